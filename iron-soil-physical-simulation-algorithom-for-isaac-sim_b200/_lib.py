@@ -1,0 +1,181 @@
+"""ctypes binding of ``libsoilb200.so`` (declarations mirror include/soilb200.h).
+
+The library is the only compute path: if it is missing or no CUDA device is
+usable, every entry point raises :class:`B200BackendUnavailable` -- there is
+no CPU fallback (the reference likewise refuses to relabel a missing Warp
+backend as a GPU pass, ``performance/warp_backend.py`` / ``probe_warp``).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libsoilb200.so"
+
+SB_OK = 0
+SB_ERR_BAD_ARG = 1
+SB_ERR_SUBSTEP_CAP = 2
+SB_ERR_POSITIVITY = 3
+SB_ERR_NONCONVERGENCE = 4
+SB_ERR_CUDA = 5
+SB_ERR_WAIT_LIMIT = 6
+SB_ERR_STATE = 7
+SB_ERR_RANGE = 8
+
+SB_FP64 = 0
+SB_FX32 = 1
+
+FIELD = {
+    "z_base": 0,
+    "b_eff": 1,
+    "mobile": 2,
+    "momentum_x": 3,
+    "momentum_y": 4,
+    "external_x": 5,
+    "external_y": 6,
+    "frontier_reached": 7,
+    "labels": 8,
+    "unstable": 9,
+    "slope": 10,
+    "severity": 11,
+    "latch": 12,
+    "previous_component": 13,
+}
+INT_FIELDS = {"frontier_reached", "labels", "unstable", "latch", "previous_component"}
+
+
+class B200BackendUnavailable(RuntimeError):
+    """The CUDA library or a usable B200 device is not available."""
+
+
+class B200DeviceError(RuntimeError):
+    """A CUDA error raised while running an operation on an existing context."""
+
+
+class NumericalNonconvergenceError(RuntimeError):
+    """Device loop exceeded its bound (reference: solvers/event_driven_slope.py:510-533)."""
+
+
+class GridDesc(C.Structure):
+    _fields_ = [
+        ("device", C.c_int), ("ny", C.c_int), ("nx", C.c_int),
+        ("dx_m", C.c_double), ("dy_m", C.c_double), ("tile_size", C.c_int),
+        ("precision", C.c_int), ("height_exponent", C.c_int), ("datum_m", C.c_double),
+    ]
+
+
+class MobileParams(C.Structure):
+    _fields_ = [
+        ("gravity_m_s2", C.c_double), ("earth_pressure_coefficient", C.c_double),
+        ("cfl", C.c_double), ("dry_tolerance_m", C.c_double),
+        ("start_angle_deg", C.c_double), ("basal_friction_coefficient", C.c_double),
+        ("maximum_substeps", C.c_int), ("use_external", C.c_int),
+        ("density_kg_m3", C.c_double),
+    ]
+
+
+class MobileLedger(C.Structure):
+    _fields_ = [
+        ("mass_m3", C.c_double), ("momentum_m4_s", C.c_double * 2),
+        ("kinetic", C.c_double), ("gravitational", C.c_double), ("internal", C.c_double),
+        ("volume_w_m3", C.c_double), ("momentum_w", C.c_double * 2),
+        ("kinetic_w_j", C.c_double), ("potential_w_j", C.c_double),
+        ("pressure_w_j", C.c_double), ("max_speed_m_s", C.c_double),
+        ("min_h_m", C.c_double), ("mass_quanta", C.c_int64),
+        ("volume_w_quanta", C.c_int64),
+    ]
+
+
+class MobileStats(C.Structure):
+    _fields_ = [
+        ("substeps", C.c_int), ("static_skip", C.c_int), ("cfl_limited", C.c_int),
+        ("status", C.c_int), ("maximum_cfl", C.c_double),
+        ("conservative_impulse_m4_s", C.c_double * 2),
+        ("friction_impulse_m4_s", C.c_double * 2),
+        ("external_impulse_m4_s", C.c_double * 2),
+        ("friction_dissipation", C.c_double), ("external_work", C.c_double),
+        ("before", MobileLedger), ("after", MobileLedger),
+    ]
+
+
+_LIB = None
+_PROTOTYPES = {
+    "sb_ctx_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
+    "sb_ctx_destroy": (C.c_int, [C.c_void_p]),
+    "sb_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "sb_download": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "sb_upload_i32": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "sb_download_i32": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "sb_synchronize": (C.c_int, [C.c_void_p]),
+    "sb_mobile_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(MobileParams),
+                                 C.POINTER(MobileStats)]),
+    "sb_mobile_ledger_of": (C.c_int, [C.c_void_p, C.POINTER(MobileParams),
+                                      C.POINTER(MobileLedger)]),
+    "sb_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "sb_kernel_launch_count": (C.c_int64, [C.c_void_p]),
+    "sb_version": (C.c_char_p, []),
+    "sb_sizeof": (C.c_size_t, [C.c_char_p]),
+}
+
+# ctypes mirror of each ABI struct, checked against sb_sizeof() in the tests.
+ABI_STRUCTS = {
+    "sb_grid_desc": GridDesc,
+    "sb_mobile_params": MobileParams,
+    "sb_mobile_ledger": MobileLedger,
+    "sb_mobile_stats": MobileStats,
+}
+
+
+def exported_symbols() -> list[str]:
+    return sorted(_PROTOTYPES)
+
+
+def load():
+    """Load the library (once).  Raises B200BackendUnavailable when absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = Path(os.environ.get("SOILB200_LIB", LIB_PATH))
+    if not path.exists():
+        raise B200BackendUnavailable(
+            f"[soilb200] {path.name} is not built; run __graft_entry__.build() "
+            "(there is no CPU fallback)")
+    lib = C.CDLL(str(path))
+    for name, (res, args) in _PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = lib
+    return lib
+
+
+def register(name: str, restype, argtypes) -> None:
+    """Add a prototype (used by modules that bind further entry points)."""
+    _PROTOTYPES[name] = (restype, argtypes)
+    if _LIB is not None:
+        fn = getattr(_LIB, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+
+
+def last_error(ctx) -> str:
+    buf = C.create_string_buffer(1024)
+    load().sb_last_error(ctx, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(ctx, status: int, what: str = "") -> None:
+    """Map a status code to the reference's exception types and messages."""
+    if status == SB_OK:
+        return
+    msg = last_error(ctx) or f"{what} failed with status {status}"
+    if status in (SB_ERR_BAD_ARG, SB_ERR_RANGE):
+        raise ValueError(msg)
+    if status == SB_ERR_NONCONVERGENCE:
+        raise NumericalNonconvergenceError(msg)
+    if status == SB_ERR_CUDA:
+        raise B200DeviceError(msg)
+    raise RuntimeError(msg)

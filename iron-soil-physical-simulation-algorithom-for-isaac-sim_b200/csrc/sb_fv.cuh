@@ -1,0 +1,527 @@
+// Mobile V2 finite-volume substep kernels.
+//
+// Equations: reference experimental/mobile_v2_reference.py, ``_face_updates``
+// (:365-431), ``_physical_flux`` (:433-449) and the substep body of ``step``
+// (:236-307).  One launch = one CFL substep over the whole grid:
+//
+//   TMA loads a (64 + 2*HX) x (16 + 2) halo tile of b, h, qx, qy into shared
+//   memory -> every face touching the tile is evaluated exactly once into
+//   shared memory (so both cells of a face see the identical flux) -> each
+//   cell gathers its four faces, applies positivity handling, dry zeroing,
+//   the external source and Coulomb friction, and writes the other buffer of
+//   the ping-pong pair -> the block reduces the next wave-speed maximum and
+//   the impulse/energy diagnostics -> the last block to finish reduces all
+//   block partials in a fixed order and computes the next substep's dt on the
+//   device, so the substep loop never returns to the host.
+//
+// Precision instantiations:
+//   FX = false : double everywhere, operation order identical to the
+//                reference NumPy code (bit-identical fields).
+//   FX = true  : int32 height quanta (b relative to a datum), float momentum;
+//                face mass fluxes are rounded to whole quanta and capped at
+//                floor(h_donor/4) per face => exact mass, h >= 0 always.
+#pragma once
+
+#include "sb_common.cuh"
+
+namespace sb {
+
+constexpr int kTileX = 64;
+constexpr int kTileY = 16;
+constexpr int kEastFaces = kTileY * (kTileX + 1);
+constexpr int kNorthFaces = (kTileY + 1) * kTileX;
+constexpr int kFvDiag = 8;      // cons x,y | ext x,y | fric x,y | fdiss | ework
+constexpr int kFvPartial = 10;  // kFvDiag + wave max + positivity flag
+
+struct FvConst {
+  int ny, nx, pitch, tiles_x, nblocks;
+  double dx, dy, K, g, cfl, dry, mu_g, c_half, kg, min_spacing;
+  // fixed-point constants
+  double Q;
+  float Kf, KGf, HKGf, Qf, invQf, dryf;
+  int max_substeps;
+  int has_external;
+};
+
+// Device-resident loop control block (one per context).
+struct FvControl {
+  double remaining;
+  double sub_dt;
+  double max_cfl;
+  double wave;
+  double diag[kFvDiag];
+  int substeps;
+  int parity;       // buffer index holding the current state
+  int done;         // 1 => substep kernels return immediately
+  int status;       // sb_status
+  int cfl_limited;
+  int static_skip;
+  unsigned int arrive;
+  int wait_fail;
+};
+
+template <bool FX>
+struct FvTypes;
+template <>
+struct FvTypes<true> {
+  using H = int32_t;  // height quanta
+  using B = int32_t;  // support quanta (datum relative)
+  using R = float;    // momentum / arithmetic
+};
+template <>
+struct FvTypes<false> {
+  using H = double;
+  using B = double;
+  using R = double;
+};
+
+template <bool FX>
+struct FvTile {
+  static constexpr int HX = 16 / sizeof(typename FvTypes<FX>::R);  // TMA x alignment
+  static constexpr int BW = kTileX + 2 * HX;                        // box width
+  static constexpr int BH = kTileY + 2;                             // box height
+  static constexpr int BOX = BW * BH;
+  static constexpr int BOX_BYTES = BOX * (int)sizeof(typename FvTypes<FX>::R);
+  __device__ static int cell(int ly, int lx) { return (ly + 1) * BW + lx + HX; }
+};
+
+template <bool FX>
+struct FvSmem {
+  using T = FvTypes<FX>;
+  using Tl = FvTile<FX>;
+  using M = typename std::conditional<FX, int32_t, double>::type;  // mass flux type
+  alignas(128) typename T::B b[Tl::BOX];
+  alignas(128) typename T::H h[Tl::BOX];
+  alignas(128) typename T::R qx[Tl::BOX];
+  alignas(128) typename T::R qy[Tl::BOX];
+  M em[kEastFaces];
+  typename T::R enm[kEastFaces], enp[kEastFaces], et[kEastFaces];
+  M nm[kNorthFaces];
+  typename T::R nnm[kNorthFaces], nnp[kNorthFaces], nt[kNorthFaces];
+  double red[kThreads / 32 * kFvPartial];
+  uint64_t bar;
+  int flag;
+};
+
+// --------------------------------------------------------------------------
+// Face fluxes.  (L, R) = (west, east) or (south, north) cell; n/t = normal and
+// tangential momentum components.  Outputs: mass flux (quanta or raw),
+// normal-momentum flux seen by L (minus) and by R (plus), tangential flux.
+// --------------------------------------------------------------------------
+__device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int br, int hlq,
+                                        int hrq, float qnl, float qtl, float qnr, float qtr,
+                                        int& m, float& fnm, float& fnp, float& ft) {
+  const int bface = max(bl, br);
+  const int dl = bface - bl;
+  const int dr = bface - br;
+  const float hl = (float)hlq * c.Qf;
+  const float hr = (float)hrq * c.Qf;
+  float hsl = hl, hsr = hr;
+  if (dl != 0) hsl = fmaxf((c.Kf * hl - (float)dl * c.Qf) / c.Kf, 0.f);
+  if (dr != 0) hsr = fmaxf((c.Kf * hr - (float)dr * c.Qf) / c.Kf, 0.f);
+  const float sl = hlq > 0 ? hsl / hl : 0.f;
+  const float sr = hrq > 0 ? hsr / hr : 0.f;
+  const float qnsl = qnl * sl, qtsl = qtl * sl;
+  const float qnsr = qnr * sr, qtsr = qtr * sr;
+  const bool wl = hsl > c.dryf, wr = hsr > c.dryf;
+  const float unl = wl ? qnsl / hsl : 0.f, utl = wl ? qtsl / hsl : 0.f;
+  const float unr = wr ? qnsr / hsr : 0.f, utr = wr ? qtsr / hsr : 0.f;
+  const float fnl = qnsl * unl + (c.HKGf * hsl) * hsl;
+  const float fnr = qnsr * unr + (c.HKGf * hsr) * hsr;
+  const float ftl = qnsl * utl, ftr = qnsr * utr;
+  const float spd = fmaxf(fabsf(unl) + sqrtf(c.KGf * hsl), fabsf(unr) + sqrtf(c.KGf * hsr));
+  const float half = 0.5f * spd;
+  const float fh = 0.5f * (qnsl + qnsr) - half * (hsr - hsl);
+  const float fn = 0.5f * (fnl + fnr) - half * (qnsr - qnsl);
+  ft = 0.5f * (ftl + ftr) - half * (qtsr - qtsl);
+  const float corl = (c.HKGf * hl) * hl - (c.HKGf * hsl) * hsl;
+  const float corr = (c.HKGf * hr) * hr - (c.HKGf * hsr) * hsr;
+  float mf = rintf((lam * fh) * c.invQf);
+  mf = fminf(fmaxf(mf, -1073741824.f), 1073741824.f);
+  int mi = (int)mf;
+  mi = mi > 0 ? min(mi, hlq >> 2) : max(mi, -(hrq >> 2));
+  m = mi;
+  fnm = fn + corl;
+  fnp = fn + corr;
+}
+
+__device__ __forceinline__ void face_fp64(const FvConst& c, double bl, double br, double hl,
+                                          double hr, double qnl, double qtl, double qnr,
+                                          double qtr, double& fh, double& fnm, double& fnp,
+                                          double& ft) {
+  const double bface = fmax(bl, br);
+  const double hsl = fmax(((bl + c.K * hl) - bface) / c.K, 0.0);
+  const double hsr = fmax(((br + c.K * hr) - bface) / c.K, 0.0);
+  const double sl = hl > c.dry ? hsl / hl : 0.0;
+  const double sr = hr > c.dry ? hsr / hr : 0.0;
+  const double qnsl = qnl * sl, qtsl = qtl * sl;
+  const double qnsr = qnr * sr, qtsr = qtr * sr;
+  const bool wl = hsl > c.dry, wr = hsr > c.dry;
+  const double unl = wl ? qnsl / hsl : 0.0, utl = wl ? qtsl / hsl : 0.0;
+  const double unr = wr ? qnsr / hsr : 0.0, utr = wr ? qtsr / hsr : 0.0;
+  const double fnl = qnsl * unl + (c.c_half * hsl) * hsl;
+  const double fnr = qnsr * unr + (c.c_half * hsr) * hsr;
+  const double ftl = qnsl * utl, ftr = qnsr * utr;
+  const double spd = fmax(fabs(unl) + sqrt(c.kg * hsl), fabs(unr) + sqrt(c.kg * hsr));
+  const double half = 0.5 * spd;
+  fh = 0.5 * (qnsl + qnsr) - half * (hsr - hsl);
+  const double fn = 0.5 * (fnl + fnr) - half * (qnsr - qnsl);
+  ft = 0.5 * (ftl + ftr) - half * (qtsr - qtsl);
+  fnm = fn + ((c.c_half * hl) * hl - (c.c_half * hsl) * hsl);
+  fnp = fn + ((c.c_half * hr) * hr - (c.c_half * hsr) * hsr);
+}
+
+// --------------------------------------------------------------------------
+// Finalisation of one substep by the last block: fixed-order reduction of the
+// block partials, loop control, next dt.
+// --------------------------------------------------------------------------
+template <int NP>
+__device__ void reduce_partials(const double* partials, int nblocks, double* out,
+                                double* scratch, const bool* is_max) {
+  double v[NP];
+#pragma unroll
+  for (int k = 0; k < NP; ++k) v[k] = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += kThreads) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      const double x = __ldcg(partials + (size_t)b * NP + k);
+      v[k] = is_max[k] ? fmax(v[k], x) : v[k] + x;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NP; ++k) v[k] = is_max[k] ? warp_max(v[k]) : warp_sum(v[k]);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) scratch[warp * NP + k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NP; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < kThreads / 32; ++w)
+        s = is_max[k] ? fmax(s, scratch[w * NP + k]) : s + scratch[w * NP + k];
+      out[k] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// Computes sub_dt/max_cfl for the next substep from ctl->wave (CPU: reference
+// step :247-257).  Called by one thread.
+__device__ __forceinline__ void plan_substep(const FvConst& c, FvControl* ctl) {
+  const double w = ctl->wave;
+  const double rem = ctl->remaining;
+  const double stable = w <= 1.0e-14 ? rem : c.cfl * c.min_spacing / w;
+  const double sub = fmin(rem, stable);
+  if (sub < rem - 1.0e-14) ctl->cfl_limited = 1;
+  ctl->max_cfl = fmax(ctl->max_cfl, w * sub / c.min_spacing);
+  ctl->sub_dt = sub;
+}
+
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    fv_substep_kernel(const FvConst c, const __grid_constant__ CUtensorMap tm_b,
+                      const __grid_constant__ CUtensorMap tm_h0,
+                      const __grid_constant__ CUtensorMap tm_h1,
+                      const __grid_constant__ CUtensorMap tm_qx0,
+                      const __grid_constant__ CUtensorMap tm_qx1,
+                      const __grid_constant__ CUtensorMap tm_qy0,
+                      const __grid_constant__ CUtensorMap tm_qy1,
+                      typename FvTypes<FX>::H* __restrict__ h0,
+                      typename FvTypes<FX>::H* __restrict__ h1,
+                      typename FvTypes<FX>::R* __restrict__ qx0,
+                      typename FvTypes<FX>::R* __restrict__ qx1,
+                      typename FvTypes<FX>::R* __restrict__ qy0,
+                      typename FvTypes<FX>::R* __restrict__ qy1,
+                      const typename FvTypes<FX>::R* __restrict__ ext_x,
+                      const typename FvTypes<FX>::R* __restrict__ ext_y, FvControl* ctl,
+                      double* __restrict__ partials, cudaGraphConditionalHandle loop_handle,
+                      int use_handle) {
+  using T = FvTypes<FX>;
+  using Tl = FvTile<FX>;
+  using R = typename T::R;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  // TMA destinations need 128-byte alignment; the launch reserves 128 spare bytes.
+  unsigned char* smem_base = smem_raw + ((128u - (smem_u32(smem_raw) & 127u)) & 127u);
+  FvSmem<FX>& s = *reinterpret_cast<FvSmem<FX>*>(smem_base);
+
+  if (*(volatile int*)&ctl->done) return;  // uniform across the grid
+  const double sub_dt = ctl->sub_dt;
+  const int parity = ctl->parity;
+  const int tile_x = blockIdx.x % c.tiles_x;
+  const int tile_y = blockIdx.x / c.tiles_x;
+  const int gx0 = tile_x * kTileX, gy0 = tile_y * kTileY;
+
+  // ---- TMA: halo tile of the four fields -------------------------------
+  if (threadIdx.x == 0) {
+    mbar_init(&s.bar, 1);
+    s.flag = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const CUtensorMap* mh = parity ? &tm_h1 : &tm_h0;
+    const CUtensorMap* mx = parity ? &tm_qx1 : &tm_qx0;
+    const CUtensorMap* my = parity ? &tm_qy1 : &tm_qy0;
+    mbar_expect_tx(&s.bar, 4 * Tl::BOX_BYTES);
+    const int x0 = gx0 - Tl::HX, y0 = gy0 - 1;
+    tma_load_2d(s.b, &tm_b, x0, y0, &s.bar);
+    tma_load_2d(s.h, mh, x0, y0, &s.bar);
+    tma_load_2d(s.qx, mx, x0, y0, &s.bar);
+    tma_load_2d(s.qy, my, x0, y0, &s.bar);
+  }
+  const bool loaded = mbar_wait(&s.bar, 0);
+  if (!loaded) {
+    if (threadIdx.x == 0) atomicExch(&ctl->wait_fail, 1);
+  }
+  const float lamx_f = (float)(sub_dt / c.dx);
+  const float lamy_f = (float)(sub_dt / c.dy);
+  const double lamx = sub_dt / c.dx;
+  const double lamy = sub_dt / c.dy;
+
+  // ---- Faces --------------------------------------------------------------
+  for (int f = threadIdx.x; f < kEastFaces + kNorthFaces; f += kThreads) {
+    const bool east = f < kEastFaces;
+    int ly, lx, la, lb;
+    bool valid;
+    if (east) {
+      ly = f / (kTileX + 1);
+      lx = f % (kTileX + 1) - 1;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      valid = loaded && gx >= 0 && gx + 1 < c.nx && gy < c.ny;
+      la = Tl::cell(ly, lx);
+      lb = la + 1;
+    } else {
+      const int g = f - kEastFaces;
+      ly = g / kTileX - 1;
+      lx = g % kTileX;
+      const int gx = gx0 + lx, gy = gy0 + ly;
+      valid = loaded && gy >= 0 && gy + 1 < c.ny && gx < c.nx;
+      la = Tl::cell(ly, lx);
+      lb = la + Tl::BW;
+    }
+    if constexpr (FX) {
+      int m = 0;
+      float fnm = 0.f, fnp = 0.f, ft = 0.f;
+      if (valid) {
+        if (east)
+          face_fx(c, lamx_f, s.b[la], s.b[lb], s.h[la], s.h[lb], s.qx[la], s.qy[la], s.qx[lb],
+                  s.qy[lb], m, fnm, fnp, ft);
+        else
+          face_fx(c, lamy_f, s.b[la], s.b[lb], s.h[la], s.h[lb], s.qy[la], s.qx[la], s.qy[lb],
+                  s.qx[lb], m, fnm, fnp, ft);
+      }
+      if (east) {
+        s.em[f] = m; s.enm[f] = fnm; s.enp[f] = fnp; s.et[f] = ft;
+      } else {
+        const int g = f - kEastFaces;
+        s.nm[g] = m; s.nnm[g] = fnm; s.nnp[g] = fnp; s.nt[g] = ft;
+      }
+    } else {
+      double fh = 0.0, fnm = 0.0, fnp = 0.0, ft = 0.0;
+      if (valid) {
+        if (east)
+          face_fp64(c, s.b[la], s.b[lb], s.h[la], s.h[lb], s.qx[la], s.qy[la], s.qx[lb],
+                    s.qy[lb], fh, fnm, fnp, ft);
+        else
+          face_fp64(c, s.b[la], s.b[lb], s.h[la], s.h[lb], s.qy[la], s.qx[la], s.qy[lb],
+                    s.qx[lb], fh, fnm, fnp, ft);
+      }
+      if (east) {
+        s.em[f] = fh; s.enm[f] = fnm; s.enp[f] = fnp; s.et[f] = ft;
+      } else {
+        const int g = f - kEastFaces;
+        s.nm[g] = fh; s.nnm[g] = fnm; s.nnp[g] = fnp; s.nt[g] = ft;
+      }
+    }
+  }
+  __syncthreads();
+
+  // ---- Cells --------------------------------------------------------------
+  typename T::H* hdst = parity ? h0 : h1;
+  R* qxdst = parity ? qx0 : qx1;
+  R* qydst = parity ? qy0 : qy1;
+  double acc[kFvDiag];
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
+  double wave = 0.0;
+  int neg = 0;
+  for (int i = threadIdx.x; i < kTileX * kTileY; i += kThreads) {
+    const int ly = i / kTileX, lx = i % kTileX;
+    const int gy = gy0 + ly, gx = gx0 + lx;
+    if (gy >= c.ny || gx >= c.nx || !loaded) continue;
+    const int e = ly * (kTileX + 1) + lx + 1;  // east face of this cell
+    const int w = e - 1;                       // west face
+    const int n = (ly + 1) * kTileX + lx;      // north face
+    const int so = n - kTileX;                 // south face
+    const int cs = Tl::cell(ly, lx);
+    const size_t gi = (size_t)gy * c.pitch + gx;
+    R ax = R(0), ay = R(0);
+    if (c.has_external) {
+      ax = ext_x[gi];
+      ay = ext_y[gi];
+    }
+    if constexpr (FX) {
+      const int dh = ((0 - s.em[e] + s.em[w]) - s.nm[n]) + s.nm[so];
+      const int hq = s.h[cs] + dh;
+      const float zero = 0.f;
+      const float dqx =
+          (((zero - lamx_f * s.enm[e]) + lamx_f * s.enp[w]) - lamy_f * s.nt[n]) + lamy_f * s.nt[so];
+      const float dqy =
+          (((zero - lamx_f * s.et[e]) + lamx_f * s.et[w]) - lamy_f * s.nnm[n]) + lamy_f * s.nnp[so];
+      const float qx_old = s.qx[cs], qy_old = s.qy[cs];
+      const float hn = (float)hq * c.Qf;
+      const bool wet = hn > c.dryf;
+      const float qxn = wet ? qx_old + dqx : 0.f;
+      const float qyn = wet ? qy_old + dqy : 0.f;
+      float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
+      if (wet) {
+        vbx = qxn / hn;
+        vby = qyn / hn;
+        if (c.has_external) {
+          const float dtf = (float)sub_dt;
+          qex = qxn + (hn * ax) * dtf;
+          qey = qyn + (hn * ay) * dtf;
+        }
+        vex = qex / hn;
+        vey = qey / hn;
+      }
+      const float spd = sqrtf(vex * vex + vey * vey);
+      const float dec = (float)(c.mu_g * sub_dt);
+      const float fac = fmaxf(0.f, 1.f - dec / fmaxf(spd, 1.0e-15f));
+      const float vax = vex * fac, vay = vey * fac;
+      const float qxo = hn * vax, qyo = hn * vay;
+      hdst[gi] = hq;
+      qxdst[gi] = qxo;
+      qydst[gi] = qyo;
+      const double h64 = (double)hn;
+      acc[0] += (double)qxn - (double)qx_old;
+      acc[1] += (double)qyn - (double)qy_old;
+      acc[2] += (double)qex - (double)qxn;
+      acc[3] += (double)qey - (double)qyn;
+      acc[4] += (double)qxo - (double)qex;
+      acc[5] += (double)qyo - (double)qey;
+      acc[6] += 0.5 * h64 *
+                ((double)spd * (double)spd - ((double)vax * (double)vax + (double)vay * (double)vay));
+      acc[7] += h64 * ((0.5 * ((double)vbx + (double)vex)) * (double)ax +
+                       (0.5 * ((double)vby + (double)vey)) * (double)ay) * sub_dt;
+      float vx = 0.f, vy = 0.f;
+      if (wet) {
+        vx = qxo / hn;
+        vy = qyo / hn;
+      }
+      const float wv = sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn);
+      wave = fmax(wave, (double)wv);
+    } else {
+      const double dh = (((0.0 - lamx * s.em[e]) + lamx * s.em[w]) - lamy * s.nm[n]) + lamy * s.nm[so];
+      const double dqx =
+          (((0.0 - lamx * s.enm[e]) + lamx * s.enp[w]) - lamy * s.nt[n]) + lamy * s.nt[so];
+      const double dqy =
+          (((0.0 - lamx * s.et[e]) + lamx * s.et[w]) - lamy * s.nnm[n]) + lamy * s.nnp[so];
+      double hn = s.h[cs] + dh;
+      const double qx_old = s.qx[cs], qy_old = s.qy[cs];
+      double qxn = qx_old + dqx, qyn = qy_old + dqy;
+      if (hn < -2.0e-13) neg = 1;
+      hn = fmax(hn, 0.0);
+      const bool wet = hn > c.dry;
+      if (!wet) {
+        qxn = 0.0;
+        qyn = 0.0;
+      }
+      double vbx = 0.0, vby = 0.0, vex = 0.0, vey = 0.0;
+      const double qex = qxn + (hn * ax) * sub_dt;
+      const double qey = qyn + (hn * ay) * sub_dt;
+      if (wet) {
+        vbx = qxn / hn;
+        vby = qyn / hn;
+        vex = qex / hn;
+        vey = qey / hn;
+      }
+      const double spd = sqrt(vex * vex + vey * vey);
+      const double dec = c.mu_g * sub_dt;
+      const double fac = fmax(0.0, 1.0 - dec / fmax(spd, 1.0e-15));
+      const double vax = vex * fac, vay = vey * fac;
+      const double qxo = hn * vax, qyo = hn * vay;
+      hdst[gi] = hn;
+      qxdst[gi] = qxo;
+      qydst[gi] = qyo;
+      acc[0] += qxn - qx_old;
+      acc[1] += qyn - qy_old;
+      acc[2] += qex - qxn;
+      acc[3] += qey - qyn;
+      acc[4] += qxo - qex;
+      acc[5] += qyo - qey;
+      acc[6] += 0.5 * (hn * (spd * spd - (vax * vax + vay * vay)));
+      acc[7] += hn * ((0.5 * (vbx + vex)) * ax + (0.5 * (vby + vey)) * ay) * sub_dt;
+      double vx = 0.0, vy = 0.0;
+      if (wet) {
+        vx = qxo / hn;
+        vy = qyo / hn;
+      }
+      wave = fmax(wave, sqrt(vx * vx + vy * vy) + sqrt(c.kg * hn));
+    }
+  }
+
+  // ---- Block partials --------------------------------------------------------
+  double v[kFvPartial];
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) v[k] = warp_sum(acc[k]);
+  v[kFvDiag] = warp_max(wave);
+  v[kFvDiag + 1] = (double)__reduce_or_sync(0xffffffffu, (unsigned)neg);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < kFvPartial; ++k) s.red[warp * kFvPartial + k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < kFvPartial) {
+    const int k = threadIdx.x;
+    double a = 0.0;
+    for (int w2 = 0; w2 < kThreads / 32; ++w2)
+      a = k >= kFvDiag ? fmax(a, s.red[w2 * kFvPartial + k]) : a + s.red[w2 * kFvPartial + k];
+    partials[(size_t)blockIdx.x * kFvPartial + k] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicAdd(&ctl->arrive, 1u);
+    s.flag = (prev == (unsigned)c.nblocks - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!s.flag) return;
+
+  // ---- Last block: loop control ---------------------------------------------
+  __threadfence();
+  __shared__ double tot[kFvPartial];
+  __shared__ bool is_max[kFvPartial];
+  if (threadIdx.x < kFvPartial) is_max[threadIdx.x] = threadIdx.x >= kFvDiag;
+  __syncthreads();
+  reduce_partials<kFvPartial>(partials, c.nblocks, tot, s.red, is_max);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] += tot[k];
+    ctl->substeps += 1;
+    ctl->remaining -= sub_dt;
+    ctl->parity = parity ^ 1;
+    ctl->wave = tot[kFvDiag];
+    ctl->arrive = 0;
+    if (ctl->wait_fail) {
+      ctl->status = 6;  // SB_ERR_WAIT_LIMIT
+      ctl->done = 1;
+    } else if (tot[kFvDiag + 1] != 0.0) {
+      ctl->status = 3;  // SB_ERR_POSITIVITY
+      ctl->done = 1;
+    } else if (!(ctl->remaining > 1.0e-14)) {
+      ctl->done = 1;
+    } else if (ctl->substeps >= c.max_substeps) {
+      ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
+      ctl->done = 1;
+    } else {
+      plan_substep(c, ctl);
+    }
+    __threadfence();
+    if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
+  }
+}
+
+}  // namespace sb

@@ -1,0 +1,277 @@
+// Per-step ledger / prologue reduction and field conversion kernels.
+//
+// One pass over the state computes, with a deterministic two-level reduction:
+//   * the FP64 ledger of MobileV2ReferenceSolver.mass/momentum/energy_terms
+//     (experimental/mobile_v2_reference.py:104-127) and of the production
+//     ``summarize`` kernel (bulk_interaction/warp_mobile_v2.py:28-54); in the
+//     fixed-point path mass and Triangle-A-C volume are exact int64 sums;
+//   * the static short-circuit of ``_globally_static_below_start`` (:353-363);
+//   * the wave speed that sets the first substep's dt (:239-253).
+#pragma once
+
+#include "sb_fv.cuh"
+
+namespace sb {
+
+enum LedgerSlot {
+  L_HSUM = 0, L_HSUM_W, L_QX, L_QY, L_QX_W, L_QY_W, L_HS2, L_HS2_W, L_HB, L_HB_W, L_HH, L_HH_W,
+  L_NSUM,
+  L_MAXSPEED = L_NSUM, L_NEGMINH, L_MAXQ, L_MAXGRAD, L_MAXWAVE, L_MAXEXT,
+  L_NP
+};
+constexpr int kLedgerI64 = 2;  // h quanta, h quanta * w6
+
+struct LedgerOut {
+  double v[L_NP];
+  long long iq[kLedgerI64];
+};
+
+struct StepIO {  // per-step device record: ledgers before/after + loop control
+  LedgerOut before;
+  LedgerOut after;
+};
+
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    ledger_kernel(const FvConst c, const typename FvTypes<FX>::B* __restrict__ b,
+                  const typename FvTypes<FX>::H* __restrict__ h0,
+                  const typename FvTypes<FX>::H* __restrict__ h1,
+                  const typename FvTypes<FX>::R* __restrict__ qx0,
+                  const typename FvTypes<FX>::R* __restrict__ qx1,
+                  const typename FvTypes<FX>::R* __restrict__ qy0,
+                  const typename FvTypes<FX>::R* __restrict__ qy1,
+                  const typename FvTypes<FX>::R* __restrict__ ext_x,
+                  const typename FvTypes<FX>::R* __restrict__ ext_y, double datum,
+                  double static_limit, int mode, FvControl* ctl, StepIO* io,
+                  double* __restrict__ partials, long long* __restrict__ ipartials,
+                  unsigned int* arrive, cudaGraphConditionalHandle loop_handle, int use_handle) {
+  using T = FvTypes<FX>;
+  const int parity = ctl->parity;
+  const typename T::H* h = parity ? h1 : h0;
+  const typename T::R* qx = parity ? qx1 : qx0;
+  const typename T::R* qy = parity ? qy1 : qy0;
+  double v[L_NP];
+#pragma unroll
+  for (int k = 0; k < L_NP; ++k) v[k] = 0.0;
+  v[L_NEGMINH] = -1.0e300;
+  long long iq0 = 0, iq1 = 0;
+  const long long ncell = (long long)c.ny * c.nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncell;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / c.nx), col = (int)(i % c.nx);
+    const size_t gi = (size_t)r * c.pitch + col;
+    const int w6 = vertex_weight6(r, col, c.ny, c.nx);
+    double hv, bv;
+    const double qxv = (double)qx[gi], qyv = (double)qy[gi];
+    // gradient of the free surface b + h (np.gradient, edge_order 1)
+    const int cl = col > 0 ? col - 1 : col, cr = col + 1 < c.nx ? col + 1 : col;
+    const int rd = r > 0 ? r - 1 : r, ru = r + 1 < c.ny ? r + 1 : r;
+    const double denx = (col > 0 && col + 1 < c.nx) ? 2.0 * c.dx : c.dx;
+    const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
+    const size_t il = (size_t)r * c.pitch + cl, ir = (size_t)r * c.pitch + cr;
+    const size_t idn = (size_t)rd * c.pitch + col, iup = (size_t)ru * c.pitch + col;
+    double grad;
+    if constexpr (FX) {
+      const int hq = h[gi];
+      hv = (double)hq * c.Q;
+      bv = (double)b[gi] * c.Q + datum;
+      iq0 += hq;
+      iq1 += (long long)hq * w6;
+      const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
+      const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
+      const double gx = ((double)(Hr - Hl) * c.Q) / denx;
+      const double gy = ((double)(Hu - Hd) * c.Q) / deny;
+      grad = sqrt(gx * gx + gy * gy);
+    } else {
+      hv = h[gi];
+      bv = b[gi];
+      v[L_HSUM] += hv;
+      v[L_HSUM_W] += hv * w6;
+      const double gx = ((b[ir] + h[ir]) - (b[il] + h[il])) / denx;
+      const double gy = ((b[iup] + h[iup]) - (b[idn] + h[idn])) / deny;
+      grad = hypot(gx, gy);
+    }
+    const bool wet = hv > c.dry;
+    double s2 = 0.0, spd = 0.0, wave;
+    if constexpr (FX) {
+      const float hn = (float)h[gi] * c.Qf;
+      float vx = 0.f, vy = 0.f;
+      if (hn > c.dryf) {
+        vx = qx[gi] / hn;
+        vy = qy[gi] / hn;
+      }
+      wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
+    } else {
+      double vx = 0.0, vy = 0.0;
+      if (wet) {
+        vx = qxv / hv;
+        vy = qyv / hv;
+      }
+      wave = sqrt(vx * vx + vy * vy) + sqrt(c.kg * fmax(hv, 0.0));
+    }
+    if (wet) {
+      s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
+      spd = sqrt(s2);
+    }
+    v[L_QX] += qxv;
+    v[L_QY] += qyv;
+    v[L_QX_W] += qxv * w6;
+    v[L_QY_W] += qyv * w6;
+    v[L_HS2] += hv * s2;
+    v[L_HS2_W] += hv * s2 * w6;
+    v[L_HB] += hv * bv;
+    v[L_HB_W] += hv * bv * w6;
+    v[L_HH] += hv * hv;
+    v[L_HH_W] += hv * hv * w6;
+    v[L_MAXSPEED] = fmax(v[L_MAXSPEED], spd);
+    v[L_NEGMINH] = fmax(v[L_NEGMINH], -hv);
+    v[L_MAXQ] = fmax(v[L_MAXQ], fmax(fabs(qxv), fabs(qyv)));
+    v[L_MAXGRAD] = fmax(v[L_MAXGRAD], grad);
+    v[L_MAXWAVE] = fmax(v[L_MAXWAVE], wave);
+    if (c.has_external)
+      v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
+  }
+  // block reduction
+  __shared__ double red[kThreads / 32 * L_NP];
+  __shared__ long long ired[kThreads / 32 * kLedgerI64];
+  __shared__ int last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < L_NP; ++k) v[k] = k < L_NSUM ? warp_sum(v[k]) : warp_max(v[k]);
+  iq0 = (long long)warp_sum_u64((unsigned long long)iq0);
+  iq1 = (long long)warp_sum_u64((unsigned long long)iq1);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < L_NP; ++k) red[warp * L_NP + k] = v[k];
+    ired[warp * 2] = iq0;
+    ired[warp * 2 + 1] = iq1;
+  }
+  __syncthreads();
+  if (threadIdx.x < L_NP) {
+    const int k = threadIdx.x;
+    double a = k == L_NEGMINH ? -1.0e300 : 0.0;
+    for (int w = 0; w < kThreads / 32; ++w)
+      a = k < L_NSUM ? a + red[w * L_NP + k] : fmax(a, red[w * L_NP + k]);
+    partials[(size_t)blockIdx.x * L_NP + k] = a;
+  } else if (threadIdx.x < L_NP + kLedgerI64) {
+    const int k = threadIdx.x - L_NP;
+    long long a = 0;
+    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * 2 + k];
+    ipartials[(size_t)blockIdx.x * kLedgerI64 + k] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(arrive, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // fixed-order final reduction (thread k handles slot k serially over blocks)
+  LedgerOut* out = mode == 0 ? &io->before : &io->after;
+  if (threadIdx.x < L_NP) {
+    const int k = threadIdx.x;
+    double a = k == L_NEGMINH ? -1.0e300 : 0.0;
+    for (unsigned bk = 0; bk < gridDim.x; ++bk) {
+      const double x = __ldcg(partials + (size_t)bk * L_NP + k);
+      a = k < L_NSUM ? a + x : fmax(a, x);
+    }
+    out->v[k] = a;
+  } else if (threadIdx.x < L_NP + kLedgerI64) {
+    const int k = threadIdx.x - L_NP;
+    long long a = 0;
+    for (unsigned bk = 0; bk < gridDim.x; ++bk) a += __ldcg(ipartials + (size_t)bk * kLedgerI64 + k);
+    out->iq[k] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *arrive = 0;
+    if (mode == 0) {
+      // prologue: static short-circuit and the first substep's dt
+      const bool no_ext = !c.has_external || out->v[L_MAXEXT] <= 1.0e-14;
+      const bool is_static =
+          no_ext && out->v[L_MAXQ] <= 1.0e-14 && out->v[L_MAXGRAD] <= static_limit;
+      ctl->wave = out->v[L_MAXWAVE];
+      if (is_static) {
+        ctl->static_skip = 1;
+        ctl->done = 1;
+      } else if (!(ctl->remaining > 1.0e-14)) {
+        ctl->done = 1;
+      } else if (c.max_substeps <= 0) {
+        ctl->status = 2;
+        ctl->done = 1;
+      } else {
+        plan_substep(c, ctl);
+      }
+      __threadfence();
+      if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
+    }
+  }
+}
+
+// Resets the loop control block for a new physics step of dt seconds.
+__global__ void fv_begin_kernel(FvControl* ctl, const double* dt) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    ctl->remaining = *dt;
+    ctl->sub_dt = 0.0;
+    ctl->max_cfl = 0.0;
+    ctl->wave = 0.0;
+    for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] = 0.0;
+    ctl->substeps = 0;
+    ctl->done = 0;
+    ctl->status = 0;
+    ctl->cfl_limited = 0;
+    ctl->static_skip = 0;
+    ctl->arrive = 0;
+    ctl->wait_fail = 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Field conversion (host float64 layout <-> device storage).
+// ---------------------------------------------------------------------------
+__global__ void to_fixed_kernel(const double* __restrict__ src, int32_t* __restrict__ dst, int ny,
+                                int nx, int pitch, double datum, double scale, int* range_error) {
+  const long long n = (long long)ny * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nx), c = (int)(i % nx);
+    const double x = rint((src[i] - datum) * scale);
+    if (!(fabs(x) < 2147483647.0)) {
+      atomicExch(range_error, 1);
+      dst[(size_t)r * pitch + c] = 0;
+    } else {
+      dst[(size_t)r * pitch + c] = (int32_t)x;
+    }
+  }
+}
+
+__global__ void from_fixed_kernel(const int32_t* __restrict__ src, double* __restrict__ dst,
+                                  int ny, int nx, int pitch, double datum, double quantum) {
+  const long long n = (long long)ny * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nx), c = (int)(i % nx);
+    dst[i] = (double)src[(size_t)r * pitch + c] * quantum + datum;
+  }
+}
+
+__global__ void to_float_kernel(const double* __restrict__ src, float* __restrict__ dst, int ny,
+                                int nx, int pitch) {
+  const long long n = (long long)ny * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nx), c = (int)(i % nx);
+    dst[(size_t)r * pitch + c] = (float)src[i];
+  }
+}
+
+__global__ void from_float_kernel(const float* __restrict__ src, double* __restrict__ dst, int ny,
+                                  int nx, int pitch) {
+  const long long n = (long long)ny * nx;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / nx), c = (int)(i % nx);
+    dst[i] = (double)src[(size_t)r * pitch + c];
+  }
+}
+
+}  // namespace sb

@@ -1,0 +1,104 @@
+"""Pin the CPU oracle against the reference's own outputs (no GPU needed).
+
+The golden fixtures were produced by running the reference's
+``MobileV2ReferenceSolver`` (tests/golden/make_golden.py); the JSON values are
+copied from the reports the reference ships
+(``outputs/mobile_v2_reference/*.json``).
+"""
+
+import json
+
+import numpy as np
+import pytest
+
+from oracle import fixed_point as fx
+from oracle import mobile_v2 as m
+
+from conftest import GOLDEN
+
+
+def _cfg():
+    return m.OracleConfig()
+
+
+def test_fv_oracle_is_bitwise_equal_to_reference_on_contract_states(fv_golden):
+    cfg = _cfg()
+    for name in fv_golden["names"]:
+        s = m.step(cfg, fv_golden[f"{name}/b"], fv_golden[f"{name}/h"], fv_golden[f"{name}/q"],
+                   float(fv_golden[f"{name}/dt"]))
+        assert s.substeps == int(fv_golden[f"{name}/substeps"]), name
+        assert np.array_equal(s.h, fv_golden[f"{name}/h_out"]), name
+        assert np.array_equal(s.q, fv_golden[f"{name}/q_out"]), name
+        sc = fv_golden[f"{name}/scalars"]
+        assert s.maximum_cfl == sc[0]
+        assert s.energy_after[3] == pytest.approx(sc[6], rel=1e-14, abs=1e-15)
+
+
+def test_fv_oracle_matches_shipped_contract_report(fv_golden):
+    rep = json.loads((GOLDEN / "reference_reports.json").read_text())["cpu_contracts"]
+    cfg = _cfg()
+    for name, want in rep.items():
+        s = m.step(cfg, fv_golden[f"{name}/b"], fv_golden[f"{name}/h"], fv_golden[f"{name}/q"],
+                   float(fv_golden[f"{name}/dt"]))
+        assert s.substeps == want["substeps"], name
+        assert s.maximum_cfl == pytest.approx(want["maximum_CFL"], abs=1e-15)
+        assert s.energy_after[3] == pytest.approx(want["energy_after"], rel=1e-13, abs=1e-15)
+        assert s.energy_before[3] == pytest.approx(want["energy_before"], rel=1e-13, abs=1e-15)
+        assert s.friction_dissipation == pytest.approx(want["friction_dissipation"], rel=1e-11,
+                                                       abs=1e-15)
+        assert abs(s.mass_after - s.mass_before) <= 2.0e-13
+
+
+def test_device_equivalence_substep_counts(fv_golden):
+    rep = json.loads((GOLDEN / "reference_reports.json").read_text())["device_equivalence"]
+    for name, want in rep.items():
+        assert int(fv_golden[f"{name}/substeps"]) == want["CPU_substeps"] == want["DEVICE_substeps"]
+
+
+def test_fv_oracle_gate_cfl04_bitwise(gate_golden):
+    cfg = m.OracleConfig(basal_friction_coefficient=float(np.tan(np.deg2rad(35.0))), cfl=0.4)
+    b, h = gate_golden["b"], gate_golden["h"]
+    q = np.zeros(h.shape + (2,))
+    for k in range(6):
+        s = m.step(cfg, b, h, q, 1.0 / 60.0)
+        h, q = s.h, s.q
+        assert s.substeps == gate_golden["substeps"][k]
+        assert np.array_equal(h, gate_golden[f"h_{k}"])
+        assert np.array_equal(q, gate_golden[f"q_{k}"])
+
+
+def test_fixed_point_mirror_tracks_fp64_and_conserves_exactly(gate_golden):
+    b, h = gate_golden["b"], gate_golden["h"]
+    datum = 0.5 * (b.min() + b.max())
+    k = fx.choose_exponent(max(b.max() - datum, h.max()))
+    p = fx.FixedParams(dx=0.05, dy=0.05, cfl=0.4, mu=float(np.tan(np.deg2rad(35.0))), exponent=k)
+    bq = fx.quantize(b, datum, k)
+    hq = fx.quantize(h, 0.0, k)
+    m0 = int(hq.sum(dtype=np.int64))
+    qx = np.zeros(h.shape, np.float32)
+    qy = qx.copy()
+    for s in range(6):
+        hq, qx, qy, n, _ = fx.step(p, bq, hq, qx, qy, 1.0 / 60.0)
+        assert n == gate_golden["substeps"][s]
+        err = np.abs(fx.dequantize(hq, 0.0, k) - gate_golden[f"h_{s}"]).max()
+        assert err <= 1.0e-6
+        assert int(hq.sum(dtype=np.int64)) == m0
+        assert hq.min() >= 0
+
+
+def test_fixed_point_donor_cap_keeps_heights_nonnegative():
+    # A thin film on a steep ramp at CFL 0.4: the cap must keep h >= 0.
+    rng = np.random.default_rng(3)
+    ny, nx = 24, 31
+    ys, xs = np.indices((ny, nx))
+    b = 0.9 * xs * 0.05 + 0.01 * rng.random((ny, nx))
+    h = np.where(rng.random((ny, nx)) < 0.3, 1e-6 * rng.random((ny, nx)), 0.0)
+    k = fx.choose_exponent(1.0)
+    p = fx.FixedParams(dx=0.05, dy=0.05, cfl=0.4, exponent=k)
+    bq = fx.quantize(b, 0.5, k)
+    hq = fx.quantize(h, 0.0, k)
+    qx = (rng.normal(0, 1e-6, (ny, nx))).astype(np.float32)
+    qy = np.zeros_like(qx)
+    m0 = int(hq.sum(dtype=np.int64))
+    hq, qx, qy, n, _ = fx.step(p, bq, hq, qx, qy, 0.05)
+    assert hq.min() >= 0 and int(hq.sum(dtype=np.int64)) == m0
