@@ -1,0 +1,367 @@
+#!/usr/bin/env python3
+"""Benchmark: Mobile V2 cell-substeps/s on the config-1 plain path (701^2).
+
+One step = one 1/60 s physics step of the plain terrain path on a 701 x 701
+grid (dx 0.05 m): bucket-cut entrainment -> Mobile V2 finite-volume step (all
+CFL substeps) -> large-avalanche labelling (38 deg start, 8-connected) ->
+gated residual frontier relaxation, through the public Python API over the C
+ABI.  Inputs: the seeded 6-octave value-noise pile (seed 1) and the straight
+bucket cut of the config; synthetic data, no dataset.
+
+  value   cell-substeps/s = 701^2 * sum(substeps) / sum(device step time), with
+          the terrain resident in HBM; device time from CUDA events on the
+          library's stream; L2 flushed (256 MiB write) between timed steps.
+  e2e     the same cell-substeps over host wall-clock time, including per step
+          the pinned-host -> device copy of the cut command (indices + target
+          surfaces) and the device -> host read of the step records.
+  roofline  dominant kernel = the fused FV substep kernel; achieved =
+          28 B/cell * cells per launch / mean launch time from CUDA events
+          recorded around the device-side substep loop.
+
+``--impl reference`` times the CPU restatement of the reference path (NumPy,
+oracle/) on the same workload, one rank only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mobile V2 cell-substeps/s at 701^2 (config-1 plain path)"
+UNIT = "cell-substeps/s"
+N = 701
+DX = 0.05
+DT = 1.0 / 60.0
+BYTES_PER_CELL_SUBSTEP = 28  # FX32: read b,h,qx,qy (16 B) + write h,qx,qy (12 B)
+
+
+def material():
+    import soilb200
+    return soilb200.MaterialScenario("config1_soil", 1600.0, 35.0, 0.0, 0.5, 38.0, 30.0, 0.55)
+
+
+def cut_schedule(cut, steps: int, pinned: bool):
+    """Per-step cut commands (flat indices, target surfaces), optionally pinned."""
+    out = []
+    for k in range(steps):
+        idx, tgt = cut.footprint((k + 1) * DT)
+        if pinned:
+            import torch
+            ti = torch.empty(idx.size, dtype=torch.int32, pin_memory=True)
+            tt = torch.empty(tgt.size, dtype=torch.float64, pin_memory=True)
+            ti.numpy()[:] = idx
+            tt.numpy()[:] = tgt
+            out.append((ti.numpy(), tt.numpy()))
+        else:
+            out.append((idx, tgt))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._thread = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}",
+                                      f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            for name, val in zip(names, s[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.samples)}
+
+
+def load_traffic():
+    p = ROOT / "profiles" / "traffic.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return None
+    return None
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def run_gpu(args, rank: int, world: int, local_rank: int):
+    import torch
+    import soilb200
+    from soilb200 import workloads
+    from soilb200.pipeline import PlainPath
+
+    torch.cuda.set_device(local_rank)
+    cfg = workloads.config1(N, seed=1, dx=DX)
+    path = PlainPath(cfg["b_eff"], cfg["z_base"], dx=DX, material=material(),
+                     device=local_rank, residual="gated")
+    grid = path.grid
+    total_steps = args.warmup + args.steps
+    sched = cut_schedule(cfg["cut"], total_steps, pinned=True)
+    stream = torch.cuda.ExternalStream(grid.stream_handle(), device=local_rank)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
+
+    for k in range(args.warmup):
+        idx, tgt = sched[k]
+        path.step(DT, idx, tgt)
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+    launches0 = grid.kernel_launches()
+    step_ms, substeps, loop_ms = [], [], []
+    h2d = d2h = 0
+    stats_bytes = 2 * 400  # MobileStats + LabelOut records read back per step (approx, fixed)
+    wall = 0.0
+    with ClockSampler(local_rank) as clocks:
+        for k in range(args.warmup, total_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            idx, tgt = sched[k]
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            e0.record(stream)
+            st = path.step(DT, idx, tgt)
+            e1.record(stream)
+            e1.synchronize()
+            wall += time.perf_counter() - t0
+            step_ms.append(e0.elapsed_time(e1))
+            substeps.append(st.substeps)
+            ls = path.mobile.last_stats
+            if ls is not None and ls.substeps:
+                loop_ms.append((ls.substep_loop_ms, ls.substeps))
+            h2d += idx.nbytes + tgt.nbytes
+            d2h += stats_bytes
+    launches = grid.kernel_launches() - launches0
+    dev_s = sum(step_ms) / 1000.0
+    cells = N * N
+    cell_substeps = cells * sum(substeps)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([dev_s, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        c = torch.tensor([float(cell_substeps)], dtype=torch.float64, device=f"cuda:{local_rank}")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        dev_s, wall = float(t[0]), float(t[1])
+        cell_substeps = float(c[0])
+    peak, peak_kind = measured_peak()
+    tot_loop = sum(m for m, _ in loop_ms)
+    tot_launch = sum(n for _, n in loop_ms)
+    per_launch_ms = tot_loop / tot_launch if tot_launch else None
+    alg_bytes = BYTES_PER_CELL_SUBSTEP * cells
+    achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms else None
+    traffic = load_traffic()
+    result = None
+    if rank == 0:
+        result = {
+            "metric": METRIC, "value": cell_substeps / dev_s if dev_s > 0 else 0.0, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev_s * 1000.0 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32-quanta+f32 (f64/i64 ledger)",
+            "data": "synthetic (seeded config-1 value-noise pile + bucket cut)",
+            "config": {"workload": "config1_plain_path_701", "grid": [N, N], "dx_m": DX,
+                       "dt_s": DT, "steps_simulated_before_timing": args.warmup,
+                       "step": "cut entrain -> Mobile V2 (all substeps) -> labelling -> "
+                               "gated residual frontier",
+                       "precision": "FX32: int32 height quanta + float32 momentum",
+                       "l2": "flushed (256 MiB write) between timed steps",
+                       "parallelism": f"replicas x{world}",
+                       "substeps_total": int(sum(substeps))},
+            "e2e": {"value": cell_substeps / wall if wall > 0 else 0.0, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d // max(args.steps, 1),
+                    "d2h_bytes_per_step": d2h // max(args.steps, 1)},
+            "roofline": {"bound": "hbm", "kernel": "fv_substep_kernel<FX32>",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "mean_launch_ms": per_launch_ms,
+                         "traffic": (traffic or {}).get("fv_substep_bytes_per_launch")},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+    return result
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle port, NumPy, 1 core)
+# ---------------------------------------------------------------------------
+def cpu_path_step(state, cut_cmd, mat):
+    from oracle import labels as L
+    from oracle import mobile_v2 as M
+
+    b, h, q, z = state
+    idx, tgt = cut_cmd
+    if len(idx):
+        fb, fh = b.ravel(), h.ravel()
+        avail = np.maximum(fb[idx] - z.ravel()[idx], 0.0)
+        d = np.minimum(np.maximum(fb[idx] - tgt, 0.0), avail)
+        fb[idx] -= d
+        fh[idx] += d
+    cfg = M.OracleConfig(dx_m=DX, dy_m=DX, start_angle_deg=mat.start_angle_deg,
+                         stop_angle_deg=mat.stop_angle_deg,
+                         basal_friction_coefficient=mat.mobile_friction_coefficient)
+    s = M.step(cfg, b, h, q, DT)
+    y = L.yield_init(b, z, s.h, s.q[..., 0], s.q[..., 1], dx=DX, dy=DX,
+                     tan_start=np.tan(np.deg2rad(mat.start_angle_deg)),
+                     tan_stop=np.tan(np.deg2rad(mat.stop_angle_deg)),
+                     density=mat.assumed_bulk_density_kg_m3, gravity=9.81, cohesion=0.0,
+                     mobilization_depth=0.08, dry=1e-8)
+    L.canonical_labels(y["unstable"], 8)
+    return (b, s.h, s.q, z), s.substeps
+
+
+def cpu_baseline(sample_steps: int = 6, warm_steps: int = 30, budget_s: float = 25.0):
+    from soilb200 import workloads
+    cfg = workloads.config1(N, seed=1, dx=DX)
+    mat = material()
+    sched = cut_schedule(cfg["cut"], warm_steps + sample_steps, pinned=False)
+    state = (cfg["b_eff"].copy(), np.zeros((N, N)), np.zeros((N, N, 2)), cfg["z_base"])
+    # warm-up cut with no flow (entrainment only) keeps the sample bounded
+    for k in range(warm_steps):
+        idx, tgt = sched[k]
+        fb, fh = state[0].ravel(), state[1].ravel()
+        d = np.maximum(fb[idx] - tgt, 0.0)
+        fb[idx] -= d
+        fh[idx] += d
+    t0 = time.perf_counter()
+    subs = 0
+    done = 0
+    for k in range(warm_steps, warm_steps + sample_steps):
+        state, n = cpu_path_step(state, sched[k], mat)
+        subs += n
+        done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": N * N * subs / el if el > 0 else 0.0, "unit": UNIT, "cores": 1,
+            "kind": "port",
+            "sample": f"{done} physics steps ({subs} substeps) of the config-1 plain path on "
+                      f"the CPU oracle (NumPy FP64 restatement of MobileV2ReferenceSolver + "
+                      f"yield/labelling), after {warm_steps} cut steps; {el:.1f} s"}
+
+
+def run_reference(args):
+    """--impl reference: the CPU restatement of the path, on this host."""
+    from soilb200 import workloads
+    cfg = workloads.config1(N, seed=1, dx=DX)
+    mat = material()
+    total = args.warmup + args.steps
+    sched = cut_schedule(cfg["cut"], total, pinned=False)
+    state = (cfg["b_eff"].copy(), np.zeros((N, N)), np.zeros((N, N, 2)), cfg["z_base"])
+    for k in range(args.warmup):
+        state, _ = cpu_path_step(state, sched[k], mat)
+    t0 = time.perf_counter()
+    subs = 0
+    for k in range(args.warmup, total):
+        state, n = cpu_path_step(state, sched[k], mat)
+        subs += n
+    el = time.perf_counter() - t0
+    value = N * N * subs / el if el > 0 else 0.0
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": el * 1000.0 / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded config-1 value-noise pile + bucket cut)",
+            "config": {"workload": "config1_plain_path_701", "grid": [N, N], "dx_m": DX,
+                       "dt_s": DT},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                             "sample": f"{args.steps} physics steps ({subs} substeps) after "
+                                       f"{args.warmup} warm-up steps, NumPy oracle, 1 core"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)))
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    result = run_gpu(args, rank, world, local_rank)
+    if rank == 0:
+        if not args.no_cpu_baseline:
+            result["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(result))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -125,6 +125,8 @@ typedef struct sb_mobile_ledger {
   double min_h_m;
   int64_t mass_quanta;         /* SB_FX32: exact sum of h quanta */
   int64_t volume_w_quanta;     /* SB_FX32: exact sum of h quanta * (6 w / dx dy) */
+  double resting_volume_w_m3;  /* sum(max(b_eff - z_base, 0) w) (reservoir_reduction) */
+  int64_t resting_w_quanta;    /* SB_FX32: exact form of resting_volume_w_m3 */
 } sb_mobile_ledger;
 
 typedef struct sb_mobile_stats {
@@ -140,6 +142,7 @@ typedef struct sb_mobile_stats {
   double external_work;            /* per unit density */
   sb_mobile_ledger before;
   sb_mobile_ledger after;
+  double substep_loop_ms;      /* device time of the substep loop (CUDA events) */
 } sb_mobile_stats;
 
 int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out);
@@ -156,9 +159,108 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params,
 int sb_mobile_ledger_of(sb_ctx* ctx, const sb_mobile_params* params,
                         sb_mobile_ledger* out);
 
+/* ---- Large-avalanche (FailureZone) labelling ---------------------------- */
+/* Material/config keys of DeviceLargeAvalancheBridge.initialize
+ * (runtime/gpu_large_avalanche.py:541-566); angles are passed both as tangents
+ * and radians so callers can compute them exactly as the reference does. */
+typedef struct sb_label_params {
+  double tan_start;
+  double tan_stop;
+  double start_rad;
+  double stop_rad;
+  double density_kg_m3;
+  double gravity_m_s2;
+  double cohesion_pa;
+  double mobilization_depth_m;
+  double dry_tolerance_m;
+  double activity_speed_m_s;
+  int connectivity;            /* 4 or 8 */
+  int release_settled_latches;
+} sb_label_params;
+
+typedef struct sb_label_stats {
+  int status;
+  int unstable_cell_count;
+  int connected_region_count;
+  int largest_connected_cell_count;
+  int winner_root;             /* canonical label (min flat index) of the winner */
+  int union_passes;
+  int previous_overlap;        /* winner cells that were in the previous component */
+  int pad;
+  double largest_connected_area_m2;
+  double largest_connected_mobilizable_volume_m3;
+  double excess_start_sum_rad; /* over winner cells */
+  double excess_start_max_rad;
+  double excess_stop_sum_rad;
+  double excess_stop_max_rad;
+} sb_label_stats;
+
+/* Yield initialisation + connected components + component reductions. */
+int sb_label(sb_ctx* ctx, const sb_label_params* params, sb_label_stats* out);
+/* Components of a caller-provided int32 mask (nonzero = member); replaces the
+ * CPU _largest_connected_region(mask, connectivity)
+ * (bulk_interaction/large_avalanche.py:711-778).  Labels via SB_FIELD_LABELS. */
+int sb_label_mask(sb_ctx* ctx, const int32_t* mask, int connectivity, sb_label_stats* out);
+/* update_previous_and_tiles (gpu_large_avalanche.py:277-306): previous-component
+ * mask and, when seed_frontier, frontier_reached + the frontier tile flags. */
+int sb_label_commit(sb_ctx* ctx, int keep_candidate, int seed_frontier);
+
+/* ---- Repose relaxation ---------------------------------------------------- */
+typedef struct sb_relax_params {
+  double spacing0_m;           /* spacing along axis 0 (rows) */
+  double spacing1_m;           /* spacing along axis 1 (columns) */
+  double critical_slope;       /* tan(critical angle) */
+  double tolerance_m;
+  int max_iterations;          /* full: iterations; frontier: rounds */
+  int weighted;                /* frontier: Triangle-A-C vertex weights, else uniform */
+} sb_relax_params;
+
+typedef struct sb_relax_stats {
+  int iterations;              /* full: iterations run; frontier: rounds */
+  int converged;
+  int status;
+  int active_tiles;            /* frontier: active tiles at the last round start */
+  int moved_edges;             /* frontier: transfers applied */
+  int pad;
+} sb_relax_stats;
+
+/* relax_critical_slope on SB_FIELD_B_EFF (slope_model.py:273-343). */
+int sb_relax_full(sb_ctx* ctx, const sb_relax_params* params, sb_relax_stats* out);
+/* Frontier seeds: reached := 1 at the cells and their 3x3-stencil tiles become
+ * active (_seed_gpu_residual_frontier, v2_physics_core.py:1153-1170). */
+int sb_frontier_seed_cells(sb_ctx* ctx, const int32_t* flat_indices, int count);
+/* Activate tiles directly (tile id = row_tile * tiles_x + col_tile). */
+int sb_frontier_seed_tiles(sb_ctx* ctx, const int32_t* tile_ids, int count);
+/* Residual frontier rounds on SB_FIELD_B_EFF until no tile is active. */
+int sb_frontier_run(sb_ctx* ctx, const sb_relax_params* params, sb_relax_stats* out);
+/* Copies the next-round active tile flags (int32 per tile) to the host. */
+int sb_frontier_active_tiles(sb_ctx* ctx, int32_t* flags, int capacity);
+int sb_frontier_tile_count(sb_ctx* ctx);
+/* out4 = {sum of values, max 8-neighbour slope, min value, sum of quanta (SB_FX32)}
+ * of SB_FIELD_B_EFF or SB_FIELD_Z_BASE (RelaxationStats volume / max_slope,
+ * slope_model.py:261-270, :331-342). */
+int sb_field_stats(sb_ctx* ctx, int field, double spacing0_m, double spacing1_m, double* out4);
+
+/* ---- Resting <-> Mobile exchange (runtime/bulk_state_authority.py:103-149,
+ *      entrain_host_indices / deposit_host_indices :920-1034) ------------ */
+/* b_eff -= d, mobile += d with d = min(max(depth,0), max(b_eff - z_base, 0));
+ * volume_m3 = sum(d * w) (exact in SB_FX32). */
+int sb_entrain(sb_ctx* ctx, const int32_t* flat_indices, const double* requested_depth_m,
+               int count, double* volume_m3);
+/* Same, with the requested depth b_eff - target_surface (a cut to a surface). */
+int sb_entrain_to_surface(sb_ctx* ctx, const int32_t* flat_indices,
+                          const double* target_surface_m, int count, double* volume_m3);
+/* mobile -= d, b_eff += d, momentum scaled by the retained fraction;
+ * out3 = {deposited volume m3, removed momentum x, y (density * q * w)}. */
+int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double* requested_depth_m,
+               int count, double density_kg_m3, double* out3);
+
 int sb_last_error(sb_ctx* ctx, char* buffer, size_t length);
 /* Number of kernels this context has launched (cumulative). */
 int64_t sb_kernel_launch_count(sb_ctx* ctx);
+/* The cudaStream_t every operation of this context is issued on (for timing
+ * with events or ordering caller work; do not destroy it). */
+void* sb_stream(sb_ctx* ctx);
 const char* sb_version(void);
 /* sizeof() of an ABI struct by name ("sb_grid_desc", "sb_mobile_params",
  * "sb_mobile_ledger", "sb_mobile_stats", ...); 0 if unknown.  Lets bindings

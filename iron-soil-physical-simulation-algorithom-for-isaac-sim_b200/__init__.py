@@ -20,6 +20,21 @@ from .mobile_v2 import (  # noqa: F401
     MobileV2Step,
 )
 
+from .avalanche import (  # noqa: F401
+    B200LargeAvalancheBridge,
+    LabelDiagnosis,
+    LargeAvalancheTransitionConfig,
+    MaterialScenario,
+    label_mask,
+    largest_connected_region,
+)
+from .relax import (  # noqa: F401
+    FrontierRelaxation,
+    FrontierStats,
+    RelaxationStats,
+    relax_critical_slope,
+)
+
 # Reference-compatible aliases: code written against the reference's Warp
 # device solver can switch by changing only the import.
 WarpMobileV2ReferenceSolver = B200MobileV2Solver
@@ -28,4 +43,7 @@ __all__ = [
     "B200BackendUnavailable", "B200DeviceError", "NumericalNonconvergenceError",
     "DeviceGrid", "choose_quantization", "B200MobileV2Solver", "MobileV2Config",
     "MobileV2State", "MobileV2Step", "WarpMobileV2ReferenceSolver",
+    "B200LargeAvalancheBridge", "LabelDiagnosis", "LargeAvalancheTransitionConfig",
+    "MaterialScenario", "FrontierRelaxation", "FrontierStats", "RelaxationStats",
+    "relax_critical_slope", "label_mask", "largest_connected_region",
 ]

@@ -85,7 +85,8 @@ class MobileLedger(C.Structure):
         ("kinetic_w_j", C.c_double), ("potential_w_j", C.c_double),
         ("pressure_w_j", C.c_double), ("max_speed_m_s", C.c_double),
         ("min_h_m", C.c_double), ("mass_quanta", C.c_int64),
-        ("volume_w_quanta", C.c_int64),
+        ("volume_w_quanta", C.c_int64), ("resting_volume_w_m3", C.c_double),
+        ("resting_w_quanta", C.c_int64),
     ]
 
 
@@ -98,6 +99,43 @@ class MobileStats(C.Structure):
         ("external_impulse_m4_s", C.c_double * 2),
         ("friction_dissipation", C.c_double), ("external_work", C.c_double),
         ("before", MobileLedger), ("after", MobileLedger),
+        ("substep_loop_ms", C.c_double),
+    ]
+
+
+class LabelParams(C.Structure):
+    _fields_ = [
+        ("tan_start", C.c_double), ("tan_stop", C.c_double), ("start_rad", C.c_double),
+        ("stop_rad", C.c_double), ("density_kg_m3", C.c_double), ("gravity_m_s2", C.c_double),
+        ("cohesion_pa", C.c_double), ("mobilization_depth_m", C.c_double),
+        ("dry_tolerance_m", C.c_double), ("activity_speed_m_s", C.c_double),
+        ("connectivity", C.c_int), ("release_settled_latches", C.c_int),
+    ]
+
+
+class LabelStats(C.Structure):
+    _fields_ = [
+        ("status", C.c_int), ("unstable_cell_count", C.c_int),
+        ("connected_region_count", C.c_int), ("largest_connected_cell_count", C.c_int),
+        ("winner_root", C.c_int), ("union_passes", C.c_int), ("previous_overlap", C.c_int),
+        ("pad", C.c_int), ("largest_connected_area_m2", C.c_double),
+        ("largest_connected_mobilizable_volume_m3", C.c_double),
+        ("excess_start_sum_rad", C.c_double), ("excess_start_max_rad", C.c_double),
+        ("excess_stop_sum_rad", C.c_double), ("excess_stop_max_rad", C.c_double),
+    ]
+
+
+class RelaxParams(C.Structure):
+    _fields_ = [
+        ("spacing0_m", C.c_double), ("spacing1_m", C.c_double), ("critical_slope", C.c_double),
+        ("tolerance_m", C.c_double), ("max_iterations", C.c_int), ("weighted", C.c_int),
+    ]
+
+
+class RelaxStats(C.Structure):
+    _fields_ = [
+        ("iterations", C.c_int), ("converged", C.c_int), ("status", C.c_int),
+        ("active_tiles", C.c_int), ("moved_edges", C.c_int), ("pad", C.c_int),
     ]
 
 
@@ -116,8 +154,25 @@ _PROTOTYPES = {
                                       C.POINTER(MobileLedger)]),
     "sb_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "sb_kernel_launch_count": (C.c_int64, [C.c_void_p]),
+    "sb_stream": (C.c_void_p, [C.c_void_p]),
     "sb_version": (C.c_char_p, []),
     "sb_sizeof": (C.c_size_t, [C.c_char_p]),
+    "sb_label": (C.c_int, [C.c_void_p, C.POINTER(LabelParams), C.POINTER(LabelStats)]),
+    "sb_label_commit": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "sb_label_mask": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LabelStats)]),
+    "sb_relax_full": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams), C.POINTER(RelaxStats)]),
+    "sb_frontier_seed_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "sb_frontier_seed_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "sb_frontier_run": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams), C.POINTER(RelaxStats)]),
+    "sb_frontier_active_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "sb_frontier_tile_count": (C.c_int, [C.c_void_p]),
+    "sb_field_stats": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p]),
+    "sb_entrain": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                             C.POINTER(C.c_double)]),
+    "sb_entrain_to_surface": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.POINTER(C.c_double)]),
+    "sb_deposit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                             C.c_void_p]),
 }
 
 # ctypes mirror of each ABI struct, checked against sb_sizeof() in the tests.
@@ -126,6 +181,10 @@ ABI_STRUCTS = {
     "sb_mobile_params": MobileParams,
     "sb_mobile_ledger": MobileLedger,
     "sb_mobile_stats": MobileStats,
+    "sb_label_params": LabelParams,
+    "sb_label_stats": LabelStats,
+    "sb_relax_params": RelaxParams,
+    "sb_relax_stats": RelaxStats,
 }
 
 

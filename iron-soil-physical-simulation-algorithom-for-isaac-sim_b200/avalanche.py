@@ -1,0 +1,237 @@
+"""Large-avalanche (FailureZone) labelling on the GPU.
+
+Mirrors the diagnosis part of the reference's ``DeviceLargeAvalancheBridge``
+(``runtime/gpu_large_avalanche.py:469-676``): cohesive start/stop yield on the
+free surface, 8- (or 4-) connected components of the unstable mask with
+canonical min-index labels, the largest component (ties -> smallest label),
+its area / mobilizable volume / slope excess, persistence in physical time
+and the classification ``NO_LARGE_EVENT`` / ``LOCAL_STATIC_INSTABILITY`` /
+``PERSISTING_LARGE_UNSTABLE_REGION`` / ``LARGE_AVALANCHE_MOBILE_PATH``
+(:645-676), then ``update_previous_and_tiles`` which seeds the residual
+frontier for local instabilities (:277-306).  ``MaterialScenario`` and
+``LargeAvalancheTransitionConfig`` are restated with the reference's fields
+(``bulk_state/models.py:51-62``; ``bulk_interaction/large_avalanche.py:38-144``).
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib
+from .grid import DeviceGrid
+
+LITERATURE_REDUCED_ORDER_UNCALIBRATED = "LITERATURE_BASED_REDUCED_ORDER_UNCALIBRATED"
+
+
+@dataclass(frozen=True)
+class MaterialScenario:
+    name: str
+    assumed_bulk_density_kg_m3: float
+    internal_friction_angle_deg: float
+    cohesion_proxy_pa: float
+    tool_friction_coefficient: float
+    start_angle_deg: float
+    stop_angle_deg: float
+    mobile_friction_coefficient: float
+
+    def __post_init__(self) -> None:
+        if not isinstance(self.name, str) or not self.name.strip():
+            raise ValueError("[MaterialScenario] name must be non-empty")
+        if not self.assumed_bulk_density_kg_m3 > 0.0:
+            raise ValueError("[MaterialScenario] assumed density must be > 0")
+        if self.cohesion_proxy_pa < 0.0:
+            raise ValueError("[MaterialScenario] cohesion must be non-negative")
+
+
+@dataclass(frozen=True)
+class LargeAvalancheTransitionConfig:
+    minimum_connected_cells: int = 32
+    minimum_connected_area_m2: float = 0.08
+    minimum_mobilizable_volume_m3: float = 0.004
+    minimum_mean_excess_start_deg: float = 0.0
+    persistence_time_s: float = 0.12
+    mobilization_depth_m: float = 0.08
+    gravity_velocity_length_m: float = 0.25
+    velocity_efficiency: float = 0.45
+    mobile_activity_speed_m_s: float = 0.05
+    mobile_activity_volume_m3: float = 1.0e-5
+    dry_tolerance_m: float = 1.0e-8
+    settled_mobile_volume_m3: float = 1.0e-5
+    settled_speed_m_s: float = 0.05
+    connectivity: int = 8
+    parameter_basis: str = LITERATURE_REDUCED_ORDER_UNCALIBRATED
+    sensitivity_case: str = "nominal_uncalibrated"
+
+    def __post_init__(self) -> None:
+        if not isinstance(self.minimum_connected_cells, int) or self.minimum_connected_cells < 1:
+            raise ValueError("[LargeAvalanche] minimum_connected_cells must be >= 1")
+        if self.connectivity not in (4, 8):
+            raise ValueError("[LargeAvalanche] connectivity must be 4 or 8")
+        numeric = np.asarray([
+            self.minimum_connected_area_m2, self.minimum_mobilizable_volume_m3,
+            self.minimum_mean_excess_start_deg, self.persistence_time_s,
+            self.mobilization_depth_m, self.gravity_velocity_length_m, self.velocity_efficiency,
+            self.mobile_activity_speed_m_s, self.mobile_activity_volume_m3, self.dry_tolerance_m,
+            self.settled_mobile_volume_m3, self.settled_speed_m_s], dtype=np.float64)
+        if not np.all(np.isfinite(numeric)) or np.any(numeric < 0.0):
+            raise ValueError("[LargeAvalanche] numeric configuration must be finite/non-negative")
+        if self.persistence_time_s <= 0.0:
+            raise ValueError("[LargeAvalanche] persistence_time_s must be positive")
+        if self.mobilization_depth_m <= 0.0 or self.gravity_velocity_length_m <= 0.0:
+            raise ValueError("[LargeAvalanche] failure depth/velocity length must be positive")
+        if not 0.0 < self.velocity_efficiency <= 1.0:
+            raise ValueError("[LargeAvalanche] velocity_efficiency must lie in (0, 1]")
+        if self.parameter_basis != LITERATURE_REDUCED_ORDER_UNCALIBRATED:
+            raise ValueError("[LargeAvalanche] transition parameters must remain explicitly "
+                             "literature-based reduced-order / uncalibrated")
+        if not self.sensitivity_case:
+            raise ValueError("[LargeAvalanche] sensitivity_case must be non-empty")
+
+    @classmethod
+    def from_mapping(cls, value: dict) -> "LargeAvalancheTransitionConfig":
+        if not isinstance(value, dict):
+            raise TypeError("[LargeAvalanche] configuration must be a mapping")
+        names = {f.name for f in fields(cls)}
+        unknown = sorted(set(value) - names)
+        if unknown:
+            raise ValueError(f"[LargeAvalanche] unknown configuration fields: {unknown}")
+        return cls(**value)
+
+
+@dataclass(frozen=True)
+class LabelDiagnosis:
+    """Diagnosis subset of the reference ``DeviceLargeAvalancheResult`` (:469-507)."""
+
+    classification: str
+    unstable_cell_count: int
+    connected_region_count: int
+    largest_connected_cell_count: int
+    largest_connected_area_m2: float
+    largest_connected_mobilizable_volume_m3: float
+    mean_excess_start_deg: float
+    maximum_excess_start_deg: float
+    mean_excess_stop_deg: float
+    maximum_excess_stop_deg: float
+    persistence_s: float
+    candidate: bool
+    transition_ready: bool
+    winner_label: int
+    union_iterations: int
+
+
+class B200LargeAvalancheBridge:
+    NO_LARGE_EVENT = "NO_LARGE_EVENT"
+    LOCAL_STATIC_INSTABILITY = "LOCAL_STATIC_INSTABILITY"
+    PERSISTING_LARGE_UNSTABLE_REGION = "PERSISTING_LARGE_UNSTABLE_REGION"
+    LARGE_AVALANCHE_MOBILE_PATH = "LARGE_AVALANCHE_MOBILE_PATH"
+
+    def __init__(self, grid: DeviceGrid, material: MaterialScenario,
+                 config: LargeAvalancheTransitionConfig | None = None, *,
+                 gravity_m_s2: float = 9.81) -> None:
+        self.grid = grid
+        self.material = material
+        self.config = config or LargeAvalancheTransitionConfig()
+        self.gravity = float(gravity_m_s2)
+        self._persistence_s = 0.0
+        self._has_previous = False
+
+    def reset(self) -> None:
+        self._persistence_s = 0.0
+        self._has_previous = False
+
+    def _params(self, release: bool) -> _lib.LabelParams:
+        start = float(np.deg2rad(self.material.start_angle_deg))
+        stop = float(np.deg2rad(self.material.stop_angle_deg))
+        return _lib.LabelParams(
+            float(np.tan(start)), float(np.tan(stop)), start, stop,
+            float(self.material.assumed_bulk_density_kg_m3), self.gravity,
+            float(self.material.cohesion_proxy_pa), float(self.config.mobilization_depth_m),
+            float(self.config.dry_tolerance_m), float(self.config.mobile_activity_speed_m_s),
+            int(self.config.connectivity), 1 if release else 0)
+
+    def label(self, *, release_settled_latches: bool = True) -> _lib.LabelStats:
+        """Yield + components + component reductions (no classification)."""
+        st = _lib.LabelStats()
+        _lib.check(self.grid.ctx, _lib.load().sb_label(
+            self.grid.ctx, self._params(release_settled_latches), st), "label")
+        return st
+
+    def labels(self) -> np.ndarray:
+        """Canonical labels: -1 for stable cells, else the component's min flat index."""
+        return self.grid.download("labels")
+
+    def observe(self, dt_s: float, *, release_settled_latches: bool = True) -> LabelDiagnosis:
+        dt = float(dt_s)
+        if not np.isfinite(dt) or dt <= 0.0:
+            raise ValueError("[GpuLargeAvalanche] dt_s must be finite/positive")
+        st = self.label(release_settled_latches=release_settled_latches)
+        cfg = self.config
+        largest = int(st.largest_connected_cell_count)
+        area = float(st.largest_connected_area_m2)
+        volume = float(st.largest_connected_mobilizable_volume_m3)
+        mean_start = float(np.rad2deg(st.excess_start_sum_rad / largest)) if largest else 0.0
+        mean_stop = float(np.rad2deg(st.excess_stop_sum_rad / largest)) if largest else 0.0
+        extent_pass = largest >= cfg.minimum_connected_cells and area >= cfg.minimum_connected_area_m2
+        volume_pass = volume >= cfg.minimum_mobilizable_volume_m3
+        excess_pass = mean_start >= cfg.minimum_mean_excess_start_deg
+        candidate = extent_pass and volume_pass and excess_pass
+        overlap = int(st.previous_overlap) > 0
+        if candidate:
+            self._persistence_s = (self._persistence_s + dt if overlap or not self._has_previous
+                                   else dt)
+        else:
+            self._persistence_s = 0.0
+        ready = candidate and self._persistence_s >= cfg.persistence_time_s
+        if ready:
+            cls = self.LARGE_AVALANCHE_MOBILE_PATH
+        elif candidate:
+            cls = self.PERSISTING_LARGE_UNSTABLE_REGION
+        elif int(st.unstable_cell_count) > 0:
+            cls = self.LOCAL_STATIC_INSTABILITY
+        else:
+            cls = self.NO_LARGE_EVENT
+        _lib.check(self.grid.ctx, _lib.load().sb_label_commit(
+            self.grid.ctx, 1 if candidate else 0,
+            1 if cls == self.LOCAL_STATIC_INSTABILITY else 0), "label commit")
+        self._has_previous = candidate
+        return LabelDiagnosis(
+            cls, int(st.unstable_cell_count), int(st.connected_region_count), largest, area,
+            volume, mean_start, float(np.rad2deg(st.excess_start_max_rad)), mean_stop,
+            float(np.rad2deg(st.excess_stop_max_rad)), self._persistence_s, candidate, ready,
+            int(st.winner_root), int(st.union_passes))
+
+
+def label_mask(grid: DeviceGrid, mask: np.ndarray, connectivity: int = 8):
+    """Connected components of ``mask`` on the GPU -> (canonical labels, LabelStats)."""
+    m = np.ascontiguousarray(np.asarray(mask, dtype=bool).astype(np.int32))
+    if m.shape != grid.shape:
+        raise ValueError("[LargeAvalanche] connected mask must match the grid shape")
+    st = _lib.LabelStats()
+    _lib.check(grid.ctx, _lib.load().sb_label_mask(grid.ctx, m.ctypes.data, int(connectivity), st),
+               "label mask")
+    return grid.download("labels"), st
+
+
+def largest_connected_region(mask: np.ndarray, connectivity: int, *, device: int = 0):
+    """GPU drop-in for ``_largest_connected_region`` (large_avalanche.py:711-778).
+
+    Returns (largest component mask, region count, largest size).  Ties resolve
+    to the component with the smallest flat index, which is also the first
+    maximum in the reference's run-order dictionary.
+    """
+    source = np.asarray(mask, dtype=bool)
+    if source.ndim != 2:
+        raise ValueError("[LargeAvalanche] connected mask must be 2-D")
+    if not np.any(source):
+        return np.zeros_like(source), 0, 0
+    if min(source.shape) < 2:
+        raise ValueError("[soilb200] masks need at least 2 rows and 2 columns")
+    grid = DeviceGrid(source.shape, 1.0, 1.0, precision="fx32", device=device)
+    try:
+        labels, st = label_mask(grid, source, connectivity)
+    finally:
+        grid.close()
+    return labels == int(st.winner_root), int(st.connected_region_count), \
+        int(st.largest_connected_cell_count)

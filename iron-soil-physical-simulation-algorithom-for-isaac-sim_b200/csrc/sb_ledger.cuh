@@ -15,11 +15,12 @@ namespace sb {
 
 enum LedgerSlot {
   L_HSUM = 0, L_HSUM_W, L_QX, L_QY, L_QX_W, L_QY_W, L_HS2, L_HS2_W, L_HB, L_HB_W, L_HH, L_HH_W,
+  L_REST_W,  // FP64: sum max(b - z, 0) * w6
   L_NSUM,
   L_MAXSPEED = L_NSUM, L_NEGMINH, L_MAXQ, L_MAXGRAD, L_MAXWAVE, L_MAXEXT,
   L_NP
 };
-constexpr int kLedgerI64 = 2;  // h quanta, h quanta * w6
+constexpr int kLedgerI64 = 3;  // h quanta, h quanta * w6, max(b - z, 0) quanta * w6
 
 struct LedgerOut {
   double v[L_NP];
@@ -34,6 +35,7 @@ struct StepIO {  // per-step device record: ledgers before/after + loop control
 template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     ledger_kernel(const FvConst c, const typename FvTypes<FX>::B* __restrict__ b,
+                  const typename FvTypes<FX>::B* __restrict__ z,
                   const typename FvTypes<FX>::H* __restrict__ h0,
                   const typename FvTypes<FX>::H* __restrict__ h1,
                   const typename FvTypes<FX>::R* __restrict__ qx0,
@@ -54,7 +56,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (int k = 0; k < L_NP; ++k) v[k] = 0.0;
   v[L_NEGMINH] = -1.0e300;
-  long long iq0 = 0, iq1 = 0;
+  long long iq0 = 0, iq1 = 0, iq2 = 0;
   const long long ncell = (long long)c.ny * c.nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncell;
        i += (long long)gridDim.x * blockDim.x) {
@@ -77,6 +79,8 @@ __global__ void __launch_bounds__(kThreads)
       bv = (double)b[gi] * c.Q + datum;
       iq0 += hq;
       iq1 += (long long)hq * w6;
+      const long long rest = (long long)b[gi] - (long long)z[gi];
+      iq2 += (rest > 0 ? rest : 0) * w6;
       const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
       const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
       const double gx = ((double)(Hr - Hl) * c.Q) / denx;
@@ -87,6 +91,7 @@ __global__ void __launch_bounds__(kThreads)
       bv = b[gi];
       v[L_HSUM] += hv;
       v[L_HSUM_W] += hv * w6;
+      v[L_REST_W] += fmax(b[gi] - z[gi], 0.0) * w6;
       const double gx = ((b[ir] + h[ir]) - (b[il] + h[il])) / denx;
       const double gy = ((b[iup] + h[iup]) - (b[idn] + h[idn])) / deny;
       grad = hypot(gx, gy);
@@ -140,11 +145,13 @@ __global__ void __launch_bounds__(kThreads)
   for (int k = 0; k < L_NP; ++k) v[k] = k < L_NSUM ? warp_sum(v[k]) : warp_max(v[k]);
   iq0 = (long long)warp_sum_u64((unsigned long long)iq0);
   iq1 = (long long)warp_sum_u64((unsigned long long)iq1);
+  iq2 = (long long)warp_sum_u64((unsigned long long)iq2);
   if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < L_NP; ++k) red[warp * L_NP + k] = v[k];
-    ired[warp * 2] = iq0;
-    ired[warp * 2 + 1] = iq1;
+    ired[warp * kLedgerI64] = iq0;
+    ired[warp * kLedgerI64 + 1] = iq1;
+    ired[warp * kLedgerI64 + 2] = iq2;
   }
   __syncthreads();
   if (threadIdx.x < L_NP) {
@@ -156,7 +163,7 @@ __global__ void __launch_bounds__(kThreads)
   } else if (threadIdx.x < L_NP + kLedgerI64) {
     const int k = threadIdx.x - L_NP;
     long long a = 0;
-    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * 2 + k];
+    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + k];
     ipartials[(size_t)blockIdx.x * kLedgerI64 + k] = a;
   }
   __threadfence();

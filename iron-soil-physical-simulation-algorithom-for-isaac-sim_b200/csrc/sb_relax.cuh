@@ -1,0 +1,463 @@
+// Repose (MiniSlope) relaxation kernels.
+//
+// Arrays are generic 2-D fields whose axis 0 (rows) uses spacing s0 and axis 1
+// (columns) spacing s1, the convention of the reference's
+// ``relax_critical_slope(height, grid_spacing)`` (slope_model.py:273-343).
+// Direction order and parity rule follow ``_neighbor_pairs`` (:744-750): for
+// (d0, d1) in ((1,0,s0), (0,1,s1), (1,1,hyp), (1,-1,hyp)), parity on the
+// axis-0 coordinate of endpoint a when d0 != 0, else on its axis-1 coordinate.
+//
+// relax_full_kernel      -- one full-domain iteration (8 colour sub-phases) per
+//                           launch with temporal blocking: a (T+2*8)^2 halo
+//                           box is TMA-loaded into shared memory, all eight
+//                           sub-phases run there (the exact region shrinks by
+//                           one cell per sub-phase), the T^2 interior is
+//                           written back; the iteration's max excess (over all
+//                           pairs of each sub-phase, before its update) feeds
+//                           the convergence test on the device.
+// frontier_*_kernel      -- production compact-frontier rounds
+//                           (runtime/v2_physics_core.py:1172-1254 over
+//                           solvers/warp_compact_frontier.py:56-130): per tile
+//                           CTAs, reached-gated weighted transfers, tile
+//                           activation of the 3x3 cell stencil around moved
+//                           endpoints, final scan -> next active tiles.
+#pragma once
+
+#include "sb_common.cuh"
+#include "sb_fv.cuh"
+
+namespace sb {
+
+constexpr int kRelaxTile = 32;
+constexpr int kRelaxHalo = 8;
+constexpr int kRelaxBox = kRelaxTile + 2 * kRelaxHalo;  // 48
+
+struct RelaxConst {
+  int n0, n1, pitch, tiles1, ntiles;
+  double s0, s1;
+  double crit[4];       // tan(angle) * L per direction
+  double crit_q[4];     // FX: crit / Q
+  double tol, tol_q;
+  int max_iterations;
+  int weighted;         // frontier: Triangle-A-C vertex weights (else uniform)
+  int ftile;            // frontier tile size
+  double f;             // weight unit s0*s1/6
+};
+
+struct RelaxControl {
+  int iterations;
+  int done;
+  int converged;
+  int status;
+  unsigned long long max_excess_bits;  // double bits of this iteration's max excess
+  unsigned int arrive;
+  int parity;        // buffer holding the current field (full relax)
+  int n_active;      // frontier: active tiles at the start of the last round
+  int rounds;
+  int moved_edges;
+  int pad;
+};
+
+__device__ __forceinline__ void dir_of(int d, int& d0, int& d1) {
+  d0 = d == 1 ? 0 : 1;
+  d1 = d == 0 ? 0 : (d == 3 ? -1 : 1);
+}
+
+// ------------------------------------------------------------------------
+// Full-domain relaxation (one iteration per launch).
+// ------------------------------------------------------------------------
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    relax_full_kernel(const RelaxConst c, const __grid_constant__ CUtensorMap tm0,
+                      const __grid_constant__ CUtensorMap tm1,
+                      typename FvTypes<FX>::H* __restrict__ f0,
+                      typename FvTypes<FX>::H* __restrict__ f1, RelaxControl* ctl,
+                      cudaGraphConditionalHandle handle, int use_handle) {
+  using H = typename FvTypes<FX>::H;
+  __shared__ alignas(128) H s[kRelaxBox * kRelaxBox];
+  __shared__ alignas(8) uint64_t bar;
+  __shared__ double red[kThreads / 32];
+  __shared__ int last;
+  if (*(volatile int*)&ctl->done) return;
+  const int parity_buf = ctl->parity;
+  const int t1 = blockIdx.x % c.tiles1, t0 = blockIdx.x / c.tiles1;
+  const int g0 = t0 * kRelaxTile - kRelaxHalo, g1 = t1 * kRelaxTile - kRelaxHalo;
+  if (threadIdx.x == 0) mbar_init(&bar, 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(&bar, kRelaxBox * kRelaxBox * (unsigned)sizeof(H));
+    tma_load_2d(s, parity_buf ? &tm1 : &tm0, g1, g0, &bar);
+  }
+  const bool loaded = mbar_wait(&bar, 0);
+  double worst = 0.0;
+  const int npairs = kRelaxBox * kRelaxBox;
+  for (int d = 0; d < 4; ++d) {
+    int d0, d1;
+    dir_of(d, d0, d1);
+    for (int par = 0; par < 2; ++par) {
+      // (1) max excess over pairs owned by the interior, both parities, pre-update
+      for (int k = threadIdx.x; k < kRelaxTile * kRelaxTile; k += kThreads) {
+        const int la0 = kRelaxHalo + k / kRelaxTile, la1 = kRelaxHalo + k % kRelaxTile;
+        const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
+        if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+        const int ia = la0 * kRelaxBox + la1, ib = (la0 + d0) * kRelaxBox + la1 + d1;
+        double ex;
+        if constexpr (FX) {
+          const long long df = (long long)s[ia] - (long long)s[ib];
+          ex = (double)(df < 0 ? -df : df) - c.crit_q[d];  // in quanta
+        } else {
+          ex = fmax(fabs(s[ia] - s[ib]) - c.crit[d], 0.0);
+        }
+        worst = fmax(worst, ex);
+      }
+      __syncthreads();
+      // (2) Jacobi update of the active-parity pairs inside the box
+      if (loaded) {
+        for (int k = threadIdx.x; k < npairs; k += kThreads) {
+          const int la0 = k / kRelaxBox, la1 = k % kRelaxBox;
+          const int lb0 = la0 + d0, lb1 = la1 + d1;
+          if (lb0 >= kRelaxBox || lb1 < 0 || lb1 >= kRelaxBox) continue;
+          const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
+          if (a0 < 0 || a1 < 0 || a0 >= c.n0 || a1 >= c.n1) continue;
+          if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+          if ((((d0 ? a0 : a1) & 1)) != par) continue;
+          const int ia = k, ib = lb0 * kRelaxBox + lb1;
+          if constexpr (FX) {
+            const long long df = (long long)s[ia] - (long long)s[ib];
+            const double ex = (double)(df < 0 ? -df : df) - c.crit_q[d];
+            if (ex > 0.0) {
+              const long long t = (long long)ceil(ex * 0.5);
+              const long long st = df < 0 ? -t : t;
+              s[ia] = (H)(s[ia] - st);
+              s[ib] = (H)(s[ib] + st);
+            }
+          } else {
+            const double diff = s[ia] - s[ib];
+            const double ex = fmax(fabs(diff) - c.crit[d], 0.0);
+            const double sg = diff > 0.0 ? 1.0 : (diff < 0.0 ? -1.0 : 0.0);
+            const double t = 0.5 * ex * sg;
+            s[ia] = s[ia] - t;
+            s[ib] = s[ib] + t;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // write back the interior into the other buffer
+  H* dst = parity_buf ? f0 : f1;
+  for (int k = threadIdx.x; k < kRelaxTile * kRelaxTile; k += kThreads) {
+    const int la0 = kRelaxHalo + k / kRelaxTile, la1 = kRelaxHalo + k % kRelaxTile;
+    const int a0 = g0 + la0, a1 = g1 + la1;
+    if (a0 < c.n0 && a1 < c.n1 && loaded) dst[(size_t)a0 * c.pitch + a1] = s[la0 * kRelaxBox + la1];
+  }
+  worst = warp_max(worst);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = worst;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) m = fmax(m, red[w]);
+    if (!loaded) atomicExch(&ctl->status, 6);
+    atomicMax(&ctl->max_excess_bits, (unsigned long long)__double_as_longlong(m));
+    __threadfence();
+    last = atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  const double m = __longlong_as_double((long long)ctl->max_excess_bits);
+  ctl->arrive = 0;
+  ctl->max_excess_bits = 0;
+  ctl->iterations += 1;
+  ctl->parity = parity_buf ^ 1;
+  if (ctl->status) {
+    ctl->done = 1;
+  } else if (m <= (FX ? c.tol_q : c.tol)) {
+    ctl->converged = 1;
+    ctl->done = 1;
+  } else if (ctl->iterations >= c.max_iterations) {
+    ctl->done = 1;
+  }
+  __threadfence();
+  if (use_handle) cudaGraphSetConditional(handle, ctl->done ? 0u : 1u);
+}
+
+// ------------------------------------------------------------------------
+// Compact frontier rounds (production schedule).
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double vertex_weight_fp64(int r, int col, int n0, int n1, double f) {
+  double w = 0.0;
+  if (r < n0 - 1 && col < n1 - 1) w += 2.0 * f;
+  if (r < n0 - 1 && col > 0) w += f;
+  if (r > 0 && col > 0) w += 2.0 * f;
+  if (r > 0 && col < n1 - 1) w += f;
+  return w;
+}
+
+__device__ __forceinline__ long long gcd_ll(long long a, long long b) {
+  while (b) {
+    const long long t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// Round start: next-active flags -> phase buffer 0; decides termination.
+__global__ void frontier_begin_kernel(const RelaxConst c, int* __restrict__ unstable,
+                                      int* __restrict__ phase0, int* __restrict__ phase1,
+                                      RelaxControl* ctl, cudaGraphConditionalHandle handle) {
+  __shared__ int cnt[kThreads / 32];
+  int n = 0;
+  for (int t = threadIdx.x; t < c.ntiles; t += blockDim.x) {
+    const int a = unstable[t];
+    phase0[t] = a;
+    phase1[t] = 0;
+    unstable[t] = 0;
+    n += a;
+  }
+  n = warp_sum(n);
+  if ((threadIdx.x & 31) == 0) cnt[threadIdx.x >> 5] = n;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int tot = 0;
+    for (int w = 0; w < kThreads / 32; ++w) tot += cnt[w];
+    ctl->n_active = tot;
+    if (tot == 0) {
+      ctl->converged = 1;
+      ctl->done = 1;
+    } else if (ctl->rounds >= c.max_iterations) {
+      ctl->status = 4;  // NONCONVERGENCE
+      ctl->done = 1;
+    } else {
+      ctl->rounds += 1;
+    }
+    __threadfence();
+    cudaGraphSetConditional(handle, ctl->done ? 0u : 1u);
+  }
+}
+
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    frontier_subphase_kernel(const RelaxConst c, int dir, int par,
+                             typename FvTypes<FX>::H* __restrict__ hfield,
+                             int* __restrict__ reached, const int* __restrict__ phase_src,
+                             int* __restrict__ phase_dst, RelaxControl* ctl) {
+  using H = typename FvTypes<FX>::H;
+  __shared__ int trig[9];
+  __shared__ int moved_count;
+  const int t = blockIdx.x;
+  if (*(volatile int*)&ctl->done || !phase_src[t]) return;
+  const int T = c.ftile;
+  const int tr = t / c.tiles1, tc = t % c.tiles1;
+  if (threadIdx.x < 9) trig[threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    moved_count = 0;
+    phase_dst[t] = 1;
+  }
+  __syncthreads();
+  int d0, d1;
+  dir_of(dir, d0, d1);
+  int moved = 0;
+  for (int k = threadIdx.x; k < T * T; k += kThreads) {
+    const int a0 = tr * T + k / T, a1 = tc * T + k % T;
+    const int b0 = a0 + d0, b1 = a1 + d1;
+    if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+    if (((d0 ? a0 : a1) & 1) != par) continue;
+    const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
+    if (!reached[ia] && !reached[ib]) continue;
+    bool did = false;
+    if constexpr (FX) {
+      const long long df = (long long)hfield[ia] - (long long)hfield[ib];
+      const double ex = (double)(df < 0 ? -df : df) - c.crit_q[dir];
+      if (ex > 0.0) {
+        long long ua = 1, ub = 1;
+        if (c.weighted) {
+          const long long wa = vertex_weight6(a0, a1, c.n0, c.n1);
+          const long long wb = vertex_weight6(b0, b1, c.n0, c.n1);
+          const long long g = gcd_ll(wa, wb);
+          ua = wb / g;
+          ub = wa / g;
+        }
+        const long long kk = (long long)ceil(ex / (double)(ua + ub));
+        const long long sg = df < 0 ? -1 : 1;
+        hfield[ia] = (H)(hfield[ia] - sg * kk * ua);
+        hfield[ib] = (H)(hfield[ib] + sg * kk * ub);
+        did = true;
+      }
+    } else {
+      const double diff = hfield[ia] - hfield[ib];
+      const double ex = fabs(diff) - c.crit[dir];
+      if (ex > 0.0) {
+        const double signed_ex = diff < 0.0 ? -ex : ex;
+        double wa = 1.0, wb = 1.0;
+        if (c.weighted) {
+          wa = vertex_weight_fp64(a0, a1, c.n0, c.n1, c.f);
+          wb = vertex_weight_fp64(b0, b1, c.n0, c.n1, c.f);
+        }
+        const double ws = wa + wb;
+        const double ta = signed_ex * wb / ws, tb = signed_ex * wa / ws;
+        hfield[ia] = hfield[ia] - ta;
+        hfield[ib] = hfield[ib] + tb;
+        did = true;
+      }
+    }
+    if (did) {
+      reached[ia] = 1;
+      reached[ib] = 1;
+      ++moved;
+      // tiles of the 3x3 cell stencil around both endpoints (within the 3x3 tile block)
+      const int ends[4] = {a0, a1, b0, b1};
+      for (int e = 0; e < 2; ++e) {
+        const int p0 = ends[2 * e], p1 = ends[2 * e + 1];
+        for (int o0 = -1; o0 <= 1; ++o0)
+          for (int o1 = -1; o1 <= 1; ++o1) {
+            const int q0 = p0 + o0, q1 = p1 + o1;
+            if (q0 < 0 || q1 < 0 || q0 >= c.n0 || q1 >= c.n1) continue;
+            const int rt = q0 / T - tr, ct = q1 / T - tc;  // in [-1, 1]
+            trig[(rt + 1) * 3 + ct + 1] = 1;
+          }
+      }
+    }
+  }
+  moved = warp_sum(moved);
+  if ((threadIdx.x & 31) == 0 && moved) atomicAdd(&moved_count, moved);
+  __syncthreads();
+  if (threadIdx.x < 9 && trig[threadIdx.x]) {
+    const int rt = tr + threadIdx.x / 3 - 1, ct = tc + threadIdx.x % 3 - 1;
+    phase_dst[rt * c.tiles1 + ct] = 1;
+  }
+  if (threadIdx.x == 0 && moved_count) atomicAdd(&ctl->moved_edges, moved_count);
+}
+
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    frontier_scan_kernel(const RelaxConst c, const typename FvTypes<FX>::H* __restrict__ hfield,
+                         const int* __restrict__ reached, const int* __restrict__ phase,
+                         int* __restrict__ unstable, RelaxControl* ctl) {
+  __shared__ int bad;
+  const int t = blockIdx.x;
+  if (*(volatile int*)&ctl->done || !phase[t]) return;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  const int T = c.ftile;
+  const int tr = t / c.tiles1, tc = t % c.tiles1;
+  int found = 0;
+  for (int k = threadIdx.x; k < T * T && !found; k += kThreads) {
+    const int a0 = tr * T + k / T, a1 = tc * T + k % T;
+    if (a0 >= c.n0 || a1 >= c.n1) continue;
+    for (int d = 0; d < 4 && !found; ++d) {
+      int d0, d1;
+      dir_of(d, d0, d1);
+      const int b0 = a0 + d0, b1 = a1 + d1;
+      if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+      const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
+      if (!reached[ia] && !reached[ib]) continue;
+      if constexpr (FX) {
+        const long long df = (long long)hfield[ia] - (long long)hfield[ib];
+        if ((double)(df < 0 ? -df : df) - c.crit_q[d] > c.tol_q) found = 1;
+      } else {
+        if (fabs(hfield[ia] - hfield[ib]) - c.crit[d] > c.tol) found = 1;
+      }
+    }
+  }
+  if (found) bad = 1;
+  __syncthreads();
+  if (threadIdx.x == 0 && bad) unstable[t] = 1;
+}
+
+__global__ void frontier_finish_kernel(const RelaxConst c, int* __restrict__ reached,
+                                       const RelaxControl* ctl) {
+  if (!ctl->converged) return;
+  const long long n = (long long)c.n0 * c.pitch;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    reached[i] = 0;
+}
+
+// sum, min and max 8-neighbour slope of a support field (RelaxationStats:
+// volume_before/after and max_slope = slope_model.max_neighbor_slope :261-270).
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    field_stats_kernel(int n0, int n1, int pitch, double s0, double s1, double Q, double datum,
+                       const typename FvTypes<FX>::H* __restrict__ f, double* __restrict__ partials,
+                       long long* __restrict__ ipartials, unsigned int* arrive, double* out) {
+  const double diag = hypot(s0, s1);
+  double sum = 0.0, mx = 0.0, mn = 1.0e300;
+  long long isum = 0;
+  const long long n = (long long)n0 * n1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int a0 = (int)(i / n1), a1 = (int)(i % n1);
+    const size_t ia = (size_t)a0 * pitch + a1;
+    double va;
+    if constexpr (FX) {
+      isum += f[ia];
+      va = (double)f[ia] * Q + datum;
+    } else {
+      va = f[ia];
+      sum += va;
+    }
+    mn = fmin(mn, va);
+    for (int d = 0; d < 4; ++d) {
+      int d0, d1;
+      dir_of(d, d0, d1);
+      const int b0 = a0 + d0, b1 = a1 + d1;
+      if (b0 >= n0 || b1 < 0 || b1 >= n1) continue;
+      const size_t ib = (size_t)b0 * pitch + b1;
+      const double dist = d == 0 ? s0 : (d == 1 ? s1 : diag);
+      double diff;
+      if constexpr (FX) diff = (double)((long long)f[ia] - (long long)f[ib]) * Q;
+      else diff = f[ia] - f[ib];
+      mx = fmax(mx, fabs(diff) / dist);
+    }
+  }
+  sum = warp_sum(sum);
+  isum = (long long)warp_sum_u64((unsigned long long)isum);
+  mx = warp_max(mx);
+  mn = warp_min(mn);
+  __shared__ double r[kThreads / 32][3];
+  __shared__ long long ri[kThreads / 32];
+  __shared__ int last;
+  if ((threadIdx.x & 31) == 0) {
+    r[threadIdx.x >> 5][0] = sum;
+    r[threadIdx.x >> 5][1] = mx;
+    r[threadIdx.x >> 5][2] = mn;
+    ri[threadIdx.x >> 5] = isum;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0, cmin = 1.0e300;
+    long long ia = 0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      a += r[w][0];
+      b = fmax(b, r[w][1]);
+      cmin = fmin(cmin, r[w][2]);
+      ia += ri[w];
+    }
+    partials[blockIdx.x * 3 + 0] = a;
+    partials[blockIdx.x * 3 + 1] = b;
+    partials[blockIdx.x * 3 + 2] = cmin;
+    ipartials[blockIdx.x] = ia;
+    __threadfence();
+    last = atomicAdd(arrive, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  double a = 0.0, b = 0.0, cmin = 1.0e300;
+  long long ia = 0;
+  for (unsigned k = 0; k < gridDim.x; ++k) {
+    a += __ldcg(partials + k * 3);
+    b = fmax(b, __ldcg(partials + k * 3 + 1));
+    cmin = fmin(cmin, __ldcg(partials + k * 3 + 2));
+    ia += __ldcg(ipartials + k);
+  }
+  *arrive = 0;
+  out[0] = FX ? (double)ia * Q + datum * (double)n : a;
+  out[1] = b;
+  out[2] = cmin;
+  out[3] = (double)ia;
+}
+
+}  // namespace sb

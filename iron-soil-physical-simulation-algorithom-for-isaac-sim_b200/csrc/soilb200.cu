@@ -25,6 +25,9 @@
 #include "sb_common.cuh"
 #include "sb_fv.cuh"
 #include "sb_ledger.cuh"
+#include "sb_labels.cuh"
+#include "sb_relax.cuh"
+#include "sb_exchange.cuh"
 
 using namespace sb;
 
@@ -54,6 +57,20 @@ struct MobileGraph {
   FvConst key{};
   double static_limit = 0.0;
   bool valid = false;
+};
+
+struct LoopGraph {  // graph whose key is a RelaxConst
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+  RelaxConst key{};
+  bool valid = false;
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    valid = false;
+  }
 };
 
 }  // namespace
@@ -90,6 +107,34 @@ struct sb_ctx {
   int fv_blocks = 0;
   int ledger_blocks = 0;
   MobileGraph mobile;
+  cudaEvent_t ev_loop[2] = {nullptr, nullptr};  // around the substep WHILE node
+  // labelling (flat ny*nx arrays)
+  int* parent = nullptr;
+  void* slope = nullptr;
+  void* severity = nullptr;
+  int* latch = nullptr;
+  int* previous = nullptr;
+  double* export_cum = nullptr;
+  double* export_base = nullptr;
+  LabelRoots roots{};
+  int* root_list = nullptr;
+  LabelOut* lout = nullptr;
+  LabelOut* lout_host = nullptr;
+  // relaxation
+  void* b_alt = nullptr;
+  CUtensorMap tm_relax[2];
+  int ftiles0 = 0, ftiles1 = 0;
+  int* ftile_next = nullptr;   // next-round active tiles (seeded by labels / seeds)
+  int* phase[2] = {nullptr, nullptr};
+  RelaxControl* rctl = nullptr;
+  RelaxControl* rctl_host = nullptr;
+  LoopGraph relax_full;
+  LoopGraph frontier;
+  // exchange command buffers
+  int32_t* xidx = nullptr;
+  double* xval = nullptr;
+  ExchangeOut* xout = nullptr;
+  ExchangeOut* xout_host = nullptr;
   long long launches = 0;
   char err[1024] = {0};
 };
@@ -137,11 +182,18 @@ int grid_for(long long n) {
   return (int)(b < 1 ? 1 : b);
 }
 
-void* field_ptr(sb_ctx* c, int field, int* is_int, int* is_height, int* is_support) {
+void* field_ptr(sb_ctx* c, int field, int* is_int, int* is_height, int* is_support,
+                int* is_flat = nullptr) {
   *is_int = 0;
   *is_height = 0;
   *is_support = 0;
+  if (is_flat) *is_flat = 0;
   switch (field) {
+    case SB_FIELD_LABELS: *is_int = 1; if (is_flat) *is_flat = 1; return c->parent;
+    case SB_FIELD_LATCH: *is_int = 1; if (is_flat) *is_flat = 1; return c->latch;
+    case SB_FIELD_PREVIOUS_COMPONENT: *is_int = 1; if (is_flat) *is_flat = 1; return c->previous;
+    case SB_FIELD_SLOPE: if (is_flat) *is_flat = 1; return c->slope;
+    case SB_FIELD_SEVERITY: if (is_flat) *is_flat = 1; return c->severity;
     case SB_FIELD_Z_BASE: *is_support = 1; return c->z;
     case SB_FIELD_B_EFF: *is_support = 1; return c->b;
     case SB_FIELD_MOBILE: *is_height = 1; return c->h[c->parity_host];
@@ -201,7 +253,7 @@ void fv_args(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle, 
 template <bool FX>
 void ledger_args(sb_ctx* ctx, const FvConst& c, double* datum, double* static_limit, int* mode,
                  cudaGraphConditionalHandle* handle, int* use_handle, std::vector<void*>& args) {
-  args = {(void*)&c,         (void*)&ctx->b,        (void*)&ctx->h[0],      (void*)&ctx->h[1],
+  args = {(void*)&c,         (void*)&ctx->b,        (void*)&ctx->z,  (void*)&ctx->h[0],      (void*)&ctx->h[1],
           (void*)&ctx->qx[0], (void*)&ctx->qx[1],   (void*)&ctx->qy[0],     (void*)&ctx->qy[1],
           (void*)&ctx->ext_x, (void*)&ctx->ext_y,   (void*)datum,           (void*)static_limit,
           (void*)mode,        (void*)&ctx->ctl,     (void*)&ctx->io,        (void*)&ctx->partials,
@@ -256,13 +308,15 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
                         dim3(ctx->ledger_blocks), 0, args.data());
     if (rc) return rc;
   }
+  cudaGraphNode_t n_ev0, n_ev1;
+  SB_CUDA(ctx, cudaGraphAddEventRecordNode(&n_ev0, g, &n_pro, 1, ctx->ev_loop[0]));
   {
     cudaGraphNodeParams cp{};
     cp.type = cudaGraphNodeTypeConditional;
     cp.conditional.handle = handle;
     cp.conditional.type = cudaGraphCondTypeWhile;
     cp.conditional.size = 1;
-    SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_pro, 1, &cp));
+    SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_ev0, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     std::vector<void*> args;
     fv_args<FX>(ctx, cc, &handle, &use_handle, args);
@@ -274,7 +328,8 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
     int no_handle = 0;
     std::vector<void*> args;
     ledger_args<FX>(ctx, cc, &datum, &limit, &mode1, &handle, &no_handle, args);
-    int rc = add_kernel(ctx, g, &n_after, &n_loop, 1, (void*)ledger_kernel<FX>,
+    SB_CUDA(ctx, cudaGraphAddEventRecordNode(&n_ev1, g, &n_loop, 1, ctx->ev_loop[1]));
+    int rc = add_kernel(ctx, g, &n_after, &n_ev1, 1, (void*)ledger_kernel<FX>,
                         dim3(ctx->ledger_blocks), 0, args.data());
     if (rc) return rc;
   }
@@ -318,6 +373,8 @@ void fill_ledger(const sb_ctx* ctx, const LedgerOut& o, const sb_mobile_params* 
   L->pressure_w_j = rho * 0.5 * K * g * o.v[L_HH_W] * f;
   L->max_speed_m_s = o.v[L_MAXSPEED];
   L->min_h_m = -o.v[L_NEGMINH];
+  L->resting_volume_w_m3 = fx(ctx) ? (double)o.iq[2] * ctx->quantum * f : o.v[L_REST_W] * f;
+  L->resting_w_quanta = fx(ctx) ? o.iq[2] : 0;
 }
 
 }  // namespace
@@ -334,6 +391,10 @@ size_t sb_sizeof(const char* type_name) {
       {"sb_mobile_params", sizeof(sb_mobile_params)},
       {"sb_mobile_ledger", sizeof(sb_mobile_ledger)},
       {"sb_mobile_stats", sizeof(sb_mobile_stats)},
+      {"sb_label_params", sizeof(sb_label_params)},
+      {"sb_label_stats", sizeof(sb_label_stats)},
+      {"sb_relax_params", sizeof(sb_relax_params)},
+      {"sb_relax_stats", sizeof(sb_relax_stats)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.name, type_name) == 0) return e.size;
@@ -348,6 +409,8 @@ int sb_last_error(sb_ctx* ctx, char* buffer, size_t length) {
 }
 
 int64_t sb_kernel_launch_count(sb_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+void* sb_stream(sb_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   if (!desc || !out) return SB_ERR_BAD_ARG;
@@ -401,8 +464,58 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMallocHost(&ctx->dt_host, sizeof(double)));
   SB_CUDA(ctx, cudaMallocHost(&ctx->ctl_host, sizeof(FvControl)));
   SB_CUDA(ctx, cudaMallocHost(&ctx->io_host, sizeof(StepIO)));
+  SB_CUDA(ctx, cudaEventCreate(&ctx->ev_loop[0]));
+  SB_CUDA(ctx, cudaEventCreate(&ctx->ev_loop[1]));
+  // labelling buffers (flat ny*nx)
+  const size_t n = (size_t)d.ny * d.nx;
+  SB_CUDA(ctx, cudaMalloc(&ctx->parent, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->slope, n * ctx->esize));
+  SB_CUDA(ctx, cudaMalloc(&ctx->severity, n * ctx->esize));
+  SB_CUDA(ctx, cudaMalloc(&ctx->latch, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->previous, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->export_cum, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->export_base, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.count, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.area6, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.volume, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.exc_start, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.exc_stop, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.max_exc_start, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.max_exc_stop, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->roots.prev_overlap, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->root_list, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->lout, sizeof(LabelOut)));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->lout_host, sizeof(LabelOut)));
+  void* zero_init[] = {ctx->parent, ctx->latch, ctx->previous, ctx->export_cum, ctx->export_base};
+  size_t zero_size[] = {n * 4, n * 4, n * 4, n * 8, n * 8};
+  for (int k = 0; k < 5; ++k) SB_CUDA(ctx, cudaMemsetAsync(zero_init[k], 0, zero_size[k], ctx->stream));
+  // relaxation buffers
+  SB_CUDA(ctx, cudaMalloc(&ctx->b_alt, field_bytes));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->b_alt, 0, field_bytes, ctx->stream));
+  ctx->ftiles0 = (d.ny + d.tile_size - 1) / d.tile_size;
+  ctx->ftiles1 = (d.nx + d.tile_size - 1) / d.tile_size;
+  const size_t nt = (size_t)ctx->ftiles0 * ctx->ftiles1;
+  SB_CUDA(ctx, cudaMalloc(&ctx->ftile_next, nt * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->phase[0], nt * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->phase[1], nt * 4));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->ftile_next, 0, nt * 4, ctx->stream));
+  SB_CUDA(ctx, cudaMalloc(&ctx->rctl, sizeof(RelaxControl)));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->rctl, 0, sizeof(RelaxControl), ctx->stream));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->rctl_host, sizeof(RelaxControl)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->xidx, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->xval, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->xout, sizeof(ExchangeOut)));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->xout_host, sizeof(ExchangeOut)));
   // TMA descriptors (box = halo tile of the FV kernel)
   int rc;
+  {
+    const CUtensorMapDataType dt =
+        fx(ctx) ? CU_TENSOR_MAP_DATA_TYPE_INT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    if ((rc = encode_2d(ctx, &ctx->tm_relax[0], ctx->b, dt, ctx->esize, kRelaxBox, kRelaxBox)))
+      return rc;
+    if ((rc = encode_2d(ctx, &ctx->tm_relax[1], ctx->b_alt, dt, ctx->esize, kRelaxBox, kRelaxBox)))
+      return rc;
+  }
   if (fx(ctx)) {
     using Tl = FvTile<true>;
     if ((rc = encode_2d(ctx, &ctx->tm_b, ctx->b, CU_TENSOR_MAP_DATA_TYPE_INT32, 4, Tl::BW, Tl::BH)))
@@ -450,12 +563,24 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->mobile.exec) cudaGraphExecDestroy(ctx->mobile.exec);
   if (ctx->mobile.graph) cudaGraphDestroy(ctx->mobile.graph);
+  ctx->relax_full.reset();
+  ctx->frontier.reset();
   void* ptrs[] = {ctx->b, ctx->z, ctx->h[0], ctx->h[1], ctx->qx[0], ctx->qx[1], ctx->qy[0],
                   ctx->qy[1], ctx->ext_x, ctx->ext_y, ctx->reached, ctx->staging,
                   ctx->range_error, ctx->ctl, ctx->io, ctx->partials, ctx->ipartials,
-                  ctx->arrive, ctx->dt_dev};
+                  ctx->arrive, ctx->dt_dev, ctx->parent, ctx->slope, ctx->severity, ctx->latch,
+                  ctx->previous, ctx->export_cum, ctx->export_base, ctx->roots.count,
+                  ctx->roots.area6, ctx->roots.volume, ctx->roots.exc_start, ctx->roots.exc_stop,
+                  ctx->roots.max_exc_start, ctx->roots.max_exc_stop, ctx->roots.prev_overlap,
+                  ctx->root_list, ctx->lout, ctx->b_alt, ctx->ftile_next, ctx->phase[0],
+                  ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
+  if (ctx->rctl_host) cudaFreeHost(ctx->rctl_host);
+  for (cudaEvent_t e : ctx->ev_loop)
+    if (e) cudaEventDestroy(e);
+  if (ctx->xout_host) cudaFreeHost(ctx->xout_host);
   if (ctx->dt_host) cudaFreeHost(ctx->dt_host);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
   if (ctx->io_host) cudaFreeHost(ctx->io_host);
@@ -472,9 +597,10 @@ int sb_synchronize(sb_ctx* ctx) {
 
 int sb_upload(sb_ctx* ctx, int field, const double* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
-  int is_int, is_h, is_s;
-  void* dst = field_ptr(ctx, field, &is_int, &is_h, &is_s);
+  int is_int, is_h, is_s, is_flat;
+  void* dst = field_ptr(ctx, field, &is_int, &is_h, &is_s, &is_flat);
   if (!dst || is_int) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is not a float field", field);
+  if (is_flat) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is read-only", field);
   const int ny = ctx->d.ny, nx = ctx->d.nx;
   if (!fx(ctx)) {
     SB_CUDA(ctx, cudaMemcpy2DAsync(dst, (size_t)ctx->pitch * 8, host, (size_t)nx * 8,
@@ -512,10 +638,24 @@ int sb_upload(sb_ctx* ctx, int field, const double* host) {
 
 int sb_download(sb_ctx* ctx, int field, double* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
-  int is_int, is_h, is_s;
-  void* src = field_ptr(ctx, field, &is_int, &is_h, &is_s);
+  int is_int, is_h, is_s, is_flat;
+  void* src = field_ptr(ctx, field, &is_int, &is_h, &is_s, &is_flat);
   if (!src || is_int) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is not a float field", field);
   const int ny = ctx->d.ny, nx = ctx->d.nx;
+  if (is_flat) {
+    if (!fx(ctx)) {
+      SB_CUDA(ctx, cudaMemcpyAsync(host, src, (size_t)ny * nx * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    } else {
+      from_float_kernel<<<grid_for((long long)ny * nx), kThreads, 0, ctx->stream>>>(
+          (const float*)src, ctx->staging, ny, nx, nx);
+      ctx->launches++;
+      SB_CUDA(ctx, cudaGetLastError());
+      SB_CUDA(ctx, cudaMemcpyAsync(host, ctx->staging, (size_t)ny * nx * 8, cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    }
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SB_OK;
+  }
   if (!fx(ctx)) {
     SB_CUDA(ctx, cudaMemcpy2DAsync(host, (size_t)nx * 8, src, (size_t)ctx->pitch * 8,
                                    (size_t)nx * 8, ny, cudaMemcpyDeviceToHost, ctx->stream));
@@ -540,9 +680,17 @@ int sb_download(sb_ctx* ctx, int field, double* host) {
 
 int sb_upload_i32(sb_ctx* ctx, int field, const int32_t* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
-  int is_int, is_h, is_s;
-  void* dst = field_ptr(ctx, field, &is_int, &is_h, &is_s);
+  int is_int, is_h, is_s, is_flat;
+  void* dst = field_ptr(ctx, field, &is_int, &is_h, &is_s, &is_flat);
   if (!dst || !is_int) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is not an int field", field);
+  if (field == SB_FIELD_LABELS)
+    return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] labels are read-only");
+  if (is_flat) {
+    SB_CUDA(ctx, cudaMemcpyAsync(dst, host, (size_t)ctx->d.ny * ctx->d.nx * 4,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SB_OK;
+  }
   SB_CUDA(ctx, cudaMemcpy2DAsync(dst, (size_t)ctx->pitch * 4, host, (size_t)ctx->d.nx * 4,
                                  (size_t)ctx->d.nx * 4, ctx->d.ny, cudaMemcpyHostToDevice,
                                  ctx->stream));
@@ -552,9 +700,15 @@ int sb_upload_i32(sb_ctx* ctx, int field, const int32_t* host) {
 
 int sb_download_i32(sb_ctx* ctx, int field, int32_t* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
-  int is_int, is_h, is_s;
-  void* src = field_ptr(ctx, field, &is_int, &is_h, &is_s);
+  int is_int, is_h, is_s, is_flat;
+  void* src = field_ptr(ctx, field, &is_int, &is_h, &is_s, &is_flat);
   if (!src || !is_int) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is not an int field", field);
+  if (is_flat) {
+    SB_CUDA(ctx, cudaMemcpyAsync(host, src, (size_t)ctx->d.ny * ctx->d.nx * 4,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SB_OK;
+  }
   SB_CUDA(ctx, cudaMemcpy2DAsync(host, (size_t)ctx->d.nx * 4, src, (size_t)ctx->pitch * 4,
                                  (size_t)ctx->d.nx * 4, ctx->d.ny, cudaMemcpyDeviceToHost,
                                  ctx->stream));
@@ -598,7 +752,10 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
   const FvControl& k = *ctx->ctl_host;
   ctx->parity_host = k.parity;
   ctx->launches += 3 + k.substeps;
+  float loop_ms = 0.f;
+  SB_CUDA(ctx, cudaEventElapsedTime(&loop_ms, ctx->ev_loop[0], ctx->ev_loop[1]));
   std::memset(out, 0, sizeof(*out));
+  out->substep_loop_ms = loop_ms;
   out->substeps = k.substeps;
   out->static_skip = k.static_skip;
   out->cfl_limited = k.cfl_limited;
@@ -648,3 +805,581 @@ int sb_mobile_ledger_of(sb_ctx* ctx, const sb_mobile_params* params, sb_mobile_l
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Labelling
+// ---------------------------------------------------------------------------
+static LabelConst make_label_const(const sb_ctx* ctx, const sb_label_params* p) {
+  LabelConst c{};
+  c.ny = ctx->d.ny;
+  c.nx = ctx->d.nx;
+  c.pitch = ctx->pitch;
+  c.tiles_x = (ctx->d.nx + kLabelTile - 1) / kLabelTile;
+  c.connectivity = p->connectivity;
+  c.dx = ctx->d.dx_m;
+  c.dy = ctx->d.dy_m;
+  c.tan_start = p->tan_start;
+  c.tan_stop = p->tan_stop;
+  c.density = p->density_kg_m3;
+  c.gravity = p->gravity_m_s2;
+  c.cohesion = p->cohesion_pa;
+  c.mob_depth = p->mobilization_depth_m;
+  c.dry = p->dry_tolerance_m;
+  c.activity_speed = p->activity_speed_m_s;
+  c.start_rad = p->start_rad;
+  c.stop_rad = p->stop_rad;
+  c.Q = ctx->quantum;
+  c.datum = ctx->d.datum_m;
+  c.release_latches = p->release_settled_latches ? 1 : 0;
+  c.tile_size = ctx->d.tile_size;
+  c.frontier_tiles_x = ctx->ftiles1;
+  return c;
+}
+
+template <bool FX>
+static int run_label(sb_ctx* ctx, const LabelConst& c) {
+  using T = FvTypes<FX>;
+  const int tiles = c.tiles_x * ((c.ny + kLabelTile - 1) / kLabelTile);
+  const int P = ctx->parity_host;
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->lout, 0, sizeof(LabelOut), ctx->stream));
+  label_init_local_kernel<FX><<<tiles, kThreads, 0, ctx->stream>>>(
+      c, (const typename T::B*)ctx->b, (const typename T::B*)ctx->z, (const typename T::H*)ctx->h[P],
+      (const typename T::R*)ctx->qx[P], (const typename T::R*)ctx->qy[P], ctx->parent,
+      (typename T::R*)ctx->slope, (typename T::R*)ctx->severity, ctx->latch, ctx->export_cum,
+      ctx->export_base, ctx->roots);
+  label_merge_kernel<<<tiles, kThreads, 0, ctx->stream>>>(c, ctx->parent, ctx->lout);
+  const int g = grid_for((long long)c.ny * c.nx);
+  label_compress_kernel<FX><<<g, kThreads, 0, ctx->stream>>>(
+      c, ctx->parent, (const typename T::B*)ctx->b, (const typename T::B*)ctx->z,
+      (const typename T::R*)ctx->slope, (const typename T::R*)ctx->severity, ctx->latch,
+      ctx->previous, ctx->roots, ctx->root_list, ctx->lout, 0);
+  label_reduce_kernel<<<148, kThreads, 0, ctx->stream>>>(ctx->roots, ctx->root_list, ctx->lout,
+                                                         ctx->arrive);
+  ctx->launches += 4;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->lout_host, ctx->lout, sizeof(LabelOut), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+extern "C" int sb_label(sb_ctx* ctx, const sb_label_params* p, sb_label_stats* out) {
+  if (!ctx || !p || !out) return SB_ERR_BAD_ARG;
+  if (p->connectivity != 4 && p->connectivity != 8)
+    return fail(ctx, SB_ERR_BAD_ARG, "[LargeAvalanche] connectivity must be 4 or 8");
+  if ((long long)ctx->d.ny * ctx->d.nx >= 0x7fffffffLL)
+    return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] grid too large for int32 labels");
+  const LabelConst c = make_label_const(ctx, p);
+  int rc = fx(ctx) ? run_label<true>(ctx, c) : run_label<false>(ctx, c);
+  if (rc) return rc;
+  const LabelOut& o = *ctx->lout_host;
+  std::memset(out, 0, sizeof(*out));
+  out->status = o.status;
+  out->unstable_cell_count = o.total_unstable;
+  out->connected_region_count = o.regions;
+  out->largest_connected_cell_count = o.largest;
+  out->winner_root = o.winner;
+  out->union_passes = 2;
+  out->previous_overlap = o.prev_overlap;
+  const double f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  out->largest_connected_area_m2 = (double)o.area6 * f;
+  out->largest_connected_mobilizable_volume_m3 =
+      fx(ctx) ? (double)o.volume * ctx->quantum * f : (double)o.volume / kVolumeScaleFp64 * f;
+  out->excess_start_sum_rad = (double)o.exc_start / kExcessScale;
+  out->excess_start_max_rad = (double)o.max_exc_start / kExcessScale;
+  out->excess_stop_sum_rad = (double)o.exc_stop / kExcessScale;
+  out->excess_stop_max_rad = (double)o.max_exc_stop / kExcessScale;
+  if (o.status)
+    return fail(ctx, SB_ERR_NONCONVERGENCE,
+                "NUMERICAL_NONCONVERGENCE: device avalanche connected components");
+  return SB_OK;
+}
+
+extern "C" int sb_label_mask(sb_ctx* ctx, const int32_t* mask, int connectivity,
+                             sb_label_stats* out) {
+  if (!ctx || !mask || !out) return SB_ERR_BAD_ARG;
+  if (connectivity != 4 && connectivity != 8)
+    return fail(ctx, SB_ERR_BAD_ARG, "[LargeAvalanche] connectivity must be 4 or 8");
+  LabelConst c{};
+  c.ny = ctx->d.ny;
+  c.nx = ctx->d.nx;
+  c.pitch = ctx->pitch;
+  c.tiles_x = (ctx->d.nx + kLabelTile - 1) / kLabelTile;
+  c.connectivity = connectivity;
+  const size_t n = (size_t)c.ny * c.nx;
+  int32_t* dmask = (int32_t*)ctx->staging;  // 8*n bytes of scratch >= 4*n
+  SB_CUDA(ctx, cudaMemcpyAsync(dmask, mask, n * 4, cudaMemcpyHostToDevice, ctx->stream));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->lout, 0, sizeof(LabelOut), ctx->stream));
+  const int tiles = c.tiles_x * ((c.ny + kLabelTile - 1) / kLabelTile);
+  label_mask_local_kernel<<<tiles, kThreads, 0, ctx->stream>>>(c, dmask, ctx->parent, ctx->roots);
+  label_merge_kernel<<<tiles, kThreads, 0, ctx->stream>>>(c, ctx->parent, ctx->lout);
+  const int g = grid_for((long long)n);
+  if (fx(ctx))
+    label_compress_kernel<true><<<g, kThreads, 0, ctx->stream>>>(
+        c, ctx->parent, nullptr, nullptr, nullptr, nullptr, ctx->latch, ctx->previous, ctx->roots,
+        ctx->root_list, ctx->lout, 1);
+  else
+    label_compress_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
+        c, ctx->parent, nullptr, nullptr, nullptr, nullptr, ctx->latch, ctx->previous, ctx->roots,
+        ctx->root_list, ctx->lout, 1);
+  label_reduce_kernel<<<148, kThreads, 0, ctx->stream>>>(ctx->roots, ctx->root_list, ctx->lout,
+                                                         ctx->arrive);
+  ctx->launches += 4;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->lout_host, ctx->lout, sizeof(LabelOut), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const LabelOut& o = *ctx->lout_host;
+  std::memset(out, 0, sizeof(*out));
+  out->status = o.status;
+  out->unstable_cell_count = o.total_unstable;
+  out->connected_region_count = o.regions;
+  out->largest_connected_cell_count = o.largest;
+  out->winner_root = o.winner;
+  out->union_passes = 2;
+  out->largest_connected_area_m2 = (double)o.area6 * (ctx->d.dx_m * ctx->d.dy_m / 6.0);
+  if (o.status)
+    return fail(ctx, SB_ERR_NONCONVERGENCE,
+                "NUMERICAL_NONCONVERGENCE: device avalanche connected components");
+  return SB_OK;
+}
+
+extern "C" int sb_label_commit(sb_ctx* ctx, int keep_candidate, int seed_frontier) {
+  if (!ctx) return SB_ERR_BAD_ARG;
+  LabelConst c{};
+  c.ny = ctx->d.ny;
+  c.nx = ctx->d.nx;
+  c.pitch = ctx->pitch;
+  c.tile_size = ctx->d.tile_size;
+  c.frontier_tiles_x = ctx->ftiles1;
+  label_update_previous_kernel<<<grid_for((long long)c.ny * c.nx), kThreads, 0, ctx->stream>>>(
+      c, ctx->parent, ctx->previous, ctx->reached, ctx->ftile_next, ctx->lout,
+      keep_candidate ? 1 : 0, seed_frontier ? 1 : 0);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Relaxation
+// ---------------------------------------------------------------------------
+static int relax_const(sb_ctx* ctx, const sb_relax_params* p, RelaxConst* c, int tile) {
+  if (!(p->spacing0_m > 0) || !(p->spacing1_m > 0) || !std::isfinite(p->spacing0_m) ||
+      !std::isfinite(p->spacing1_m))
+    return fail(ctx, SB_ERR_BAD_ARG, "grid spacing must be positive");
+  if (!(p->critical_slope > 0) || !std::isfinite(p->critical_slope))
+    return fail(ctx, SB_ERR_BAD_ARG, "critical slope must be finite/positive");
+  if (!(p->tolerance_m >= 0) || p->max_iterations < 1)
+    return fail(ctx, SB_ERR_BAD_ARG, "tolerance/max_iterations invalid");
+  std::memset(c, 0, sizeof(*c));
+  c->n0 = ctx->d.ny;
+  c->n1 = ctx->d.nx;
+  c->pitch = ctx->pitch;
+  c->tiles1 = (ctx->d.nx + tile - 1) / tile;
+  c->ntiles = c->tiles1 * ((ctx->d.ny + tile - 1) / tile);
+  c->s0 = p->spacing0_m;
+  c->s1 = p->spacing1_m;
+  const double diag = std::hypot(p->spacing0_m, p->spacing1_m);
+  const double dist[4] = {p->spacing0_m, p->spacing1_m, diag, diag};
+  for (int k = 0; k < 4; ++k) {
+    c->crit[k] = p->critical_slope * dist[k];
+    c->crit_q[k] = c->crit[k] / ctx->quantum;
+  }
+  c->tol = p->tolerance_m;
+  c->tol_q = p->tolerance_m / ctx->quantum;
+  c->max_iterations = p->max_iterations;
+  c->weighted = p->weighted ? 1 : 0;
+  c->ftile = tile;
+  c->f = p->spacing0_m * p->spacing1_m / 6.0;
+  if (fx(ctx)) {
+    // the rounded-up transfer rule needs crit*L >= 8 quanta (no overshoot past level)
+    for (int k = 0; k < 2; ++k)
+      if (c->crit_q[k] < 8.0)
+        return fail(ctx, SB_ERR_BAD_ARG,
+                    "[soilb200] critical height difference below 8 quanta; use a finer quantum");
+  }
+  return SB_OK;
+}
+
+__global__ void relax_reset_kernel(RelaxControl* ctl) {
+  if (threadIdx.x == 0) {
+    ctl->iterations = 0;
+    ctl->done = 0;
+    ctl->converged = 0;
+    ctl->status = 0;
+    ctl->max_excess_bits = 0;
+    ctl->arrive = 0;
+    ctl->parity = 0;
+    ctl->n_active = 0;
+    ctl->rounds = 0;
+    ctl->moved_edges = 0;
+  }
+}
+
+template <bool FX>
+static int build_relax_full(sb_ctx* ctx, const RelaxConst& c) {
+  LoopGraph& lg = ctx->relax_full;
+  lg.reset();
+  cudaGraph_t g;
+  SB_CUDA(ctx, cudaGraphCreate(&g, 0));
+  lg.graph = g;
+  cudaGraphConditionalHandle handle;
+  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNode_t n_reset, n_loop, n_body;
+  {
+    void* args[] = {(void*)&ctx->rctl};
+    int rc = add_kernel(ctx, g, &n_reset, nullptr, 0, (void*)relax_reset_kernel, dim3(1), 0, args);
+    if (rc) return rc;
+  }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_reset, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  RelaxConst cc = c;
+  int use_handle = 1;
+  const int tiles1 = (c.n1 + kRelaxTile - 1) / kRelaxTile;
+  const int tiles0 = (c.n0 + kRelaxTile - 1) / kRelaxTile;
+  RelaxConst ck = cc;
+  ck.tiles1 = tiles1;
+  void* args[] = {(void*)&ck, (void*)&ctx->tm_relax[0], (void*)&ctx->tm_relax[1],
+                  (void*)&ctx->b, (void*)&ctx->b_alt, (void*)&ctx->rctl, (void*)&handle,
+                  (void*)&use_handle};
+  int rc = add_kernel(ctx, body, &n_body, nullptr, 0, (void*)relax_full_kernel<FX>,
+                      dim3(tiles0 * tiles1), 0, args);
+  if (rc) return rc;
+  SB_CUDA(ctx, cudaGraphInstantiate(&lg.exec, g, 0));
+  lg.key = c;
+  lg.valid = true;
+  return SB_OK;
+}
+
+extern "C" int sb_relax_full(sb_ctx* ctx, const sb_relax_params* p, sb_relax_stats* out) {
+  if (!ctx || !p || !out) return SB_ERR_BAD_ARG;
+  RelaxConst c;
+  int rc = relax_const(ctx, p, &c, kRelaxTile);
+  if (rc) return rc;
+  LoopGraph& lg = ctx->relax_full;
+  if (!lg.valid || std::memcmp(&lg.key, &c, sizeof(RelaxConst)) != 0) {
+    rc = fx(ctx) ? build_relax_full<true>(ctx, c) : build_relax_full<false>(ctx, c);
+    if (rc) return rc;
+  }
+  SB_CUDA(ctx, cudaGraphLaunch(lg.exec, ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->rctl_host, ctx->rctl, sizeof(RelaxControl),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const RelaxControl& k = *ctx->rctl_host;
+  ctx->launches += 1 + k.iterations;
+  if (k.parity) {  // result lives in the alternate buffer: copy it back
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->b, ctx->b_alt, (size_t)ctx->pitch * ctx->d.ny * ctx->esize,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->iterations = k.iterations;
+  out->converged = k.converged;
+  out->status = k.status;
+  if (k.status == SB_ERR_WAIT_LIMIT)
+    return fail(ctx, SB_ERR_WAIT_LIMIT, "[soilb200] a bounded device wait gave up (TMA tile load)");
+  return SB_OK;
+}
+
+__global__ void frontier_seed_cells_kernel(const int32_t* __restrict__ idx, int count, int ny,
+                                           int nx, int pitch, int tile, int tiles1,
+                                           int* __restrict__ reached, int* __restrict__ flags,
+                                           int* bad) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const int i = idx[k];
+    if (i < 0 || i >= ny * nx) {
+      atomicExch(bad, 1);
+      continue;
+    }
+    const int r = i / nx, c = i % nx;
+    reached[(size_t)r * pitch + c] = 1;
+    for (int o0 = -1; o0 <= 1; ++o0)
+      for (int o1 = -1; o1 <= 1; ++o1) {
+        const int q0 = r + o0, q1 = c + o1;
+        if (q0 < 0 || q1 < 0 || q0 >= ny || q1 >= nx) continue;
+        flags[(q0 / tile) * tiles1 + q1 / tile] = 1;
+      }
+  }
+}
+
+__global__ void frontier_seed_tiles_kernel(const int32_t* __restrict__ ids, int count, int ntiles,
+                                           int* __restrict__ flags, int* bad) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const int t = ids[k];
+    if (t < 0 || t >= ntiles) {
+      atomicExch(bad, 1);
+      continue;
+    }
+    flags[t] = 1;
+  }
+}
+
+static int upload_ints(sb_ctx* ctx, const int32_t* host, int count) {
+  // staging holds ny*nx doubles = 2*ny*nx int32 >= count for any valid request
+  if ((long long)count > 2LL * ctx->d.ny * ctx->d.nx)
+    return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] seed list longer than the grid");
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->staging, host, (size_t)count * 4, cudaMemcpyHostToDevice,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->range_error, 0, sizeof(int), ctx->stream));
+  return SB_OK;
+}
+
+static int check_bad(sb_ctx* ctx, const char* what) {
+  int herr = 0;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(&herr, ctx->range_error, sizeof(int), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (herr) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] %s index outside state", what);
+  return SB_OK;
+}
+
+extern "C" int sb_frontier_seed_cells(sb_ctx* ctx, const int32_t* flat, int count) {
+  if (!ctx || (!flat && count)) return SB_ERR_BAD_ARG;
+  if (count <= 0) return SB_OK;
+  int rc = upload_ints(ctx, flat, count);
+  if (rc) return rc;
+  frontier_seed_cells_kernel<<<grid_for(count), kThreads, 0, ctx->stream>>>(
+      (const int32_t*)ctx->staging, count, ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->d.tile_size,
+      ctx->ftiles1, ctx->reached, ctx->ftile_next, ctx->range_error);
+  ctx->launches++;
+  return check_bad(ctx, "frontier seed");
+}
+
+extern "C" int sb_frontier_seed_tiles(sb_ctx* ctx, const int32_t* ids, int count) {
+  if (!ctx || (!ids && count)) return SB_ERR_BAD_ARG;
+  if (count <= 0) return SB_OK;
+  int rc = upload_ints(ctx, ids, count);
+  if (rc) return rc;
+  frontier_seed_tiles_kernel<<<grid_for(count), kThreads, 0, ctx->stream>>>(
+      (const int32_t*)ctx->staging, count, ctx->ftiles0 * ctx->ftiles1, ctx->ftile_next,
+      ctx->range_error);
+  ctx->launches++;
+  return check_bad(ctx, "frontier tile");
+}
+
+extern "C" int sb_frontier_tile_count(sb_ctx* ctx) { return ctx ? ctx->ftiles0 * ctx->ftiles1 : 0; }
+
+extern "C" int sb_frontier_active_tiles(sb_ctx* ctx, int32_t* flags, int capacity) {
+  if (!ctx || !flags) return SB_ERR_BAD_ARG;
+  const int nt = ctx->ftiles0 * ctx->ftiles1;
+  if (capacity < nt) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] tile flag buffer too small");
+  SB_CUDA(ctx, cudaMemcpyAsync(flags, ctx->ftile_next, (size_t)nt * 4, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+template <bool FX>
+static int build_frontier(sb_ctx* ctx, const RelaxConst& c) {
+  LoopGraph& lg = ctx->frontier;
+  lg.reset();
+  cudaGraph_t g;
+  SB_CUDA(ctx, cudaGraphCreate(&g, 0));
+  lg.graph = g;
+  cudaGraphConditionalHandle handle;
+  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+  static RelaxConst cc;  // copied into the node parameters at add time
+  cc = c;
+  cudaGraphNode_t n_reset, n_begin0, n_loop, n_finish;
+  int rc;
+  {
+    void* args[] = {(void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_reset, nullptr, 0, (void*)relax_reset_kernel, dim3(1), 0, args)))
+      return rc;
+  }
+  void* begin_args[] = {(void*)&cc, (void*)&ctx->ftile_next, (void*)&ctx->phase[0],
+                        (void*)&ctx->phase[1], (void*)&ctx->rctl, (void*)&handle};
+  if ((rc = add_kernel(ctx, g, &n_begin0, &n_reset, 1, (void*)frontier_begin_kernel, dim3(1), 0,
+                       begin_args)))
+    return rc;
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_begin0, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraphNode_t prev = nullptr;
+  int dirs[8], pars[8];
+  for (int k = 0; k < 8; ++k) {
+    dirs[k] = k / 2;
+    pars[k] = k % 2;
+  }
+  typename FvTypes<FX>::H* hf = (typename FvTypes<FX>::H*)ctx->b;
+  for (int k = 0; k < 8; ++k) {
+    cudaGraphNode_t node;
+    void* args[] = {(void*)&cc, (void*)&dirs[k], (void*)&pars[k], (void*)&hf,
+                    (void*)&ctx->reached, (void*)&ctx->phase[k & 1],
+                    (void*)&ctx->phase[(k + 1) & 1], (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, body, &node, prev ? &prev : nullptr, prev ? 1 : 0,
+                         (void*)frontier_subphase_kernel<FX>, dim3(c.ntiles), 0, args)))
+      return rc;
+    prev = node;
+  }
+  cudaGraphNode_t n_scan, n_begin;
+  {
+    void* args[] = {(void*)&cc, (void*)&hf, (void*)&ctx->reached, (void*)&ctx->phase[0],
+                    (void*)&ctx->ftile_next, (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, body, &n_scan, &prev, 1, (void*)frontier_scan_kernel<FX>,
+                         dim3(c.ntiles), 0, args)))
+      return rc;
+  }
+  if ((rc = add_kernel(ctx, body, &n_begin, &n_scan, 1, (void*)frontier_begin_kernel, dim3(1), 0,
+                       begin_args)))
+    return rc;
+  {
+    void* args[] = {(void*)&cc, (void*)&ctx->reached, (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_finish, &n_loop, 1, (void*)frontier_finish_kernel,
+                         dim3(grid_for((long long)c.n0 * c.pitch)), 0, args)))
+      return rc;
+  }
+  SB_CUDA(ctx, cudaGraphInstantiate(&lg.exec, g, 0));
+  lg.key = c;
+  lg.valid = true;
+  return SB_OK;
+}
+
+extern "C" int sb_frontier_run(sb_ctx* ctx, const sb_relax_params* p, sb_relax_stats* out) {
+  if (!ctx || !p || !out) return SB_ERR_BAD_ARG;
+  RelaxConst c;
+  int rc = relax_const(ctx, p, &c, ctx->d.tile_size);
+  if (rc) return rc;
+  LoopGraph& lg = ctx->frontier;
+  if (!lg.valid || std::memcmp(&lg.key, &c, sizeof(RelaxConst)) != 0) {
+    rc = fx(ctx) ? build_frontier<true>(ctx, c) : build_frontier<false>(ctx, c);
+    if (rc) return rc;
+  }
+  SB_CUDA(ctx, cudaGraphLaunch(lg.exec, ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->rctl_host, ctx->rctl, sizeof(RelaxControl),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const RelaxControl& k = *ctx->rctl_host;
+  ctx->launches += 3 + 10LL * k.rounds;
+  std::memset(out, 0, sizeof(*out));
+  out->iterations = k.rounds;
+  out->converged = k.converged;
+  out->status = k.status;
+  out->active_tiles = k.n_active;
+  out->moved_edges = k.moved_edges;
+  if (k.status == SB_ERR_NONCONVERGENCE)
+    return fail(ctx, SB_ERR_NONCONVERGENCE,
+                "NUMERICAL_NONCONVERGENCE: GPU residual MiniSlope exceeded the numerical safety limit");
+  return SB_OK;
+}
+
+extern "C" int sb_field_stats(sb_ctx* ctx, int field, double spacing0, double spacing1,
+                              double* out4) {
+  if (!ctx || !out4) return SB_ERR_BAD_ARG;
+  if (field != SB_FIELD_B_EFF && field != SB_FIELD_Z_BASE)
+    return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field statistics support b_eff / z_base");
+  void* f = field == SB_FIELD_B_EFF ? ctx->b : ctx->z;
+  const int g = ctx->ledger_blocks;
+  double* dout = (double*)ctx->staging;  // 4 doubles of scratch
+  if (fx(ctx))
+    field_stats_kernel<true><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, spacing0, spacing1, ctx->quantum, ctx->d.datum_m,
+        (const int32_t*)f, ctx->partials, ctx->ipartials, ctx->arrive, dout);
+  else
+    field_stats_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, spacing0, spacing1, ctx->quantum, ctx->d.datum_m,
+        (const double*)f, ctx->partials, ctx->ipartials, ctx->arrive, dout);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(out4, dout, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Resting <-> Mobile exchange
+// ---------------------------------------------------------------------------
+static int exchange_upload(sb_ctx* ctx, const int32_t* idx, const double* val, int count) {
+  if (count < 0 || (long long)count > (long long)ctx->d.ny * ctx->d.nx)
+    return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] invalid exchange request size");
+  for (int k = 0; k < count; ++k)
+    if (!std::isfinite(val[k]))
+      return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] invalid exchange request");
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->xidx, idx, (size_t)count * 4, cudaMemcpyHostToDevice, ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->xval, val, (size_t)count * 8, cudaMemcpyHostToDevice, ctx->stream));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->xout, 0, sizeof(ExchangeOut), ctx->stream));
+  return SB_OK;
+}
+
+static int exchange_finish(sb_ctx* ctx) {
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->xout_host, ctx->xout, sizeof(ExchangeOut),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->xout_host->bad_index)
+    return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] exchange index outside state");
+  return SB_OK;
+}
+
+static int entrain_common(sb_ctx* ctx, const int32_t* idx, const double* val, int count, int mode,
+                          double* volume_m3) {
+  if (!ctx || (count > 0 && (!idx || !val))) return SB_ERR_BAD_ARG;
+  if (volume_m3) *volume_m3 = 0.0;
+  if (count == 0) return SB_OK;
+  int rc = exchange_upload(ctx, idx, val, count);
+  if (rc) return rc;
+  const int P = ctx->parity_host;
+  const double f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  if (fx(ctx))
+    entrain_kernel<true><<<grid_for(count), kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, f, (int32_t*)ctx->b,
+        (const int32_t*)ctx->z, (int32_t*)ctx->h[P], ctx->xidx, ctx->xval, count, mode, ctx->xout);
+  else
+    entrain_kernel<false><<<grid_for(count), kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, f, (double*)ctx->b,
+        (const double*)ctx->z, (double*)ctx->h[P], ctx->xidx, ctx->xval, count, mode, ctx->xout);
+  ctx->launches++;
+  if ((rc = exchange_finish(ctx))) return rc;
+  if (volume_m3)
+    *volume_m3 = fx(ctx) ? (double)ctx->xout_host->volume_w6_quanta * ctx->quantum * f
+                         : ctx->xout_host->volume_w_fp64;
+  return SB_OK;
+}
+
+extern "C" int sb_entrain(sb_ctx* ctx, const int32_t* flat_indices, const double* depth_m,
+                          int count, double* volume_m3) {
+  return entrain_common(ctx, flat_indices, depth_m, count, 0, volume_m3);
+}
+
+extern "C" int sb_entrain_to_surface(sb_ctx* ctx, const int32_t* flat_indices,
+                                     const double* target_m, int count, double* volume_m3) {
+  return entrain_common(ctx, flat_indices, target_m, count, 1, volume_m3);
+}
+
+extern "C" int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double* depth_m,
+                          int count, double density_kg_m3, double* out3) {
+  if (!ctx || (count > 0 && (!flat_indices || !depth_m)) || !out3) return SB_ERR_BAD_ARG;
+  if (!(density_kg_m3 > 0.0)) return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] invalid deposition indices/density");
+  out3[0] = out3[1] = out3[2] = 0.0;
+  if (count == 0) return SB_OK;
+  int rc = exchange_upload(ctx, flat_indices, depth_m, count);
+  if (rc) return rc;
+  const int P = ctx->parity_host;
+  const double f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  if (fx(ctx))
+    deposit_kernel<true><<<grid_for(count), kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, f, (int32_t*)ctx->b, (int32_t*)ctx->h[P],
+        (float*)ctx->qx[P], (float*)ctx->qy[P], ctx->xidx, ctx->xval, count, ctx->xout);
+  else
+    deposit_kernel<false><<<grid_for(count), kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, f, (double*)ctx->b, (double*)ctx->h[P],
+        (double*)ctx->qx[P], (double*)ctx->qy[P], ctx->xidx, ctx->xval, count, ctx->xout);
+  ctx->launches++;
+  if ((rc = exchange_finish(ctx))) return rc;
+  const ExchangeOut& o = *ctx->xout_host;
+  out3[0] = fx(ctx) ? (double)o.volume_w6_quanta * ctx->quantum * f : o.volume_w_fp64;
+  out3[1] = density_kg_m3 * o.momentum_w[0];
+  out3[2] = density_kg_m3 * o.momentum_w[1];
+  return SB_OK;
+}

@@ -148,5 +148,9 @@ class DeviceGrid:
     def synchronize(self) -> None:
         _lib.check(self.ctx, _lib.load().sb_synchronize(self.ctx), "synchronize")
 
+    def stream_handle(self) -> int:
+        """Integer cudaStream_t of this context (e.g. for torch.cuda.ExternalStream)."""
+        return int(_lib.load().sb_stream(self.ctx) or 0)
+
     def kernel_launches(self) -> int:
         return int(_lib.load().sb_kernel_launch_count(self.ctx))

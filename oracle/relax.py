@@ -102,6 +102,42 @@ def relax_critical_slope(height, grid_spacing, critical_angle_deg=34.0, max_iter
     return h, it, converged, vol0, float(h.sum() * area)
 
 
+def relax_critical_slope_fixed(hq, grid_spacing, crit_tan: float, quantum: float,
+                               max_iterations=20000, tolerance=1e-8):
+    """Fixed-point mirror of the production full-domain kernel.
+
+    Heights are integer quanta; each active pair with excess e > 0 (in quanta)
+    moves ceil(e/2) quanta, so the pair ends at or below critical; the
+    convergence max is taken in quanta.  Returns (hq, iterations, converged).
+    """
+    h = np.asarray(hq, dtype=np.int64).copy()
+    s0, s1 = grid_spacing
+    pairs = neighbor_pairs(s0, s1)
+    crit_q = [(crit_tan * dist) / quantum for _, _, dist in pairs]
+    tol_q = tolerance / quantum
+    it = 0
+    converged = False
+    for it in range(1, max_iterations + 1):
+        worst = 0.0
+        for d, (d0, d1, _) in enumerate(pairs):
+            a, b = paired_views(h, d0, d1)
+            coord = (np.arange(a.shape[0])[:, None] if d0 else np.arange(a.shape[1])[None, :])
+            for par in (0, 1):
+                a, b = paired_views(h, d0, d1)
+                diff = a - b
+                ex = np.abs(diff).astype(np.float64) - crit_q[d]
+                worst = max(worst, float(ex.max(initial=0.0)))
+                active = ((coord & 1) == par) & (ex > 0.0)
+                t = np.where(active, np.ceil(ex * 0.5), 0.0).astype(np.int64)
+                st = np.where(diff < 0, -t, t)
+                a -= st
+                b += st
+        if worst <= tol_q:
+            converged = True
+            break
+    return h, it, converged
+
+
 # ---------------------------------------------------------------------------
 # Compact frontier (production schedule)
 # ---------------------------------------------------------------------------

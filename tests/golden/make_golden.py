@@ -162,6 +162,119 @@ def make_fv_gate():
     np.savez_compressed(HERE / "fv_gate.npz", **arrays)
 
 
+def make_relax():
+    """relax_critical_slope cases and compact-frontier events (CPU adapter)."""
+    import slope_model as sm
+    from isaac_bulk_pipeline.config import SolverConfig
+    from isaac_bulk_pipeline.solvers import SparseTileFrontierMinimumSlopeAdapter
+    from isaac_bulk_pipeline.terrain import TerrainGrid
+
+    arrays = {}
+    full = []
+    # full-domain relax_critical_slope (H[axis0, axis1], spacing per axis)
+    pile = sm.random_pile(40, 48, 0.05, 0.05, seed=5, peak_height=0.6)
+    full.append(("PILE_40x48", pile, (0.05, 0.05), 34.0))
+    ys, xs = np.indices((30, 25))
+    cone = np.maximum(0.0, 0.9 - 0.09 * np.hypot(xs - 12.0, ys - 15.0))
+    full.append(("CONE_30x25_ANISO", cone, (0.05, 0.08), 30.0))
+    noise = 0.25 * (sm.fractal_perlin_noise(32, 32, seed=11) + 1.0)
+    full.append(("NOISE_32", noise, (0.05, 0.05), 35.0))
+    for name, h, spacing, angle in full:
+        out, stats = sm.relax_critical_slope(h, spacing, critical_angle_deg=angle,
+                                             max_iterations=20000, tolerance=1e-8)
+        arrays[f"full/{name}/h"] = h
+        arrays[f"full/{name}/spacing"] = np.asarray(spacing)
+        arrays[f"full/{name}/angle"] = np.float64(angle)
+        arrays[f"full/{name}/out"] = out
+        arrays[f"full/{name}/iterations"] = np.int64(stats.iterations)
+    arrays["full_names"] = np.asarray([n for n, *_ in full])
+
+    events = []
+    base = np.ones((33, 33))
+    dist = base.copy()
+    dist[16, 16] += 0.30
+    seeds = np.zeros((33, 33), dtype=bool)
+    seeds[16, 16] = True
+    events.append(("DISTURB_33", base, dist, seeds, 8, 30.0))
+    rng = np.random.default_rng(77)
+    ys, xs = np.indices((40, 56))
+    base2 = 0.5 + 0.2 * np.tan(np.deg2rad(20.0)) * xs * 0.05 + 0.002 * rng.random((40, 56))
+    dist2 = base2.copy()
+    seeds2 = np.zeros((40, 56), dtype=bool)
+    for (r, c, a) in ((10, 12, 0.25), (30, 40, 0.35), (22, 27, -0.2)):
+        dist2[r - 1:r + 2, c - 1:c + 2] += a
+        seeds2[r - 1:r + 2, c - 1:c + 2] = True
+    events.append(("MULTI_40x56", base2, dist2, seeds2, 8, 32.0))
+    for name, b0, d, sd, tile, angle in events:
+        ny, nx = d.shape
+        grid = TerrainGrid(nx, ny, 0.05, 0.05, 0.0, 0.0, "/World/Terrain")
+        cfg = SolverConfig(critical_angle_deg=angle, max_iterations=2000,
+                           large_avalanche_iteration_threshold=1000,
+                           numerical_safety_max_iterations=2000, tolerance=1.0e-8,
+                           boundary_condition="closed", conservation_tolerance_m3=1.0e-7)
+        cpu = SparseTileFrontierMinimumSlopeAdapter(grid, cfg, tile_size=tile)
+        cpu.set_reference_height(b0)
+        cpu.mark_changed(sd)
+        res = cpu.solve(d)
+        arrays[f"event/{name}/h"] = d
+        arrays[f"event/{name}/seeds"] = sd
+        arrays[f"event/{name}/tile"] = np.int64(tile)
+        arrays[f"event/{name}/angle"] = np.float64(angle)
+        arrays[f"event/{name}/out"] = res.heightmap_stable
+        arrays[f"event/{name}/iterations"] = np.int64(res.iteration_count)
+    arrays["event_names"] = np.asarray([n for n, *_ in events])
+    np.savez_compressed(HERE / "relax.npz", **arrays)
+
+
+def make_labels():
+    """Connected-component and yield fixtures from the CPU avalanche detector."""
+    from isaac_bulk_pipeline.bulk_interaction.large_avalanche import _largest_connected_region
+    from isaac_bulk_pipeline.bulk_interaction.yield_criterion import evaluate_cohesive_yield
+    from isaac_bulk_pipeline.bulk_state import MaterialScenario, TerrainVolumeIntegrator
+    from isaac_bulk_pipeline.terrain import TerrainGrid
+
+    arrays = {}
+    names = []
+    rng = np.random.default_rng(2024)
+    masks = {
+        "RANDOM_60x70_p045": rng.random((60, 70)) < 0.45,
+        "RANDOM_64x64_p060": rng.random((64, 64)) < 0.60,
+        "STRIPES_50x33": (np.indices((50, 33))[1] % 3) == 0,
+        "CHECKER_31x31": (np.indices((31, 31)).sum(axis=0) % 2) == 0,
+        "EMPTY_8x9": np.zeros((8, 9), dtype=bool),
+        "FULL_9x8": np.ones((9, 8), dtype=bool),
+    }
+    for name, mask in masks.items():
+        for conn in (4, 8):
+            largest, count, size = _largest_connected_region(mask, conn)
+            key = f"{name}/c{conn}"
+            names.append(key)
+            arrays[f"{key}/mask"] = mask
+            arrays[f"{key}/largest"] = largest
+            arrays[f"{key}/regions"] = np.int64(count)
+            arrays[f"{key}/largest_size"] = np.int64(size)
+    arrays["mask_names"] = np.asarray(names)
+    # cohesive yield on a seeded noise pile (start 38, stop 30, cohesion 0)
+    import slope_model as sm
+    ny, nx = 48, 52
+    grid = TerrainGrid(nx, ny, 0.05, 0.05, 0.0, 0.0, "/World/Terrain")
+    integ = TerrainVolumeIntegrator.from_grid(grid)
+    resting = 0.2 + 0.3 * (sm.fractal_perlin_noise(ny, nx, seed=3) + 1.0)
+    mobile = np.zeros((ny, nx))
+    material = MaterialScenario("golden", 1370.0, 29.8, 0.0, 0.5, 38.0, 30.0, 0.35)
+    depth = np.minimum(resting, 0.08)
+    ys = evaluate_cohesive_yield(resting, mobile, material, grid, integ, layer_depth_m=depth)
+    arrays["yield/resting"] = resting
+    arrays["yield/start_mask"] = ys.start_mask
+    arrays["yield/slope_rad"] = ys.slope_rad
+    arrays["yield/stop_margin"] = ys.yield_stop_margin_pa
+    largest, count, size = _largest_connected_region(ys.start_mask, 8)
+    arrays["yield/largest"] = largest
+    arrays["yield/regions"] = np.int64(count)
+    arrays["yield/largest_size"] = np.int64(size)
+    np.savez_compressed(HERE / "labels.npz", **arrays)
+
+
 def make_report_values():
     """Copy the numbers the reference ships in its own JSON reports."""
     import json
