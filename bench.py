@@ -241,6 +241,52 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     return result
 
 
+def run_mobile_large(args, n: int = 4096):
+    """Mobile V2 steps alone on an n^2 grid that is wet everywhere (HBM-bound:
+    the 28 B/cell working set of n = 4096 is 470 MB, well above the 126 MB L2)."""
+    import torch
+    import soilb200
+    from soilb200.bulk_state import B200BulkState, B200ProductionMobileV2Solver
+
+    ys, xs = np.indices((n, n), dtype=np.float64)
+    b = np.tan(np.deg2rad(10.0)) * xs * DX + 0.2 * np.sin(xs / 37.0) * np.cos(ys / 29.0)
+    h = 0.15 + 0.1 * np.cos(xs / 53.0) * np.sin(ys / 41.0)
+    state = B200BulkState((n, n), DX, DX, b, mobile_headroom_m=1.0)
+    state.grid.upload("mobile", h)
+    cfg = soilb200.MobileV2Config(dx_m=DX, dy_m=DX)
+    solver = B200ProductionMobileV2Solver(state=state, config=cfg)
+    solver.bind_device_state(state, material())
+    stream = torch.cuda.ExternalStream(state.grid.stream_handle())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        solver.step_resident(DT)
+    torch.cuda.synchronize()
+    dev_ms, subs, loop = 0.0, 0, []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        rec = solver.step_resident(DT)
+        e1.record(stream)
+        e1.synchronize()
+        dev_ms += e0.elapsed_time(e1)
+        subs += rec.substeps
+        ls = solver.last_stats
+        loop.append((ls.substep_loop_ms, ls.substeps))
+    peak, kind = measured_peak()
+    per = sum(m for m, _ in loop) / max(sum(k for _, k in loop), 1)
+    alg = BYTES_PER_CELL_SUBSTEP * n * n
+    ach = alg / (per * 1e-3) / 1e9
+    return {"metric": f"Mobile V2 cell-substeps/s at {n}^2 (FV step only, wet everywhere)",
+            "value": n * n * subs / (dev_ms * 1e-3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+            "substeps": subs, "higher_is_better": True,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "peak_source": kind, "mean_launch_ms": per,
+                         "algorithmic_bytes_per_launch": alg}}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle port, NumPy, 1 core)
 # ---------------------------------------------------------------------------
@@ -337,6 +383,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="config1_plain_path_701",
+                    choices=["config1_plain_path_701", "mobile_v2_4096"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -345,6 +393,9 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)))
+        return
+    if args.workload == "mobile_v2_4096":
+        print(json.dumps(run_mobile_large(args)))
         return
     if world > 1:
         import datetime

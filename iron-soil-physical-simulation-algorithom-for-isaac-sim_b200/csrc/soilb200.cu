@@ -108,6 +108,8 @@ struct sb_ctx {
   int ledger_blocks = 0;
   MobileGraph mobile;
   cudaEvent_t ev_loop[2] = {nullptr, nullptr};  // around the substep WHILE node
+  bool use_graphs = true;  // false: host-driven launches (profilers that cannot see
+                           // kernels inside conditional graphs)
   // labelling (flat ny*nx arrays)
   int* parent = nullptr;
   void* slope = nullptr;
@@ -377,6 +379,42 @@ void fill_ledger(const sb_ctx* ctx, const LedgerOut& o, const sb_mobile_params* 
   L->resting_w_quanta = fx(ctx) ? o.iq[2] : 0;
 }
 
+template <bool FX>
+static int mobile_step_host_loop(sb_ctx* ctx, const FvConst& c, double static_limit) {
+  // Same kernels as the graph, launched from the host; the loop flag is read
+  // back after every substep (one synchronisation per substep).
+  double datum = ctx->d.datum_m, limit = static_limit;
+  int mode0 = 0, mode1 = 1, no_handle = 0;
+  cudaGraphConditionalHandle handle{};
+  FvConst cc = c;
+  {
+    void* args[] = {(void*)&ctx->ctl, (void*)&ctx->dt_dev};
+    SB_CUDA(ctx, cudaLaunchKernel((void*)fv_begin_kernel, dim3(1), dim3(kThreads), args, 0,
+                                  ctx->stream));
+  }
+  std::vector<void*> args;
+  ledger_args<FX>(ctx, cc, &datum, &limit, &mode0, &handle, &no_handle, args);
+  SB_CUDA(ctx, cudaLaunchKernel((void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks), dim3(kThreads),
+                                args.data(), 0, ctx->stream));
+  SB_CUDA(ctx, cudaEventRecord(ctx->ev_loop[0], ctx->stream));
+  std::vector<void*> fargs;
+  fv_args<FX>(ctx, cc, &handle, &no_handle, fargs);
+  for (int it = 0; it <= c.max_substeps; ++it) {
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(FvControl), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->ctl_host->done) break;
+    SB_CUDA(ctx, cudaLaunchKernel((void*)fv_substep_kernel<FX>, dim3(c.nblocks), dim3(kThreads),
+                                  fargs.data(), fv_smem_bytes<FX>(), ctx->stream));
+  }
+  SB_CUDA(ctx, cudaEventRecord(ctx->ev_loop[1], ctx->stream));
+  std::vector<void*> a2;
+  ledger_args<FX>(ctx, cc, &datum, &limit, &mode1, &handle, &no_handle, a2);
+  SB_CUDA(ctx, cudaLaunchKernel((void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks), dim3(kThreads),
+                                a2.data(), 0, ctx->stream));
+  return SB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -433,6 +471,10 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   *out = ctx;
   SB_CUDA(ctx, cudaSetDevice(d.device));
   SB_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  {
+    const char* env = std::getenv("SOILB200_NO_GRAPH");
+    ctx->use_graphs = !(env && env[0] == '1');
+  }
   ctx->quantum = std::ldexp(1.0, -d.height_exponent);
   ctx->pitch = (d.nx + 31) / 32 * 32;
   ctx->esize = fx(ctx) ? 4 : 8;
@@ -734,8 +776,8 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
   const double static_limit =
       std::tan(params->start_angle_deg * (M_PI / 180.0)) + 1.0e-14;
   MobileGraph& mg = ctx->mobile;
-  if (!mg.valid || std::memcmp(&mg.key, &c, sizeof(FvConst)) != 0 ||
-      mg.static_limit != static_limit) {
+  if (ctx->use_graphs && (!mg.valid || std::memcmp(&mg.key, &c, sizeof(FvConst)) != 0 ||
+                          mg.static_limit != static_limit)) {
     rc = fx(ctx) ? build_mobile_graph<true>(ctx, c, static_limit)
                  : build_mobile_graph<false>(ctx, c, static_limit);
     if (rc) return rc;
@@ -743,7 +785,13 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
   *ctx->dt_host = dt_s;
   SB_CUDA(ctx, cudaMemcpyAsync(ctx->dt_dev, ctx->dt_host, sizeof(double), cudaMemcpyHostToDevice,
                                ctx->stream));
-  SB_CUDA(ctx, cudaGraphLaunch(mg.exec, ctx->stream));
+  if (ctx->use_graphs) {
+    SB_CUDA(ctx, cudaGraphLaunch(mg.exec, ctx->stream));
+  } else {
+    rc = fx(ctx) ? mobile_step_host_loop<true>(ctx, c, static_limit)
+                 : mobile_step_host_loop<false>(ctx, c, static_limit);
+    if (rc) return rc;
+  }
   SB_CUDA(ctx, cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(FvControl), cudaMemcpyDeviceToHost,
                                ctx->stream));
   SB_CUDA(ctx, cudaMemcpyAsync(ctx->io_host, ctx->io, sizeof(StepIO), cudaMemcpyDeviceToHost,
