@@ -253,6 +253,8 @@ def run_mobile_large(args, n: int = 4096):
     h = 0.15 + 0.1 * np.cos(xs / 53.0) * np.sin(ys / 41.0)
     state = B200BulkState((n, n), DX, DX, b, mobile_headroom_m=1.0)
     state.grid.upload("mobile", h)
+    state.grid.upload("momentum_x", 0.8 * h)   # 0.8 m/s downslope: never static
+    state.grid.upload("momentum_y", 0.3 * h)
     cfg = soilb200.MobileV2Config(dx_m=DX, dy_m=DX)
     solver = B200ProductionMobileV2Solver(state=state, config=cfg)
     solver.bind_device_state(state, material())

@@ -235,3 +235,4 @@ def largest_connected_region(mask: np.ndarray, connectivity: int, *, device: int
         grid.close()
     return labels == int(st.winner_root), int(st.connected_region_count), \
         int(st.largest_connected_cell_count)
+

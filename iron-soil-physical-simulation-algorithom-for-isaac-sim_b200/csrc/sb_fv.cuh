@@ -38,7 +38,7 @@ struct FvConst {
   double dx, dy, K, g, cfl, dry, mu_g, c_half, kg, min_spacing;
   // fixed-point constants
   double Q;
-  float Kf, KGf, HKGf, Qf, invQf, dryf;
+  float Kf, KGf, HKGf, Qf, invQf, dryf, QKf;  // QKf = float(Q / K)
   int max_substeps;
   int has_external;
 };
@@ -94,6 +94,8 @@ struct FvSmem {
   alignas(128) typename T::H h[Tl::BOX];
   alignas(128) typename T::R qx[Tl::BOX];
   alignas(128) typename T::R qy[Tl::BOX];
+  // FX only: per-cell velocity q/h and celerity sqrt(K g h) of the loaded tile
+  typename T::R u[Tl::BOX], v[Tl::BOX], cel[Tl::BOX];
   M em[kEastFaces];
   typename T::R enm[kEastFaces], enp[kEastFaces], et[kEastFaces];
   M nm[kNorthFaces];
@@ -108,34 +110,43 @@ struct FvSmem {
 // tangential momentum components.  Outputs: mass flux (quanta or raw),
 // normal-momentum flux seen by L (minus) and by R (plus), tangential flux.
 // --------------------------------------------------------------------------
+// FX face: un/ut are the cells' velocity components q/h (0 for empty cells), cl/cr
+// their celerities sqrt(K g h).  The hydrostatic depth only differs from h on
+// the lower side of a face (d > 0), so only that side needs a square root.
+// Reconstructed discharge is u * hs (= q * hs / h of the reference).
 __device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int br, int hlq,
-                                        int hrq, float qnl, float qtl, float qnr, float qtr,
-                                        int& m, float& fnm, float& fnp, float& ft) {
+                                        int hrq, float unl, float utl, float unr, float utr,
+                                        float cl, float cr, int& m, float& fnm, float& fnp,
+                                        float& ft) {
   const int bface = max(bl, br);
   const int dl = bface - bl;
   const int dr = bface - br;
   const float hl = (float)hlq * c.Qf;
   const float hr = (float)hrq * c.Qf;
-  float hsl = hl, hsr = hr;
-  if (dl != 0) hsl = fmaxf((c.Kf * hl - (float)dl * c.Qf) / c.Kf, 0.f);
-  if (dr != 0) hsr = fmaxf((c.Kf * hr - (float)dr * c.Qf) / c.Kf, 0.f);
-  const float sl = hlq > 0 ? hsl / hl : 0.f;
-  const float sr = hrq > 0 ? hsr / hr : 0.f;
-  const float qnsl = qnl * sl, qtsl = qtl * sl;
-  const float qnsr = qnr * sr, qtsr = qtr * sr;
+  float hsl = hl, hsr = hr, csl = cl, csr = cr, corl = 0.f, corr = 0.f;
+  if (dl != 0) {
+    hsl = fmaxf(hl - (float)dl * c.QKf, 0.f);
+    csl = sqrtf(c.KGf * hsl);
+    corl = (c.HKGf * hl) * hl - (c.HKGf * hsl) * hsl;
+  }
+  if (dr != 0) {
+    hsr = fmaxf(hr - (float)dr * c.QKf, 0.f);
+    csr = sqrtf(c.KGf * hsr);
+    corr = (c.HKGf * hr) * hr - (c.HKGf * hsr) * hsr;
+  }
+  const float qnsl = unl * hsl, qtsl = utl * hsl;
+  const float qnsr = unr * hsr, qtsr = utr * hsr;
   const bool wl = hsl > c.dryf, wr = hsr > c.dryf;
-  const float unl = wl ? qnsl / hsl : 0.f, utl = wl ? qtsl / hsl : 0.f;
-  const float unr = wr ? qnsr / hsr : 0.f, utr = wr ? qtsr / hsr : 0.f;
-  const float fnl = qnsl * unl + (c.HKGf * hsl) * hsl;
-  const float fnr = qnsr * unr + (c.HKGf * hsr) * hsr;
-  const float ftl = qnsl * utl, ftr = qnsr * utr;
-  const float spd = fmaxf(fabsf(unl) + sqrtf(c.KGf * hsl), fabsf(unr) + sqrtf(c.KGf * hsr));
+  const float vnl = wl ? unl : 0.f, vtl = wl ? utl : 0.f;
+  const float vnr = wr ? unr : 0.f, vtr = wr ? utr : 0.f;
+  const float fnl = qnsl * vnl + (c.HKGf * hsl) * hsl;
+  const float fnr = qnsr * vnr + (c.HKGf * hsr) * hsr;
+  const float ftl = qnsl * vtl, ftr = qnsr * vtr;
+  const float spd = fmaxf(fabsf(vnl) + csl, fabsf(vnr) + csr);
   const float half = 0.5f * spd;
   const float fh = 0.5f * (qnsl + qnsr) - half * (hsr - hsl);
   const float fn = 0.5f * (fnl + fnr) - half * (qnsr - qnsl);
   ft = 0.5f * (ftl + ftr) - half * (qtsr - qtsl);
-  const float corl = (c.HKGf * hl) * hl - (c.HKGf * hsl) * hsl;
-  const float corr = (c.HKGf * hr) * hr - (c.HKGf * hsr) * hsr;
   float mf = rintf((lam * fh) * c.invQf);
   mf = fminf(fmaxf(mf, -1073741824.f), 1073741824.f);
   int mi = (int)mf;
@@ -275,6 +286,17 @@ __global__ void __launch_bounds__(kThreads)
   if (!loaded) {
     if (threadIdx.x == 0) atomicExch(&ctl->wait_fail, 1);
   }
+  if constexpr (FX) {
+    // per-cell velocity and celerity of the whole halo box
+    for (int j = threadIdx.x; j < Tl::BOX; j += kThreads) {
+      const float hf = (float)s.h[j] * c.Qf;
+      const float inv = s.h[j] > 0 ? 1.0f / hf : 0.f;
+      s.u[j] = s.qx[j] * inv;
+      s.v[j] = s.qy[j] * inv;
+      s.cel[j] = sqrtf(c.KGf * hf);
+    }
+    __syncthreads();
+  }
   const float lamx_f = (float)(sub_dt / c.dx);
   const float lamy_f = (float)(sub_dt / c.dy);
   const double lamx = sub_dt / c.dx;
@@ -306,11 +328,11 @@ __global__ void __launch_bounds__(kThreads)
       float fnm = 0.f, fnp = 0.f, ft = 0.f;
       if (valid) {
         if (east)
-          face_fx(c, lamx_f, s.b[la], s.b[lb], s.h[la], s.h[lb], s.qx[la], s.qy[la], s.qx[lb],
-                  s.qy[lb], m, fnm, fnp, ft);
+          face_fx(c, lamx_f, s.b[la], s.b[lb], s.h[la], s.h[lb], s.u[la], s.v[la], s.u[lb],
+                  s.v[lb], s.cel[la], s.cel[lb], m, fnm, fnp, ft);
         else
-          face_fx(c, lamy_f, s.b[la], s.b[lb], s.h[la], s.h[lb], s.qy[la], s.qx[la], s.qy[lb],
-                  s.qx[lb], m, fnm, fnp, ft);
+          face_fx(c, lamy_f, s.b[la], s.b[lb], s.h[la], s.h[lb], s.v[la], s.u[la], s.v[lb],
+                  s.u[lb], s.cel[la], s.cel[lb], m, fnm, fnp, ft);
       }
       if (east) {
         s.em[f] = m; s.enm[f] = fnm; s.enp[f] = fnp; s.et[f] = ft;
@@ -377,15 +399,19 @@ __global__ void __launch_bounds__(kThreads)
       const float qyn = wet ? qy_old + dqy : 0.f;
       float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
       if (wet) {
-        vbx = qxn / hn;
-        vby = qyn / hn;
+        const float inv = 1.0f / hn;
+        vbx = qxn * inv;
+        vby = qyn * inv;
         if (c.has_external) {
           const float dtf = (float)sub_dt;
           qex = qxn + (hn * ax) * dtf;
           qey = qyn + (hn * ay) * dtf;
+          vex = qex * inv;
+          vey = qey * inv;
+        } else {
+          vex = vbx;
+          vey = vby;
         }
-        vex = qex / hn;
-        vey = qey / hn;
       }
       const float spd = sqrtf(vex * vex + vey * vey);
       const float dec = (float)(c.mu_g * sub_dt);
@@ -406,12 +432,7 @@ __global__ void __launch_bounds__(kThreads)
                 ((double)spd * (double)spd - ((double)vax * (double)vax + (double)vay * (double)vay));
       acc[7] += h64 * ((0.5 * ((double)vbx + (double)vex)) * (double)ax +
                        (0.5 * ((double)vby + (double)vey)) * (double)ay) * sub_dt;
-      float vx = 0.f, vy = 0.f;
-      if (wet) {
-        vx = qxo / hn;
-        vy = qyo / hn;
-      }
-      const float wv = sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn);
+      const float wv = spd * fac + sqrtf(c.KGf * hn);  // |new velocity| + celerity
       wave = fmax(wave, (double)wv);
     } else {
       const double dh = (((0.0 - lamx * s.em[e]) + lamx * s.em[w]) - lamy * s.nm[n]) + lamy * s.nm[so];

@@ -102,8 +102,9 @@ __global__ void __launch_bounds__(kThreads)
       const float hn = (float)h[gi] * c.Qf;
       float vx = 0.f, vy = 0.f;
       if (hn > c.dryf) {
-        vx = qx[gi] / hn;
-        vy = qy[gi] / hn;
+        const float inv = 1.0f / hn;
+        vx = qx[gi] * inv;
+        vy = qy[gi] * inv;
       }
       wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
     } else {
@@ -172,21 +173,28 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // fixed-order final reduction (thread k handles slot k serially over blocks)
+  // fixed-order final reduction: every thread folds a strided subset of the
+  // block partials, then a fixed shuffle/shared-memory tree combines them
   LedgerOut* out = mode == 0 ? &io->before : &io->after;
-  if (threadIdx.x < L_NP) {
-    const int k = threadIdx.x;
-    double a = k == L_NEGMINH ? -1.0e300 : 0.0;
-    for (unsigned bk = 0; bk < gridDim.x; ++bk) {
-      const double x = __ldcg(partials + (size_t)bk * L_NP + k);
-      a = k < L_NSUM ? a + x : fmax(a, x);
-    }
-    out->v[k] = a;
-  } else if (threadIdx.x < L_NP + kLedgerI64) {
-    const int k = threadIdx.x - L_NP;
+  __shared__ bool is_max[L_NP];
+  __shared__ double tot[L_NP];
+  if (threadIdx.x < L_NP) is_max[threadIdx.x] = threadIdx.x >= L_NSUM;
+  __syncthreads();
+  reduce_partials<L_NP>(partials, gridDim.x, tot, red, is_max);
+  {
+    long long a[kLedgerI64] = {0, 0, 0};
+    for (unsigned bk = threadIdx.x; bk < gridDim.x; bk += kThreads)
+      for (int k = 0; k < kLedgerI64; ++k) a[k] += __ldcg(ipartials + (size_t)bk * kLedgerI64 + k);
+    for (int k = 0; k < kLedgerI64; ++k) a[k] = (long long)warp_sum_u64((unsigned long long)a[k]);
+    if (lane == 0)
+      for (int k = 0; k < kLedgerI64; ++k) ired[warp * kLedgerI64 + k] = a[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < L_NP) out->v[threadIdx.x] = tot[threadIdx.x];
+  if (threadIdx.x < kLedgerI64) {
     long long a = 0;
-    for (unsigned bk = 0; bk < gridDim.x; ++bk) a += __ldcg(ipartials + (size_t)bk * kLedgerI64 + k);
-    out->iq[k] = a;
+    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + threadIdx.x];
+    out->iq[threadIdx.x] = a;
   }
   __syncthreads();
   if (threadIdx.x == 0) {

@@ -232,6 +232,7 @@ FvConst make_const(const sb_ctx* ctx, const sb_mobile_params* p) {
   c.Qf = (float)ctx->quantum;
   c.invQf = (float)(1.0 / ctx->quantum);
   c.dryf = (float)c.dry;
+  c.QKf = (float)(ctx->quantum / c.K);
   c.max_substeps = p->maximum_substeps;
   c.has_external = p->use_external ? 1 : 0;
   return c;
@@ -1431,3 +1432,4 @@ extern "C" int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double
   out3[2] = density_kg_m3 * o.momentum_w[1];
   return SB_OK;
 }
+

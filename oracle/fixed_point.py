@@ -8,8 +8,11 @@ exactly; each donor may lose at most ``floor(h/4)`` quanta per face, so heights
 can never become negative (the reference equations are positivity-preserving
 for CFL <= 0.25, where this cap never binds; it only limits faces at CFL 0.4).
 
-The operation order below is the specification of the kernel in
-``csrc/fv_kernels.cuh`` (``Fx32`` traits).  All float32 operations are single
+The operation order below is the specification of the FX instantiation of
+the kernel in ``csrc/sb_fv.cuh``.  Velocities are computed once per cell
+(u = q * (1/h)) and reused by its faces: the reference's reconstructed
+discharge q * (hs/h) equals u * hs and its face velocity qs/hs equals u, so
+this is the same mathematics with no division per face.  All float32 operations are single
 IEEE operations (the library is compiled with ``-fmad=false``), so this mirror
 and the kernel agree bit for bit.
 
@@ -67,68 +70,85 @@ def _div(num, den, wet):
     return out
 
 
-def face_fluxes(p: FixedParams, lam: np.float32, bl, br, hlq, hrq, qnl, qtl, qnr, qtr):
-    """Fluxes of one face family.  Returns (mass quanta int32, Fn_minus, Fn_plus, Ft)."""
-    KF = F32(p.K)
+def cell_velocity(p: FixedParams, hq, qx, qy):
+    """Per-cell velocity q/h (0 where h == 0) and celerity sqrt(K g h)."""
+    QF = F32(p.quantum)
+    hf = hq.astype(F32) * QF
+    inv = _div(np.ones_like(hf), hf, hq > 0)
+    return qx * inv, qy * inv, np.sqrt(F32(p.K * p.gravity) * hf)
+
+
+def face_fluxes(p: FixedParams, lam: np.float32, bl, br, hlq, hrq, unl, utl, unr, utr, cl, cr):
+    """Fluxes of one face family from cell velocities (un, ut) and celerities c.
+
+    Returns (mass quanta int32, Fn_minus, Fn_plus, Ft)."""
     KGF = F32(p.K * p.gravity)
     HKGF = F32(0.5 * p.K * p.gravity)
     QF = F32(p.quantum)
+    QKF = F32(p.quantum / p.K)
     INVQ = F32(2.0 ** p.exponent)
     DRYF = F32(p.dry)
+    zero = F32(0)
     bface = np.maximum(bl, br)
     dl = (bface - bl).astype(np.int32)
     dr = (bface - br).astype(np.int32)
     hl = hlq.astype(F32) * QF
     hr = hrq.astype(F32) * QF
-    hsl = np.where(dl == 0, hl, np.maximum((KF * hl - dl.astype(F32) * QF) / KF, F32(0)))
-    hsr = np.where(dr == 0, hr, np.maximum((KF * hr - dr.astype(F32) * QF) / KF, F32(0)))
-    sl = _div(hsl, hl, hlq > 0)
-    sr = _div(hsr, hr, hrq > 0)
-    qnsl, qtsl = qnl * sl, qtl * sl
-    qnsr, qtsr = qnr * sr, qtr * sr
-    wl = hsl > DRYF
-    wr = hsr > DRYF
-    unl, utl = _div(qnsl, hsl, wl), _div(qtsl, hsl, wl)
-    unr, utr = _div(qnsr, hsr, wr), _div(qtsr, hsr, wr)
-    fnl = qnsl * unl + (HKGF * hsl) * hsl
-    fnr = qnsr * unr + (HKGF * hsr) * hsr
-    ftl = qnsl * utl
-    ftr = qnsr * utr
-    spd = np.maximum(np.abs(unl) + np.sqrt(KGF * hsl), np.abs(unr) + np.sqrt(KGF * hsr))
+    low_l, low_r = dl != 0, dr != 0
+    hsl = np.where(low_l, np.maximum(hl - dl.astype(F32) * QKF, zero), hl)
+    hsr = np.where(low_r, np.maximum(hr - dr.astype(F32) * QKF, zero), hr)
+    csl = np.where(low_l, np.sqrt(KGF * hsl), cl)
+    csr = np.where(low_r, np.sqrt(KGF * hsr), cr)
+    corl = np.where(low_l, (HKGF * hl) * hl - (HKGF * hsl) * hsl, zero)
+    corr = np.where(low_r, (HKGF * hr) * hr - (HKGF * hsr) * hsr, zero)
+    qnsl, qtsl = unl * hsl, utl * hsl
+    qnsr, qtsr = unr * hsr, utr * hsr
+    wl, wr = hsl > DRYF, hsr > DRYF
+    vnl, vtl = np.where(wl, unl, zero), np.where(wl, utl, zero)
+    vnr, vtr = np.where(wr, unr, zero), np.where(wr, utr, zero)
+    fnl = qnsl * vnl + (HKGF * hsl) * hsl
+    fnr = qnsr * vnr + (HKGF * hsr) * hsr
+    ftl = qnsl * vtl
+    ftr = qnsr * vtr
+    spd = np.maximum(np.abs(vnl) + csl, np.abs(vnr) + csr)
     half = F32(0.5) * spd
     fh = F32(0.5) * (qnsl + qnsr) - half * (hsr - hsl)
     fn = F32(0.5) * (fnl + fnr) - half * (qnsr - qnsl)
     ft = F32(0.5) * (ftl + ftr) - half * (qtsr - qtsl)
-    corr_l = (HKGF * hl) * hl - (HKGF * hsl) * hsl
-    corr_r = (HKGF * hr) * hr - (HKGF * hsr) * hsr
     m = np.rint((lam * fh) * INVQ)
     m = np.clip(m, F32(-(2.0 ** 30)), F32(2.0 ** 30)).astype(np.int32)
     m = np.where(m > 0, np.minimum(m, hlq >> 2), np.maximum(m, -(hrq >> 2))).astype(np.int32)
-    return m, fn + corr_l, fn + corr_r, ft
+    return m, fn + corl, fn + corr, ft
 
 
 def wave_speed(p: FixedParams, hq: np.ndarray, qx: np.ndarray, qy: np.ndarray) -> np.ndarray:
+    """Wave speed of a state as evaluated by the step prologue."""
     QF = F32(p.quantum)
     KGF = F32(p.K * p.gravity)
     hn = hq.astype(F32) * QF
     wet = hn > F32(p.dry)
-    vx = _div(qx, hn, wet)
-    vy = _div(qy, hn, wet)
+    inv = _div(np.ones_like(hn), hn, wet)
+    vx = qx * inv
+    vy = qy * inv
     return np.sqrt(vx * vx + vy * vy) + np.sqrt(KGF * hn)
 
 
 def substep(p: FixedParams, bq, hq, qx, qy, sub_dt: float, ax=None, ay=None):
-    """One substep on int32/float32 fields; returns new fields and FP64 diagnostics."""
+    """One substep on int32/float32 fields; returns new fields, FP64 diagnostics
+    and the wave speed of the new state (which sets the next dt)."""
     ny, nx = hq.shape
     lamx = F32(sub_dt / p.dx)
     lamy = F32(sub_dt / p.dy)
     QF = F32(p.quantum)
+    u, v, cel = cell_velocity(p, hq, qx, qy)
     # x faces: between (r, c) and (r, c+1); normal = x, tangential = y.
     mx, fnmx, fnpx, ftx = face_fluxes(p, lamx, bq[:, :-1], bq[:, 1:], hq[:, :-1], hq[:, 1:],
-                                      qx[:, :-1], qy[:, :-1], qx[:, 1:], qy[:, 1:])
+                                      u[:, :-1], v[:, :-1], u[:, 1:], v[:, 1:],
+                                      cel[:, :-1], cel[:, 1:])
     # y faces: between (r, c) and (r+1, c); normal = y, tangential = x.
     my, fnmy, fnpy, fty = face_fluxes(p, lamy, bq[:-1, :], bq[1:, :], hq[:-1, :], hq[1:, :],
-                                      qy[:-1, :], qx[:-1, :], qy[1:, :], qx[1:, :])
+                                      v[:-1, :], u[:-1, :], v[1:, :], u[1:, :],
+                                      cel[:-1, :], cel[1:, :])
 
     def pad_e(a):  # east face value per cell (zero on the last column)
         out = np.zeros((ny, nx), dtype=a.dtype)
@@ -156,22 +176,21 @@ def substep(p: FixedParams, bq, hq, qx, qy, sub_dt: float, ax=None, ay=None):
     dqy = (((zero - lamx * pad_e(ftx)) + lamx * pad_w(ftx)) - lamy * pad_n(fnmy)) + lamy * pad_s(fnpy)
     hnq = (hq + dh).astype(np.int32)
     assert int(hnq.min(initial=0)) >= 0
-    qxn = qx + dqx
-    qyn = qy + dqy
     hn = hnq.astype(F32) * QF
     wet = hn > F32(p.dry)
-    qxn = np.where(wet, qxn, zero)
-    qyn = np.where(wet, qyn, zero)
-    vbx = _div(qxn, hn, wet)
-    vby = _div(qyn, hn, wet)
+    qxn = np.where(wet, qx + dqx, zero)
+    qyn = np.where(wet, qy + dqy, zero)
+    inv = _div(np.ones_like(hn), hn, wet)
+    vbx = qxn * inv
+    vby = qyn * inv
     if ax is not None:
         dtf = F32(sub_dt)
-        qex = qxn + (hn * ax) * dtf
-        qey = qyn + (hn * ay) * dtf
+        qex = np.where(wet, qxn + (hn * ax) * dtf, qxn)
+        qey = np.where(wet, qyn + (hn * ay) * dtf, qyn)
+        vex = qex * inv
+        vey = qey * inv
     else:
-        qex, qey = qxn, qyn
-    vex = _div(qex, hn, wet)
-    vey = _div(qey, hn, wet)
+        qex, qey, vex, vey = qxn, qyn, vbx, vby
     spd = np.sqrt(vex * vex + vey * vey)
     dec = F32(p.mu * p.gravity * sub_dt)
     fac = np.maximum(zero, F32(1) - dec / np.maximum(spd, F32(1.0e-15)))
@@ -179,6 +198,7 @@ def substep(p: FixedParams, bq, hq, qx, qy, sub_dt: float, ax=None, ay=None):
     vay = vey * fac
     qxo = hn * vax
     qyo = hn * vay
+    wave = spd * fac + np.sqrt(F32(p.K * p.gravity) * hn)
     h64 = hn.astype(np.float64)
     diag = {
         "cons": np.asarray([np.sum(qxn.astype(np.float64) - qx), np.sum(qyn.astype(np.float64) - qy)]),
@@ -186,6 +206,7 @@ def substep(p: FixedParams, bq, hq, qx, qy, sub_dt: float, ax=None, ay=None):
         "fric": np.asarray([np.sum(qxo.astype(np.float64) - qex), np.sum(qyo.astype(np.float64) - qey)]),
         "fdiss": 0.5 * float(np.sum(h64 * (spd.astype(np.float64) ** 2
                                            - (vax.astype(np.float64) ** 2 + vay.astype(np.float64) ** 2)))),
+        "wave": float(np.max(wave, initial=F32(0))),
     }
     return hnq, qxo.astype(F32), qyo.astype(F32), diag
 
@@ -211,13 +232,14 @@ def step(p: FixedParams, bq, hq, qx, qy, dt_s: float, ax=None, ay=None):
     remaining = float(dt_s)
     smin = min(p.dx, p.dy)
     dts = []
+    w = float(np.max(wave_speed(p, hq, qx, qy), initial=F32(0)))
     while remaining > 1.0e-14:
         if len(dts) >= p.maximum_substeps:
             raise RuntimeError("MobileV2 maximum_substeps exceeded")
-        w = float(np.max(wave_speed(p, hq, qx, qy), initial=F32(0)))
         stable = remaining if w <= 1.0e-14 else p.cfl * smin / w
         sub = min(remaining, stable)
-        hq, qx, qy, _ = substep(p, bq, hq, qx, qy, sub, ax, ay)
+        hq, qx, qy, diag = substep(p, bq, hq, qx, qy, sub, ax, ay)
+        w = diag["wave"]
         dts.append(sub)
         remaining -= sub
     return hq, qx, qy, len(dts), dts
