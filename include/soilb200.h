@@ -59,7 +59,8 @@ enum sb_status {
   SB_ERR_CUDA = 5,            /* CUDA runtime/driver error */
   SB_ERR_WAIT_LIMIT = 6,      /* a bounded device-side wait gave up */
   SB_ERR_STATE = 7,           /* call order / missing data */
-  SB_ERR_RANGE = 8            /* value outside the fixed-point range */
+  SB_ERR_RANGE = 8,           /* value outside the fixed-point range */
+  SB_ERR_CAPACITY = 9         /* request larger than a fixed, preallocated capacity */
 };
 
 enum sb_precision { SB_FP64 = 0, SB_FX32 = 1 };
@@ -254,6 +255,28 @@ int sb_entrain_to_surface(sb_ctx* ctx, const int32_t* flat_indices,
  * out3 = {deposited volume m3, removed momentum x, y (density * q * w)}. */
 int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double* requested_depth_m,
                int count, double density_kg_m3, double* out3);
+
+/* ---- Allocation-free connected components --------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory once running -- e.g. a simulator plugin whose frame callbacks forbid
+ * cudaMalloc (it can block, synchronise the device and break real-time step
+ * budgets), or code issuing work into a CUDA stream capture it does not own,
+ * where allocation calls are not permitted.  The caller passes device
+ * pointers for the int32 mask (nonzero = member) and the int32 output labels
+ * (canonical: -1 outside the mask, else the component's minimum flat index),
+ * both ny*nx row-major, plus the stream to run on.  Scratch (per-root counters
+ * and the root list) is a file-scope static device array reserved on every
+ * GPU that loads the library until process exit; it is never allocated by
+ * this call.  Limit: ny*nx <= 524288 cells (SB_ERR_CAPACITY beyond).  The
+ * first call on a device looks up the scratch address with the device
+ * current, so make that first call before any stream capture.  Every call
+ * shares the one scratch array (its contents persist; each call clears what
+ * must start at zero), so calls that overlap on the GPU race: serialise them
+ * (one stream, or wait between calls).  Blocks until the stats are read.
+ * dx_m/dy_m only scale largest_connected_area_m2. */
+int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, int ny, int nx,
+                         int connectivity, double dx_m, double dy_m, void* stream,
+                         sb_label_stats* out);
 
 int sb_last_error(sb_ctx* ctx, char* buffer, size_t length);
 /* Number of kernels this context has launched (cumulative). */

@@ -26,6 +26,7 @@ from .avalanche import (  # noqa: F401
     LargeAvalancheTransitionConfig,
     MaterialScenario,
     label_mask,
+    label_mask_preallocated,
     largest_connected_region,
 )
 from .relax import (  # noqa: F401
@@ -46,4 +47,5 @@ __all__ = [
     "B200LargeAvalancheBridge", "LabelDiagnosis", "LargeAvalancheTransitionConfig",
     "MaterialScenario", "FrontierRelaxation", "FrontierStats", "RelaxationStats",
     "relax_critical_slope", "label_mask", "largest_connected_region",
+    "label_mask_preallocated",
 ]

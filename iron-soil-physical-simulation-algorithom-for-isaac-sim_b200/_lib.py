@@ -24,6 +24,7 @@ SB_ERR_CUDA = 5
 SB_ERR_WAIT_LIMIT = 6
 SB_ERR_STATE = 7
 SB_ERR_RANGE = 8
+SB_ERR_CAPACITY = 9
 
 SB_FP64 = 0
 SB_FX32 = 1
@@ -160,6 +161,9 @@ _PROTOTYPES = {
     "sb_label": (C.c_int, [C.c_void_p, C.POINTER(LabelParams), C.POINTER(LabelStats)]),
     "sb_label_commit": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "sb_label_mask": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LabelStats)]),
+    "sb_label_mask_static": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                       C.c_double, C.c_double, C.c_void_p,
+                                       C.POINTER(LabelStats)]),
     "sb_relax_full": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams), C.POINTER(RelaxStats)]),
     "sb_frontier_seed_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "sb_frontier_seed_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

@@ -236,3 +236,31 @@ def largest_connected_region(mask: np.ndarray, connectivity: int, *, device: int
     return labels == int(st.winner_root), int(st.connected_region_count), \
         int(st.largest_connected_cell_count)
 
+
+def label_mask_preallocated(mask_ptr: int, labels_ptr: int, shape, connectivity: int = 8, *,
+                            dx_m: float = 1.0, dy_m: float = 1.0, stream: int = 0):
+    """Connected components with no device allocation by this library.
+
+    For callers that cannot allocate device memory while they run (a plugin
+    frame callback with a fixed memory budget, or work recorded into a CUDA
+    stream capture owned by someone else).  ``mask_ptr`` / ``labels_ptr`` are
+    device addresses of int32 row-major ``shape`` arrays (e.g. from
+    ``tensor.data_ptr()``); the scratch is a fixed static device array, so
+    ``shape`` may hold at most 524288 cells and concurrent calls must not
+    overlap on the GPU.  Returns the ``LabelStats`` record.
+    """
+    ny, nx = int(shape[0]), int(shape[1])
+    st = _lib.LabelStats()
+    rc = _lib.load().sb_label_mask_static(mask_ptr, labels_ptr, ny, nx, int(connectivity),
+                                          float(dx_m), float(dy_m), stream, st)
+    if rc == _lib.SB_ERR_CAPACITY:
+        raise ValueError(f"[soilb200] {ny}x{nx} = {ny * nx} cells exceeds the static "
+                         "scratch capacity of 524288 cells")
+    if rc == _lib.SB_ERR_BAD_ARG:
+        raise ValueError("[soilb200] invalid pointers, shape or connectivity")
+    if rc == _lib.SB_ERR_NONCONVERGENCE:
+        raise _lib.NumericalNonconvergenceError(
+            "NUMERICAL_NONCONVERGENCE: device avalanche connected components")
+    if rc != _lib.SB_OK:
+        raise _lib.B200DeviceError(f"[soilb200] sb_label_mask_static failed with status {rc}")
+    return st

@@ -1433,3 +1433,151 @@ extern "C" int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double
   return SB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free connected components (sb_label_mask_static).
+//
+// For callers that may not allocate device memory themselves or through this
+// library: the union-find needs per-root counters and a root list beyond its
+// input mask and output labels, and here that scratch lives in one file-scope
+// static device array sized for kStaticLabelMaxCells cells (8 MiB + header,
+// reserved on every GPU that loads the library, until process exit).
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int kStaticLabelMaxCells = 1 << 19;  // 524288 cells (701 x 701 fits)
+constexpr size_t kStaticHeaderBytes = 256;     // LabelOut + arrive counter, zeroed per call
+constexpr size_t kStaticCountOffset = kStaticHeaderBytes;
+constexpr size_t kStaticAreaOffset = kStaticCountOffset + (size_t)kStaticLabelMaxCells * 4;
+constexpr size_t kStaticRootOffset = kStaticAreaOffset + (size_t)kStaticLabelMaxCells * 8;
+constexpr size_t kStaticScratchBytes = kStaticRootOffset + (size_t)kStaticLabelMaxCells * 4;
+static_assert(sizeof(LabelOut) + sizeof(unsigned int) <= kStaticHeaderBytes, "header too small");
+
+static __device__ __align__(256) unsigned char g_label_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+unsigned char* g_label_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Per-cell init of the static variant: only the counters it uses are cleared.
+__global__ void __launch_bounds__(kThreads)
+    label_mask_local_static_kernel(const LabelConst c, const int* __restrict__ mask,
+                                   int* __restrict__ parent, int* __restrict__ count,
+                                   long long* __restrict__ area6) {
+  __shared__ int lab[kLabelTile * kLabelTile];
+  const int tx = blockIdx.x % c.tiles_x, ty = blockIdx.x / c.tiles_x;
+  const int gx0 = tx * kLabelTile, gy0 = ty * kLabelTile;
+  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kThreads) {
+    const int ly = li / kLabelTile, lx = li % kLabelTile;
+    const int r = gy0 + ly, col = gx0 + lx;
+    int u = 0;
+    if (r < c.ny && col < c.nx) {
+      const long long flat = (long long)r * c.nx + col;
+      u = mask[flat] != 0;
+      parent[flat] = u ? (int)flat : -1;
+      if (u) {
+        count[flat] = 0;
+        area6[flat] = 0;
+      }
+    }
+    lab[li] = u ? li : -1;
+  }
+  local_ccl(lab, c.connectivity, gy0, gx0, c.nx, parent);
+}
+
+// Region count / total / winner over the root list (count and area only).
+__global__ void __launch_bounds__(kThreads)
+    label_reduce_static_kernel(const int* __restrict__ count, const long long* __restrict__ area6,
+                               const int* __restrict__ root_list, LabelOut* out,
+                               unsigned int* arrive) {
+  const int nroots = out->root_count;
+  unsigned long long best = 0;
+  int total = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nroots; k += gridDim.x * blockDim.x) {
+    const int root = root_list[k];
+    const int cnt = count[root];
+    total += cnt;
+    const unsigned long long key = ((unsigned long long)(unsigned)cnt << 32) |
+                                   (unsigned long long)(0x7fffffffu - (unsigned)root);
+    best = key > best ? key : best;
+  }
+  total = warp_sum(total);
+  best = warp_max(best);
+  if ((threadIdx.x & 31) == 0) {
+    if (total) atomicAdd(&out->total_unstable, total);
+    if (best) atomicMax(&out->best_key, best);
+  }
+  __threadfence();
+  __syncthreads();
+  __shared__ int last;
+  if (threadIdx.x == 0) last = atomicAdd(arrive, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  *arrive = 0;
+  out->regions = nroots;
+  const unsigned long long key = *(volatile unsigned long long*)&out->best_key;
+  if (key == 0) {
+    out->largest = 0;
+    out->winner = -1;
+    return;
+  }
+  const int winner = (int)(0x7fffffffu - (unsigned)(key & 0xffffffffu));
+  out->largest = (int)(key >> 32);
+  out->winner = winner;
+  out->area6 = area6[winner];
+}
+
+}  // namespace
+
+extern "C" int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, int ny, int nx,
+                                    int connectivity, double dx_m, double dy_m, void* stream,
+                                    sb_label_stats* out) {
+  if (!d_mask || !d_labels || !out || ny < 1 || nx < 1) return SB_ERR_BAD_ARG;
+  if (connectivity != 4 && connectivity != 8) return SB_ERR_BAD_ARG;
+  if ((long long)ny * nx > kStaticLabelMaxCells) return SB_ERR_CAPACITY;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SB_ERR_CUDA;
+  if (!g_label_scratch_ptr[dev]) {
+    // one-time set-up on this device (the device is current): the host-side
+    // symbol is only a stand-in, the kernels need its device address
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_label_scratch) != cudaSuccess || !p) return SB_ERR_CUDA;
+    g_label_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+  }
+  unsigned char* base = g_label_scratch_ptr[dev];
+  LabelOut* lout = reinterpret_cast<LabelOut*>(base);
+  unsigned int* arrive = reinterpret_cast<unsigned int*>(base + sizeof(LabelOut));
+  int* count = reinterpret_cast<int*>(base + kStaticCountOffset);
+  long long* area6 = reinterpret_cast<long long*>(base + kStaticAreaOffset);
+  int* root_list = reinterpret_cast<int*>(base + kStaticRootOffset);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  LabelConst c{};
+  c.ny = ny;
+  c.nx = nx;
+  c.pitch = nx;
+  c.tiles_x = (nx + kLabelTile - 1) / kLabelTile;
+  c.connectivity = connectivity;
+  LabelRoots roots{};
+  roots.count = count;
+  roots.area6 = area6;
+  if (cudaMemsetAsync(base, 0, kStaticHeaderBytes, s) != cudaSuccess) return SB_ERR_CUDA;
+  const int tiles = c.tiles_x * ((ny + kLabelTile - 1) / kLabelTile);
+  label_mask_local_static_kernel<<<tiles, kThreads, 0, s>>>(c, d_mask, d_labels, count, area6);
+  label_merge_kernel<<<tiles, kThreads, 0, s>>>(c, d_labels, lout);
+  label_compress_kernel<true><<<grid_for((long long)ny * nx), kThreads, 0, s>>>(
+      c, d_labels, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, roots, root_list, lout, 1);
+  label_reduce_static_kernel<<<148, kThreads, 0, s>>>(count, area6, root_list, lout, arrive);
+  if (cudaGetLastError() != cudaSuccess) return SB_ERR_CUDA;
+  LabelOut host;
+  if (cudaMemcpyAsync(&host, lout, sizeof(LabelOut), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return SB_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return SB_ERR_CUDA;
+  std::memset(out, 0, sizeof(*out));
+  out->status = host.status;
+  out->unstable_cell_count = host.total_unstable;
+  out->connected_region_count = host.regions;
+  out->largest_connected_cell_count = host.largest;
+  out->winner_root = host.winner;
+  out->union_passes = 2;
+  out->largest_connected_area_m2 = (double)host.area6 * (dx_m * dy_m / 6.0);
+  return host.status ? SB_ERR_NONCONVERGENCE : SB_OK;
+}
