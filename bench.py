@@ -149,8 +149,11 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
 
     torch.cuda.set_device(local_rank)
     cfg = workloads.config1(N, seed=1, dx=DX)
+    # one CUDA graph per step; with SOILB200_NO_GRAPH=1 (profilers) the same
+    # kernels are launched operator by operator instead
+    fused = os.environ.get("SOILB200_NO_GRAPH") != "1"
     path = PlainPath(cfg["b_eff"], cfg["z_base"], dx=DX, material=material(),
-                     device=local_rank, residual="gated")
+                     device=local_rank, residual="gated", fused=fused)
     grid = path.grid
     total_steps = args.warmup + args.steps
     sched = cut_schedule(cfg["cut"], total_steps, pinned=True)
@@ -224,6 +227,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                        "precision": "FX32: int32 height quanta + float32 momentum",
                        "l2": "flushed (256 MiB write) between timed steps",
                        "parallelism": f"replicas x{world}",
+                       "launch": "one CUDA graph per step" if fused else "operator by operator",
                        "substeps_total": int(sum(substeps))},
             "e2e": {"value": cell_substeps / wall if wall > 0 else 0.0, "unit": UNIT,
                     "h2d_bytes_per_step": h2d // max(args.steps, 1),

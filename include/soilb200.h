@@ -256,6 +256,49 @@ int sb_entrain_to_surface(sb_ctx* ctx, const int32_t* flat_indices,
 int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double* requested_depth_m,
                int count, double density_kg_m3, double* out3);
 
+/* ---- Fused plain terrain step ----------------------------------------------
+ * One call = one physics step of the production GPU core restricted to this
+ * library's operators (runtime/v2_physics_core.py:708-1003): tool cut
+ * entrainment to target surfaces -> Mobile V2 step (all CFL substeps) ->
+ * large-avalanche labelling, classification and persistence
+ * (gpu_large_avalanche.py:541-676) -> frontier seeding for local
+ * instabilities -> residual MiniSlope frontier rounds, gated as the
+ * reference gates them (quiet mobile layer, no mobilizable yield).  The whole
+ * step is one CUDA graph launch with one host synchronisation. */
+typedef struct sb_path_params {
+  sb_mobile_params mobile;
+  sb_label_params label;
+  sb_relax_params relax;       /* residual frontier: spacing, tan(stop angle), tolerance, rounds */
+  int minimum_connected_cells; /* LargeAvalancheTransitionConfig thresholds */
+  int residual_mode;           /* 0 never, 1 gated like the reference, 2 every step */
+  double minimum_connected_area_m2;
+  double minimum_mobilizable_volume_m3;
+  double minimum_mean_excess_start_deg;
+  double persistence_time_s;
+  double settled_mobile_volume_m3;
+  double settled_speed_m_s;
+} sb_path_params;
+
+typedef struct sb_path_stats {
+  sb_mobile_stats mobile;
+  sb_label_stats label;
+  sb_relax_stats relax;
+  double entrained_m3;
+  double persistence_s;
+  double mean_excess_start_deg;
+  int classification;          /* 0 NO_LARGE_EVENT, 1 LOCAL_STATIC_INSTABILITY,
+                                  2 PERSISTING_LARGE_UNSTABLE_REGION, 3 LARGE_AVALANCHE_MOBILE_PATH */
+  int candidate;
+  int transition_ready;
+  int residual_ran;
+} sb_path_stats;
+
+int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_flat_indices,
+                 const double* cut_target_surface_m, int cut_count, const sb_path_params* params,
+                 sb_path_stats* out);
+/* Clears the persistence state of the fused step (reset of the bridge). */
+int sb_path_reset(sb_ctx* ctx);
+
 /* ---- Allocation-free connected components --------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory once running -- e.g. a simulator plugin whose frame callbacks forbid

@@ -140,6 +140,25 @@ class RelaxStats(C.Structure):
     ]
 
 
+class PathParams(C.Structure):
+    _fields_ = [
+        ("mobile", MobileParams), ("label", LabelParams), ("relax", RelaxParams),
+        ("minimum_connected_cells", C.c_int), ("residual_mode", C.c_int),
+        ("minimum_connected_area_m2", C.c_double), ("minimum_mobilizable_volume_m3", C.c_double),
+        ("minimum_mean_excess_start_deg", C.c_double), ("persistence_time_s", C.c_double),
+        ("settled_mobile_volume_m3", C.c_double), ("settled_speed_m_s", C.c_double),
+    ]
+
+
+class PathStats(C.Structure):
+    _fields_ = [
+        ("mobile", MobileStats), ("label", LabelStats), ("relax", RelaxStats),
+        ("entrained_m3", C.c_double), ("persistence_s", C.c_double),
+        ("mean_excess_start_deg", C.c_double), ("classification", C.c_int),
+        ("candidate", C.c_int), ("transition_ready", C.c_int), ("residual_ran", C.c_int),
+    ]
+
+
 _LIB = None
 _PROTOTYPES = {
     "sb_ctx_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
@@ -171,6 +190,9 @@ _PROTOTYPES = {
     "sb_frontier_active_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "sb_frontier_tile_count": (C.c_int, [C.c_void_p]),
     "sb_field_stats": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_void_p]),
+    "sb_path_step": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int,
+                               C.POINTER(PathParams), C.POINTER(PathStats)]),
+    "sb_path_reset": (C.c_int, [C.c_void_p]),
     "sb_entrain": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                              C.POINTER(C.c_double)]),
     "sb_entrain_to_surface": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
@@ -189,6 +211,8 @@ ABI_STRUCTS = {
     "sb_label_stats": LabelStats,
     "sb_relax_params": RelaxParams,
     "sb_relax_stats": RelaxStats,
+    "sb_path_params": PathParams,
+    "sb_path_stats": PathStats,
 }
 
 

@@ -138,9 +138,12 @@ template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     label_init_local_kernel(const LabelConst c, const typename FvTypes<FX>::B* __restrict__ b,
                             const typename FvTypes<FX>::B* __restrict__ z,
-                            const typename FvTypes<FX>::H* __restrict__ h,
-                            const typename FvTypes<FX>::R* __restrict__ qx,
-                            const typename FvTypes<FX>::R* __restrict__ qy,
+                            const typename FvTypes<FX>::H* __restrict__ h0,
+                            const typename FvTypes<FX>::H* __restrict__ h1,
+                            const typename FvTypes<FX>::R* __restrict__ qx0,
+                            const typename FvTypes<FX>::R* __restrict__ qx1,
+                            const typename FvTypes<FX>::R* __restrict__ qy0,
+                            const typename FvTypes<FX>::R* __restrict__ qy1, const FvControl* ctl,
                             int* __restrict__ parent, typename FvTypes<FX>::R* __restrict__ slope_out,
                             typename FvTypes<FX>::R* __restrict__ severity_out,
                             int* __restrict__ latch, const double* __restrict__ export_cum,
@@ -148,6 +151,10 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ int lab[kLabelTile * kLabelTile];
   const int tx = blockIdx.x % c.tiles_x, ty = blockIdx.x / c.tiles_x;
   const int gx0 = tx * kLabelTile, gy0 = ty * kLabelTile;
+  const int P = ctl->parity;  // buffer holding the current mobile state
+  const typename FvTypes<FX>::H* h = P ? h1 : h0;
+  const typename FvTypes<FX>::R* qx = P ? qx1 : qx0;
+  const typename FvTypes<FX>::R* qy = P ? qy1 : qy0;
   for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kThreads) {
     const int ly = li / kLabelTile, lx = li % kLabelTile;
     const int r = gy0 + ly, col = gx0 + lx;

@@ -1,0 +1,175 @@
+// Kernels that glue the plain terrain step into one CUDA graph.
+//
+// The reference takes every decision of the step on the host between blocking
+// synchronisations (runtime/v2_physics_core.py:708-1003,
+// runtime/gpu_large_avalanche.py:620-676).  Here the same decisions run in a
+// single-thread device kernel between the graph's kernels: the large-avalanche
+// classification and persistence, the frontier seeding flags and the
+// residual-MiniSlope gate.
+#pragma once
+
+#include "sb_exchange.cuh"
+#include "sb_labels.cuh"
+#include "sb_ledger.cuh"
+#include "sb_relax.cuh"
+
+namespace sb {
+
+struct PathConst {
+  double dt;                  // unused in kernels (dt comes from the device copy)
+  double f;                   // weight unit dx*dy/6
+  double Q;
+  double dx, dy;
+  int min_cells;
+  double min_area, min_volume, min_mean_excess_deg, persistence_time;
+  double settled_volume, settled_speed, dry_tol;
+  int residual_mode;          // 0 off, 1 gated as the reference, 2 always
+  int fx;
+};
+
+// Device-resident state of the step pipeline (persistence across steps).
+struct PathState {
+  double persistence_s;
+  double entrained_m3;
+  double mean_excess_start_deg;
+  double area_m2;
+  double volume_m3;
+  int has_previous;
+  int candidate;
+  int ready;
+  int classification;         // 0 NO_LARGE_EVENT, 1 LOCAL_STATIC, 2 PERSISTING, 3 MOBILE_PATH
+  int keep_candidate;
+  int seed_frontier;
+  int residual_enable;
+  int pad;
+};
+
+// Bucket-cut entrainment to target surfaces; the command length is read on
+// the device so the graph is independent of it (mode 1 of entrain_kernel).
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    path_entrain_kernel(int ny, int nx, int pitch, double Q, double datum, double f,
+                        typename FvTypes<FX>::B* __restrict__ b,
+                        const typename FvTypes<FX>::B* __restrict__ z,
+                        typename FvTypes<FX>::H* __restrict__ h0,
+                        typename FvTypes<FX>::H* __restrict__ h1,
+                        const FvControl* ctl, const int32_t* __restrict__ idx,
+                        const double* __restrict__ target, const int* count_dev,
+                        ExchangeOut* out) {
+  const int count = *count_dev;
+  typename FvTypes<FX>::H* h = ctl->parity ? h1 : h0;
+  long long vq = 0;
+  double vs = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const int i = idx[k];
+    if (i < 0 || i >= ny * nx) {
+      atomicExch(&out->bad_index, 1);
+      continue;
+    }
+    const int r = i / nx, c = i % nx;
+    const size_t gi = (size_t)r * pitch + c;
+    const int w6 = vertex_weight6(r, c, ny, nx);
+    if constexpr (FX) {
+      const long long avail = (long long)b[gi] - (long long)z[gi];
+      const long long req = (long long)b[gi] - (long long)rint((target[k] - datum) / Q);
+      long long d = req < avail ? req : avail;
+      if (d < 0) d = 0;
+      b[gi] = (int32_t)(b[gi] - d);
+      h[gi] = (int32_t)(h[gi] + d);
+      vq += d * w6;
+    } else {
+      const double avail = fmax(b[gi] - z[gi], 0.0);
+      const double d = fmin(fmax(b[gi] - target[k], 0.0), avail);
+      b[gi] = b[gi] - d;
+      h[gi] = h[gi] + d;
+      vs += d * ((double)w6 * f);
+    }
+  }
+  vq = (long long)warp_sum_u64((unsigned long long)vq);
+  vs = warp_sum(vs);
+  if ((threadIdx.x & 31) == 0) {
+    if (vq) atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
+    if (vs != 0.0) atomicAdd(&out->volume_w_fp64, vs);
+  }
+}
+
+// Classification, persistence and gating (reference gpu_large_avalanche.py
+// :620-676 and the residual gate of v2_physics_core.py:930-1003).
+__global__ void path_classify_kernel(const PathConst c, const LabelOut* lo, const StepIO* io,
+                                     const ExchangeOut* xo, PathState* ps, const double* dt_dev) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double dt = *dt_dev;
+  const int largest = lo->winner >= 0 ? lo->largest : 0;
+  const double area = (double)lo->area6 * c.f;
+  const double volume = c.fx ? (double)lo->volume * c.Q * c.f : (double)lo->volume / kVolumeScaleFp64 * c.f;
+  const double mean_start =
+      largest ? ((double)lo->exc_start / kExcessScale / (double)largest) * (180.0 / 3.141592653589793)
+              : 0.0;
+  const bool extent = largest >= c.min_cells && area >= c.min_area;
+  const bool vol_pass = volume >= c.min_volume;
+  const bool exc_pass = mean_start >= c.min_mean_excess_deg;
+  const bool candidate = extent && vol_pass && exc_pass;
+  const bool overlap = lo->prev_overlap > 0;
+  if (candidate)
+    ps->persistence_s = (overlap || !ps->has_previous) ? ps->persistence_s + dt : dt;
+  else
+    ps->persistence_s = 0.0;
+  const bool ready = candidate && ps->persistence_s >= c.persistence_time;
+  int cls = 0;
+  if (ready) cls = 3;
+  else if (candidate) cls = 2;
+  else if (lo->total_unstable > 0) cls = 1;
+  ps->candidate = candidate;
+  ps->ready = ready;
+  ps->classification = cls;
+  ps->keep_candidate = candidate;
+  ps->seed_frontier = cls == 1;
+  ps->has_previous = candidate;
+  ps->mean_excess_start_deg = mean_start;
+  ps->area_m2 = area;
+  ps->volume_m3 = volume;
+  ps->entrained_m3 = c.fx ? (double)xo->volume_w6_quanta * c.Q * c.f : xo->volume_w_fp64;
+  const LedgerOut& a = io->after;
+  const double mobile_volume = c.fx ? (double)a.iq[1] * c.Q * c.f : a.v[L_HSUM_W] * c.f;
+  const bool quiet = mobile_volume <= c.settled_volume && a.v[L_MAXSPEED] <= c.settled_speed;
+  const bool yield_present = lo->total_unstable > 0 && volume > c.dry_tol * c.dx * c.dy;
+  ps->residual_enable = c.residual_mode == 2 || (c.residual_mode == 1 && quiet && !yield_present);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    path_update_previous_kernel(const LabelConst c, const int* __restrict__ parent,
+                                int* __restrict__ previous, int* __restrict__ reached,
+                                int* __restrict__ tile_flags, const LabelOut* out,
+                                const PathState* ps) {
+  const int n = c.ny * c.nx;
+  const int winner = out->winner;
+  const int keep = ps->keep_candidate, seed = ps->seed_frontier;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const bool belongs = winner >= 0 && parent[i] == winner;
+    previous[i] = (belongs && keep) ? 1 : 0;
+    if (belongs && seed) {
+      const int r = i / c.nx, col = i % c.nx;
+      reached[(size_t)r * c.pitch + col] = 1;
+      tile_flags[(r / c.tile_size) * c.frontier_tiles_x + col / c.tile_size] = 1;
+    }
+  }
+}
+
+// Frontier reset for the step graph: a disabled residual leaves the pending
+// tile flags untouched for a later step (the reference keeps them queued).
+__global__ void path_frontier_reset_kernel(RelaxControl* ctl, const PathState* ps) {
+  if (threadIdx.x == 0) {
+    ctl->iterations = 0;
+    ctl->done = ps->residual_enable ? 0 : 1;
+    ctl->converged = 0;
+    ctl->status = 0;
+    ctl->max_excess_bits = 0;
+    ctl->arrive = 0;
+    ctl->parity = 0;
+    ctl->n_active = 0;
+    ctl->rounds = 0;
+    ctl->moved_edges = 0;
+  }
+}
+
+}  // namespace sb

@@ -208,6 +208,10 @@ __global__ void frontier_begin_kernel(const RelaxConst c, int* __restrict__ unst
                                       int* __restrict__ phase0, int* __restrict__ phase1,
                                       RelaxControl* ctl, cudaGraphConditionalHandle handle) {
   __shared__ int cnt[kThreads / 32];
+  if (*(volatile int*)&ctl->done) {  // loop disabled before it started: keep the flags
+    if (threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
+    return;
+  }
   int n = 0;
   for (int t = threadIdx.x; t < c.ntiles; t += blockDim.x) {
     const int a = unstable[t];

@@ -14,6 +14,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -28,6 +29,7 @@
 #include "sb_labels.cuh"
 #include "sb_relax.cuh"
 #include "sb_exchange.cuh"
+#include "sb_path.cuh"
 
 using namespace sb;
 
@@ -132,6 +134,15 @@ struct sb_ctx {
   RelaxControl* rctl_host = nullptr;
   LoopGraph relax_full;
   LoopGraph frontier;
+  // fused plain-path step
+  PathState* pstate = nullptr;
+  PathState* pstate_host = nullptr;
+  int* path_count = nullptr;
+  int* path_count_host = nullptr;
+  cudaGraphExec_t path_exec = nullptr;
+  cudaGraph_t path_graph = nullptr;
+  unsigned char path_key[512] = {0};
+  bool path_valid = false;
   // exchange command buffers
   int32_t* xidx = nullptr;
   double* xval = nullptr;
@@ -416,6 +427,31 @@ static int mobile_step_host_loop(sb_ctx* ctx, const FvConst& c, double static_li
   return SB_OK;
 }
 
+int fill_mobile_stats(sb_ctx* ctx, const sb_mobile_params* params, sb_mobile_stats* out) {
+  const FvControl& k = *ctx->ctl_host;
+  ctx->parity_host = k.parity;
+  float loop_ms = 0.f;
+  SB_CUDA(ctx, cudaEventElapsedTime(&loop_ms, ctx->ev_loop[0], ctx->ev_loop[1]));
+  std::memset(out, 0, sizeof(*out));
+  out->substep_loop_ms = loop_ms;
+  out->substeps = k.substeps;
+  out->static_skip = k.static_skip;
+  out->cfl_limited = k.cfl_limited;
+  out->status = k.status;
+  out->maximum_cfl = k.max_cfl;
+  const double area = ctx->d.dx_m * ctx->d.dy_m;
+  for (int i = 0; i < 2; ++i) {
+    out->conservative_impulse_m4_s[i] = k.diag[i] * area;
+    out->external_impulse_m4_s[i] = k.diag[2 + i] * area;
+    out->friction_impulse_m4_s[i] = k.diag[4 + i] * area;
+  }
+  out->friction_dissipation = k.diag[6] * area;
+  out->external_work = k.diag[7] * area;
+  fill_ledger(ctx, ctx->io_host->before, params, &out->before);
+  fill_ledger(ctx, ctx->io_host->after, params, &out->after);
+  return SB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -434,6 +470,8 @@ size_t sb_sizeof(const char* type_name) {
       {"sb_label_stats", sizeof(sb_label_stats)},
       {"sb_relax_params", sizeof(sb_relax_params)},
       {"sb_relax_stats", sizeof(sb_relax_stats)},
+      {"sb_path_params", sizeof(sb_path_params)},
+      {"sb_path_stats", sizeof(sb_path_stats)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.name, type_name) == 0) return e.size;
@@ -549,6 +587,11 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMalloc(&ctx->xval, n * 8));
   SB_CUDA(ctx, cudaMalloc(&ctx->xout, sizeof(ExchangeOut)));
   SB_CUDA(ctx, cudaMallocHost(&ctx->xout_host, sizeof(ExchangeOut)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->pstate, sizeof(PathState)));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->pstate, 0, sizeof(PathState), ctx->stream));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->pstate_host, sizeof(PathState)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->path_count, sizeof(int)));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->path_count_host, sizeof(int)));
   // TMA descriptors (box = halo tile of the FV kernel)
   int rc;
   {
@@ -616,7 +659,8 @@ int sb_ctx_destroy(sb_ctx* ctx) {
                   ctx->roots.area6, ctx->roots.volume, ctx->roots.exc_start, ctx->roots.exc_stop,
                   ctx->roots.max_exc_start, ctx->roots.max_exc_stop, ctx->roots.prev_overlap,
                   ctx->root_list, ctx->lout, ctx->b_alt, ctx->ftile_next, ctx->phase[0],
-                  ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout};
+                  ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout, ctx->pstate,
+                  ctx->path_count};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
@@ -624,6 +668,10 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   for (cudaEvent_t e : ctx->ev_loop)
     if (e) cudaEventDestroy(e);
   if (ctx->xout_host) cudaFreeHost(ctx->xout_host);
+  if (ctx->pstate_host) cudaFreeHost(ctx->pstate_host);
+  if (ctx->path_count_host) cudaFreeHost(ctx->path_count_host);
+  if (ctx->path_exec) cudaGraphExecDestroy(ctx->path_exec);
+  if (ctx->path_graph) cudaGraphDestroy(ctx->path_graph);
   if (ctx->dt_host) cudaFreeHost(ctx->dt_host);
   if (ctx->ctl_host) cudaFreeHost(ctx->ctl_host);
   if (ctx->io_host) cudaFreeHost(ctx->io_host);
@@ -799,27 +847,9 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
                                ctx->stream));
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const FvControl& k = *ctx->ctl_host;
-  ctx->parity_host = k.parity;
   ctx->launches += 3 + k.substeps;
-  float loop_ms = 0.f;
-  SB_CUDA(ctx, cudaEventElapsedTime(&loop_ms, ctx->ev_loop[0], ctx->ev_loop[1]));
-  std::memset(out, 0, sizeof(*out));
-  out->substep_loop_ms = loop_ms;
-  out->substeps = k.substeps;
-  out->static_skip = k.static_skip;
-  out->cfl_limited = k.cfl_limited;
-  out->status = k.status;
-  out->maximum_cfl = k.max_cfl;
-  const double area = ctx->d.dx_m * ctx->d.dy_m;
-  for (int i = 0; i < 2; ++i) {
-    out->conservative_impulse_m4_s[i] = k.diag[i] * area;
-    out->external_impulse_m4_s[i] = k.diag[2 + i] * area;
-    out->friction_impulse_m4_s[i] = k.diag[4 + i] * area;
-  }
-  out->friction_dissipation = k.diag[6] * area;
-  out->external_work = k.diag[7] * area;
-  fill_ledger(ctx, ctx->io_host->before, params, &out->before);
-  fill_ledger(ctx, ctx->io_host->after, params, &out->after);
+  rc = fill_mobile_stats(ctx, params, out);
+  if (rc) return rc;
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
   if (k.status == SB_ERR_SUBSTEP_CAP)
     return fail(ctx, SB_ERR_SUBSTEP_CAP, "MobileV2 maximum_substeps exceeded");
@@ -889,11 +919,12 @@ template <bool FX>
 static int run_label(sb_ctx* ctx, const LabelConst& c) {
   using T = FvTypes<FX>;
   const int tiles = c.tiles_x * ((c.ny + kLabelTile - 1) / kLabelTile);
-  const int P = ctx->parity_host;
   SB_CUDA(ctx, cudaMemsetAsync(ctx->lout, 0, sizeof(LabelOut), ctx->stream));
   label_init_local_kernel<FX><<<tiles, kThreads, 0, ctx->stream>>>(
-      c, (const typename T::B*)ctx->b, (const typename T::B*)ctx->z, (const typename T::H*)ctx->h[P],
-      (const typename T::R*)ctx->qx[P], (const typename T::R*)ctx->qy[P], ctx->parent,
+      c, (const typename T::B*)ctx->b, (const typename T::B*)ctx->z,
+      (const typename T::H*)ctx->h[0], (const typename T::H*)ctx->h[1],
+      (const typename T::R*)ctx->qx[0], (const typename T::R*)ctx->qx[1],
+      (const typename T::R*)ctx->qy[0], (const typename T::R*)ctx->qy[1], ctx->ctl, ctx->parent,
       (typename T::R*)ctx->slope, (typename T::R*)ctx->severity, ctx->latch, ctx->export_cum,
       ctx->export_base, ctx->roots);
   label_merge_kernel<<<tiles, kThreads, 0, ctx->stream>>>(c, ctx->parent, ctx->lout);
@@ -1430,6 +1461,336 @@ extern "C" int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double
   out3[0] = fx(ctx) ? (double)o.volume_w6_quanta * ctx->quantum * f : o.volume_w_fp64;
   out3[1] = density_kg_m3 * o.momentum_w[0];
   out3[2] = density_kg_m3 * o.momentum_w[1];
+  return SB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Fused plain terrain step (one graph per step)
+// ---------------------------------------------------------------------------
+namespace {
+
+int add_memset(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps,
+               size_t ndeps, void* dst, size_t bytes) {
+  cudaMemsetParams mp{};
+  mp.dst = dst;
+  mp.value = 0;
+  mp.elementSize = 4;
+  mp.width = bytes / 4;
+  mp.height = 1;
+  mp.pitch = 0;
+  SB_CUDA(ctx, cudaGraphAddMemsetNode(node, g, deps, ndeps, &mp));
+  return SB_OK;
+}
+
+template <bool FX>
+int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
+  using T = FvTypes<FX>;
+  if (ctx->path_exec) cudaGraphExecDestroy(ctx->path_exec);
+  if (ctx->path_graph) cudaGraphDestroy(ctx->path_graph);
+  ctx->path_exec = nullptr;
+  ctx->path_graph = nullptr;
+  ctx->path_valid = false;
+  cudaGraph_t g;
+  SB_CUDA(ctx, cudaGraphCreate(&g, 0));
+  ctx->path_graph = g;
+  cudaGraphConditionalHandle h_mob, h_front;
+  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_mob, g, 0, cudaGraphCondAssignDefault));
+  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_front, g, 0, cudaGraphCondAssignDefault));
+  int rc, one = 1, zero = 0;
+  const int ny = ctx->d.ny, nx = ctx->d.nx;
+  double Q = ctx->quantum, datum = ctx->d.datum_m, f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  cudaGraphNode_t prev, node;
+  // 1. cut entrainment
+  if ((rc = add_memset(ctx, g, &prev, nullptr, 0, ctx->xout, sizeof(ExchangeOut)))) return rc;
+  {
+    int pitch = ctx->pitch;
+    int nyv = ny, nxv = nx;
+    void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
+                    &ctx->ctl, &ctx->xidx, &ctx->xval, &ctx->path_count, &ctx->xout};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_entrain_kernel<FX>, dim3(64), 0, args)))
+      return rc;
+    prev = node;
+  }
+  // 2. Mobile V2 (same kernels as the standalone step graph)
+  static FvConst fc;
+  fc = make_const(ctx, &p->mobile);
+  static double static_limit, dat;
+  static_limit = std::tan(p->mobile.start_angle_deg * (M_PI / 180.0)) + 1.0e-14;
+  dat = ctx->d.datum_m;
+  static int mode0 = 0, mode1 = 1, use_h = 1, no_h = 0;
+  {
+    void* args[] = {(void*)&ctx->ctl, (void*)&ctx->dt_dev};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)fv_begin_kernel, dim3(1), 0, args))) return rc;
+    prev = node;
+  }
+  {
+    std::vector<void*> args;
+    ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode0, &h_mob, &use_h, args);
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks),
+                         0, args.data())))
+      return rc;
+    prev = node;
+  }
+  SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[0]));
+  prev = node;
+  {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_mob;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    SB_CUDA(ctx, cudaGraphAddNode(&node, g, &prev, 1, &cp));
+    prev = node;
+    std::vector<void*> args;
+    fv_args<FX>(ctx, fc, &h_mob, &use_h, args);
+    cudaGraphNode_t body_node;
+    if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node, nullptr, 0,
+                         (void*)fv_substep_kernel<FX>, dim3(fc.nblocks), fv_smem_bytes<FX>(),
+                         args.data())))
+      return rc;
+  }
+  SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[1]));
+  prev = node;
+  {
+    std::vector<void*> args;
+    ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode1, &h_mob, &no_h, args);
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks),
+                         0, args.data())))
+      return rc;
+    prev = node;
+  }
+  // 3. labelling
+  static LabelConst lc;
+  lc = make_label_const(ctx, &p->label);
+  const int ltiles = lc.tiles_x * ((ny + kLabelTile - 1) / kLabelTile);
+  if ((rc = add_memset(ctx, g, &node, &prev, 1, ctx->lout, sizeof(LabelOut)))) return rc;
+  prev = node;
+  {
+    void* args[] = {&lc, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1], &ctx->qx[0], &ctx->qx[1],
+                    &ctx->qy[0], &ctx->qy[1], &ctx->ctl, &ctx->parent, &ctx->slope, &ctx->severity,
+                    &ctx->latch, &ctx->export_cum, &ctx->export_base, &ctx->roots};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_init_local_kernel<FX>, dim3(ltiles),
+                         0, args)))
+      return rc;
+    prev = node;
+  }
+  {
+    void* args[] = {&lc, &ctx->parent, &ctx->lout};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_merge_kernel, dim3(ltiles), 0, args)))
+      return rc;
+    prev = node;
+  }
+  {
+    static int mask_only = 0;
+    void* args[] = {&lc, &ctx->parent, &ctx->b, &ctx->z, &ctx->slope, &ctx->severity, &ctx->latch,
+                    &ctx->previous, &ctx->roots, &ctx->root_list, &ctx->lout, &mask_only};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_compress_kernel<FX>,
+                         dim3(grid_for((long long)ny * nx)), 0, args)))
+      return rc;
+    prev = node;
+  }
+  {
+    void* args[] = {&ctx->roots, &ctx->root_list, &ctx->lout, &ctx->arrive};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_reduce_kernel, dim3(148), 0, args)))
+      return rc;
+    prev = node;
+  }
+  // 4. classification / persistence / gate, then previous mask + seeding
+  static PathConst pc;
+  pc = PathConst{};
+  pc.f = f;
+  pc.Q = ctx->quantum;
+  pc.dx = ctx->d.dx_m;
+  pc.dy = ctx->d.dy_m;
+  pc.min_cells = p->minimum_connected_cells;
+  pc.min_area = p->minimum_connected_area_m2;
+  pc.min_volume = p->minimum_mobilizable_volume_m3;
+  pc.min_mean_excess_deg = p->minimum_mean_excess_start_deg;
+  pc.persistence_time = p->persistence_time_s;
+  pc.settled_volume = p->settled_mobile_volume_m3;
+  pc.settled_speed = p->settled_speed_m_s;
+  pc.dry_tol = p->label.dry_tolerance_m;
+  pc.residual_mode = p->residual_mode;
+  pc.fx = FX ? 1 : 0;
+  {
+    void* args[] = {&pc, &ctx->lout, &ctx->io, &ctx->xout, &ctx->pstate, &ctx->dt_dev};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_classify_kernel, dim3(1), 0, args)))
+      return rc;
+    prev = node;
+  }
+  {
+    void* args[] = {&lc, &ctx->parent, &ctx->previous, &ctx->reached, &ctx->ftile_next, &ctx->lout,
+                    &ctx->pstate};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_update_previous_kernel,
+                         dim3(grid_for((long long)ny * nx)), 0, args)))
+      return rc;
+    prev = node;
+  }
+  // 5. gated residual frontier (same kernels as sb_frontier_run)
+  static RelaxConst rcn;
+  if ((rc = relax_const(ctx, &p->relax, &rcn, ctx->d.tile_size))) return rc;
+  {
+    void* args[] = {&ctx->rctl, &ctx->pstate};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_frontier_reset_kernel, dim3(1), 0,
+                         args)))
+      return rc;
+    prev = node;
+  }
+  void* begin_args[] = {&rcn, &ctx->ftile_next, &ctx->phase[0], &ctx->phase[1], &ctx->rctl,
+                        &h_front};
+  if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)frontier_begin_kernel, dim3(1), 0,
+                       begin_args)))
+    return rc;
+  prev = node;
+  {
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h_front;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    SB_CUDA(ctx, cudaGraphAddNode(&node, g, &prev, 1, &cp));
+    prev = node;
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    static int dirs[8], pars[8];
+    static typename T::H* hf;
+    hf = (typename T::H*)ctx->b;
+    cudaGraphNode_t bprev = nullptr, bnode;
+    for (int k = 0; k < 8; ++k) {
+      dirs[k] = k / 2;
+      pars[k] = k % 2;
+      void* args[] = {&rcn, &dirs[k], &pars[k], &hf, &ctx->reached, &ctx->phase[k & 1],
+                      &ctx->phase[(k + 1) & 1], &ctx->rctl};
+      if ((rc = add_kernel(ctx, body, &bnode, bprev ? &bprev : nullptr, bprev ? 1 : 0,
+                           (void*)frontier_subphase_kernel<FX>, dim3(rcn.ntiles), 0, args)))
+        return rc;
+      bprev = bnode;
+    }
+    void* sargs[] = {&rcn, &hf, &ctx->reached, &ctx->phase[0], &ctx->ftile_next, &ctx->rctl};
+    if ((rc = add_kernel(ctx, body, &bnode, &bprev, 1, (void*)frontier_scan_kernel<FX>,
+                         dim3(rcn.ntiles), 0, sargs)))
+      return rc;
+    bprev = bnode;
+    if ((rc = add_kernel(ctx, body, &bnode, &bprev, 1, (void*)frontier_begin_kernel, dim3(1), 0,
+                         begin_args)))
+      return rc;
+  }
+  {
+    void* args[] = {&rcn, &ctx->reached, &ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)frontier_finish_kernel,
+                         dim3(grid_for((long long)rcn.n0 * rcn.pitch)), 0, args)))
+      return rc;
+    prev = node;
+  }
+  // 6. records back to pinned host memory
+  struct Copy { void* dst; const void* src; size_t n; };
+  const Copy copies[] = {{ctx->ctl_host, ctx->ctl, sizeof(FvControl)},
+                         {ctx->io_host, ctx->io, sizeof(StepIO)},
+                         {ctx->lout_host, ctx->lout, sizeof(LabelOut)},
+                         {ctx->rctl_host, ctx->rctl, sizeof(RelaxControl)},
+                         {ctx->pstate_host, ctx->pstate, sizeof(PathState)},
+                         {ctx->xout_host, ctx->xout, sizeof(ExchangeOut)}};
+  for (const Copy& cpy : copies) {
+    SB_CUDA(ctx, cudaGraphAddMemcpyNode1D(&node, g, &prev, 1, cpy.dst, cpy.src, cpy.n,
+                                          cudaMemcpyDeviceToHost));
+    prev = node;
+  }
+  (void)one;
+  (void)zero;
+  SB_CUDA(ctx, cudaGraphInstantiate(&ctx->path_exec, g, 0));
+  ctx->path_valid = true;
+  return SB_OK;
+}
+
+}  // namespace
+
+extern "C" int sb_path_reset(sb_ctx* ctx) {
+  if (!ctx) return SB_ERR_BAD_ARG;
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->pstate, 0, sizeof(PathState), ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
+                            const double* cut_target, int cut_count, const sb_path_params* p,
+                            sb_path_stats* out) {
+  if (!ctx || !p || !out) return SB_ERR_BAD_ARG;
+  if (!std::isfinite(dt_s) || dt_s <= 0.0) return fail(ctx, SB_ERR_BAD_ARG, "dt must be finite/positive");
+  if (cut_count < 0 || (cut_count > 0 && (!cut_idx || !cut_target)) ||
+      (long long)cut_count > (long long)ctx->d.ny * ctx->d.nx)
+    return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] invalid entrainment request");
+  if (p->label.connectivity != 4 && p->label.connectivity != 8)
+    return fail(ctx, SB_ERR_BAD_ARG, "[LargeAvalanche] connectivity must be 4 or 8");
+  int rc = check_params(ctx, &p->mobile);
+  if (rc) return rc;
+  if (!ctx->use_graphs)
+    return fail(ctx, SB_ERR_STATE, "[soilb200] the fused step needs CUDA graphs (unset SOILB200_NO_GRAPH)");
+  if (!ctx->path_valid || std::memcmp(ctx->path_key, p, sizeof(*p)) != 0) {
+    static_assert(sizeof(sb_path_params) <= sizeof(((sb_ctx*)nullptr)->path_key), "key size");
+    rc = fx(ctx) ? build_path_graph<true>(ctx, p) : build_path_graph<false>(ctx, p);
+    if (rc) return rc;
+    std::memcpy(ctx->path_key, p, sizeof(*p));
+    // the standalone Mobile graph shares the control block; force its rebuild check
+    ctx->mobile.valid = false;
+  }
+  *ctx->dt_host = dt_s;
+  *ctx->path_count_host = cut_count;
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->dt_dev, ctx->dt_host, sizeof(double), cudaMemcpyHostToDevice,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->path_count, ctx->path_count_host, sizeof(int),
+                               cudaMemcpyHostToDevice, ctx->stream));
+  if (cut_count > 0) {
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->xidx, cut_idx, (size_t)cut_count * 4, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->xval, cut_target, (size_t)cut_count * 8,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+  }
+  SB_CUDA(ctx, cudaGraphLaunch(ctx->path_exec, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  std::memset(out, 0, sizeof(*out));
+  if ((rc = fill_mobile_stats(ctx, &p->mobile, &out->mobile))) return rc;
+  const LabelOut& o = *ctx->lout_host;
+  out->label.status = o.status;
+  out->label.unstable_cell_count = o.total_unstable;
+  out->label.connected_region_count = o.regions;
+  out->label.largest_connected_cell_count = o.largest;
+  out->label.winner_root = o.winner;
+  out->label.union_passes = 2;
+  out->label.previous_overlap = o.prev_overlap;
+  const double f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  out->label.largest_connected_area_m2 = (double)o.area6 * f;
+  out->label.largest_connected_mobilizable_volume_m3 =
+      fx(ctx) ? (double)o.volume * ctx->quantum * f : (double)o.volume / kVolumeScaleFp64 * f;
+  out->label.excess_start_sum_rad = (double)o.exc_start / kExcessScale;
+  out->label.excess_start_max_rad = (double)o.max_exc_start / kExcessScale;
+  out->label.excess_stop_sum_rad = (double)o.exc_stop / kExcessScale;
+  out->label.excess_stop_max_rad = (double)o.max_exc_stop / kExcessScale;
+  const RelaxControl& r = *ctx->rctl_host;
+  out->relax.iterations = r.rounds;
+  out->relax.converged = r.converged;
+  out->relax.status = r.status;
+  out->relax.active_tiles = r.n_active;
+  out->relax.moved_edges = r.moved_edges;
+  const PathState& ps = *ctx->pstate_host;
+  out->entrained_m3 = ps.entrained_m3;
+  out->persistence_s = ps.persistence_s;
+  out->mean_excess_start_deg = ps.mean_excess_start_deg;
+  out->classification = ps.classification;
+  out->candidate = ps.candidate;
+  out->transition_ready = ps.ready;
+  out->residual_ran = ps.residual_enable;
+  const FvControl& k = *ctx->ctl_host;
+  ctx->launches += 12 + k.substeps + 10LL * r.rounds;
+  if (ctx->xout_host->bad_index)
+    return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] entrainment index outside state");
+  if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
+  if (k.status == SB_ERR_SUBSTEP_CAP)
+    return fail(ctx, SB_ERR_SUBSTEP_CAP, "MobileV2 maximum_substeps exceeded");
+  if (k.status) return fail(ctx, k.status, "[soilb200] device status %d", k.status);
+  if (o.status)
+    return fail(ctx, SB_ERR_NONCONVERGENCE, "NUMERICAL_NONCONVERGENCE: device avalanche connected components");
+  if (r.status == SB_ERR_NONCONVERGENCE)
+    return fail(ctx, SB_ERR_NONCONVERGENCE,
+                "NUMERICAL_NONCONVERGENCE: GPU residual MiniSlope exceeded the numerical safety limit");
   return SB_OK;
 }
 

@@ -15,10 +15,16 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import _lib
+
 from .avalanche import B200LargeAvalancheBridge, LargeAvalancheTransitionConfig, MaterialScenario
 from .bulk_state import B200BulkState, B200ProductionMobileV2Solver
-from .mobile_v2 import MobileV2Config
+from .mobile_v2 import MobileV2Config, mobile_params
 from .relax import FrontierRelaxation
+
+CLASSIFICATIONS = ("NO_LARGE_EVENT", "LOCAL_STATIC_INSTABILITY",
+                   "PERSISTING_LARGE_UNSTABLE_REGION", "LARGE_AVALANCHE_MOBILE_PATH")
+RESIDUAL_MODES = {"never": 0, "gated": 1, "always": 2}
 
 
 @dataclass
@@ -35,11 +41,17 @@ class PathStepStats:
 
 
 class PlainPath:
+    """The plain step on one device.  ``fused=True`` (default) runs the whole
+    step as one CUDA graph (``sb_path_step``, one host synchronisation);
+    ``fused=False`` calls the operators one by one (same kernels, same results)."""
+
     def __init__(self, b_eff: np.ndarray, z_base: np.ndarray, *, dx: float,
                  material: MaterialScenario, mobile_config: MobileV2Config | None = None,
                  avalanche_config: LargeAvalancheTransitionConfig | None = None,
                  tile_size: int = 64, precision: str = "fx32", device: int = 0,
-                 residual: str = "gated", mobile_headroom_m: float = 1.0) -> None:
+                 residual: str = "gated", mobile_headroom_m: float = 1.0,
+                 fused: bool = True, tolerance_m: float = 1e-8,
+                 max_rounds: int = 4096) -> None:
         self.state = B200BulkState(b_eff.shape, dx, dx, b_eff, z_base_m=z_base, device=device,
                                    tile_size=tile_size, precision=precision,
                                    mobile_headroom_m=mobile_headroom_m)
@@ -51,14 +63,63 @@ class PlainPath:
         self.mobile.bind_device_state(self.state, material)
         self.avalanche = B200LargeAvalancheBridge(self.state.grid, material, avalanche_config)
         self.frontier = FrontierRelaxation(self.state.grid, weighted=True)
+        if residual not in RESIDUAL_MODES:
+            raise ValueError(f"[soilb200] residual must be one of {sorted(RESIDUAL_MODES)}")
         self.residual = residual
         self.critical_slope = float(np.tan(np.deg2rad(material.stop_angle_deg)))
+        self.fused = bool(fused)
+        self.tolerance_m = float(tolerance_m)
+        self.max_rounds = int(max_rounds)
+        self.last_stats: _lib.PathStats | None = None
+        self._params = self._path_params()
+
+    def _path_params(self) -> _lib.PathParams:
+        cfg = self.avalanche.config
+        relax = _lib.RelaxParams(float(self.frontier.spacing[0]), float(self.frontier.spacing[1]),
+                                 self.critical_slope, self.tolerance_m, self.max_rounds, 1)
+        return _lib.PathParams(
+            mobile_params(self.mobile.config,
+                          density_kg_m3=float(self.material.assumed_bulk_density_kg_m3)),
+            self.avalanche._params(True), relax, int(cfg.minimum_connected_cells),
+            RESIDUAL_MODES[self.residual], float(cfg.minimum_connected_area_m2),
+            float(cfg.minimum_mobilizable_volume_m3), float(cfg.minimum_mean_excess_start_deg),
+            float(cfg.persistence_time_s), float(cfg.settled_mobile_volume_m3),
+            float(cfg.settled_speed_m_s))
 
     @property
     def grid(self):
         return self.state.grid
 
     def step(self, dt_s: float, cut_cells=None, cut_targets=None) -> PathStepStats:
+        if self.fused:
+            return self._step_fused(dt_s, cut_cells, cut_targets)
+        return self._step_operators(dt_s, cut_cells, cut_targets)
+
+    def _step_fused(self, dt_s, cut_cells, cut_targets) -> PathStepStats:
+        n = 0 if cut_cells is None else int(len(cut_cells))
+        idx = tgt = None
+        if n:
+            idx = np.ascontiguousarray(cut_cells, dtype=np.int32)
+            tgt = np.ascontiguousarray(cut_targets, dtype=np.float64)
+            if tgt.shape != idx.shape or not np.all(np.isfinite(tgt)):
+                raise ValueError("[DeviceBulkState] invalid entrainment request")
+        st = _lib.PathStats()
+        g = self.grid
+        _lib.check(g.ctx, _lib.load().sb_path_step(
+            g.ctx, float(dt_s), idx.ctypes.data if n else None, tgt.ctypes.data if n else None,
+            n, self._params, st), "sb_path_step")
+        self.last_stats = st
+        self.mobile.last_stats = st.mobile
+        self.state.advance_time(dt_s)
+        return PathStepStats(int(st.mobile.substeps), float(st.entrained_m3),
+                             CLASSIFICATIONS[st.classification], int(st.label.unstable_cell_count),
+                             int(st.label.connected_region_count),
+                             int(st.label.largest_connected_cell_count),
+                             int(st.relax.iterations) if st.residual_ran else 0,
+                             float(st.mobile.after.volume_w_m3),
+                             float(st.mobile.after.max_speed_m_s))
+
+    def _step_operators(self, dt_s, cut_cells, cut_targets) -> PathStepStats:
         entrained = 0.0
         if cut_cells is not None and len(cut_cells):
             entrained = self.state.entrain_to_surface(cut_cells, cut_targets, reason="bucket_cut")
@@ -74,7 +135,7 @@ class PlainPath:
                          > cfg.dry_tolerance_m * self.grid.dx * self.grid.dy)
         run = self.residual == "always" or (self.residual == "gated" and quiet and not yield_present)
         if run:
-            rounds = self.frontier.run(self.critical_slope, 1e-8).rounds
+            rounds = self.frontier.run(self.critical_slope, self.tolerance_m, self.max_rounds).rounds
         return PathStepStats(int(mob.substeps), entrained, diag.classification,
                              diag.unstable_cell_count, diag.connected_region_count,
                              diag.largest_connected_cell_count, rounds,

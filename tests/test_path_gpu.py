@@ -1,0 +1,78 @@
+"""GPU tests of the plain terrain step (config-1 path on a small grid).
+
+* The fused step (one CUDA graph per physics step, classification and gating
+  on the device) must reproduce the operator-by-operator path bit for bit:
+  fields, substeps, classifications, residual rounds.
+* FX32: the total material volume sum(w*(b-z)+) + sum(w*h) is conserved
+  exactly (entrainment, transport and relaxation all move whole quanta).
+"""
+
+import numpy as np
+import pytest
+
+import soilb200
+from soilb200 import workloads
+from soilb200.pipeline import PlainPath
+
+pytestmark = pytest.mark.gpu
+
+DT = 1.0 / 60.0
+
+
+def _material():
+    return soilb200.MaterialScenario("path_test", 1600.0, 35.0, 0.0, 0.5, 38.0, 30.0, 0.55)
+
+
+def _setup(n, seed=1):
+    b = workloads.noise_pile(n, seed, 0.05)
+    cut = workloads.BucketCut((n, n), 0.05, b, start=(0.25 * n * 0.05, 0.5 * n * 0.05))
+    return b, cut
+
+
+def _fields(path):
+    g = path.grid
+    return [g.download(k) for k in ("b_eff", "mobile", "momentum_x", "momentum_y")]
+
+
+@pytest.mark.parametrize("precision,residual", [("fx32", "gated"), ("fx32", "always"),
+                                                ("fp64", "always")])
+def test_fused_step_equals_operator_path(precision, residual):
+    n = 160
+    b, cut = _setup(n)
+    z = np.zeros_like(b)
+    fused = PlainPath(b, z, dx=0.05, material=_material(), precision=precision, tile_size=32,
+                      residual=residual, fused=True)
+    ops = PlainPath(b, z, dx=0.05, material=_material(), precision=precision, tile_size=32,
+                    residual=residual, fused=False)
+    for k in range(24):
+        idx, tgt = cut.footprint((k + 1) * DT)
+        a = fused.step(DT, idx, tgt)
+        o = ops.step(DT, idx, tgt)
+        assert a.substeps == o.substeps, k
+        assert a.classification == o.classification, k
+        assert (a.unstable_cells, a.regions, a.largest) == (o.unstable_cells, o.regions, o.largest)
+        assert a.residual_rounds == o.residual_rounds, k
+        if k % 6 == 5:
+            for fa, fo in zip(_fields(fused), _fields(ops)):
+                assert np.array_equal(fa, fo), k
+    fused.close()
+    ops.close()
+
+
+def test_fx32_path_conserves_total_volume_exactly():
+    n = 192
+    b, cut = _setup(n, seed=3)
+    path = PlainPath(b, np.zeros_like(b), dx=0.05, material=_material(), precision="fx32",
+                     tile_size=32, residual="always")
+    r0 = path.state.reservoir_reduction(1600.0)
+    total0 = r0["resting_quanta_w6"] + r0["mobile_quanta_w6"]
+    moved = 0.0
+    for k in range(40):
+        idx, tgt = cut.footprint((k + 1) * DT)
+        st = path.step(DT, idx, tgt)
+        moved += st.entrained_m3
+        r = path.state.reservoir_reduction(1600.0)
+        assert r["resting_quanta_w6"] + r["mobile_quanta_w6"] == total0, k
+    assert moved > 0.0
+    assert path.state.reservoir_reduction(1600.0)["mobile_quanta_w6"] > 0
+    path.close()
