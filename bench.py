@@ -70,29 +70,78 @@ def cut_schedule(cut, steps: int, pinned: bool):
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock / throttle-reason sampling during the timed region.
 
+    NVML is read from a thread every 2 ms (a timed region of a few tens of
+    milliseconds still gets a median); nvidia-smi polling is the fallback when
+    NVML cannot be opened.  Only reads: no clock or power setting is touched.
+    """
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device = device
-        self.samples = []
+        self.period = period_s
+        self.samples = []            # (sm_mhz, sm_max_mhz, reasons bitmask)
+        self.source = None
         self._stop = threading.Event()
         self._thread = None
+        self._nvml = None
+        self._handle = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            self._nvml = pynvml
+            try:
+                uuid = str(torch.cuda.get_device_properties(device).uuid)
+                self._handle = pynvml.nvmlDeviceGetHandleByUUID(
+                    uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+            except Exception:
+                self._handle = pynvml.nvmlDeviceGetHandleByIndex(device)
+            self.source = "nvml"
+        except Exception:
+            self._nvml = None
+            self.source = "nvidia-smi"
+
+    def _sample_nvml(self):
+        n = self._nvml
+        sm = n.nvmlDeviceGetClockInfo(self._handle, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(self._handle, n.NVML_CLOCK_SM)
+        get = getattr(n, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            n.nvmlDeviceGetCurrentClocksThrottleReasons
+        self.samples.append((float(sm), float(mx), int(get(self._handle))))
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                              "--format=csv,noheader,nounits"],
+                             capture_output=True, text=True, timeout=5).stdout.strip()
+        if not out:
+            return
+        f = [x.strip() for x in out.split(",")]
+        mask = 0
+        for (name, bit), val in zip(self.REASONS, f[5:9]):
+            if val.lower().startswith("active"):
+                mask |= bit
+        try:
+            self.samples.append((float(f[1]), float(f[2]), mask))
+        except ValueError:
+            pass
 
     def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.device}",
-                                      f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
+                if self._nvml is not None:
+                    self._sample_nvml()
+                else:
+                    self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(self.period if self._nvml is not None else 0.2)
 
     def __enter__(self):
         self._thread = threading.Thread(target=self._run, daemon=True)
@@ -107,17 +156,11 @@ class ClockSampler:
     def summary(self):
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for s in self.samples:
-            for name, val in zip(names, s[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.samples)}
+        reasons = sorted({name for _, _, m in self.samples for name, bit in self.REASONS
+                          if m & bit})
+        return {"sm_mhz": statistics.median(s[0] for s in self.samples),
+                "sm_max_mhz": max(s[1] for s in self.samples), "reasons": reasons,
+                "samples": len(self.samples), "source": self.source}
 
 
 def load_traffic():

@@ -34,7 +34,8 @@ constexpr int kFvDiag = 8;      // cons x,y | ext x,y | fric x,y | fdiss | ework
 constexpr int kFvPartial = 10;  // kFvDiag + wave max + positivity flag
 
 struct FvConst {
-  int ny, nx, pitch, tiles_x, nblocks;
+  int ny, nx, pitch, tiles_x, nblocks;  // FX: tiles_x = column strips, nblocks = launch grid
+  int rows_per_warp;                    // FX streaming kernel: rows of one warp's strip
   double dx, dy, K, g, cfl, dry, mu_g, c_half, kg, min_spacing;
   // fixed-point constants
   double Q;
@@ -229,6 +230,74 @@ __device__ __forceinline__ void plan_substep(const FvConst& c, FvControl* ctl) {
   if (sub < rem - 1.0e-14) ctl->cfl_limited = 1;
   ctl->max_cfl = fmax(ctl->max_cfl, w * sub / c.min_spacing);
   ctl->sub_dt = sub;
+}
+
+// Block partials of one substep (impulse/energy sums, wave maximum,
+// positivity flag) and, in the last block to arrive, the fixed-order grid
+// reduction and loop control: substep count, remaining time, ping-pong parity,
+// error status and the next substep's dt; the graph's while-condition is set
+// from here.
+__device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, double* partials,
+                                          const double* acc, double wave, int neg, double* red,
+                                          int* flag, double sub_dt, int parity,
+                                          cudaGraphConditionalHandle loop_handle, int use_handle) {
+  double v[kFvPartial];
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) v[k] = warp_sum(acc[k]);
+  v[kFvDiag] = warp_max(wave);
+  v[kFvDiag + 1] = (double)__reduce_or_sync(0xffffffffu, (unsigned)neg);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < kFvPartial; ++k) red[warp * kFvPartial + k] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < kFvPartial) {
+    const int k = threadIdx.x;
+    double a = 0.0;
+    for (int w2 = 0; w2 < kThreads / 32; ++w2)
+      a = k >= kFvDiag ? fmax(a, red[w2 * kFvPartial + k]) : a + red[w2 * kFvPartial + k];
+    partials[(size_t)blockIdx.x * kFvPartial + k] = a;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicAdd(&ctl->arrive, 1u);
+    *flag = (prev == (unsigned)c.nblocks - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!*flag) return;
+
+  __threadfence();
+  __shared__ double tot[kFvPartial];
+  __shared__ bool is_max[kFvPartial];
+  if (threadIdx.x < kFvPartial) is_max[threadIdx.x] = threadIdx.x >= kFvDiag;
+  __syncthreads();
+  reduce_partials<kFvPartial>(partials, c.nblocks, tot, red, is_max);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] += tot[k];
+    ctl->substeps += 1;
+    ctl->remaining -= sub_dt;
+    ctl->parity = parity ^ 1;
+    ctl->wave = tot[kFvDiag];
+    ctl->arrive = 0;
+    if (ctl->wait_fail) {
+      ctl->status = 6;  // SB_ERR_WAIT_LIMIT
+      ctl->done = 1;
+    } else if (tot[kFvDiag + 1] != 0.0) {
+      ctl->status = 3;  // SB_ERR_POSITIVITY
+      ctl->done = 1;
+    } else if (!(ctl->remaining > 1.0e-14)) {
+      ctl->done = 1;
+    } else if (ctl->substeps >= c.max_substeps) {
+      ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
+      ctl->done = 1;
+    } else {
+      plan_substep(c, ctl);
+    }
+    __threadfence();
+    if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
+  }
 }
 
 template <bool FX>
@@ -484,65 +553,201 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
 
-  // ---- Block partials --------------------------------------------------------
-  double v[kFvPartial];
-#pragma unroll
-  for (int k = 0; k < kFvDiag; ++k) v[k] = warp_sum(acc[k]);
-  v[kFvDiag] = warp_max(wave);
-  v[kFvDiag + 1] = (double)__reduce_or_sync(0xffffffffu, (unsigned)neg);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < kFvPartial; ++k) s.red[warp * kFvPartial + k] = v[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < kFvPartial) {
-    const int k = threadIdx.x;
-    double a = 0.0;
-    for (int w2 = 0; w2 < kThreads / 32; ++w2)
-      a = k >= kFvDiag ? fmax(a, s.red[w2 * kFvPartial + k]) : a + s.red[w2 * kFvPartial + k];
-    partials[(size_t)blockIdx.x * kFvPartial + k] = a;
-  }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const unsigned prev = atomicAdd(&ctl->arrive, 1u);
-    s.flag = (prev == (unsigned)c.nblocks - 1) ? 1 : 0;
-  }
-  __syncthreads();
-  if (!s.flag) return;
+  fv_finish(c, ctl, partials, acc, wave, neg, s.red, &s.flag, sub_dt, parity, loop_handle,
+            use_handle);
+}
 
-  // ---- Last block: loop control ---------------------------------------------
-  __threadfence();
-  __shared__ double tot[kFvPartial];
-  __shared__ bool is_max[kFvPartial];
-  if (threadIdx.x < kFvPartial) is_max[threadIdx.x] = threadIdx.x >= kFvDiag;
-  __syncthreads();
-  reduce_partials<kFvPartial>(partials, c.nblocks, tot, s.red, is_max);
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] += tot[k];
-    ctl->substeps += 1;
-    ctl->remaining -= sub_dt;
-    ctl->parity = parity ^ 1;
-    ctl->wave = tot[kFvDiag];
-    ctl->arrive = 0;
-    if (ctl->wait_fail) {
-      ctl->status = 6;  // SB_ERR_WAIT_LIMIT
-      ctl->done = 1;
-    } else if (tot[kFvDiag + 1] != 0.0) {
-      ctl->status = 3;  // SB_ERR_POSITIVITY
-      ctl->done = 1;
-    } else if (!(ctl->remaining > 1.0e-14)) {
-      ctl->done = 1;
-    } else if (ctl->substeps >= c.max_substeps) {
-      ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
-      ctl->done = 1;
-    } else {
-      plan_substep(c, ctl);
-    }
-    __threadfence();
-    if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
+// --------------------------------------------------------------------------
+// FX32 substep as a register-streaming stencil.
+//
+// A warp owns a strip of 32 columns (lanes 1..30 are output columns, lanes 0
+// and 31 their west/east neighbours) and walks down rows_per_warp rows.  Per
+// row every lane evaluates the east face of its column (the east neighbour's
+// state arrives by shuffle) and the north face (the next row is already in
+// registers); the west face is the previous lane's east face (one more
+// shuffle) and the south face is the previous row's north face, carried in
+// registers.  Each interior face is therefore evaluated once, in registers:
+// nothing is staged in shared memory, the only shared memory use is the
+// block reduction.  The row after next is loaded while the current row is
+// computed.  The face and cell arithmetic is the same as the tile kernel's,
+// so both produce identical fields.
+// --------------------------------------------------------------------------
+constexpr int kStripOut = 30;
+
+struct FxCell {
+  int b, h;
+  float qx, qy, u, v, cel;
+};
+
+__device__ __forceinline__ void fx_load(const FvConst& c, const int32_t* __restrict__ b,
+                                        const int32_t* __restrict__ h,
+                                        const float* __restrict__ qx,
+                                        const float* __restrict__ qy, int row, int gx, bool colok,
+                                        FxCell& x) {
+  if (colok && row >= 0 && row < c.ny) {
+    const size_t gi = (size_t)row * c.pitch + gx;
+    x.b = __ldg(b + gi);
+    x.h = __ldg(h + gi);
+    x.qx = __ldg(qx + gi);
+    x.qy = __ldg(qy + gi);
+  } else {
+    x.b = 0;
+    x.h = 0;
+    x.qx = 0.f;
+    x.qy = 0.f;
   }
+}
+
+// Per-cell velocity q/h (0 for an empty cell) and celerity sqrt(K g h).
+__device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
+  const float hf = (float)x.h * c.Qf;
+  const float inv = x.h > 0 ? 1.0f / hf : 0.f;
+  x.u = x.qx * inv;
+  x.v = x.qy * inv;
+  x.cel = sqrtf(c.KGf * hf);
+}
+
+__global__ void __launch_bounds__(kThreads, 4)
+    fv_stream_kernel(const FvConst c, const int32_t* __restrict__ bsrc, int32_t* __restrict__ h0,
+                     int32_t* __restrict__ h1, float* __restrict__ qx0, float* __restrict__ qx1,
+                     float* __restrict__ qy0, float* __restrict__ qy1,
+                     const float* __restrict__ ext_x, const float* __restrict__ ext_y,
+                     FvControl* ctl, double* __restrict__ partials,
+                     cudaGraphConditionalHandle loop_handle, int use_handle) {
+  __shared__ double red[kThreads / 32 * kFvPartial];
+  __shared__ int flag;
+  if (*(volatile int*)&ctl->done) return;  // uniform across the grid
+  const double sub_dt = ctl->sub_dt;
+  const int parity = ctl->parity;
+  const int32_t* __restrict__ hsrc = parity ? h1 : h0;
+  const float* __restrict__ qxsrc = parity ? qx1 : qx0;
+  const float* __restrict__ qysrc = parity ? qy1 : qy0;
+  int32_t* __restrict__ hdst = parity ? h0 : h1;
+  float* __restrict__ qxdst = parity ? qx0 : qx1;
+  float* __restrict__ qydst = parity ? qy0 : qy1;
+
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  const int strip = gw % c.tiles_x;
+  const int y0 = (gw / c.tiles_x) * c.rows_per_warp;
+  const int y1 = min(y0 + c.rows_per_warp, c.ny);
+  const int gx = strip * kStripOut - 1 + lane;
+  const bool colok = gx >= 0 && gx < c.nx;
+  const bool out_lane = lane >= 1 && lane <= kStripOut && colok;
+  const bool east_ok = gx >= 0 && gx + 1 < c.nx && lane < 31;
+  const float lamx_f = (float)(sub_dt / c.dx);
+  const float lamy_f = (float)(sub_dt / c.dy);
+  const float dtf = (float)sub_dt;
+  const float dec = (float)(c.mu_g * sub_dt);
+
+  double acc[kFvDiag];
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
+  double wave = 0.0;
+
+  if (y0 < c.ny) {  // warp-uniform
+    FxCell cur, nxt, nn;
+    fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0, gx, colok, cur);
+    fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 + 1, gx, colok, nxt);
+    // south face of the first row (the previous row's north face)
+    int ms = 0;
+    float nts = 0.f, nnps = 0.f;
+    {
+      FxCell prv;
+      fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 - 1, gx, colok, prv);
+      fx_prepare(c, prv);
+      fx_prepare(c, cur);
+      if (y0 > 0 && colok) {
+        float fnm;
+        face_fx(c, lamy_f, prv.b, cur.b, prv.h, cur.h, prv.v, prv.u, cur.v, cur.u, prv.cel,
+                cur.cel, ms, fnm, nnps, nts);
+      }
+    }
+    fx_prepare(c, nxt);
+    for (int r = y0; r < y1; ++r) {
+      fx_load(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
+      // east face: this column and the next lane's
+      const int eb = __shfl_down_sync(0xffffffffu, cur.b, 1);
+      const int eh = __shfl_down_sync(0xffffffffu, cur.h, 1);
+      const float eu = __shfl_down_sync(0xffffffffu, cur.u, 1);
+      const float ev = __shfl_down_sync(0xffffffffu, cur.v, 1);
+      const float ec = __shfl_down_sync(0xffffffffu, cur.cel, 1);
+      int me = 0;
+      float enm = 0.f, enp = 0.f, et = 0.f;
+      if (east_ok)
+        face_fx(c, lamx_f, cur.b, eb, cur.h, eh, cur.u, cur.v, eu, ev, cur.cel, ec, me, enm, enp,
+                et);
+      // west face = the previous lane's east face
+      const int mw = __shfl_up_sync(0xffffffffu, me, 1);
+      const float enpw = __shfl_up_sync(0xffffffffu, enp, 1);
+      const float etw = __shfl_up_sync(0xffffffffu, et, 1);
+      // north face: this row and the next
+      int mn = 0;
+      float nnm = 0.f, nnp = 0.f, nt = 0.f;
+      if (colok && r + 1 < c.ny)
+        face_fx(c, lamy_f, cur.b, nxt.b, cur.h, nxt.h, cur.v, cur.u, nxt.v, nxt.u, cur.cel,
+                nxt.cel, mn, nnm, nnp, nt);
+      if (out_lane) {
+        const size_t gi = (size_t)r * c.pitch + gx;
+        float ax = 0.f, ay = 0.f;
+        if (c.has_external) {
+          ax = ext_x[gi];
+          ay = ext_y[gi];
+        }
+        const int dh = ((0 - me + mw) - mn) + ms;
+        const int hq = cur.h + dh;
+        const float zero = 0.f;
+        const float dqx = (((zero - lamx_f * enm) + lamx_f * enpw) - lamy_f * nt) + lamy_f * nts;
+        const float dqy = (((zero - lamx_f * et) + lamx_f * etw) - lamy_f * nnm) + lamy_f * nnps;
+        const float hn = (float)hq * c.Qf;
+        const bool wet = hn > c.dryf;
+        const float qxn = wet ? cur.qx + dqx : 0.f;
+        const float qyn = wet ? cur.qy + dqy : 0.f;
+        float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
+        if (wet) {
+          const float inv = 1.0f / hn;
+          vbx = qxn * inv;
+          vby = qyn * inv;
+          if (c.has_external) {
+            qex = qxn + (hn * ax) * dtf;
+            qey = qyn + (hn * ay) * dtf;
+            vex = qex * inv;
+            vey = qey * inv;
+          } else {
+            vex = vbx;
+            vey = vby;
+          }
+        }
+        const float spd = sqrtf(vex * vex + vey * vey);
+        const float fac = fmaxf(0.f, 1.f - dec / fmaxf(spd, 1.0e-15f));
+        const float vax = vex * fac, vay = vey * fac;
+        const float qxo = hn * vax, qyo = hn * vay;
+        hdst[gi] = hq;
+        qxdst[gi] = qxo;
+        qydst[gi] = qyo;
+        const double h64 = (double)hn;
+        acc[0] += (double)qxn - (double)cur.qx;
+        acc[1] += (double)qyn - (double)cur.qy;
+        acc[2] += (double)qex - (double)qxn;
+        acc[3] += (double)qey - (double)qyn;
+        acc[4] += (double)qxo - (double)qex;
+        acc[5] += (double)qyo - (double)qey;
+        acc[6] += 0.5 * h64 *
+                  ((double)spd * (double)spd - ((double)vax * (double)vax + (double)vay * (double)vay));
+        acc[7] += h64 * ((0.5 * ((double)vbx + (double)vex)) * (double)ax +
+                         (0.5 * ((double)vby + (double)vey)) * (double)ay) * sub_dt;
+        const float wv = spd * fac + sqrtf(c.KGf * hn);  // |new velocity| + celerity
+        wave = fmax(wave, (double)wv);
+      }
+      ms = mn;
+      nts = nt;
+      nnps = nnp;
+      cur = nxt;
+      nxt = nn;
+      fx_prepare(c, nxt);
+    }
+  }
+  fv_finish(c, ctl, partials, acc, wave, 0, red, &flag, sub_dt, parity, loop_handle, use_handle);
 }
 
 }  // namespace sb

@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(kThreads)
     const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
     const size_t il = (size_t)r * c.pitch + cl, ir = (size_t)r * c.pitch + cr;
     const size_t idn = (size_t)rd * c.pitch + col, iup = (size_t)ru * c.pitch + col;
-    double grad;
+    double grad;  // FX: squared gradient (sqrt taken once, after the max)
     if constexpr (FX) {
       const int hq = h[gi];
       hv = (double)hq * c.Q;
@@ -83,9 +83,10 @@ __global__ void __launch_bounds__(kThreads)
       iq2 += (rest > 0 ? rest : 0) * w6;
       const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
       const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
-      const double gx = ((double)(Hr - Hl) * c.Q) / denx;
-      const double gy = ((double)(Hu - Hd) * c.Q) / deny;
-      grad = sqrt(gx * gx + gy * gy);
+      // (H difference) * Q / spacing with the spacing folded into one constant
+      const double gx = (double)(Hr - Hl) * ((col > 0 && col + 1 < c.nx) ? c.Q / (2.0 * c.dx) : c.Q / c.dx);
+      const double gy = (double)(Hu - Hd) * ((r > 0 && r + 1 < c.ny) ? c.Q / (2.0 * c.dy) : c.Q / c.dy);
+      grad = gx * gx + gy * gy;
     } else {
       hv = h[gi];
       bv = b[gi];
@@ -97,7 +98,7 @@ __global__ void __launch_bounds__(kThreads)
       grad = hypot(gx, gy);
     }
     const bool wet = hv > c.dry;
-    double s2 = 0.0, spd = 0.0, wave;
+    double s2 = 0.0, spd = 0.0, e = 0.0, wave;
     if constexpr (FX) {
       const float hn = (float)h[gi] * c.Qf;
       float vx = 0.f, vy = 0.f;
@@ -107,6 +108,12 @@ __global__ void __launch_bounds__(kThreads)
         vy = qy[gi] * inv;
       }
       wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
+      if (wet) {  // one reciprocal: e = |q|^2 / h (= h |u|^2), s2 = e / h
+        const double inv = 1.0 / hv;
+        e = (qxv * qxv + qyv * qyv) * inv;
+        s2 = e * inv;
+      }
+      spd = s2;  // squared speed; sqrt after the max
     } else {
       double vx = 0.0, vy = 0.0;
       if (wet) {
@@ -114,17 +121,18 @@ __global__ void __launch_bounds__(kThreads)
         vy = qyv / hv;
       }
       wave = sqrt(vx * vx + vy * vy) + sqrt(c.kg * fmax(hv, 0.0));
-    }
-    if (wet) {
-      s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
-      spd = sqrt(s2);
+      if (wet) {
+        s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
+        spd = sqrt(s2);
+        e = hv * s2;
+      }
     }
     v[L_QX] += qxv;
     v[L_QY] += qyv;
     v[L_QX_W] += qxv * w6;
     v[L_QY_W] += qyv * w6;
-    v[L_HS2] += hv * s2;
-    v[L_HS2_W] += hv * s2 * w6;
+    v[L_HS2] += e;
+    v[L_HS2_W] += e * w6;
     v[L_HB] += hv * bv;
     v[L_HB_W] += hv * bv * w6;
     v[L_HH] += hv * hv;
@@ -190,7 +198,12 @@ __global__ void __launch_bounds__(kThreads)
       for (int k = 0; k < kLedgerI64; ++k) ired[warp * kLedgerI64 + k] = a[k];
   }
   __syncthreads();
-  if (threadIdx.x < L_NP) out->v[threadIdx.x] = tot[threadIdx.x];
+  if (threadIdx.x < L_NP) {
+    double val = tot[threadIdx.x];
+    // FX accumulates squared gradient / speed maxima; monotone sqrt after the max
+    if (FX && (threadIdx.x == L_MAXGRAD || threadIdx.x == L_MAXSPEED)) val = sqrt(val);
+    out->v[threadIdx.x] = val;
+  }
   if (threadIdx.x < kLedgerI64) {
     long long a = 0;
     for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + threadIdx.x];

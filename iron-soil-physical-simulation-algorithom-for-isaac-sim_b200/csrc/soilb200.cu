@@ -107,6 +107,12 @@ struct sb_ctx {
   int parity_host = 0;            // mirror of ctl->parity after the last sync
   CUtensorMap tm_b, tm_h[2], tm_qx[2], tm_qy[2];
   int fv_blocks = 0;
+  // FX32 substep kernel: register-streaming strips (default) or the TMA tile
+  // kernel (SOILB200_FV_TILE=1); strips of 30 output columns x fv_rows rows
+  int fv_stream = 0;
+  int fv_rows = 0;
+  int fv_strips = 0;
+  int fv_stream_blocks = 0;
   int ledger_blocks = 0;
   MobileGraph mobile;
   cudaEvent_t ev_loop[2] = {nullptr, nullptr};  // around the substep WHILE node
@@ -226,6 +232,11 @@ FvConst make_const(const sb_ctx* ctx, const sb_mobile_params* p) {
   c.pitch = ctx->pitch;
   c.tiles_x = (ctx->d.nx + kTileX - 1) / kTileX;
   c.nblocks = c.tiles_x * ((ctx->d.ny + kTileY - 1) / kTileY);
+  if (ctx->fv_stream) {
+    c.tiles_x = ctx->fv_strips;
+    c.nblocks = ctx->fv_stream_blocks;
+    c.rows_per_warp = ctx->fv_rows;
+  }
   c.dx = ctx->d.dx_m;
   c.dy = ctx->d.dy_m;
   c.K = p->earth_pressure_coefficient;
@@ -254,14 +265,34 @@ size_t fv_smem_bytes() {
   return sizeof(FvSmem<FX>) + 128;
 }
 
+// Kernel, grid, shared memory and argument list of one substep launch.
+struct FvLaunch {
+  void* func = nullptr;
+  dim3 grid;
+  size_t smem = 0;
+  std::vector<void*> args;
+};
+
 template <bool FX>
-void fv_args(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle, int* use_handle,
-             std::vector<void*>& args) {
-  args = {(void*)&c,           (void*)&ctx->tm_b,     (void*)&ctx->tm_h[0], (void*)&ctx->tm_h[1],
-          (void*)&ctx->tm_qx[0], (void*)&ctx->tm_qx[1], (void*)&ctx->tm_qy[0], (void*)&ctx->tm_qy[1],
-          (void*)&ctx->h[0],   (void*)&ctx->h[1],     (void*)&ctx->qx[0],   (void*)&ctx->qx[1],
-          (void*)&ctx->qy[0],  (void*)&ctx->qy[1],    (void*)&ctx->ext_x,   (void*)&ctx->ext_y,
-          (void*)&ctx->ctl,    (void*)&ctx->partials, (void*)handle,        (void*)use_handle};
+void fv_launch(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle, int* use_handle,
+               FvLaunch& L) {
+  if (FX && ctx->fv_stream) {
+    L.func = (void*)fv_stream_kernel;
+    L.smem = 0;
+    L.args = {(void*)&c,         (void*)&ctx->b,     (void*)&ctx->h[0],  (void*)&ctx->h[1],
+              (void*)&ctx->qx[0], (void*)&ctx->qx[1], (void*)&ctx->qy[0], (void*)&ctx->qy[1],
+              (void*)&ctx->ext_x, (void*)&ctx->ext_y, (void*)&ctx->ctl,   (void*)&ctx->partials,
+              (void*)handle,      (void*)use_handle};
+  } else {
+    L.func = (void*)fv_substep_kernel<FX>;
+    L.smem = fv_smem_bytes<FX>();
+    L.args = {(void*)&c,           (void*)&ctx->tm_b,     (void*)&ctx->tm_h[0], (void*)&ctx->tm_h[1],
+              (void*)&ctx->tm_qx[0], (void*)&ctx->tm_qx[1], (void*)&ctx->tm_qy[0], (void*)&ctx->tm_qy[1],
+              (void*)&ctx->h[0],   (void*)&ctx->h[1],     (void*)&ctx->qx[0],   (void*)&ctx->qx[1],
+              (void*)&ctx->qy[0],  (void*)&ctx->qy[1],    (void*)&ctx->ext_x,   (void*)&ctx->ext_y,
+              (void*)&ctx->ctl,    (void*)&ctx->partials, (void*)handle,        (void*)use_handle};
+  }
+  L.grid = dim3(c.nblocks);
 }
 
 template <bool FX>
@@ -332,10 +363,9 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
     cp.conditional.size = 1;
     SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_ev0, 1, &cp));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    std::vector<void*> args;
-    fv_args<FX>(ctx, cc, &handle, &use_handle, args);
-    int rc = add_kernel(ctx, body, &n_body, nullptr, 0, (void*)fv_substep_kernel<FX>,
-                        dim3(c.nblocks), fv_smem_bytes<FX>(), args.data());
+    FvLaunch L;
+    fv_launch<FX>(ctx, cc, &handle, &use_handle, L);
+    int rc = add_kernel(ctx, body, &n_body, nullptr, 0, L.func, L.grid, L.smem, L.args.data());
     if (rc) return rc;
   }
   {
@@ -409,15 +439,15 @@ static int mobile_step_host_loop(sb_ctx* ctx, const FvConst& c, double static_li
   SB_CUDA(ctx, cudaLaunchKernel((void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks), dim3(kThreads),
                                 args.data(), 0, ctx->stream));
   SB_CUDA(ctx, cudaEventRecord(ctx->ev_loop[0], ctx->stream));
-  std::vector<void*> fargs;
-  fv_args<FX>(ctx, cc, &handle, &no_handle, fargs);
+  FvLaunch L;
+  fv_launch<FX>(ctx, cc, &handle, &no_handle, L);
   for (int it = 0; it <= c.max_substeps; ++it) {
     SB_CUDA(ctx, cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(FvControl), cudaMemcpyDeviceToHost,
                                  ctx->stream));
     SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (ctx->ctl_host->done) break;
-    SB_CUDA(ctx, cudaLaunchKernel((void*)fv_substep_kernel<FX>, dim3(c.nblocks), dim3(kThreads),
-                                  fargs.data(), fv_smem_bytes<FX>(), ctx->stream));
+    SB_CUDA(ctx, cudaLaunchKernel(L.func, L.grid, dim3(kThreads), L.args.data(), L.smem,
+                                  ctx->stream));
   }
   SB_CUDA(ctx, cudaEventRecord(ctx->ev_loop[1], ctx->stream));
   std::vector<void*> a2;
@@ -534,8 +564,25 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMemsetAsync(ctx->io, 0, sizeof(StepIO), ctx->stream));
   const int tiles = ((d.nx + kTileX - 1) / kTileX) * ((d.ny + kTileY - 1) / kTileY);
   ctx->fv_blocks = tiles;
-  ctx->ledger_blocks = grid_for((long long)d.ny * d.nx);
-  const size_t np = (size_t)(tiles > ctx->ledger_blocks ? tiles : ctx->ledger_blocks) *
+  if (d.precision == SB_FX32) {
+    const char* tile_env = std::getenv("SOILB200_FV_TILE");
+    ctx->fv_stream = !(tile_env && tile_env[0] == '1');
+    ctx->fv_strips = (d.nx + kStripOut - 1) / kStripOut;
+    // rows per warp: enough warps for ~48 resident per SM, 4..64 rows each
+    const long long want_warps = 148LL * 48;
+    long long rows = ((long long)d.ny * ctx->fv_strips + want_warps - 1) / want_warps;
+    rows = rows < 4 ? 4 : (rows > 64 ? 64 : rows);
+    if (const char* rows_env = std::getenv("SOILB200_FV_ROWS")) {
+      const long long r = std::atoll(rows_env);
+      if (r >= 1 && r <= 4096) rows = r;
+    }
+    ctx->fv_rows = (int)rows;
+    const long long warps = (long long)ctx->fv_strips * ((d.ny + rows - 1) / rows);
+    ctx->fv_stream_blocks = (int)((warps + kThreads / 32 - 1) / (kThreads / 32));
+  }
+  // grid-stride reductions: two CTAs per SM keep the final fold short
+  ctx->ledger_blocks = std::min(grid_for((long long)d.ny * d.nx), 2 * 148);
+  const size_t np = (size_t)std::max({tiles, ctx->ledger_blocks, ctx->fv_stream_blocks}) *
                     (kFvPartial > L_NP ? kFvPartial : L_NP);
   SB_CUDA(ctx, cudaMalloc(&ctx->partials, np * sizeof(double)));
   SB_CUDA(ctx, cudaMalloc(&ctx->ipartials, (size_t)ctx->ledger_blocks * kLedgerI64 * 8));
@@ -1541,12 +1588,11 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     cp.conditional.size = 1;
     SB_CUDA(ctx, cudaGraphAddNode(&node, g, &prev, 1, &cp));
     prev = node;
-    std::vector<void*> args;
-    fv_args<FX>(ctx, fc, &h_mob, &use_h, args);
+    FvLaunch L;
+    fv_launch<FX>(ctx, fc, &h_mob, &use_h, L);
     cudaGraphNode_t body_node;
-    if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node, nullptr, 0,
-                         (void*)fv_substep_kernel<FX>, dim3(fc.nblocks), fv_smem_bytes<FX>(),
-                         args.data())))
+    if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node, nullptr, 0, L.func,
+                         L.grid, L.smem, L.args.data())))
       return rc;
   }
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[1]));

@@ -215,10 +215,32 @@ def static_check(p: FixedParams, bq, hq, qx, qy) -> bool:
     if max(float(np.max(np.abs(qx), initial=0.0)), float(np.max(np.abs(qy), initial=0.0))) > 1.0e-14:
         return False
     H = bq.astype(np.int64) + hq.astype(np.int64)
+    return bool(max_surface_gradient(p, H) <= np.tan(np.deg2rad(p.start_angle_deg)) + 1.0e-14)
+
+
+def _diff_axis(H, axis, spacing, Q):
+    """np.gradient's differences (central inside, one-sided at the edges, edge_order 1)
+    of an integer surface, scaled by Q / (2 spacing) resp. Q / spacing as one
+    rounded constant: (H[i+1] - H[i-1]) * (Q / (2 d))."""
+    H = np.moveaxis(H, axis, 0)
+    d = np.zeros(H.shape, dtype=np.float64)
+    n = H.shape[0]
+    if n < 2:
+        return np.moveaxis(d, 0, axis)
+    d[1:-1] = (H[2:] - H[:-2]).astype(np.float64) * (Q / (2.0 * spacing))
+    d[0] = (H[1] - H[0]).astype(np.float64) * (Q / spacing)
+    d[-1] = (H[-1] - H[-2]).astype(np.float64) * (Q / spacing)
+    return np.moveaxis(d, 0, axis)
+
+
+def max_surface_gradient(p: FixedParams, H) -> float:
+    """Largest free-surface slope |grad(b + h)| of the fixed-point path (the
+    static short-circuit of mobile_v2_reference.py:199-205 on quantised
+    heights): the maximum of gx^2 + gy^2 is taken first, its square root last."""
     Q = p.quantum
-    gy, gx = np.gradient(H.astype(np.float64) * Q, p.dy, p.dx)
-    mag = np.sqrt(gx * gx + gy * gy)
-    return bool(np.max(mag, initial=0.0) <= np.tan(np.deg2rad(p.start_angle_deg)) + 1.0e-14)
+    gx = _diff_axis(H, 1, p.dx, Q)
+    gy = _diff_axis(H, 0, p.dy, Q)
+    return float(np.sqrt(np.max(gx * gx + gy * gy, initial=0.0)))
 
 
 def step(p: FixedParams, bq, hq, qx, qy, dt_s: float, ax=None, ay=None):
