@@ -163,14 +163,16 @@ class ClockSampler:
                 "samples": len(self.samples), "source": self.source}
 
 
-def load_traffic():
-    p = ROOT / "profiles" / "traffic.json"
-    if p.exists():
-        try:
-            return json.loads(p.read_text())
-        except Exception:
-            return None
-    return None
+# DRAM bytes (read + write) of one FV substep launch, from one ncu capture of
+# the same workload (dram__bytes_read.sum + dram__bytes_write.sum); the
+# captures and their commands are summarised in profiles/.
+NCU_TRAFFIC_BYTES = {
+    # profiles/plain_path_step_701_launches.md: 8.504320 MB read + 256 B write
+    # (cold L2 under ncu; the state fits in L2, so writes stay there)
+    "config1_plain_path_701": 8_504_576,
+    # profiles/fv_stream_kernel_mobile_v2_4096.md: 282.211584 MB + 167.329280 MB
+    "mobile_v2_4096": 449_540_864,
+}
 
 
 def measured_peak():
@@ -254,7 +256,6 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     per_launch_ms = tot_loop / tot_launch if tot_launch else None
     alg_bytes = BYTES_PER_CELL_SUBSTEP * cells
     achieved = alg_bytes / (per_launch_ms * 1e-3) / 1e9 if per_launch_ms else None
-    traffic = load_traffic()
     result = None
     if rank == 0:
         result = {
@@ -275,13 +276,14 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             "e2e": {"value": cell_substeps / wall if wall > 0 else 0.0, "unit": UNIT,
                     "h2d_bytes_per_step": h2d // max(args.steps, 1),
                     "d2h_bytes_per_step": d2h // max(args.steps, 1)},
-            "roofline": {"bound": "hbm", "kernel": "fv_substep_kernel<FX32>",
+            "roofline": {"bound": "hbm", "kernel": "fv_stream_kernel (FX32 substep)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "mean_launch_ms": per_launch_ms,
-                         "traffic": (traffic or {}).get("fv_substep_bytes_per_launch")},
+                         "traffic": NCU_TRAFFIC_BYTES["config1_plain_path_701"],
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
         }
@@ -333,7 +335,9 @@ def run_mobile_large(args, n: int = 4096):
             "substeps": subs, "higher_is_better": True,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                          "frac": ach / peak, "peak_source": kind, "mean_launch_ms": per,
-                         "algorithmic_bytes_per_launch": alg}}
+                         "algorithmic_bytes_per_launch": alg,
+                         "traffic": NCU_TRAFFIC_BYTES["mobile_v2_4096"],
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"}}
 
 
 # ---------------------------------------------------------------------------

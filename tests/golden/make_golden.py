@@ -21,6 +21,11 @@ need the reference at run time.  Cases:
   ``tests/test_warp_gpu_backends.py:166-259``.
 * ``labels.npz``        -- ``_largest_connected_region`` and
   ``evaluate_cohesive_yield`` on seeded slope fields.
+* ``gate0.npz``         -- the 5 s config-0 gate: 256x256, seed 0, 300 steps of
+  1/60 s at CFL 0.4 and mu = tan 35 deg, each followed by
+  ``relax_critical_slope`` of ``b_eff`` at 35 deg (row-major array, spacing
+  (dy, dx), tolerance 1e-8 m); final fields stored as float32 (the comparison
+  bound is 1e-5 m), per-step substeps and relaxation iterations as integers.
 """
 
 from __future__ import annotations
@@ -299,7 +304,40 @@ def make_report_values():
         {"cpu_contracts": out, "device_equivalence": device}, indent=1, sort_keys=True) + "\n")
 
 
+def make_gate0(n: int = 256, steps: int = 300):
+    import time
+
+    import slope_model as sm
+
+    cfg = MobileV2Config(basal_friction_coefficient=float(np.tan(np.deg2rad(35.0))))
+    object.__setattr__(cfg, "cfl", 0.4)
+    solver = MobileV2ReferenceSolver(cfg)
+    b, h = config0_terrain(n, seed=0)
+    state = MobileV2State(b, h, np.zeros(h.shape + (2,)))
+    subs, iters = [], []
+    t0 = time.time()
+    for k in range(steps):
+        step = solver.step(state, 1.0 / 60.0)
+        subs.append(step.substeps)
+        relaxed, rs = sm.relax_critical_slope(step.state.b_eff_m, (cfg.dy_m, cfg.dx_m),
+                                              critical_angle_deg=35.0, max_iterations=20000,
+                                              tolerance=1e-8)
+        iters.append(rs.iterations)
+        state = MobileV2State(relaxed, step.state.h_m, step.state.q_m2_s)
+        if k in (59, 299):
+            print(f"gate0 step {k + 1}: {time.time() - t0:.1f} s", flush=True)
+    np.savez_compressed(HERE / "gate0.npz", b0_sum=np.float64(b.sum()), h0_sum=np.float64(h.sum()),
+                        b_final=state.b_eff_m.astype(np.float32),
+                        h_final=state.h_m.astype(np.float32),
+                        substeps=np.asarray(subs, np.int32), relax_iterations=np.asarray(iters, np.int32),
+                        mass_final=np.float64(np.sum(state.h_m) * cfg.dx_m * cfg.dy_m),
+                        resting_final=np.float64(np.sum(state.b_eff_m) * cfg.dx_m * cfg.dy_m))
+
+
 if __name__ == "__main__":
+    if "--gate0" in sys.argv:
+        make_gate0()
+        sys.exit(0)
     make_report_values()
     make_fv_contracts()
     make_fv_gate()

@@ -102,3 +102,17 @@ def test_fixed_point_donor_cap_keeps_heights_nonnegative():
     m0 = int(hq.sum(dtype=np.int64))
     hq, qx, qy, n, _ = fx.step(p, bq, hq, qx, qy, 0.05)
     assert hq.min() >= 0 and int(hq.sum(dtype=np.int64)) == m0
+
+
+def test_config0_generator_matches_gate_fixture_inputs():
+    """The 256x256 config-0 inputs are regenerated from the seed; the gate
+    fixture records their exact sums."""
+    from pathlib import Path
+
+    from soilb200 import workloads
+
+    z = np.load(Path(__file__).resolve().parent / "golden" / "gate0.npz")
+    t = workloads.config0_terrain(256, seed=0, dx=0.05)
+    assert float(t["b_eff"].sum()) == float(z["b0_sum"])
+    assert float(t["h"].sum()) == float(z["h0_sum"])
+    assert z["substeps"].shape == (300,) and z["relax_iterations"].shape == (300,)
