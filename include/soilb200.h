@@ -321,6 +321,48 @@ int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, int ny, int n
                          int connectivity, double dx_m, double dy_m, void* stream,
                          sb_label_stats* out);
 
+/* ---- Batched terrain patches ----------------------------------------------
+ * Many independent Mobile V2 grids ("patches": parallel dig environments of
+ * uneven sizes) advanced by shared launches.  The reference steps one
+ * DeviceBulkState per call (WarpProductionMobileV2Solver.step_resident,
+ * bulk_interaction/warp_mobile_v2.py:188-245; MobileV2ReferenceSolver.step,
+ * experimental/mobile_v2_reference.py:191-314); a batch runs that step for
+ * every patch with the SB_FX32 arithmetic of sb_mobile_step, each patch with
+ * its own quantum, CFL substeps and ledgers.  Patch fields are those of a
+ * context: SB_FIELD_Z_BASE, SB_FIELD_B_EFF, SB_FIELD_MOBILE,
+ * SB_FIELD_MOMENTUM_X/Y (row-major ny*nx float64 on the host).  No external
+ * acceleration.  One stream per batch; calls are synchronous at return. */
+typedef struct sb_batch sb_batch;
+
+typedef struct sb_patch_desc {
+  int ny, nx;
+  double dx_m, dy_m;
+  int height_exponent;         /* patch quantum 2^-k m, 4 <= k <= 40 */
+  int pad;
+  double datum_m;              /* datum of the patch's b_eff / z_base quanta */
+} sb_patch_desc;
+
+int sb_batch_create(int device, int n_patches, const sb_patch_desc* patches, sb_batch** out);
+int sb_batch_destroy(sb_batch* batch);
+int sb_batch_upload(sb_batch* batch, int patch, int field, const double* host);
+int sb_batch_download(sb_batch* batch, int patch, int field, double* host);
+/* Tile shape: rows per warp strip for every patch (4..256; default 16). */
+int sb_batch_set_rows(sb_batch* batch, const int* rows_per_warp);
+int sb_batch_get_rows(sb_batch* batch, int* rows_per_warp);
+/* One physics step of dt_s for every patch; per_patch[n_patches] receives each
+ * patch's record (as sb_mobile_step's).  The first failing patch's status is
+ * returned, its index in the message. */
+int sb_batch_step(sb_batch* batch, double dt_s, const sb_mobile_params* params,
+                  sb_mobile_stats* per_patch);
+/* Times every candidate rows-per-warp for each group of equal-height patches
+ * (trials steps each, on the live state, which is copied first and put back)
+ * and keeps the fastest; best_ms = substep-loop time of one step with it. */
+int sb_batch_autotune(sb_batch* batch, double dt_s, const sb_mobile_params* params, int trials,
+                      double* best_ms);
+int sb_batch_last_error(sb_batch* batch, char* buffer, size_t length);
+int64_t sb_batch_kernel_launch_count(sb_batch* batch);
+void* sb_batch_stream(sb_batch* batch);
+
 int sb_last_error(sb_ctx* ctx, char* buffer, size_t length);
 /* Number of kernels this context has launched (cumulative). */
 int64_t sb_kernel_launch_count(sb_ctx* ctx);

@@ -36,6 +36,8 @@ from .relax import (  # noqa: F401
     relax_critical_slope,
 )
 
+from .batch import B200PatchBatch  # noqa: E402,F401
+
 # Reference-compatible aliases: code written against the reference's Warp
 # device solver can switch by changing only the import.
 WarpMobileV2ReferenceSolver = B200MobileV2Solver
@@ -47,5 +49,5 @@ __all__ = [
     "B200LargeAvalancheBridge", "LabelDiagnosis", "LargeAvalancheTransitionConfig",
     "MaterialScenario", "FrontierRelaxation", "FrontierStats", "RelaxationStats",
     "relax_critical_slope", "label_mask", "largest_connected_region",
-    "label_mask_preallocated",
+    "label_mask_preallocated", "B200PatchBatch",
 ]

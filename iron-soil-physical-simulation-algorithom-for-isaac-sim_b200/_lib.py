@@ -160,6 +160,13 @@ class PathStats(C.Structure):
 
 
 _LIB = None
+class PatchDesc(C.Structure):
+    _fields_ = [
+        ("ny", C.c_int), ("nx", C.c_int), ("dx_m", C.c_double), ("dy_m", C.c_double),
+        ("height_exponent", C.c_int), ("pad", C.c_int), ("datum_m", C.c_double),
+    ]
+
+
 _PROTOTYPES = {
     "sb_ctx_create": (C.c_int, [C.POINTER(GridDesc), C.POINTER(C.c_void_p)]),
     "sb_ctx_destroy": (C.c_int, [C.c_void_p]),
@@ -199,6 +206,19 @@ _PROTOTYPES = {
                                         C.POINTER(C.c_double)]),
     "sb_deposit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
                              C.c_void_p]),
+    "sb_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(PatchDesc),
+                                  C.POINTER(C.c_void_p)]),
+    "sb_batch_destroy": (C.c_int, [C.c_void_p]),
+    "sb_batch_upload": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "sb_batch_download": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "sb_batch_set_rows": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "sb_batch_get_rows": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "sb_batch_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(MobileParams), C.c_void_p]),
+    "sb_batch_autotune": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(MobileParams), C.c_int,
+                                    C.POINTER(C.c_double)]),
+    "sb_batch_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "sb_batch_kernel_launch_count": (C.c_int64, [C.c_void_p]),
+    "sb_batch_stream": (C.c_void_p, [C.c_void_p]),
 }
 
 # ctypes mirror of each ABI struct, checked against sb_sizeof() in the tests.
@@ -213,6 +233,7 @@ ABI_STRUCTS = {
     "sb_relax_stats": RelaxStats,
     "sb_path_params": PathParams,
     "sb_path_stats": PathStats,
+    "sb_patch_desc": PatchDesc,
 }
 
 
@@ -254,11 +275,18 @@ def last_error(ctx) -> str:
     return buf.value.decode(errors="replace")
 
 
-def check(ctx, status: int, what: str = "") -> None:
+def batch_last_error(batch) -> str:
+    buf = C.create_string_buffer(1024)
+    load().sb_batch_last_error(batch, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check(ctx, status: int, what: str = "", *, batch=None) -> None:
     """Map a status code to the reference's exception types and messages."""
     if status == SB_OK:
         return
-    msg = last_error(ctx) or f"{what} failed with status {status}"
+    msg = (batch_last_error(batch) if batch is not None else last_error(ctx)) or \
+        f"{what} failed with status {status}"
     if status in (SB_ERR_BAD_ARG, SB_ERR_RANGE):
         raise ValueError(msg)
     if status == SB_ERR_NONCONVERGENCE:

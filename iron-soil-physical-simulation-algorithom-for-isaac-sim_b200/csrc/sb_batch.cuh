@@ -1,0 +1,250 @@
+// Batched Mobile V2 runtime: many independent terrain patches (parallel dig
+// environments of uneven sizes) advanced by the same launches.
+//
+// Every patch keeps its own quantisation, CFL substep dt, substep count and
+// ping-pong parity (the per-patch loop of MobileV2ReferenceSolver.step,
+// experimental/mobile_v2_reference.py:191-314).  A patch table drives the
+// launches:
+//   * FV work items are warps (one 30-column strip x rows_per_warp rows of one
+//     patch, the same strip code as the single-grid kernel); item_patch maps
+//     a global warp index to its patch, and rows_per_warp is chosen per patch
+//     by the autotuner;
+//   * ledger work items are CTAs over bands of kBandRows rows of one patch.
+// Each substep round is two launches: all active patches' strips, then one
+// warp per patch that reduces that patch's item partials in a fixed order,
+// advances its loop control and plans its next dt; the last CTA of that
+// launch sets the graph's while-condition to "some patch still active".
+// The arithmetic is the single-grid FX32 kernel's, so every patch's fields
+// are identical to stepping it alone.
+#pragma once
+
+#include "sb_ledger.cuh"
+
+namespace sb {
+
+constexpr int kBandRows = 32;  // ledger band height (one CTA per band)
+
+struct BatchPatch {
+  FvConst c;          // geometry (ny, nx, pitch, strips in tiles_x, rows_per_warp) + constants
+  long long base;     // element offset of the patch's row 0 in the field arenas
+  double datum;       // support datum of the patch's b / z quanta
+  double static_limit;
+  int first_item, n_items;  // FV warps
+  int first_band, n_bands;  // ledger CTAs
+};
+
+struct BatchCtl {  // per patch, device resident
+  FvControl k;
+  LedgerOut before;
+  LedgerOut after;
+};
+
+struct BatchGlobal {
+  unsigned arrive;
+  int active;
+};
+
+struct BatchArena {
+  const int32_t* b;
+  const int32_t* z;
+  int32_t* h[2];
+  float* qx[2];
+  float* qy[2];
+};
+
+__global__ void batch_begin_kernel(int npatch, BatchCtl* ctl, const double* dt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npatch) return;
+  FvControl& k = ctl[p].k;
+  k.remaining = *dt;
+  k.sub_dt = 0.0;
+  k.max_cfl = 0.0;
+  k.wave = 0.0;
+  for (int i = 0; i < kFvDiag; ++i) k.diag[i] = 0.0;
+  k.substeps = 0;
+  k.done = 0;
+  k.status = 0;
+  k.cfl_limited = 0;
+  k.static_skip = 0;
+  k.arrive = 0;
+  k.wait_fail = 0;
+}
+
+// One CTA per ledger band.
+__global__ void __launch_bounds__(kThreads)
+    batch_ledger_kernel(const BatchPatch* __restrict__ patches, const int* __restrict__ band_patch,
+                        int nbands, BatchArena a, const BatchCtl* __restrict__ ctl,
+                        double* __restrict__ partials, long long* __restrict__ ipartials) {
+  __shared__ double red[kThreads / 32 * L_NP];
+  __shared__ long long ired[kThreads / 32 * kLedgerI64];
+  const int band = blockIdx.x;
+  if (band >= nbands) return;
+  const int p = band_patch[band];
+  const BatchPatch& P = patches[p];
+  const FvConst c = P.c;
+  const int parity = ctl[p].k.parity;
+  const long long base = P.base;
+  const int r0 = (band - P.first_band) * kBandRows;
+  const int r1 = min(r0 + kBandRows, c.ny);
+  double v[L_NP];
+#pragma unroll
+  for (int k = 0; k < L_NP; ++k) v[k] = 0.0;
+  v[L_NEGMINH] = -1.0e300;
+  long long iq0 = 0, iq1 = 0, iq2 = 0;
+  const int n = (r1 - r0) * c.nx;
+  for (int i = threadIdx.x; i < n; i += kThreads)
+    ledger_cell<true>(c, a.b + base, a.z + base, a.h[parity] + base, a.qx[parity] + base,
+                      a.qy[parity] + base, nullptr, nullptr, P.datum, r0 + i / c.nx, i % c.nx, v,
+                      iq0, iq1, iq2);
+  ledger_block_store(v, iq0, iq1, iq2, red, ired, partials + (size_t)band * L_NP,
+                     ipartials + (size_t)band * kLedgerI64);
+}
+
+// One warp per patch: fixed-order fold of the patch's band partials into its
+// ledger; mode 0 also runs the prologue (static check, first dt) and counts
+// the patches that have substeps to run.
+__global__ void __launch_bounds__(kThreads)
+    batch_ledger_finish_kernel(int npatch, const BatchPatch* __restrict__ patches,
+                               BatchCtl* ctl, const double* __restrict__ partials,
+                               const long long* __restrict__ ipartials, int mode, BatchGlobal* g,
+                               cudaGraphConditionalHandle handle, int use_handle) {
+  __shared__ int last;
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (p < npatch) {
+    const BatchPatch& P = patches[p];
+    double v[L_NP];
+#pragma unroll
+    for (int k = 0; k < L_NP; ++k) v[k] = 0.0;
+    v[L_NEGMINH] = -1.0e300;
+    long long iq[kLedgerI64] = {0, 0, 0};
+    for (int j = lane; j < P.n_bands; j += 32) {
+      const size_t bidx = (size_t)(P.first_band + j);
+#pragma unroll
+      for (int k = 0; k < L_NP; ++k) {
+        const double x = partials[bidx * L_NP + k];
+        v[k] = k < L_NSUM ? v[k] + x : fmax(v[k], x);
+      }
+      for (int k = 0; k < kLedgerI64; ++k) iq[k] += ipartials[bidx * kLedgerI64 + k];
+    }
+#pragma unroll
+    for (int k = 0; k < L_NP; ++k) v[k] = k < L_NSUM ? warp_sum(v[k]) : warp_max(v[k]);
+    for (int k = 0; k < kLedgerI64; ++k) iq[k] = (long long)warp_sum_u64((unsigned long long)iq[k]);
+    if (lane == 0) {
+      LedgerOut* out = mode == 0 ? &ctl[p].before : &ctl[p].after;
+      for (int k = 0; k < L_NP; ++k) out->v[k] = ledger_final_value<true>(k, v[k]);
+      for (int k = 0; k < kLedgerI64; ++k) out->iq[k] = iq[k];
+      if (mode == 0) {
+        ledger_prologue(P.c, out, P.static_limit, &ctl[p].k);
+        if (!ctl[p].k.done) atomicAdd(&g->active, 1);
+      }
+    }
+  }
+  if (mode != 0) return;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&g->arrive, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const int active = *(volatile int*)&g->active;
+    g->arrive = 0;
+    g->active = 0;
+    __threadfence();
+    if (use_handle) cudaGraphSetConditional(handle, active > 0 ? 1u : 0u);
+  }
+}
+
+// One substep of every active patch; a warp per work item.
+__global__ void __launch_bounds__(kThreads, 3)
+    batch_fv_kernel(const BatchPatch* __restrict__ patches, const int* __restrict__ item_patch,
+                    int nitems, BatchArena a, const BatchCtl* __restrict__ ctl,
+                    double* __restrict__ item_partials) {
+  const int gw = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  if (gw >= nitems) return;  // warp-uniform
+  const int p = item_patch[gw];
+  if (ctl[p].k.done) return;
+  const BatchPatch& P = patches[p];
+  const FvConst& c = P.c;  // read through the read-only cache, not copied
+  const long long base = P.base;
+  const double sub_dt = ctl[p].k.sub_dt;
+  const int parity = ctl[p].k.parity;
+  const int local = gw - P.first_item;
+  double acc[kFvDiag];
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
+  double wave = 0.0;
+  fx_strip_run(c, a.b + base, a.h[parity] + base, a.qx[parity] + base, a.qy[parity] + base,
+               a.h[parity ^ 1] + base, a.qx[parity ^ 1] + base, a.qy[parity ^ 1] + base, nullptr,
+               nullptr, local % c.tiles_x, (local / c.tiles_x) * c.rows_per_warp, sub_dt, acc,
+               wave);
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) acc[k] = warp_sum(acc[k]);
+  wave = warp_max(wave);
+  if ((threadIdx.x & 31) == 0) {
+    double* out = item_partials + (size_t)gw * (kFvDiag + 1);
+    for (int k = 0; k < kFvDiag; ++k) out[k] = acc[k];
+    out[kFvDiag] = wave;
+  }
+}
+
+// End of a substep round: one warp per still-active patch folds its item
+// partials (fixed order) and advances the patch's loop control exactly as
+// the single-grid last-block finalisation does.
+__global__ void __launch_bounds__(kThreads)
+    batch_round_kernel(int npatch, const BatchPatch* __restrict__ patches, BatchCtl* ctl,
+                       const double* __restrict__ item_partials, BatchGlobal* g,
+                       cudaGraphConditionalHandle handle, int use_handle) {
+  __shared__ int last;
+  const int lane = threadIdx.x & 31;
+  const int p = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+  // the warp's lanes agree on the patch's state before lane 0 updates it
+  int run = 0;
+  if (p < npatch) run = __shfl_sync(0xffffffffu, lane == 0 ? !ctl[p].k.done : 0, 0);
+  if (run) {
+    const BatchPatch& P = patches[p];
+    double v[kFvDiag + 1];
+#pragma unroll
+    for (int k = 0; k <= kFvDiag; ++k) v[k] = 0.0;
+    for (int j = lane; j < P.n_items; j += 32) {
+      const double* in = item_partials + (size_t)(P.first_item + j) * (kFvDiag + 1);
+#pragma unroll
+      for (int k = 0; k < kFvDiag; ++k) v[k] += in[k];
+      v[kFvDiag] = fmax(v[kFvDiag], in[kFvDiag]);
+    }
+#pragma unroll
+    for (int k = 0; k < kFvDiag; ++k) v[k] = warp_sum(v[k]);
+    v[kFvDiag] = warp_max(v[kFvDiag]);
+    if (lane == 0) {
+      FvControl* k = &ctl[p].k;
+      for (int i = 0; i < kFvDiag; ++i) k->diag[i] += v[i];
+      k->substeps += 1;
+      k->remaining -= k->sub_dt;
+      k->parity ^= 1;
+      k->wave = v[kFvDiag];
+      if (!(k->remaining > 1.0e-14)) {
+        k->done = 1;
+      } else if (k->substeps >= P.c.max_substeps) {
+        k->status = 2;  // SB_ERR_SUBSTEP_CAP
+        k->done = 1;
+      } else {
+        plan_substep(P.c, k);
+      }
+      if (!k->done) atomicAdd(&g->active, 1);
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&g->arrive, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    const int active = *(volatile int*)&g->active;
+    g->arrive = 0;
+    g->active = 0;
+    __threadfence();
+    if (use_handle) cudaGraphSetConditional(handle, active > 0 ? 1u : 0u);
+  }
+}
+
+}  // namespace sb

@@ -607,6 +607,132 @@ __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
   x.cel = sqrtf(c.KGf * hf);
 }
 
+// One warp's strip: columns strip*30-1 .. strip*30+30, rows y0 .. y0+rows-1
+// of a grid whose row 0 starts at the given field pointers (row pitch
+// c.pitch).  Accumulates the impulse/energy sums into acc and the largest
+// next-substep wave speed into wave.  Every lane of the warp must call it.
+__device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __restrict__ bsrc,
+                                             const int32_t* __restrict__ hsrc,
+                                             const float* __restrict__ qxsrc,
+                                             const float* __restrict__ qysrc,
+                                             int32_t* __restrict__ hdst, float* __restrict__ qxdst,
+                                             float* __restrict__ qydst,
+                                             const float* __restrict__ ext_x,
+                                             const float* __restrict__ ext_y, int strip, int y0,
+                                             double sub_dt, double* acc, double& wave) {
+  const int lane = threadIdx.x & 31;
+  const int y1 = min(y0 + c.rows_per_warp, c.ny);
+  const int gx = strip * kStripOut - 1 + lane;
+  const bool colok = gx >= 0 && gx < c.nx;
+  const bool out_lane = lane >= 1 && lane <= kStripOut && colok;
+  const bool east_ok = gx >= 0 && gx + 1 < c.nx && lane < 31;
+  const float lamx_f = (float)(sub_dt / c.dx);
+  const float lamy_f = (float)(sub_dt / c.dy);
+  const float dtf = (float)sub_dt;
+  const float dec = (float)(c.mu_g * sub_dt);
+  if (y0 >= c.ny) return;  // warp-uniform
+  FxCell cur, nxt, nn;
+  fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0, gx, colok, cur);
+  fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 + 1, gx, colok, nxt);
+  // south face of the first row (the previous row's north face)
+  int ms = 0;
+  float nts = 0.f, nnps = 0.f;
+  {
+    FxCell prv;
+    fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 - 1, gx, colok, prv);
+    fx_prepare(c, prv);
+    fx_prepare(c, cur);
+    if (y0 > 0 && colok) {
+      float fnm;
+      face_fx(c, lamy_f, prv.b, cur.b, prv.h, cur.h, prv.v, prv.u, cur.v, cur.u, prv.cel,
+              cur.cel, ms, fnm, nnps, nts);
+    }
+  }
+  fx_prepare(c, nxt);
+  for (int r = y0; r < y1; ++r) {
+    fx_load(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
+    // east face: this column and the next lane's
+    const int eb = __shfl_down_sync(0xffffffffu, cur.b, 1);
+    const int eh = __shfl_down_sync(0xffffffffu, cur.h, 1);
+    const float eu = __shfl_down_sync(0xffffffffu, cur.u, 1);
+    const float ev = __shfl_down_sync(0xffffffffu, cur.v, 1);
+    const float ec = __shfl_down_sync(0xffffffffu, cur.cel, 1);
+    int me = 0;
+    float enm = 0.f, enp = 0.f, et = 0.f;
+    if (east_ok)
+      face_fx(c, lamx_f, cur.b, eb, cur.h, eh, cur.u, cur.v, eu, ev, cur.cel, ec, me, enm, enp,
+              et);
+    // west face = the previous lane's east face
+    const int mw = __shfl_up_sync(0xffffffffu, me, 1);
+    const float enpw = __shfl_up_sync(0xffffffffu, enp, 1);
+    const float etw = __shfl_up_sync(0xffffffffu, et, 1);
+    // north face: this row and the next
+    int mn = 0;
+    float nnm = 0.f, nnp = 0.f, nt = 0.f;
+    if (colok && r + 1 < c.ny)
+      face_fx(c, lamy_f, cur.b, nxt.b, cur.h, nxt.h, cur.v, cur.u, nxt.v, nxt.u, cur.cel,
+              nxt.cel, mn, nnm, nnp, nt);
+    if (out_lane) {
+      const size_t gi = (size_t)r * c.pitch + gx;
+      float ax = 0.f, ay = 0.f;
+      if (c.has_external) {
+        ax = ext_x[gi];
+        ay = ext_y[gi];
+      }
+      const int dh = ((0 - me + mw) - mn) + ms;
+      const int hq = cur.h + dh;
+      const float zero = 0.f;
+      const float dqx = (((zero - lamx_f * enm) + lamx_f * enpw) - lamy_f * nt) + lamy_f * nts;
+      const float dqy = (((zero - lamx_f * et) + lamx_f * etw) - lamy_f * nnm) + lamy_f * nnps;
+      const float hn = (float)hq * c.Qf;
+      const bool wet = hn > c.dryf;
+      const float qxn = wet ? cur.qx + dqx : 0.f;
+      const float qyn = wet ? cur.qy + dqy : 0.f;
+      float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
+      if (wet) {
+        const float inv = 1.0f / hn;
+        vbx = qxn * inv;
+        vby = qyn * inv;
+        if (c.has_external) {
+          qex = qxn + (hn * ax) * dtf;
+          qey = qyn + (hn * ay) * dtf;
+          vex = qex * inv;
+          vey = qey * inv;
+        } else {
+          vex = vbx;
+          vey = vby;
+        }
+      }
+      const float spd = sqrtf(vex * vex + vey * vey);
+      const float fac = fmaxf(0.f, 1.f - dec / fmaxf(spd, 1.0e-15f));
+      const float vax = vex * fac, vay = vey * fac;
+      const float qxo = hn * vax, qyo = hn * vay;
+      hdst[gi] = hq;
+      qxdst[gi] = qxo;
+      qydst[gi] = qyo;
+      const double h64 = (double)hn;
+      acc[0] += (double)qxn - (double)cur.qx;
+      acc[1] += (double)qyn - (double)cur.qy;
+      acc[2] += (double)qex - (double)qxn;
+      acc[3] += (double)qey - (double)qyn;
+      acc[4] += (double)qxo - (double)qex;
+      acc[5] += (double)qyo - (double)qey;
+      acc[6] += 0.5 * h64 *
+                ((double)spd * (double)spd - ((double)vax * (double)vax + (double)vay * (double)vay));
+      acc[7] += h64 * ((0.5 * ((double)vbx + (double)vex)) * (double)ax +
+                       (0.5 * ((double)vby + (double)vey)) * (double)ay) * sub_dt;
+      const float wv = spd * fac + sqrtf(c.KGf * hn);  // |new velocity| + celerity
+      wave = fmax(wave, (double)wv);
+    }
+    ms = mn;
+    nts = nt;
+    nnps = nnp;
+    cur = nxt;
+    nxt = nn;
+    fx_prepare(c, nxt);
+  }
+}
+
 __global__ void __launch_bounds__(kThreads, 4)
     fv_stream_kernel(const FvConst c, const int32_t* __restrict__ bsrc, int32_t* __restrict__ h0,
                      int32_t* __restrict__ h1, float* __restrict__ qx0, float* __restrict__ qx1,
@@ -619,134 +745,14 @@ __global__ void __launch_bounds__(kThreads, 4)
   if (*(volatile int*)&ctl->done) return;  // uniform across the grid
   const double sub_dt = ctl->sub_dt;
   const int parity = ctl->parity;
-  const int32_t* __restrict__ hsrc = parity ? h1 : h0;
-  const float* __restrict__ qxsrc = parity ? qx1 : qx0;
-  const float* __restrict__ qysrc = parity ? qy1 : qy0;
-  int32_t* __restrict__ hdst = parity ? h0 : h1;
-  float* __restrict__ qxdst = parity ? qx0 : qx1;
-  float* __restrict__ qydst = parity ? qy0 : qy1;
-
-  const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
-  const int strip = gw % c.tiles_x;
-  const int y0 = (gw / c.tiles_x) * c.rows_per_warp;
-  const int y1 = min(y0 + c.rows_per_warp, c.ny);
-  const int gx = strip * kStripOut - 1 + lane;
-  const bool colok = gx >= 0 && gx < c.nx;
-  const bool out_lane = lane >= 1 && lane <= kStripOut && colok;
-  const bool east_ok = gx >= 0 && gx + 1 < c.nx && lane < 31;
-  const float lamx_f = (float)(sub_dt / c.dx);
-  const float lamy_f = (float)(sub_dt / c.dy);
-  const float dtf = (float)sub_dt;
-  const float dec = (float)(c.mu_g * sub_dt);
-
   double acc[kFvDiag];
 #pragma unroll
   for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
   double wave = 0.0;
-
-  if (y0 < c.ny) {  // warp-uniform
-    FxCell cur, nxt, nn;
-    fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0, gx, colok, cur);
-    fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 + 1, gx, colok, nxt);
-    // south face of the first row (the previous row's north face)
-    int ms = 0;
-    float nts = 0.f, nnps = 0.f;
-    {
-      FxCell prv;
-      fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 - 1, gx, colok, prv);
-      fx_prepare(c, prv);
-      fx_prepare(c, cur);
-      if (y0 > 0 && colok) {
-        float fnm;
-        face_fx(c, lamy_f, prv.b, cur.b, prv.h, cur.h, prv.v, prv.u, cur.v, cur.u, prv.cel,
-                cur.cel, ms, fnm, nnps, nts);
-      }
-    }
-    fx_prepare(c, nxt);
-    for (int r = y0; r < y1; ++r) {
-      fx_load(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
-      // east face: this column and the next lane's
-      const int eb = __shfl_down_sync(0xffffffffu, cur.b, 1);
-      const int eh = __shfl_down_sync(0xffffffffu, cur.h, 1);
-      const float eu = __shfl_down_sync(0xffffffffu, cur.u, 1);
-      const float ev = __shfl_down_sync(0xffffffffu, cur.v, 1);
-      const float ec = __shfl_down_sync(0xffffffffu, cur.cel, 1);
-      int me = 0;
-      float enm = 0.f, enp = 0.f, et = 0.f;
-      if (east_ok)
-        face_fx(c, lamx_f, cur.b, eb, cur.h, eh, cur.u, cur.v, eu, ev, cur.cel, ec, me, enm, enp,
-                et);
-      // west face = the previous lane's east face
-      const int mw = __shfl_up_sync(0xffffffffu, me, 1);
-      const float enpw = __shfl_up_sync(0xffffffffu, enp, 1);
-      const float etw = __shfl_up_sync(0xffffffffu, et, 1);
-      // north face: this row and the next
-      int mn = 0;
-      float nnm = 0.f, nnp = 0.f, nt = 0.f;
-      if (colok && r + 1 < c.ny)
-        face_fx(c, lamy_f, cur.b, nxt.b, cur.h, nxt.h, cur.v, cur.u, nxt.v, nxt.u, cur.cel,
-                nxt.cel, mn, nnm, nnp, nt);
-      if (out_lane) {
-        const size_t gi = (size_t)r * c.pitch + gx;
-        float ax = 0.f, ay = 0.f;
-        if (c.has_external) {
-          ax = ext_x[gi];
-          ay = ext_y[gi];
-        }
-        const int dh = ((0 - me + mw) - mn) + ms;
-        const int hq = cur.h + dh;
-        const float zero = 0.f;
-        const float dqx = (((zero - lamx_f * enm) + lamx_f * enpw) - lamy_f * nt) + lamy_f * nts;
-        const float dqy = (((zero - lamx_f * et) + lamx_f * etw) - lamy_f * nnm) + lamy_f * nnps;
-        const float hn = (float)hq * c.Qf;
-        const bool wet = hn > c.dryf;
-        const float qxn = wet ? cur.qx + dqx : 0.f;
-        const float qyn = wet ? cur.qy + dqy : 0.f;
-        float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
-        if (wet) {
-          const float inv = 1.0f / hn;
-          vbx = qxn * inv;
-          vby = qyn * inv;
-          if (c.has_external) {
-            qex = qxn + (hn * ax) * dtf;
-            qey = qyn + (hn * ay) * dtf;
-            vex = qex * inv;
-            vey = qey * inv;
-          } else {
-            vex = vbx;
-            vey = vby;
-          }
-        }
-        const float spd = sqrtf(vex * vex + vey * vey);
-        const float fac = fmaxf(0.f, 1.f - dec / fmaxf(spd, 1.0e-15f));
-        const float vax = vex * fac, vay = vey * fac;
-        const float qxo = hn * vax, qyo = hn * vay;
-        hdst[gi] = hq;
-        qxdst[gi] = qxo;
-        qydst[gi] = qyo;
-        const double h64 = (double)hn;
-        acc[0] += (double)qxn - (double)cur.qx;
-        acc[1] += (double)qyn - (double)cur.qy;
-        acc[2] += (double)qex - (double)qxn;
-        acc[3] += (double)qey - (double)qyn;
-        acc[4] += (double)qxo - (double)qex;
-        acc[5] += (double)qyo - (double)qey;
-        acc[6] += 0.5 * h64 *
-                  ((double)spd * (double)spd - ((double)vax * (double)vax + (double)vay * (double)vay));
-        acc[7] += h64 * ((0.5 * ((double)vbx + (double)vex)) * (double)ax +
-                         (0.5 * ((double)vby + (double)vey)) * (double)ay) * sub_dt;
-        const float wv = spd * fac + sqrtf(c.KGf * hn);  // |new velocity| + celerity
-        wave = fmax(wave, (double)wv);
-      }
-      ms = mn;
-      nts = nt;
-      nnps = nnp;
-      cur = nxt;
-      nxt = nn;
-      fx_prepare(c, nxt);
-    }
-  }
+  fx_strip_run(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
+               parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x, ext_y,
+               gw % c.tiles_x, (gw / c.tiles_x) * c.rows_per_warp, sub_dt, acc, wave);
   fv_finish(c, ctl, partials, acc, wave, 0, red, &flag, sub_dt, parity, loop_handle, use_handle);
 }
 

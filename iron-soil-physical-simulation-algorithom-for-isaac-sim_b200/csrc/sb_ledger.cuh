@@ -32,6 +32,165 @@ struct StepIO {  // per-step device record: ledgers before/after + loop control
   LedgerOut after;
 };
 
+// Ledger contributions of cell (r, col): sums into v[0 .. L_NSUM), maxima
+// into v[L_NSUM .. L_NP), exact quanta sums into iq0..iq2 (FX).
+template <bool FX>
+__device__ __forceinline__ void ledger_cell(const FvConst& c,
+                                            const typename FvTypes<FX>::B* __restrict__ b,
+                                            const typename FvTypes<FX>::B* __restrict__ z,
+                                            const typename FvTypes<FX>::H* __restrict__ h,
+                                            const typename FvTypes<FX>::R* __restrict__ qx,
+                                            const typename FvTypes<FX>::R* __restrict__ qy,
+                                            const typename FvTypes<FX>::R* __restrict__ ext_x,
+                                            const typename FvTypes<FX>::R* __restrict__ ext_y,
+                                            double datum, int r, int col, double* v,
+                                            long long& iq0, long long& iq1, long long& iq2) {
+  const size_t gi = (size_t)r * c.pitch + col;
+  const int w6 = vertex_weight6(r, col, c.ny, c.nx);
+  double hv, bv;
+  const double qxv = (double)qx[gi], qyv = (double)qy[gi];
+  // gradient of the free surface b + h (np.gradient, edge_order 1)
+  const int cl = col > 0 ? col - 1 : col, cr = col + 1 < c.nx ? col + 1 : col;
+  const int rd = r > 0 ? r - 1 : r, ru = r + 1 < c.ny ? r + 1 : r;
+  const double denx = (col > 0 && col + 1 < c.nx) ? 2.0 * c.dx : c.dx;
+  const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
+  const size_t il = (size_t)r * c.pitch + cl, ir = (size_t)r * c.pitch + cr;
+  const size_t idn = (size_t)rd * c.pitch + col, iup = (size_t)ru * c.pitch + col;
+  double grad;  // FX: squared gradient (sqrt taken once, after the max)
+  if constexpr (FX) {
+    const int hq = h[gi];
+    hv = (double)hq * c.Q;
+    bv = (double)b[gi] * c.Q + datum;
+    iq0 += hq;
+    iq1 += (long long)hq * w6;
+    const long long rest = (long long)b[gi] - (long long)z[gi];
+    iq2 += (rest > 0 ? rest : 0) * w6;
+    const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
+    const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
+    // (H difference) * Q / spacing with the spacing folded into one constant
+    const double gx = (double)(Hr - Hl) * ((col > 0 && col + 1 < c.nx) ? c.Q / (2.0 * c.dx) : c.Q / c.dx);
+    const double gy = (double)(Hu - Hd) * ((r > 0 && r + 1 < c.ny) ? c.Q / (2.0 * c.dy) : c.Q / c.dy);
+    grad = gx * gx + gy * gy;
+  } else {
+    hv = h[gi];
+    bv = b[gi];
+    v[L_HSUM] += hv;
+    v[L_HSUM_W] += hv * w6;
+    v[L_REST_W] += fmax(b[gi] - z[gi], 0.0) * w6;
+    const double gx = ((b[ir] + h[ir]) - (b[il] + h[il])) / denx;
+    const double gy = ((b[iup] + h[iup]) - (b[idn] + h[idn])) / deny;
+    grad = hypot(gx, gy);
+  }
+  const bool wet = hv > c.dry;
+  double s2 = 0.0, spd = 0.0, e = 0.0, wave;
+  if constexpr (FX) {
+    const float hn = (float)h[gi] * c.Qf;
+    float vx = 0.f, vy = 0.f;
+    if (hn > c.dryf) {
+      const float inv = 1.0f / hn;
+      vx = qx[gi] * inv;
+      vy = qy[gi] * inv;
+    }
+    wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
+    if (wet) {  // one reciprocal: e = |q|^2 / h (= h |u|^2), s2 = e / h
+      const double inv = 1.0 / hv;
+      e = (qxv * qxv + qyv * qyv) * inv;
+      s2 = e * inv;
+    }
+    spd = s2;  // squared speed; sqrt after the max
+  } else {
+    double vx = 0.0, vy = 0.0;
+    if (wet) {
+      vx = qxv / hv;
+      vy = qyv / hv;
+    }
+    wave = sqrt(vx * vx + vy * vy) + sqrt(c.kg * fmax(hv, 0.0));
+    if (wet) {
+      s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
+      spd = sqrt(s2);
+      e = hv * s2;
+    }
+  }
+  v[L_QX] += qxv;
+  v[L_QY] += qyv;
+  v[L_QX_W] += qxv * w6;
+  v[L_QY_W] += qyv * w6;
+  v[L_HS2] += e;
+  v[L_HS2_W] += e * w6;
+  v[L_HB] += hv * bv;
+  v[L_HB_W] += hv * bv * w6;
+  v[L_HH] += hv * hv;
+  v[L_HH_W] += hv * hv * w6;
+  v[L_MAXSPEED] = fmax(v[L_MAXSPEED], spd);
+  v[L_NEGMINH] = fmax(v[L_NEGMINH], -hv);
+  v[L_MAXQ] = fmax(v[L_MAXQ], fmax(fabs(qxv), fabs(qyv)));
+  v[L_MAXGRAD] = fmax(v[L_MAXGRAD], grad);
+  v[L_MAXWAVE] = fmax(v[L_MAXWAVE], wave);
+  if (c.has_external)
+    v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
+}
+
+// Block reduction of per-thread ledger values into one block's partials
+// (L_NP doubles at part, kLedgerI64 integers at ipart), in a fixed order.
+__device__ __forceinline__ void ledger_block_store(double* v, long long iq0, long long iq1,
+                                                   long long iq2, double* red, long long* ired,
+                                                   double* part, long long* ipart) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < L_NP; ++k) v[k] = k < L_NSUM ? warp_sum(v[k]) : warp_max(v[k]);
+  iq0 = (long long)warp_sum_u64((unsigned long long)iq0);
+  iq1 = (long long)warp_sum_u64((unsigned long long)iq1);
+  iq2 = (long long)warp_sum_u64((unsigned long long)iq2);
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < L_NP; ++k) red[warp * L_NP + k] = v[k];
+    ired[warp * kLedgerI64] = iq0;
+    ired[warp * kLedgerI64 + 1] = iq1;
+    ired[warp * kLedgerI64 + 2] = iq2;
+  }
+  __syncthreads();
+  if (threadIdx.x < L_NP) {
+    const int k = threadIdx.x;
+    double a = k == L_NEGMINH ? -1.0e300 : 0.0;
+    for (int w = 0; w < kThreads / 32; ++w)
+      a = k < L_NSUM ? a + red[w * L_NP + k] : fmax(a, red[w * L_NP + k]);
+    part[k] = a;
+  } else if (threadIdx.x < L_NP + kLedgerI64) {
+    const int k = threadIdx.x - L_NP;
+    long long a = 0;
+    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + k];
+    ipart[k] = a;
+  }
+}
+
+// Final value of ledger slot k: the FX path accumulates squared gradient and
+// squared speed maxima and takes the (monotone) square root after the max.
+template <bool FX>
+__device__ __forceinline__ double ledger_final_value(int k, double val) {
+  if (FX && (k == L_MAXGRAD || k == L_MAXSPEED)) return sqrt(val);
+  return val;
+}
+
+// Static short-circuit and the first substep's dt from a "before" ledger
+// (reference step :199-205, :239-253).  One thread.
+__device__ __forceinline__ void ledger_prologue(const FvConst& c, const LedgerOut* out,
+                                                double static_limit, FvControl* ctl) {
+  const bool no_ext = !c.has_external || out->v[L_MAXEXT] <= 1.0e-14;
+  const bool is_static = no_ext && out->v[L_MAXQ] <= 1.0e-14 && out->v[L_MAXGRAD] <= static_limit;
+  ctl->wave = out->v[L_MAXWAVE];
+  if (is_static) {
+    ctl->static_skip = 1;
+    ctl->done = 1;
+  } else if (!(ctl->remaining > 1.0e-14)) {
+    ctl->done = 1;
+  } else if (c.max_substeps <= 0) {
+    ctl->status = 2;
+    ctl->done = 1;
+  } else {
+    plan_substep(c, ctl);
+  }
+}
+
 template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     ledger_kernel(const FvConst c, const typename FvTypes<FX>::B* __restrict__ b,
@@ -59,122 +218,15 @@ __global__ void __launch_bounds__(kThreads)
   long long iq0 = 0, iq1 = 0, iq2 = 0;
   const long long ncell = (long long)c.ny * c.nx;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncell;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int r = (int)(i / c.nx), col = (int)(i % c.nx);
-    const size_t gi = (size_t)r * c.pitch + col;
-    const int w6 = vertex_weight6(r, col, c.ny, c.nx);
-    double hv, bv;
-    const double qxv = (double)qx[gi], qyv = (double)qy[gi];
-    // gradient of the free surface b + h (np.gradient, edge_order 1)
-    const int cl = col > 0 ? col - 1 : col, cr = col + 1 < c.nx ? col + 1 : col;
-    const int rd = r > 0 ? r - 1 : r, ru = r + 1 < c.ny ? r + 1 : r;
-    const double denx = (col > 0 && col + 1 < c.nx) ? 2.0 * c.dx : c.dx;
-    const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
-    const size_t il = (size_t)r * c.pitch + cl, ir = (size_t)r * c.pitch + cr;
-    const size_t idn = (size_t)rd * c.pitch + col, iup = (size_t)ru * c.pitch + col;
-    double grad;  // FX: squared gradient (sqrt taken once, after the max)
-    if constexpr (FX) {
-      const int hq = h[gi];
-      hv = (double)hq * c.Q;
-      bv = (double)b[gi] * c.Q + datum;
-      iq0 += hq;
-      iq1 += (long long)hq * w6;
-      const long long rest = (long long)b[gi] - (long long)z[gi];
-      iq2 += (rest > 0 ? rest : 0) * w6;
-      const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
-      const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
-      // (H difference) * Q / spacing with the spacing folded into one constant
-      const double gx = (double)(Hr - Hl) * ((col > 0 && col + 1 < c.nx) ? c.Q / (2.0 * c.dx) : c.Q / c.dx);
-      const double gy = (double)(Hu - Hd) * ((r > 0 && r + 1 < c.ny) ? c.Q / (2.0 * c.dy) : c.Q / c.dy);
-      grad = gx * gx + gy * gy;
-    } else {
-      hv = h[gi];
-      bv = b[gi];
-      v[L_HSUM] += hv;
-      v[L_HSUM_W] += hv * w6;
-      v[L_REST_W] += fmax(b[gi] - z[gi], 0.0) * w6;
-      const double gx = ((b[ir] + h[ir]) - (b[il] + h[il])) / denx;
-      const double gy = ((b[iup] + h[iup]) - (b[idn] + h[idn])) / deny;
-      grad = hypot(gx, gy);
-    }
-    const bool wet = hv > c.dry;
-    double s2 = 0.0, spd = 0.0, e = 0.0, wave;
-    if constexpr (FX) {
-      const float hn = (float)h[gi] * c.Qf;
-      float vx = 0.f, vy = 0.f;
-      if (hn > c.dryf) {
-        const float inv = 1.0f / hn;
-        vx = qx[gi] * inv;
-        vy = qy[gi] * inv;
-      }
-      wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
-      if (wet) {  // one reciprocal: e = |q|^2 / h (= h |u|^2), s2 = e / h
-        const double inv = 1.0 / hv;
-        e = (qxv * qxv + qyv * qyv) * inv;
-        s2 = e * inv;
-      }
-      spd = s2;  // squared speed; sqrt after the max
-    } else {
-      double vx = 0.0, vy = 0.0;
-      if (wet) {
-        vx = qxv / hv;
-        vy = qyv / hv;
-      }
-      wave = sqrt(vx * vx + vy * vy) + sqrt(c.kg * fmax(hv, 0.0));
-      if (wet) {
-        s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
-        spd = sqrt(s2);
-        e = hv * s2;
-      }
-    }
-    v[L_QX] += qxv;
-    v[L_QY] += qyv;
-    v[L_QX_W] += qxv * w6;
-    v[L_QY_W] += qyv * w6;
-    v[L_HS2] += e;
-    v[L_HS2_W] += e * w6;
-    v[L_HB] += hv * bv;
-    v[L_HB_W] += hv * bv * w6;
-    v[L_HH] += hv * hv;
-    v[L_HH_W] += hv * hv * w6;
-    v[L_MAXSPEED] = fmax(v[L_MAXSPEED], spd);
-    v[L_NEGMINH] = fmax(v[L_NEGMINH], -hv);
-    v[L_MAXQ] = fmax(v[L_MAXQ], fmax(fabs(qxv), fabs(qyv)));
-    v[L_MAXGRAD] = fmax(v[L_MAXGRAD], grad);
-    v[L_MAXWAVE] = fmax(v[L_MAXWAVE], wave);
-    if (c.has_external)
-      v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
-  }
-  // block reduction
+       i += (long long)gridDim.x * blockDim.x)
+    ledger_cell<FX>(c, b, z, h, qx, qy, ext_x, ext_y, datum, (int)(i / c.nx), (int)(i % c.nx), v,
+                    iq0, iq1, iq2);
   __shared__ double red[kThreads / 32 * L_NP];
   __shared__ long long ired[kThreads / 32 * kLedgerI64];
   __shared__ int last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < L_NP; ++k) v[k] = k < L_NSUM ? warp_sum(v[k]) : warp_max(v[k]);
-  iq0 = (long long)warp_sum_u64((unsigned long long)iq0);
-  iq1 = (long long)warp_sum_u64((unsigned long long)iq1);
-  iq2 = (long long)warp_sum_u64((unsigned long long)iq2);
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < L_NP; ++k) red[warp * L_NP + k] = v[k];
-    ired[warp * kLedgerI64] = iq0;
-    ired[warp * kLedgerI64 + 1] = iq1;
-    ired[warp * kLedgerI64 + 2] = iq2;
-  }
-  __syncthreads();
-  if (threadIdx.x < L_NP) {
-    const int k = threadIdx.x;
-    double a = k == L_NEGMINH ? -1.0e300 : 0.0;
-    for (int w = 0; w < kThreads / 32; ++w)
-      a = k < L_NSUM ? a + red[w * L_NP + k] : fmax(a, red[w * L_NP + k]);
-    partials[(size_t)blockIdx.x * L_NP + k] = a;
-  } else if (threadIdx.x < L_NP + kLedgerI64) {
-    const int k = threadIdx.x - L_NP;
-    long long a = 0;
-    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + k];
-    ipartials[(size_t)blockIdx.x * kLedgerI64 + k] = a;
-  }
+  ledger_block_store(v, iq0, iq1, iq2, red, ired, partials + (size_t)blockIdx.x * L_NP,
+                     ipartials + (size_t)blockIdx.x * kLedgerI64);
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = (atomicAdd(arrive, 1u) == gridDim.x - 1) ? 1 : 0;
@@ -199,10 +251,7 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
   if (threadIdx.x < L_NP) {
-    double val = tot[threadIdx.x];
-    // FX accumulates squared gradient / speed maxima; monotone sqrt after the max
-    if (FX && (threadIdx.x == L_MAXGRAD || threadIdx.x == L_MAXSPEED)) val = sqrt(val);
-    out->v[threadIdx.x] = val;
+    out->v[threadIdx.x] = ledger_final_value<FX>(threadIdx.x, tot[threadIdx.x]);
   }
   if (threadIdx.x < kLedgerI64) {
     long long a = 0;
@@ -214,21 +263,7 @@ __global__ void __launch_bounds__(kThreads)
     *arrive = 0;
     if (mode == 0) {
       // prologue: static short-circuit and the first substep's dt
-      const bool no_ext = !c.has_external || out->v[L_MAXEXT] <= 1.0e-14;
-      const bool is_static =
-          no_ext && out->v[L_MAXQ] <= 1.0e-14 && out->v[L_MAXGRAD] <= static_limit;
-      ctl->wave = out->v[L_MAXWAVE];
-      if (is_static) {
-        ctl->static_skip = 1;
-        ctl->done = 1;
-      } else if (!(ctl->remaining > 1.0e-14)) {
-        ctl->done = 1;
-      } else if (c.max_substeps <= 0) {
-        ctl->status = 2;
-        ctl->done = 1;
-      } else {
-        plan_substep(c, ctl);
-      }
+      ledger_prologue(c, out, static_limit, ctl);
       __threadfence();
       if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
     }

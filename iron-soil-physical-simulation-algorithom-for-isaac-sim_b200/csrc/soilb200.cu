@@ -30,6 +30,7 @@
 #include "sb_relax.cuh"
 #include "sb_exchange.cuh"
 #include "sb_path.cuh"
+#include "sb_batch.cuh"
 
 using namespace sb;
 
@@ -384,17 +385,18 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
   return SB_OK;
 }
 
-void fill_ledger(const sb_ctx* ctx, const LedgerOut& o, const sb_mobile_params* p,
-                 sb_mobile_ledger* L) {
-  const double dx = ctx->d.dx_m, dy = ctx->d.dy_m;
+// Host form of a device ledger for a grid of spacing dx, dy; fixed-point
+// grids (fxp) convert their exact quanta sums with the grid's quantum.
+void fill_ledger_geom(bool fxp, double dx, double dy, double quantum, const LedgerOut& o,
+                      const sb_mobile_params* p, sb_mobile_ledger* L) {
   const double area = dx * dy;
   const double f = dx * dy / 6.0;  // one weight unit
   const double rho = p->density_kg_m3;
   const double K = p->earth_pressure_coefficient, g = p->gravity_m_s2;
   double hsum, hsum_w;
-  if (fx(ctx)) {
-    hsum = (double)o.iq[0] * ctx->quantum;
-    hsum_w = (double)o.iq[1] * ctx->quantum;
+  if (fxp) {
+    hsum = (double)o.iq[0] * quantum;
+    hsum_w = (double)o.iq[1] * quantum;
     L->mass_quanta = o.iq[0];
     L->volume_w_quanta = o.iq[1];
   } else {
@@ -417,8 +419,13 @@ void fill_ledger(const sb_ctx* ctx, const LedgerOut& o, const sb_mobile_params* 
   L->pressure_w_j = rho * 0.5 * K * g * o.v[L_HH_W] * f;
   L->max_speed_m_s = o.v[L_MAXSPEED];
   L->min_h_m = -o.v[L_NEGMINH];
-  L->resting_volume_w_m3 = fx(ctx) ? (double)o.iq[2] * ctx->quantum * f : o.v[L_REST_W] * f;
-  L->resting_w_quanta = fx(ctx) ? o.iq[2] : 0;
+  L->resting_volume_w_m3 = fxp ? (double)o.iq[2] * quantum * f : o.v[L_REST_W] * f;
+  L->resting_w_quanta = fxp ? o.iq[2] : 0;
+}
+
+void fill_ledger(const sb_ctx* ctx, const LedgerOut& o, const sb_mobile_params* p,
+                 sb_mobile_ledger* L) {
+  fill_ledger_geom(fx(ctx), ctx->d.dx_m, ctx->d.dy_m, ctx->quantum, o, p, L);
 }
 
 template <bool FX>
@@ -502,6 +509,7 @@ size_t sb_sizeof(const char* type_name) {
       {"sb_relax_stats", sizeof(sb_relax_stats)},
       {"sb_path_params", sizeof(sb_path_params)},
       {"sb_path_stats", sizeof(sb_path_stats)},
+      {"sb_patch_desc", sizeof(sb_patch_desc)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.name, type_name) == 0) return e.size;
@@ -1988,3 +1996,5 @@ extern "C" int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, in
   out->largest_connected_area_m2 = (double)host.area6 * (dx_m * dy_m / 6.0);
   return host.status ? SB_ERR_NONCONVERGENCE : SB_OK;
 }
+
+#include "sb_batch_host.cuh"

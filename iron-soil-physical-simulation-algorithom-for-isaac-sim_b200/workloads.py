@@ -12,6 +12,10 @@ No public dataset is involved: every terrain is generated from
   footprint moving 6 m in a straight line at 0.5 m/s) entrains resting
   material down to 0.4 m below the initial surface; labelling at 38 deg,
   8-connected; 10 s simulated.
+* config 2 -- 512 patches (seeds 1000 + i) with sides from
+  {64, 96, 128, 192, 256, 384, 512} and aspect <= 2:1, each a config-0-style
+  terrain (10 deg tilt + 8 bumps) with a mound of mobile material at a seeded
+  position; every patch takes its own CFL substeps.
 """
 
 from __future__ import annotations
@@ -130,3 +134,33 @@ def config1(n: int = 701, seed: int = 1, dx: float = 0.05):
     b = noise_pile(n, seed, dx)
     cut = BucketCut((n, n), dx, b, start=(0.3 * n * dx, 0.5 * n * dx))
     return {"b_eff": b, "z_base": np.zeros((n, n)), "cut": cut}
+
+
+C2_SIDES = (64, 96, 128, 192, 256, 384, 512)
+
+
+def config2_patch(i: int, dx: float = 0.05):
+    """Patch i of config 2: (b_eff, h, q) with shape (ny, nx), seed 1000 + i."""
+    rng = np.random.default_rng(1000 + i)
+    ny = int(rng.choice(C2_SIDES))
+    nx = int(rng.choice([s for s in C2_SIDES if max(s, ny) <= 2 * min(s, ny)]))
+    ys, xs = np.indices((ny, nx), dtype=np.float64)
+    x, y = xs * dx, ys * dx
+    z = np.tan(np.deg2rad(10.0)) * x
+    for _ in range(8):
+        amp = rng.uniform(0.05, 0.3)
+        sig = rng.uniform(0.2, 1.0)
+        cx = rng.uniform(0.0, nx * dx)
+        cy = rng.uniform(0.0, ny * dx)
+        z = z + amp * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2.0 * sig * sig))
+    mx = rng.uniform(0.2, 0.8) * (nx - 1) * dx
+    my = rng.uniform(0.2, 0.8) * (ny - 1) * dx
+    sm = min(1.5, 0.2 * min(ny, nx) * dx)
+    h = 0.4 * np.exp(-((x - mx) ** 2 + (y - my) ** 2) / (2.0 * sm * sm))
+    return z, h, np.zeros((ny, nx, 2))
+
+
+def config2(n_patches: int = 512, dx: float = 0.05):
+    """The config-2 patch list [(b_eff, h, q), ...]."""
+    return [config2_patch(i, dx) for i in range(n_patches)]
+
