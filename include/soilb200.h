@@ -363,6 +363,39 @@ int sb_batch_last_error(sb_batch* batch, char* buffer, size_t length);
 int64_t sb_batch_kernel_launch_count(sb_batch* batch);
 void* sb_batch_stream(sb_batch* batch);
 
+/* ---- Learned repose proposal ------------------------------------------------
+ * No counterpart in the reference (its repose relaxation is the plain sweep,
+ * slope_model.py:273-343, alone).  A 4-layer 3x3 convolution net proposes
+ * per-edge outflows of b_eff; they are applied in flux form and the plain
+ * sweeps (sb_relax_full / sb_frontier_run) finish to the tolerance.
+ * Convolutions: BF16 NHWC activations (channels 16 or 32), FP32 accumulate on
+ * the tensor cores; weights prepacked per row offset dy in the canonical
+ * K-major layout (n = dx*cout + co rows, k = ci).  Device pointers, 16-byte
+ * aligned; work is queued on `stream`; d_status (device int, may be null)
+ * becomes 1 if a bounded device wait gave up. */
+const char* sb_learned_last_error(void);
+int sb_learned_conv(const void* in, void* out, const void* wpk, const void* mask, int batch, int h,
+                    int w, int cin, int cout, int relu, int out_f32, int rows_per_cta,
+                    int* d_status, void* stream);
+/* dW[3][3][cin][cout] (f32) of a layer from its input and output gradient;
+ * partial: ceil(w/128)*ceil(h/rows)*batch*3*128*cout floats of scratch. */
+int sb_learned_wgrad(const void* in, const void* grad, float* partial, size_t partial_floats,
+                     float* dw, int batch, int h, int w, int cin, int cout, int rows_per_cta,
+                     int* d_status, void* stream);
+/* Features (bf16 [batch][h][w][16]: channels 0..3 = height drop along the
+ * east, north, north-east, north-west edges over L*tan_crit) of float64
+ * heights; training loss of f32 fluxes against target height changes. */
+int sb_learned_features_f64(const double* heights, void* feat, int batch, int h, int w, double dx,
+                            double dy, double tan_crit, void* stream);
+int sb_learned_loss(const float* flux, const float* target_dh, float* resid, void* dflux,
+                    double* loss_part, int batch, int h, int w, double dx, double dy,
+                    double tan_crit, float inv_scale2_n, void* stream);
+int sb_learned_loss_blocks(int batch, int h, int w);
+/* On a context's resident b_eff (SB_FX32): features, then the network's
+ * fluxes applied in whole height quanta (tq: int32 [ny][nx][4] scratch). */
+int sb_learned_features(sb_ctx* ctx, void* feat, double tan_crit);
+int sb_learned_apply(sb_ctx* ctx, const float* flux, int32_t* tq, double tan_crit);
+
 int sb_last_error(sb_ctx* ctx, char* buffer, size_t length);
 /* Number of kernels this context has launched (cumulative). */
 int64_t sb_kernel_launch_count(sb_ctx* ctx);

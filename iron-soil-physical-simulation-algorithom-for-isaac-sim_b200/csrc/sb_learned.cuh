@@ -1,0 +1,592 @@
+// Learned repose proposal: a 4-layer 3x3 convolution net (4 -> 32 -> 32 ->
+// 32 -> 4 channels, ReLU between, no bias, BF16 operands, FP32 accumulate)
+// proposes per-edge outflows of a height field; they are applied in flux
+// form (every transfer leaves one cell and enters its neighbour, in whole
+// height quanta in the fixed-point state), and plain relaxation sweeps then
+// finish to the repose tolerance.  The reference has no counterpart: its
+// repose relaxation is the plain sweep (slope_model.py:273-343) alone.
+//
+// Convolutions are implicit GEMMs on the 5th-generation tensor cores
+// (tcgen05.mma, kind::f16, operands in shared memory, accumulator in TMEM):
+//
+//   forward / data gradient: per output row of a 126-pixel tile, the input
+//     rows y-1, y, y+1 (128 pixels each, K = input channels) are multiplied
+//     by the weights of that row offset with N = (dx, out channel) = 3*COUT,
+//     accumulating D[pixel, (dx, co)] over the three rows; the epilogue adds
+//     the dx = 0 / 2 partial sums of the neighbouring pixels (exchanged in
+//     shared memory).  The data gradient is the same kernel run with the
+//     flipped, transposed weights and the ReLU mask of the layer's input.
+//   weight gradient: per input row, A = the row shifted by dx (M = (dx, ci),
+//     K = 128 pixels) times B = output-gradient rows (N = co), accumulated in
+//     TMEM over the CTA's band for the three row offsets; per-CTA partials
+//     are summed in a fixed order by a second kernel.
+//
+// Operands use the canonical no-swizzle K-major layout: 8 x 16-byte core
+// matrices, element (r, k) at ((r/8)*(K/8) + k/8)*128 + (r%8)*16 + (k%8)*2.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "sb_common.cuh"
+
+namespace sb {
+
+constexpr int kConvThreads = 128;   // 4 warps: TMEM lanes 0..127 = tile pixels
+constexpr int kConvTileOut = 126;   // output pixels per 128-pixel input tile
+
+// ---------------------------------------------------------------- tcgen05
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100; no swizzle, base offset 0
+  return d;
+}
+
+// kind::f16 instruction descriptor: D f32, A/B bf16, both K-major.
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                          int accumulate) {
+  const uint32_t z = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+          tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Warp 0 allocates ncols TMEM columns; the base address lands in *slot.
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                   smem_u32(slot)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t base, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(ncols)
+               : "memory");
+}
+
+// 16 consecutive f32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t core_off(int r, int k, int kdim) {
+  return (uint32_t)(((r >> 3) * (kdim >> 3) + (k >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+struct ConvArgs {
+  const __nv_bfloat16* in;      // [batch][h][w][cin]
+  void* out;                    // [batch][h][w][cout], bf16 or f32 (out_f32)
+  const __nv_bfloat16* wpk;     // 3 row offsets x canonical B (n = dx*cout + co, k = ci)
+  const __nv_bfloat16* mask;    // optional [batch][h][w][cout]: out *= (mask > 0)
+  int batch, h, w;
+  int rows_per_cta;
+  int relu;
+  int out_f32;
+  int* status;                  // set to 1 if a bounded wait gave up
+};
+
+template <int CIN, int COUT>
+struct ConvSmem {
+  static constexpr int N = 3 * COUT;
+  static constexpr int W_BYTES = 3 * N * CIN * 2;   // packed weights, three row offsets
+  static constexpr int ROW_BYTES = 128 * CIN * 2;  // one input row of the tile
+  static constexpr int XCH_FLOATS = 128 * 2 * COUT;
+  static constexpr int BYTES = W_BYTES + 3 * ROW_BYTES + XCH_FLOATS * 4 + 64;
+  static constexpr uint32_t TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
+};
+
+// Loads input row r of the tile (pixels x0 .. x0+127) into ring slot dst in
+// canonical A layout; zeros outside the image.
+template <int CIN>
+__device__ __forceinline__ void conv_load_row(const __nv_bfloat16* __restrict__ in, int b, int h,
+                                              int w, int r, int x0, unsigned char* dst) {
+  const int m = threadIdx.x;
+  const int x = x0 + m;
+  const bool ok = r >= 0 && r < h && x >= 0 && x < w;
+  const uint4* src = reinterpret_cast<const uint4*>(in + (((size_t)b * h + (ok ? r : 0)) * w +
+                                                          (ok ? x : 0)) * CIN);
+#pragma unroll
+  for (int kb = 0; kb < CIN / 8; ++kb) {
+    const uint4 v = ok ? src[kb] : make_uint4(0, 0, 0, 0);
+    *reinterpret_cast<uint4*>(dst + core_off(m, kb * 8, CIN)) = v;
+  }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs a) {
+  using S = ConvSmem<CIN, COUT>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* wsm = smem;
+  unsigned char* ring = smem + S::W_BYTES;
+  float* xch = reinterpret_cast<float*>(ring + 3 * S::ROW_BYTES);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(xch + S::XCH_FLOATS);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int x0 = blockIdx.x * kConvTileOut - 1;
+  const int y0 = blockIdx.y * a.rows_per_cta;
+  const int y1 = min(y0 + a.rows_per_cta, a.h);
+  const int b = blockIdx.z;
+
+  // weights -> shared memory (already in canonical layout)
+  {
+    const uint4* src = reinterpret_cast<const uint4*>(a.wpk);
+    uint4* dst = reinterpret_cast<uint4*>(wsm);
+    for (int i = tid; i < S::W_BYTES / 16; i += kConvThreads) dst[i] = src[i];
+  }
+  if (tid == 0) mbar_init(bar, 1);
+  if (warp == 0) tmem_alloc(tslot, S::TMEM_COLS);
+  conv_load_row<CIN>(a.in, b, a.h, a.w, y0 - 1, x0, ring + ((y0 - 1 + 3) % 3) * S::ROW_BYTES);
+  conv_load_row<CIN>(a.in, b, a.h, a.w, y0, x0, ring + (y0 % 3) * S::ROW_BYTES);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(128, S::N);
+  const uint32_t lbo = 128, sbo = (CIN / 8) * 128;
+  const uint32_t w_base = smem_u32(wsm), ring_base = smem_u32(ring);
+  unsigned phase = 0;
+  bool ok = true;
+
+  for (int y = y0; y < y1; ++y) {
+    conv_load_row<CIN>(a.in, b, a.h, a.w, y + 1, x0, ring + ((y + 1) % 3) * S::ROW_BYTES);
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        const uint32_t a_row = ring_base + ((y - 1 + dy + 3) % 3) * S::ROW_BYTES;
+        const uint32_t b_off = w_base + dy * (S::N * CIN * 2);
+#pragma unroll
+        for (int kk = 0; kk < CIN / 16; ++kk)
+          umma_bf16(tmem, umma_desc(a_row + kk * 256, lbo, sbo), umma_desc(b_off + kk * 256, lbo, sbo),
+                    idesc, (dy | kk) != 0);
+      }
+      umma_commit(bar);
+    }
+    ok = mbar_wait(bar, phase) && ok;
+    phase ^= 1;
+    tc_fence_after();
+    // this thread's row of D: columns (dx, co)
+    float d[S::N];
+    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+    for (int c = 0; c < S::N; c += 16) tmem_ld16(lane_addr + c, d + c);
+    tc_fence_before();
+#pragma unroll
+    for (int co = 0; co < COUT; ++co) {
+      xch[tid * 2 * COUT + co] = d[co];                    // dx = 0 partial
+      xch[tid * 2 * COUT + COUT + co] = d[2 * COUT + co];  // dx = 2 partial
+    }
+    __syncthreads();
+    const int xo = x0 + tid;
+    if (tid >= 1 && tid <= kConvTileOut && xo < a.w) {
+      const size_t pix = ((size_t)b * a.h + y) * a.w + xo;
+#pragma unroll
+      for (int c8 = 0; c8 < COUT; c8 += 8) {
+        float o[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const int co = c8 + j;
+          float v = (xch[(tid - 1) * 2 * COUT + co] + d[COUT + co]) +
+                    xch[(tid + 1) * 2 * COUT + COUT + co];
+          if (a.relu) v = fmaxf(v, 0.f);
+          o[j] = v;
+        }
+        if (a.mask) {
+          const __nv_bfloat16* mk = a.mask + pix * COUT + c8;
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (!(__bfloat162float(mk[j]) > 0.f)) o[j] = 0.f;
+        }
+        if (a.out_f32) {
+          float* op = reinterpret_cast<float*>(a.out) + pix * COUT + c8;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) op[j] = o[j];
+        } else {
+          __align__(16) __nv_bfloat16 ob[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) ob[j] = __float2bfloat16_rn(o[j]);
+          *reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(a.out) + pix * COUT + c8) =
+              *reinterpret_cast<const uint4*>(ob);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!ok && tid == 0 && a.status) atomicExch(a.status, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, S::TMEM_COLS);
+}
+
+// ----------------------------------------------------------- weight grad
+struct WgradArgs {
+  const __nv_bfloat16* in;    // layer input [batch][h][w][cin]
+  const __nv_bfloat16* grad;  // gradient at the layer output [batch][h][w][cout]
+  float* partial;             // per CTA: [3 dy][128 (dx, ci)][cout]
+  int batch, h, w;
+  int rows_per_cta;
+  int* status;
+};
+
+template <int CIN, int COUT>
+struct WgradSmem {
+  static constexpr int T_BYTES = 128 * 128 * 2;       // A: (dx, ci) rows x 128 pixels
+  static constexpr int G_BYTES = COUT * 128 * 2;      // B: co rows x 128 pixels
+  static constexpr int BYTES = T_BYTES + 3 * G_BYTES + 64;
+  static constexpr uint32_t TMEM_COLS = 3 * COUT <= 64 ? 64 : 128;
+};
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kConvThreads) conv3x3_wgrad_tc_kernel(const WgradArgs a) {
+  using S = WgradSmem<CIN, COUT>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* tbuf = smem;
+  unsigned char* gring = smem + S::T_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(gring + 3 * S::G_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int x0 = blockIdx.x * 128;
+  const int y0 = blockIdx.y * a.rows_per_cta;
+  const int y1 = min(y0 + a.rows_per_cta, a.h);
+  const int b = blockIdx.z;
+  const size_t cta = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+
+  // zero A (the (dx, ci) rows beyond 3*CIN stay zero)
+  for (int i = tid; i < S::T_BYTES / 16; i += kConvThreads)
+    reinterpret_cast<uint4*>(tbuf)[i] = make_uint4(0, 0, 0, 0);
+  if (tid == 0) mbar_init(bar, 1);
+  if (warp == 0) tmem_alloc(tslot, S::TMEM_COLS);
+
+  // gradient row r -> ring slot (B operand: element (co, pixel k))
+  auto load_grad = [&](int r) {
+    unsigned char* dst = gring + ((r + 3) % 3) * S::G_BYTES;
+    const int k = tid, x = x0 + k;
+    const bool okp = r >= 0 && r < a.h && x < a.w;
+    const __nv_bfloat16* src = a.grad + (((size_t)b * a.h + (okp ? r : 0)) * a.w + (okp ? x : 0)) * COUT;
+#pragma unroll
+    for (int co = 0; co < COUT; ++co) {
+      const __nv_bfloat16 v = okp ? src[co] : __float2bfloat16_rn(0.f);
+      *reinterpret_cast<__nv_bfloat16*>(dst + core_off(co, k, 128)) = v;
+    }
+  };
+  load_grad(y0 - 1);
+  load_grad(y0);
+  fence_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(128, COUT);
+  const uint32_t t_base = smem_u32(tbuf), g_base = smem_u32(gring);
+  const uint32_t lbo = 128;
+  unsigned phase = 0;
+  bool ok = true;
+  int started[3] = {0, 0, 0};
+
+  // input rows r contribute to output rows y = r - dy + 1 in [y0, y1)
+  for (int r = y0 - 1; r <= y1; ++r) {
+    if (r + 1 <= y1) load_grad(r + 1);
+    // A: element ((dx, ci), k) = input[r][x0 + k + dx - 1][ci]
+    if (r >= 0 && r < a.h) {
+      for (int j = tid; j < 130; j += kConvThreads) {
+        const int x = x0 + j - 1;
+        const bool okp = x >= 0 && x < a.w;
+        const __nv_bfloat16* src = a.in + (((size_t)b * a.h + r) * a.w + (okp ? x : 0)) * CIN;
+        for (int ci = 0; ci < CIN; ++ci) {
+          const __nv_bfloat16 v = okp ? src[ci] : __float2bfloat16_rn(0.f);
+#pragma unroll
+          for (int dx = 0; dx < 3; ++dx) {
+            const int k = j - dx;
+            if (k >= 0 && k < 128)
+              *reinterpret_cast<__nv_bfloat16*>(tbuf + core_off(dx * CIN + ci, k, 128)) = v;
+          }
+        }
+      }
+    } else {
+      for (int i = tid; i < (3 * CIN) * 128 / 8; i += kConvThreads) {
+        const int row = i / 16, kb = i % 16;
+        *reinterpret_cast<uint4*>(tbuf + core_off(row, kb * 8, 128)) = make_uint4(0, 0, 0, 0);
+      }
+    }
+    fence_async_smem();
+    __syncthreads();
+    bool issued = false;
+    if (tid == 0) {
+      tc_fence_after();
+      for (int dy = 0; dy < 3; ++dy) {
+        const int y = r - dy + 1;
+        if (y < y0 || y >= y1) continue;
+        const uint32_t g_row = g_base + ((y + 3) % 3) * S::G_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < 8; ++kk)
+          umma_bf16(tmem + dy * COUT, umma_desc(t_base + kk * 256, lbo, 16 * 128),
+                    umma_desc(g_row + kk * 256, lbo, 16 * 128), idesc, started[dy] | (kk > 0));
+        started[dy] = 1;
+        issued = true;
+      }
+      if (issued) umma_commit(bar);
+    }
+    issued = __syncthreads_or(issued ? 1 : 0);
+    if (issued) {
+      ok = mbar_wait(bar, phase) && ok;
+      phase ^= 1;
+    }
+    tc_fence_after();
+    __syncthreads();
+  }
+  // epilogue: lane m = (dx, ci), columns (dy, co)
+  tc_fence_after();
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  float* out = a.partial + cta * (size_t)(3 * 128 * COUT);
+  for (int dy = 0; dy < 3; ++dy) {
+#pragma unroll
+    for (int c = 0; c < COUT; c += 16) {
+      float v[16];
+      tmem_ld16(lane_addr + dy * COUT + c, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) out[((size_t)dy * 128 + tid) * COUT + c + j] = y0 < y1 ? v[j] : 0.f;
+    }
+  }
+  if (!ok && tid == 0 && a.status) atomicExch(a.status, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, S::TMEM_COLS);
+}
+
+// dW[dy][dx][ci][co] = sum over CTAs (fixed order) of partial[cta][dy][dx*cin+ci][co].
+__global__ void wgrad_reduce_kernel(const float* __restrict__ partial, int nctas, int cin, int cout,
+                                    float* __restrict__ dw) {
+  const int n = 9 * cin * cout;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int co = i % cout;
+    const int ci = (i / cout) % cin;
+    const int dx = (i / (cout * cin)) % 3;
+    const int dy = i / (3 * cout * cin);
+    const size_t off = ((size_t)dy * 128 + dx * cin + ci) * cout + co;
+    double s = 0.0;
+    for (int c = 0; c < nctas; ++c) s += (double)partial[(size_t)c * 3 * 128 * cout + off];
+    dw[i] = (float)s;
+  }
+}
+
+// --------------------------------------------------- features and fluxes
+// Edges of cell (r, c): 0 east (r, c+1), 1 north (r+1, c), 2 north-east
+// (r+1, c+1), 3 north-west (r+1, c-1); lengths dx, dy, and the diagonal.
+__device__ __forceinline__ void edge_of(int k, int& dr, int& dc) {
+  dr = k == 0 ? 0 : 1;
+  dc = k == 0 ? 1 : (k == 1 ? 0 : (k == 2 ? 1 : -1));
+}
+
+struct LearnedGeom {
+  int batch, h, w, pitch;       // height fields [batch][h][pitch]
+  double dx, dy, tan_crit;
+  double Q;                     // FX quantum (0 for FP64 heights)
+  double datum;
+};
+
+// Features: per edge k, (H[c] - H[n_k]) / (L_k tan_crit) as BF16 channels
+// 0..3 of a 16-channel pixel (12 zero channels); 0 for edges leaving the grid.
+template <typename HT>
+__global__ void learned_features_kernel(const LearnedGeom g, const HT* __restrict__ hgt,
+                                        __nv_bfloat16* __restrict__ feat) {
+  const long long n = (long long)g.batch * g.h * g.w;
+  const double diag = sqrt(g.dx * g.dx + g.dy * g.dy);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % g.w);
+    const int r = (int)((i / g.w) % g.h);
+    const int bb = (int)(i / ((long long)g.w * g.h));
+    const HT* H = hgt + (size_t)bb * g.h * g.pitch;
+    const double hc = (double)H[(size_t)r * g.pitch + c];
+    __align__(16) __nv_bfloat16 f[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) f[k] = __float2bfloat16_rn(0.f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      int dr, dc;
+      edge_of(k, dr, dc);
+      const int rn = r + dr, cn = c + dc;
+      if (rn < g.h && cn >= 0 && cn < g.w) {
+        const double L = k == 0 ? g.dx : (k == 1 ? g.dy : diag);
+        const double scale = g.Q > 0.0 ? g.Q : 1.0;
+        const double d = (hc - (double)H[(size_t)rn * g.pitch + cn]) * scale / (L * g.tan_crit);
+        f[k] = __float2bfloat16_rn((float)d);
+      }
+    }
+    uint4* dst = reinterpret_cast<uint4*>(feat + i * 16);
+    dst[0] = reinterpret_cast<const uint4*>(f)[0];
+    dst[1] = reinterpret_cast<const uint4*>(f)[1];
+  }
+}
+
+// Proposed transfer on edge k of cell c, in metres: flux * tan_crit * dx,
+// limited to half the height difference across that edge (the proposal never
+// reverses a difference on its own).  Edges leaving the grid carry nothing.
+__device__ __forceinline__ double learned_transfer(const LearnedGeom& g, double flux, double hc,
+                                                   double hn) {
+  const double t = flux * g.tan_crit * g.dx;
+  const double lim = 0.5 * fabs(hc - hn);
+  return fmin(fmax(t, -lim), lim);
+}
+
+// Fixed point: transfers rounded to whole quanta per edge (int32 [pixel][4]),
+// then gathered -- every quantum leaves one cell and enters one neighbour.
+__global__ void learned_quantize_kernel(const LearnedGeom g, const int32_t* __restrict__ hq,
+                                        const float* __restrict__ flux /*[pixel][16]*/,
+                                        int32_t* __restrict__ tq /*[pixel][4]*/) {
+  const long long n = (long long)g.batch * g.h * g.w;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % g.w);
+    const int r = (int)((i / g.w) % g.h);
+    const int bb = (int)(i / ((long long)g.w * g.h));
+    const int32_t* H = hq + (size_t)bb * g.h * g.pitch;
+    const double hc = (double)H[(size_t)r * g.pitch + c] * g.Q;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      int dr, dc;
+      edge_of(k, dr, dc);
+      const int rn = r + dr, cn = c + dc;
+      int q = 0;
+      if (rn < g.h && cn >= 0 && cn < g.w) {
+        const double hn = (double)H[(size_t)rn * g.pitch + cn] * g.Q;
+        const double t = learned_transfer(g, (double)flux[i * 16 + k], hc, hn);
+        q = (int)trunc(t / g.Q);  // toward zero: stays within the half-difference limit
+      }
+      tq[i * 4 + k] = q;
+    }
+  }
+}
+
+__global__ void learned_apply_fx_kernel(const LearnedGeom g, int32_t* __restrict__ hq,
+                                        const int32_t* __restrict__ tq) {
+  const long long n = (long long)g.batch * g.h * g.w;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % g.w);
+    const int r = (int)((i / g.w) % g.h);
+    const int bb = (int)(i / ((long long)g.w * g.h));
+    long long d = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      d -= tq[i * 4 + k];
+      int dr, dc;
+      edge_of(k, dr, dc);
+      const int rs = r - dr, cs = c - dc;  // the cell whose edge k ends here
+      if (rs >= 0 && cs >= 0 && cs < g.w)
+        d += tq[(((long long)bb * g.h + rs) * g.w + cs) * 4 + k];
+    }
+    int32_t* H = hq + (size_t)bb * g.h * g.pitch;
+    H[(size_t)r * g.pitch + c] = (int32_t)((long long)H[(size_t)r * g.pitch + c] + d);
+  }
+}
+
+// Training loss: predicted height change dH = -div(t) (unlimited transfers,
+// f32) against the plain relaxation's change; writes the residual per pixel
+// and the loss partial per block (blockDim a multiple of 32, at most 1024).
+__global__ void learned_loss_kernel(const LearnedGeom g, const float* __restrict__ flux,
+                                    const float* __restrict__ target_dh /*[pixel] metres*/,
+                                    float* __restrict__ resid /*[pixel]*/,
+                                    double* __restrict__ loss_part, float inv_scale2_n) {
+  const long long n = (long long)g.batch * g.h * g.w;
+  const float s = (float)(g.tan_crit * g.dx);
+  double acc = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % g.w);
+    const int r = (int)((i / g.w) % g.h);
+    const int bb = (int)(i / ((long long)g.w * g.h));
+    float dh = 0.f;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      int dr, dc;
+      edge_of(k, dr, dc);
+      if (r + dr < g.h && c + dc >= 0 && c + dc < g.w) dh -= flux[i * 16 + k] * s;
+      const int rs = r - dr, cs = c - dc;
+      if (rs >= 0 && cs >= 0 && cs < g.w)
+        dh += flux[(((long long)bb * g.h + rs) * g.w + cs) * 16 + k] * s;
+    }
+    const float e = dh - target_dh[i];
+    resid[i] = e;
+    acc += (double)e * (double)e;
+  }
+  acc = warp_sum(acc);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w2 = 0; w2 < (int)(blockDim.x >> 5); ++w2) t += red[w2];
+    loss_part[blockIdx.x] = t * (double)inv_scale2_n;
+  }
+}
+
+// dL/dflux[c][k] = 2 s (e[n_k] - e[c]) / (scale^2 N) for edges inside the grid.
+__global__ void learned_dflux_kernel(const LearnedGeom g, const float* __restrict__ resid,
+                                     __nv_bfloat16* __restrict__ dflux, float inv_scale2_n) {
+  const long long n = (long long)g.batch * g.h * g.w;
+  const float s = (float)(g.tan_crit * g.dx);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % g.w);
+    const int r = (int)((i / g.w) % g.h);
+    const int bb = (int)(i / ((long long)g.w * g.h));
+    __align__(16) __nv_bfloat16 f[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) f[k] = __float2bfloat16_rn(0.f);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      int dr, dc;
+      edge_of(k, dr, dc);
+      const int rn = r + dr, cn = c + dc;
+      if (rn < g.h && cn >= 0 && cn < g.w) {
+        const float en = resid[((long long)bb * g.h + rn) * g.w + cn];
+        f[k] = __float2bfloat16_rn(2.f * s * (en - resid[i]) * inv_scale2_n);
+      }
+    }
+    uint4* dst = reinterpret_cast<uint4*>(dflux + i * 16);
+    dst[0] = reinterpret_cast<const uint4*>(f)[0];
+    dst[1] = reinterpret_cast<const uint4*>(f)[1];
+  }
+}
+
+}  // namespace sb

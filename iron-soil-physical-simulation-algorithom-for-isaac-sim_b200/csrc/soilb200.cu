@@ -31,6 +31,7 @@
 #include "sb_exchange.cuh"
 #include "sb_path.cuh"
 #include "sb_batch.cuh"
+#include "sb_learned.cuh"
 
 using namespace sb;
 
@@ -1998,3 +1999,4 @@ extern "C" int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, in
 }
 
 #include "sb_batch_host.cuh"
+#include "sb_learned_host.cuh"

@@ -164,3 +164,21 @@ def config2(n_patches: int = 512, dx: float = 0.05):
     """The config-2 patch list [(b_eff, h, q), ...]."""
     return [config2_patch(i, dx) for i in range(n_patches)]
 
+
+def config3_patch(i: int, n: int = 128, dx: float = 0.05) -> np.ndarray:
+    """Training patch i of config 3: steepened fractal noise (non-negative heights)."""
+    rng = np.random.default_rng(i)
+    acc = np.zeros((n, n))
+    weight, amp = 0.0, 1.0
+    for o in range(5):
+        acc += amp * value_noise((n, n), 4 * 2 ** o, rng)
+        weight += amp
+        amp *= 0.5
+    h = acc / weight
+    target = np.tan(np.deg2rad(rng.uniform(45.0, 60.0)))
+    # steepest of the four neighbour directions (slope_model.max_neighbor_slope's measure)
+    diag = np.hypot(dx, dx)
+    s = max(np.abs(np.diff(h, axis=0)).max() / dx, np.abs(np.diff(h, axis=1)).max() / dx,
+            np.abs(h[1:, 1:] - h[:-1, :-1]).max() / diag, np.abs(h[1:, :-1] - h[:-1, 1:]).max() / diag)
+    return (h - h.min()) * (target / s)
+
