@@ -219,6 +219,22 @@ _PROTOTYPES = {
     "sb_batch_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
     "sb_batch_kernel_launch_count": (C.c_int64, [C.c_void_p]),
     "sb_batch_stream": (C.c_void_p, [C.c_void_p]),
+    "sb_learned_last_error": (C.c_char_p, []),
+    "sb_learned_conv": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                           C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_int, C.c_void_p, C.c_void_p]),
+    "sb_learned_wgrad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t,
+                                            C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_void_p, C.c_void_p]),
+    "sb_learned_features_f64": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                                   C.c_int, C.c_double, C.c_double, C.c_double,
+                                                   C.c_void_p]),
+    "sb_learned_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
+                                           C.c_double, C.c_double, C.c_float, C.c_void_p]),
+    "sb_learned_loss_blocks": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "sb_learned_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
+    "sb_learned_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
 }
 
 # ctypes mirror of each ABI struct, checked against sb_sizeof() in the tests.
