@@ -428,6 +428,76 @@ def run_batched_c2(args, n_patches: int = 512):
     return out
 
 
+def c1_after_cut(n: int = N):
+    """b_eff of config 1 after the whole 12 s straight cut (every footprint
+    lowered to its target surface)."""
+    from soilb200 import workloads
+    cfg = workloads.config1(n, seed=1, dx=DX)
+    b = cfg["b_eff"].copy()
+    cut = cfg["cut"]
+    for k in range(1, 721):
+        idx, tgt = cut.footprint(k * DT)
+        b.flat[idx] = np.minimum(b.flat[idx], tgt)
+    return b
+
+
+def run_repose(args, rounds: int = 4, eps_slope: float = 1e-4):
+    """Second headline metric: ms to repose at 701^2 after the cut, the learned
+    proposal (tensor-core conv net, flux form, exact quanta) + plain sweeps
+    against plain sweeps alone, same tolerance (eps * dx m), same start."""
+    import torch
+    import soilb200
+    from soilb200 import learned
+    from soilb200.train_repose import DEFAULT_WEIGHTS
+
+    if not DEFAULT_WEIGHTS.exists():
+        raise SystemExit(f"trained weights missing: {DEFAULT_WEIGHTS} (python -m soilb200.train_repose)")
+    net = learned.ReposeNet.load(DEFAULT_WEIGHTS)
+    b = c1_after_cut()
+    k, datum = soilb200.choose_quantization(b)
+    tol = eps_slope * DX
+    q = 2.0 ** k
+
+    def one(r):
+        g = soilb200.DeviceGrid(b.shape, DX, DX, precision="fx32", height_exponent=k, datum_m=datum)
+        g.upload("b_eff", b)
+        g.upload("z_base", np.zeros_like(b))
+        lr = learned.LearnedRelaxation(g, net, 35.0)
+        s0 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
+        stream = torch.cuda.ExternalStream(g.stream_handle())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        st = lr.relax(tol, max_iterations=400000, rounds=r)
+        e1.record(stream)
+        e1.synchronize()
+        s1 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
+        launches = g.kernel_launches()
+        g.close()
+        return e0.elapsed_time(e1), int(st.iterations), bool(st.converged), s0 == s1, launches
+
+    for _ in range(args.warmup):
+        one(0)
+        one(rounds)
+    plain, learn = [], []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            plain.append(one(0))
+            learn.append(one(rounds))
+    pm = statistics.median(p[0] for p in plain)
+    lm = statistics.median(p[0] for p in learn)
+    return {"metric": "ms to repose at 701^2 after the cut, learned proposal + plain sweeps (35 deg, eps 1e-4)",
+            "value": lm, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": lm, "higher_is_better": False, "dtype": "int32-quanta (bf16 net, f32 accumulate)",
+            "data": "synthetic (config-1 pile after the full straight cut)",
+            "config": {"workload": "repose_701", "proposal_rounds": rounds, "tolerance_m": tol,
+                       "plain_ms": pm, "speedup_vs_plain": pm / lm,
+                       "plain_iterations": plain[0][1], "learned_iterations": learn[0][1],
+                       "converged": all(p[2] for p in plain + learn),
+                       "mass_ledger_exact": all(p[3] for p in plain + learn)},
+            "gpu_launches": learn[0][4], "clocks": clocks.summary()}
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline (oracle port, NumPy, 1 core)
 # ---------------------------------------------------------------------------
@@ -525,7 +595,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="config1_plain_path_701",
-                    choices=["config1_plain_path_701", "mobile_v2_4096", "batched_c2_512"])
+                    choices=["config1_plain_path_701", "mobile_v2_4096", "batched_c2_512",
+                             "repose_701"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
@@ -540,6 +611,9 @@ def main():
         return
     if args.workload == "batched_c2_512":
         print(json.dumps(run_batched_c2(args)))
+        return
+    if args.workload == "repose_701":
+        print(json.dumps(run_repose(args)))
         return
     if world > 1:
         import datetime

@@ -80,7 +80,9 @@ enum sb_field {
   SB_FIELD_SLOPE = 10,             /* read-only, radians */
   SB_FIELD_SEVERITY = 11,          /* read-only */
   SB_FIELD_LATCH = 12,             /* int32 */
-  SB_FIELD_PREVIOUS_COMPONENT = 13 /* int32 */
+  SB_FIELD_PREVIOUS_COMPONENT = 13, /* int32 */
+  SB_FIELD_FORCING = 14,            /* int32 flat: nonzero = tool forcing (no deposition) */
+  SB_FIELD_M2R_CUMULATIVE = 15      /* read-only float64 flat: settled volume per cell, m^3 */
 };
 
 typedef struct sb_ctx sb_ctx;
@@ -320,6 +322,36 @@ int sb_path_reset(sb_ctx* ctx);
 int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, int ny, int nx,
                          int connectivity, double dx_m, double dy_m, void* stream,
                          sb_label_stats* out);
+
+/* ---- Mobile -> Resting deposition (bulk_interaction/warp_deposition.py:23-130,
+ *      WarpDepositionOperator.step_resident :183-238) -------------------------
+ * Every cell with mobile material, no tool forcing (SB_FIELD_FORCING) and
+ * speed |q/h| <= speed_threshold whose free surface is below the cohesive
+ * stop yield settles min(h, rate*dt) into b_eff (all of h when
+ * settle_subcell_tail), momentum shrinking in proportion; b_eff + h is
+ * unchanged.  All cells read the pre-step surface.  Sums as the reference's
+ * weighted_sum: volume sum(settled * w), momentum density * sum(removed q * w). */
+typedef struct sb_deposition_params {
+  double settling_rate_m_s;    /* 0.30 */
+  double speed_threshold_m_s;  /* 0.18 */
+  double density_kg_m3;        /* MaterialScenario.assumed_bulk_density_kg_m3 */
+  double gravity_m_s2;         /* 9.81 */
+  double cohesion_pa;          /* MaterialScenario.cohesion_proxy_pa */
+  double stop_angle_deg;       /* MaterialScenario.stop_angle_deg */
+  int settle_subcell_tail;
+  int pad;
+} sb_deposition_params;
+
+typedef struct sb_deposition_stats {
+  double deposited_volume_m3;
+  double removed_momentum_kg_m_s[2];
+  int64_t deposited_w6_quanta;  /* SB_FX32: exact sum of settled quanta * (6 w / dx dy) */
+  int cells;                    /* cells that settled material */
+  int pad;
+} sb_deposition_stats;
+
+int sb_deposition_step(sb_ctx* ctx, double dt_s, const sb_deposition_params* params,
+                       sb_deposition_stats* out);
 
 /* ---- Batched terrain patches ----------------------------------------------
  * Many independent Mobile V2 grids ("patches": parallel dig environments of

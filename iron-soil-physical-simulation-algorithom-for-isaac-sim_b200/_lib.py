@@ -44,8 +44,10 @@ FIELD = {
     "severity": 11,
     "latch": 12,
     "previous_component": 13,
+    "forcing": 14,
+    "m2r_cumulative": 15,
 }
-INT_FIELDS = {"frontier_reached", "labels", "unstable", "latch", "previous_component"}
+INT_FIELDS = {"frontier_reached", "labels", "unstable", "latch", "previous_component", "forcing"}
 
 
 class B200BackendUnavailable(RuntimeError):
@@ -160,6 +162,21 @@ class PathStats(C.Structure):
 
 
 _LIB = None
+class DepositionParams(C.Structure):
+    _fields_ = [
+        ("settling_rate_m_s", C.c_double), ("speed_threshold_m_s", C.c_double),
+        ("density_kg_m3", C.c_double), ("gravity_m_s2", C.c_double), ("cohesion_pa", C.c_double),
+        ("stop_angle_deg", C.c_double), ("settle_subcell_tail", C.c_int), ("pad", C.c_int),
+    ]
+
+
+class DepositionStats(C.Structure):
+    _fields_ = [
+        ("deposited_volume_m3", C.c_double), ("removed_momentum_kg_m_s", C.c_double * 2),
+        ("deposited_w6_quanta", C.c_int64), ("cells", C.c_int), ("pad", C.c_int),
+    ]
+
+
 class PatchDesc(C.Structure):
     _fields_ = [
         ("ny", C.c_int), ("nx", C.c_int), ("dx_m", C.c_double), ("dy_m", C.c_double),
@@ -206,6 +223,8 @@ _PROTOTYPES = {
                                         C.POINTER(C.c_double)]),
     "sb_deposit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
                              C.c_void_p]),
+    "sb_deposition_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(DepositionParams),
+                                     C.POINTER(DepositionStats)]),
     "sb_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(PatchDesc),
                                   C.POINTER(C.c_void_p)]),
     "sb_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -250,6 +269,8 @@ ABI_STRUCTS = {
     "sb_path_params": PathParams,
     "sb_path_stats": PathStats,
     "sb_patch_desc": PatchDesc,
+    "sb_deposition_params": DepositionParams,
+    "sb_deposition_stats": DepositionStats,
 }
 
 

@@ -150,6 +150,11 @@ class B200BulkState:
         return {"deposited_volume_m3": float(out[0]),
                 "removed_mobile_momentum_kg_m_s": np.asarray([out[1], out[2], 0.0])}
 
+    def set_tool_forcing_mask(self, mask) -> None:
+        """Cells under active tool forcing (the reference's ``material_mask``):
+        deposition leaves them alone."""
+        self.grid.upload("forcing", np.asarray(mask, dtype=bool).astype(np.int32))
+
     # ------------------------------------------------------------ host view
     def explicit_host_view(self, *, source: str = "acceptance") -> dict:
         """Full-field download at an explicit boundary (never in the step path)."""
@@ -231,6 +236,64 @@ class B200ProductionMobileV2Solver:
             "state": ["z_base", "b_eff", "mobile", "momentum_x", "momentum_y"],
             "pressure_flux": "0.5*K*g*h^2_CONSERVATIVE_FACE_FLUX",
             "K_classification": "ENGINEERING_CLOSURE_UNCALIBRATED",
+        }
+
+
+@dataclass(frozen=True)
+class WarpDepositionStep:
+    """Record of one deposition step (reference warp_deposition.py:136-140)."""
+
+    deposited_volume_m3: float
+    parameter_status: str
+    removed_mobile_momentum_terrain_kg_m_s: np.ndarray
+
+
+class B200DepositionOperator:
+    """Incremental Mobile -> Resting deposition on the resident state
+    (reference bulk_interaction/warp_deposition.py:143-255)."""
+
+    backend_name = "GPU_B200_INCREMENTAL_DEPOSITION"
+
+    def __init__(self, *, settling_rate_m_s: float = 0.30, speed_threshold_m_s: float = 0.18,
+                 device=0, runtime=None) -> None:
+        del device, runtime
+        if settling_rate_m_s <= 0.0 or speed_threshold_m_s < 0.0:
+            raise ValueError("[WarpDeposition] invalid configuration")
+        self.settling_rate_m_s = float(settling_rate_m_s)
+        self.speed_threshold_m_s = float(speed_threshold_m_s)
+        self._state: B200BulkState | None = None
+
+    def bind_device_state(self, state: B200BulkState) -> None:
+        if not isinstance(state, B200BulkState):
+            raise ValueError("[WarpDeposition] state/runtime ownership mismatch")
+        self._state = state
+
+    def step_resident(self, material, dt_s: float, *,
+                      settle_subcell_tail: bool = False) -> WarpDepositionStep:
+        if self._state is None:
+            raise RuntimeError("[WarpDeposition] bind DeviceBulkState first")
+        dt = float(dt_s)
+        if not np.isfinite(dt) or dt <= 0.0:
+            raise ValueError("[WarpDeposition] dt_s must be finite/positive")
+        p = _lib.DepositionParams(self.settling_rate_m_s, self.speed_threshold_m_s,
+                                  float(material.assumed_bulk_density_kg_m3), 9.81,
+                                  float(material.cohesion_proxy_pa),
+                                  float(material.stop_angle_deg), int(bool(settle_subcell_tail)), 0)
+        out = _lib.DepositionStats()
+        g = self._state.grid
+        _lib.check(g.ctx, _lib.load().sb_deposition_step(g.ctx, dt, p, out), "deposition")
+        return WarpDepositionStep(
+            deposited_volume_m3=float(out.deposited_volume_m3),
+            parameter_status="LITERATURE_BASED_REDUCED_ORDER_UNCALIBRATED",
+            removed_mobile_momentum_terrain_kg_m_s=np.asarray(
+                [out.removed_momentum_kg_m_s[0], out.removed_momentum_kg_m_s[1], 0.0]))
+
+    def diagnostics(self) -> dict:
+        return {
+            "backend_name": self.backend_name,
+            "resident_state": ["b_eff", "mobile", "momentum_x", "momentum_y"],
+            "semantics": "incremental_mobile_to_resting_below_cohesive_stop_yield",
+            "momentum_removal": "EXPLICITLY_REPORTED",
         }
 
 

@@ -29,6 +29,7 @@
 #include "sb_labels.cuh"
 #include "sb_relax.cuh"
 #include "sb_exchange.cuh"
+#include "sb_deposition.cuh"
 #include "sb_path.cuh"
 #include "sb_batch.cuh"
 #include "sb_learned.cuh"
@@ -156,6 +157,12 @@ struct sb_ctx {
   double* xval = nullptr;
   ExchangeOut* xout = nullptr;
   ExchangeOut* xout_host = nullptr;
+  // deposition: tool-forcing mask (int32, flat), per-cell settled volume
+  // record (double m^3, flat), device/host result records
+  int32_t* forcing = nullptr;
+  double* m2r = nullptr;
+  DepositionOut* dep_out = nullptr;
+  DepositionOut* dep_out_host = nullptr;
   long long launches = 0;
   char err[1024] = {0};
 };
@@ -223,6 +230,7 @@ void* field_ptr(sb_ctx* c, int field, int* is_int, int* is_height, int* is_suppo
     case SB_FIELD_EXTERNAL_X: return c->ext_x;
     case SB_FIELD_EXTERNAL_Y: return c->ext_y;
     case SB_FIELD_FRONTIER_REACHED: *is_int = 1; return c->reached;
+    case SB_FIELD_FORCING: *is_int = 1; if (is_flat) *is_flat = 1; return c->forcing;
     default: return nullptr;
   }
 }
@@ -511,6 +519,8 @@ size_t sb_sizeof(const char* type_name) {
       {"sb_path_params", sizeof(sb_path_params)},
       {"sb_path_stats", sizeof(sb_path_stats)},
       {"sb_patch_desc", sizeof(sb_patch_desc)},
+      {"sb_deposition_params", sizeof(sb_deposition_params)},
+      {"sb_deposition_stats", sizeof(sb_deposition_stats)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.name, type_name) == 0) return e.size;
@@ -623,6 +633,12 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMalloc(&ctx->root_list, n * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->lout, sizeof(LabelOut)));
   SB_CUDA(ctx, cudaMallocHost(&ctx->lout_host, sizeof(LabelOut)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->forcing, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->m2r, n * 8));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->forcing, 0, n * 4, ctx->stream));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->m2r, 0, n * 8, ctx->stream));
+  SB_CUDA(ctx, cudaMalloc(&ctx->dep_out, sizeof(DepositionOut)));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->dep_out_host, sizeof(DepositionOut)));
   void* zero_init[] = {ctx->parent, ctx->latch, ctx->previous, ctx->export_cum, ctx->export_base};
   size_t zero_size[] = {n * 4, n * 4, n * 4, n * 8, n * 8};
   for (int k = 0; k < 5; ++k) SB_CUDA(ctx, cudaMemsetAsync(zero_init[k], 0, zero_size[k], ctx->stream));
@@ -716,7 +732,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
                   ctx->roots.max_exc_start, ctx->roots.max_exc_stop, ctx->roots.prev_overlap,
                   ctx->root_list, ctx->lout, ctx->b_alt, ctx->ftile_next, ctx->phase[0],
                   ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout, ctx->pstate,
-                  ctx->path_count};
+                  ctx->path_count, ctx->forcing, ctx->m2r, ctx->dep_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
@@ -724,6 +740,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   for (cudaEvent_t e : ctx->ev_loop)
     if (e) cudaEventDestroy(e);
   if (ctx->xout_host) cudaFreeHost(ctx->xout_host);
+  if (ctx->dep_out_host) cudaFreeHost(ctx->dep_out_host);
   if (ctx->pstate_host) cudaFreeHost(ctx->pstate_host);
   if (ctx->path_count_host) cudaFreeHost(ctx->path_count_host);
   if (ctx->path_exec) cudaGraphExecDestroy(ctx->path_exec);
@@ -785,6 +802,12 @@ int sb_upload(sb_ctx* ctx, int field, const double* host) {
 
 int sb_download(sb_ctx* ctx, int field, double* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
+  if (field == SB_FIELD_M2R_CUMULATIVE) {  // flat double in both precisions
+    SB_CUDA(ctx, cudaMemcpyAsync(host, ctx->m2r, (size_t)ctx->d.ny * ctx->d.nx * 8,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SB_OK;
+  }
   int is_int, is_h, is_s, is_flat;
   void* src = field_ptr(ctx, field, &is_int, &is_h, &is_s, &is_flat);
   if (!src || is_int) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is not a float field", field);
@@ -1517,6 +1540,68 @@ extern "C" int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double
   out3[0] = fx(ctx) ? (double)o.volume_w6_quanta * ctx->quantum * f : o.volume_w_fp64;
   out3[1] = density_kg_m3 * o.momentum_w[0];
   out3[2] = density_kg_m3 * o.momentum_w[1];
+  return SB_OK;
+}
+
+extern "C" int sb_deposition_step(sb_ctx* ctx, double dt_s, const sb_deposition_params* p,
+                                  sb_deposition_stats* out) {
+  if (!ctx || !p || !out) return SB_ERR_BAD_ARG;
+  if (!(p->settling_rate_m_s > 0.0) || !(p->speed_threshold_m_s >= 0.0) ||
+      !std::isfinite(p->settling_rate_m_s) || !std::isfinite(p->speed_threshold_m_s))
+    return fail(ctx, SB_ERR_BAD_ARG, "[WarpDeposition] invalid configuration");
+  if (!std::isfinite(dt_s) || dt_s <= 0.0)
+    return fail(ctx, SB_ERR_BAD_ARG, "[WarpDeposition] dt_s must be finite/positive");
+  if (!(p->density_kg_m3 > 0.0) || !std::isfinite(p->gravity_m_s2) || !std::isfinite(p->cohesion_pa))
+    return fail(ctx, SB_ERR_BAD_ARG, "[WarpDeposition] invalid material");
+  DepositionConst c{};
+  c.ny = ctx->d.ny;
+  c.nx = ctx->d.nx;
+  c.pitch = ctx->pitch;
+  c.dx = ctx->d.dx_m;
+  c.dy = ctx->d.dy_m;
+  c.dt = dt_s;
+  c.rate = p->settling_rate_m_s;
+  c.speed_threshold = p->speed_threshold_m_s;
+  c.density = p->density_kg_m3;
+  c.gravity = p->gravity_m_s2;
+  c.cohesion = p->cohesion_pa;
+  c.stop_tan = std::tan(p->stop_angle_deg * (M_PI / 180.0));
+  c.settle_tail = p->settle_subcell_tail ? 1 : 0;
+  c.Q = ctx->quantum;
+  c.Qf = (float)ctx->quantum;
+  const double rq = std::floor(p->settling_rate_m_s * dt_s / ctx->quantum);
+  c.rate_q = rq > 2147483647.0 ? 2147483647LL : (long long)rq;
+  const int P = ctx->parity_host;
+  const int grid = ctx->ledger_blocks;
+  double* amount = ctx->staging;
+  if (fx(ctx)) {
+    deposition_decide_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (const int32_t*)ctx->b, (const int32_t*)ctx->h[P], (const float*)ctx->qx[P],
+        (const float*)ctx->qy[P], ctx->forcing, amount);
+    deposition_apply_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (int32_t*)ctx->b, (int32_t*)ctx->h[P], (float*)ctx->qx[P], (float*)ctx->qy[P], amount,
+        ctx->m2r, ctx->partials, ctx->arrive, ctx->dep_out);
+  } else {
+    deposition_decide_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (const double*)ctx->b, (const double*)ctx->h[P], (const double*)ctx->qx[P],
+        (const double*)ctx->qy[P], ctx->forcing, amount);
+    deposition_apply_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (double*)ctx->b, (double*)ctx->h[P], (double*)ctx->qx[P], (double*)ctx->qy[P], amount,
+        ctx->m2r, ctx->partials, ctx->arrive, ctx->dep_out);
+  }
+  ctx->launches += 2;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->dep_out_host, ctx->dep_out, sizeof(DepositionOut),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const DepositionOut& o = *ctx->dep_out_host;
+  const double f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  out->deposited_volume_m3 = fx(ctx) ? (double)o.volume_w6_quanta * ctx->quantum * f : o.volume_w;
+  out->removed_momentum_kg_m_s[0] = o.momentum_w[0];
+  out->removed_momentum_kg_m_s[1] = o.momentum_w[1];
+  out->deposited_w6_quanta = fx(ctx) ? o.volume_w6_quanta : 0;
+  out->cells = o.cells;
+  out->pad = 0;
   return SB_OK;
 }
 

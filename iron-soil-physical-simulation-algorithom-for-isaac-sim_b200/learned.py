@@ -107,11 +107,18 @@ class ReposeNet:
         return cls(device=device, weights=ws)
 
 
+def conv_rows(b: int, h: int, w: int) -> int:
+    """Rows per CTA: about one wave of 4 resident CTAs on each of 148 SMs."""
+    tiles = (w + 125) // 126
+    return int(min(32, max(4, -(-b * h * tiles // (148 * 4)))))
+
+
 def conv(x, wpk, cin: int, cout: int, *, relu: bool, out_f32: bool = False, mask=None,
-         status=None, stream=None, rows: int = 16):
+         status=None, stream=None, rows: int | None = None):
     """One tensor-core 3x3 convolution of a BF16 NHWC tensor [B, H, W, cin]."""
     torch = _torch()
     b, h, w, c = x.shape
+    rows = conv_rows(b, h, w) if rows is None else int(rows)
     if c != cin:
         raise ValueError(f"[soilb200] conv input has {c} channels, expected {cin}")
     out = torch.empty(b, h, w, cout, dtype=torch.float32 if out_f32 else torch.bfloat16,
@@ -260,16 +267,24 @@ class LearnedRelaxation:
         self._tq = torch.empty(ny * nx * 4, dtype=torch.int32, device=dev)
         self._packed = net.packed()
         self._stream = grid.stream_handle()
+        # buffers made during a proposal belong to the grid's stream, so the
+        # allocator never hands them out while that stream still reads them
+        self._torch_stream = torch.cuda.ExternalStream(self._stream, device=dev)
+        torch.cuda.current_stream(dev).synchronize()
 
     def propose(self, rounds: int = 1) -> None:
+        torch = _torch()
         lib = _lib.load()
-        for _ in range(rounds):
-            _lib.check(self.grid.ctx, lib.sb_learned_features(self.grid.ctx, self._feat.data_ptr(),
-                                                              self.tan_crit), "features")
-            _, flux = network_forward(self.net, self._feat, self._packed, stream=self._stream)
-            _lib.check(self.grid.ctx, lib.sb_learned_apply(self.grid.ctx, flux.data_ptr(),
-                                                           self._tq.data_ptr(), self.tan_crit),
-                       "apply")
+        with torch.cuda.stream(self._torch_stream):
+            for _ in range(rounds):
+                _lib.check(self.grid.ctx, lib.sb_learned_features(self.grid.ctx,
+                                                                  self._feat.data_ptr(),
+                                                                  self.tan_crit), "features")
+                _, flux = network_forward(self.net, self._feat, self._packed,
+                                          stream=self._stream)
+                _lib.check(self.grid.ctx, lib.sb_learned_apply(self.grid.ctx, flux.data_ptr(),
+                                                               self._tq.data_ptr(),
+                                                               self.tan_crit), "apply")
 
     def relax(self, tolerance_m: float, max_iterations: int = 20000, rounds: int = 1,
               spacing=None):

@@ -21,6 +21,10 @@ need the reference at run time.  Cases:
   ``tests/test_warp_gpu_backends.py:166-259``.
 * ``labels.npz``        -- ``_largest_connected_region`` and
   ``evaluate_cohesive_yield`` on seeded slope fields.
+* ``deposition.npz``    -- the CPU ``DepositionOperator.apply``
+  (bulk_interaction/deposition.py:67-160) on the three scenarios of the
+  reference's device-deposition tests (tests/test_device_bulk_state.py:150-230)
+  and a seeded static blanket below the stop angle.
 * ``gate0.npz``         -- the 5 s config-0 gate: 256x256, seed 0, 300 steps of
   1/60 s at CFL 0.4 and mu = tan 35 deg, each followed by
   ``relax_critical_slope`` of ``b_eff`` at 35 deg (row-major array, spacing
@@ -304,6 +308,53 @@ def make_report_values():
         {"cpu_contracts": out, "device_equivalence": device}, indent=1, sort_keys=True) + "\n")
 
 
+def make_deposition():
+    from isaac_bulk_pipeline.bulk_interaction import DepositionOperator
+    from isaac_bulk_pipeline.bulk_state import MaterialScenario, TerrainVolumeIntegrator
+    from isaac_bulk_pipeline.terrain import TerrainGrid
+
+    material = MaterialScenario("device_state", 1370.0, 29.8, 800.0, 0.5, 38.0, 30.0, 0.35)
+    arrays = {}
+    cases = []
+    grid16 = TerrainGrid(16, 16, 0.05, 0.05, 0.0, 0.0, "/World/Terrain")
+    resting = np.ones(grid16.shape)
+    mobile = np.zeros(grid16.shape)
+    mobile[6:10, 6:10] = 0.03
+    cases.append(("PATCH", grid16, resting, mobile, np.zeros(grid16.shape + (2,))))
+    cols = np.arange(grid16.nx, dtype=np.float64)[None, :]
+    resting = np.repeat(0.08 * cols, grid16.ny, axis=0)
+    cases.append(("BLANKET", grid16, resting, np.max(resting) - resting + 0.02,
+                  np.zeros(grid16.shape + (2,))))
+    resting = np.zeros(grid16.shape)
+    resting[8, 8] = 0.20
+    mobile = np.zeros(grid16.shape)
+    mobile[8, 9] = 0.01
+    mom = np.zeros(grid16.shape + (2,))
+    mom[8, 9, 0] = 0.02
+    cases.append(("TAIL", grid16, resting, mobile, mom))
+    grid = TerrainGrid(40, 32, 0.05, 0.05, 0.0, 0.0, "/World/Terrain")
+    rng = np.random.default_rng(21)
+    ys, xs = np.indices(grid.shape)
+    resting = 0.5 + 0.02 * np.sin(xs / 3.0) + 0.02 * np.cos(ys / 4.0)
+    mobile = np.where(rng.random(grid.shape) < 0.6, 0.004 + 0.03 * rng.random(grid.shape), 0.0)
+    cases.append(("STATIC_NOISE", grid, resting, mobile, np.zeros(grid.shape + (2,))))
+    names = []
+    for name, g, rest, mob, q in cases:
+        integ = TerrainVolumeIntegrator.from_grid(g)
+        res = DepositionOperator().apply(rest, mob, q, material, g, integ, 1.0 / 60.0)
+        names.append(name)
+        arrays[f"{name}/resting"] = rest
+        arrays[f"{name}/mobile"] = mob
+        arrays[f"{name}/momentum"] = q
+        arrays[f"{name}/resting_out"] = res.H_resting_m
+        arrays[f"{name}/mobile_out"] = res.mobile_height_m
+        arrays[f"{name}/volume"] = np.float64(res.deposited_volume_m3)
+        arrays[f"{name}/tail"] = np.int32(integ.integrate(mob) <= g.dx * g.dy * min(g.dx, g.dy))
+    arrays["names"] = np.asarray(names)
+    arrays["material"] = np.asarray([1370.0, 29.8, 800.0, 0.5, 38.0, 30.0, 0.35])
+    np.savez_compressed(HERE / "deposition.npz", **arrays)
+
+
 def make_gate0(n: int = 256, steps: int = 300):
     import time
 
@@ -337,6 +388,9 @@ def make_gate0(n: int = 256, steps: int = 300):
 if __name__ == "__main__":
     if "--gate0" in sys.argv:
         make_gate0()
+        sys.exit(0)
+    if "--deposition" in sys.argv:
+        make_deposition()
         sys.exit(0)
     make_report_values()
     make_fv_contracts()

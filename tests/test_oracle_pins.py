@@ -116,3 +116,21 @@ def test_config0_generator_matches_gate_fixture_inputs():
     assert float(t["b_eff"].sum()) == float(z["b0_sum"])
     assert float(t["h"].sum()) == float(z["h0_sum"])
     assert z["substeps"].shape == (300,) and z["relax_iterations"].shape == (300,)
+
+
+def test_deposition_oracle_matches_reference_cpu_operator():
+    """oracle/deposition.py (device-kernel semantics) equals the reference's CPU
+    DepositionOperator.apply on its device-test scenarios (fixture)."""
+    from oracle import deposition as D
+
+    z = np.load(GOLDEN / "deposition.npz")
+    m = z["material"]
+    for n in z["names"]:
+        q = z[f"{n}/momentum"]
+        b, h, _, _, vol, _, _ = D.step(z[f"{n}/resting"], z[f"{n}/mobile"], q[..., 0], q[..., 1],
+                                       dx=0.05, dy=0.05, dt=1.0 / 60.0, density=m[0],
+                                       cohesion=m[2], stop_angle_deg=m[5],
+                                       settle_tail=bool(z[f"{n}/tail"]))
+        assert np.array_equal(b, z[f"{n}/resting_out"]), n
+        assert np.array_equal(h, z[f"{n}/mobile_out"]), n
+        assert vol == pytest.approx(float(z[f"{n}/volume"]), abs=1e-15), n
