@@ -125,7 +125,7 @@ struct ConvSmem {
   static constexpr int N = 3 * COUT;
   static constexpr int W_BYTES = 3 * N * CIN * 2;   // packed weights, three row offsets
   static constexpr int ROW_BYTES = 128 * CIN * 2;  // one input row of the tile
-  static constexpr int XCH_FLOATS = 128 * 2 * COUT;
+  static constexpr int XCH_FLOATS = 4 * 2 * COUT;  // warp-boundary partial sums
   static constexpr int BYTES = W_BYTES + 3 * ROW_BYTES + XCH_FLOATS * 4 + 64;
   static constexpr uint32_t TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
 };
@@ -210,26 +210,32 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
 #pragma unroll
     for (int c = 0; c < S::N; c += 16) tmem_ld16(lane_addr + c, d + c);
     tc_fence_before();
-#pragma unroll
-    for (int co = 0; co < COUT; ++co) {
-      xch[tid * 2 * COUT + co] = d[co];                    // dx = 0 partial
-      xch[tid * 2 * COUT + COUT + co] = d[2 * COUT + co];  // dx = 2 partial
-    }
+    // neighbours' dx = 0 / dx = 2 partial sums: shuffles inside a warp, shared
+    // memory across the three warp boundaries
+    const int lane = tid & 31;
+    if (lane == 31)
+      for (int co = 0; co < COUT; ++co) xch[(warp * 2) * COUT + co] = d[co];
+    if (lane == 0)
+      for (int co = 0; co < COUT; ++co) xch[(warp * 2 + 1) * COUT + co] = d[2 * COUT + co];
     __syncthreads();
     const int xo = x0 + tid;
-    if (tid >= 1 && tid <= kConvTileOut && xo < a.w) {
-      const size_t pix = ((size_t)b * a.h + y) * a.w + xo;
+    const bool store = tid >= 1 && tid <= kConvTileOut && xo < a.w;
+    const size_t pix = ((size_t)b * a.h + y) * a.w + (store ? xo : 0);
 #pragma unroll
-      for (int c8 = 0; c8 < COUT; c8 += 8) {
-        float o[8];
+    for (int c8 = 0; c8 < COUT; c8 += 8) {
+      float o[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const int co = c8 + j;
-          float v = (xch[(tid - 1) * 2 * COUT + co] + d[COUT + co]) +
-                    xch[(tid + 1) * 2 * COUT + COUT + co];
-          if (a.relu) v = fmaxf(v, 0.f);
-          o[j] = v;
-        }
+      for (int j = 0; j < 8; ++j) {
+        const int co = c8 + j;
+        float left = __shfl_up_sync(0xffffffffu, d[co], 1);
+        float right = __shfl_down_sync(0xffffffffu, d[2 * COUT + co], 1);
+        if (lane == 0 && warp > 0) left = xch[((warp - 1) * 2) * COUT + co];
+        if (lane == 31 && warp < 3) right = xch[((warp + 1) * 2 + 1) * COUT + co];
+        float v = (left + d[COUT + co]) + right;
+        if (a.relu) v = fmaxf(v, 0.f);
+        o[j] = v;
+      }
+      if (store) {
         if (a.mask) {
           const __nv_bfloat16* mk = a.mask + pix * COUT + c8;
 #pragma unroll
