@@ -82,7 +82,15 @@ enum sb_field {
   SB_FIELD_LATCH = 12,             /* int32 */
   SB_FIELD_PREVIOUS_COMPONENT = 13, /* int32 */
   SB_FIELD_FORCING = 14,            /* int32 flat: nonzero = tool forcing (no deposition) */
-  SB_FIELD_M2R_CUMULATIVE = 15      /* read-only float64 flat: settled volume per cell, m^3 */
+  SB_FIELD_M2R_CUMULATIVE = 15,     /* float64 flat: settled volume per cell (deposition), m^3 */
+  /* large-avalanche per-cell history (flat; float64 in both precisions) */
+  SB_FIELD_R2M_CUMULATIVE = 16,         /* activated volume per cell, m^3 */
+  SB_FIELD_FIRST_ACTIVATION_TIME = 17,  /* s */
+  SB_FIELD_LAST_ACTIVATION_TIME = 18,   /* s */
+  SB_FIELD_OWNED_SURFACE = 19,          /* free surface at activation, m */
+  SB_FIELD_OWNED_EXPORT_BASELINE = 20,
+  SB_FIELD_EXPORT_CUMULATIVE = 21,
+  SB_FIELD_ACTIVATION_COUNT = 22        /* int32 flat */
 };
 
 typedef struct sb_ctx sb_ctx;
@@ -322,6 +330,56 @@ int sb_path_reset(sb_ctx* ctx);
 int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, int ny, int nx,
                          int connectivity, double dx_m, double dy_m, void* stream,
                          sb_label_stats* out);
+
+/* ---- Large-avalanche activation and lifecycle (runtime/gpu_large_avalanche.py
+ *      kernels mobilize :308-372, reduce_persistence :374-451; host
+ *      observe_and_maybe_mobilize :541-676, _persistence_summary :785-840) ----
+ * sb_avalanche_mobilize acts on the component selected by the last sb_label:
+ * each unlatched cell moves min(max(b_eff - z_base, 0), depth * severity)
+ * Resting -> Mobile at zero momentum (above the dry tolerance), latches, and
+ * records its activation history.  sb_avalanche_persistence reduces the
+ * lifecycle sums; net terrain change is against the b_eff snapshot taken by
+ * sb_avalanche_set_initial_resting (zeros before the first snapshot). */
+typedef struct sb_mobilize_stats {
+  double transferred_volume_m3;      /* sum(transfer * w) */
+  double newly_activated_volume_m3;
+  double reactivated_volume_m3;
+  double newly_activated_area_m2;
+  double reactivated_area_step_m2;
+  int64_t transferred_w6_quanta;     /* SB_FX32: exact */
+  int cells;
+  int pad;
+} sb_mobilize_stats;
+
+typedef struct sb_persistence_stats {
+  int unique_cells_ever_activated;
+  int cells_activated_more_than_once;
+  int current_mobile_cell_count;
+  int retired_candidate_cell_count;
+  int active_tile_count;
+  int pad;
+  double cumulative_r2m_m3;
+  double cumulative_m2r_m3;
+  double unique_activated_area_m2;
+  double reactivated_area_m2;
+  double current_mobile_volume_m3;
+  double maximum_mobile_speed_m_s;
+  double net_terrain_volume_change_m3;
+  double net_spatial_transfer_m3;
+  double activated_slope_sum_rad;
+  double activated_slope_max_rad;
+  double slope_minus_stop_sum_rad;
+  double start_minus_slope_sum_rad;
+  double retired_candidate_area_m2;
+  double moving_mobile_volume_m3;
+} sb_persistence_stats;
+
+int sb_avalanche_set_initial_resting(sb_ctx* ctx);
+int sb_avalanche_mobilize(sb_ctx* ctx, double activation_time_s, double mobilization_depth_m,
+                          double dry_tolerance_m, sb_mobilize_stats* out);
+int sb_avalanche_persistence(sb_ctx* ctx, double start_angle_rad, double stop_angle_rad,
+                             double dry_tolerance_m, double activity_speed_m_s,
+                             sb_persistence_stats* out);
 
 /* ---- Mobile -> Resting deposition (bulk_interaction/warp_deposition.py:23-130,
  *      WarpDepositionOperator.step_resident :183-238) -------------------------

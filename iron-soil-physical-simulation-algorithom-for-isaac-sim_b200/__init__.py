@@ -22,6 +22,7 @@ from .mobile_v2 import (  # noqa: F401
 
 from .avalanche import (  # noqa: F401
     B200LargeAvalancheBridge,
+    DeviceLargeAvalancheResult,
     LabelDiagnosis,
     LargeAvalancheTransitionConfig,
     MaterialScenario,
@@ -49,5 +50,5 @@ __all__ = [
     "B200LargeAvalancheBridge", "LabelDiagnosis", "LargeAvalancheTransitionConfig",
     "MaterialScenario", "FrontierRelaxation", "FrontierStats", "RelaxationStats",
     "relax_critical_slope", "label_mask", "largest_connected_region",
-    "label_mask_preallocated", "B200PatchBatch",
+    "label_mask_preallocated", "B200PatchBatch", "DeviceLargeAvalancheResult",
 ]

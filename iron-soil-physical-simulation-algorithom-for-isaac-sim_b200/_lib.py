@@ -46,8 +46,16 @@ FIELD = {
     "previous_component": 13,
     "forcing": 14,
     "m2r_cumulative": 15,
+    "r2m_cumulative": 16,
+    "first_activation_time": 17,
+    "last_activation_time": 18,
+    "owned_surface": 19,
+    "owned_export_baseline": 20,
+    "export_cumulative": 21,
+    "activation_count": 22,
 }
-INT_FIELDS = {"frontier_reached", "labels", "unstable", "latch", "previous_component", "forcing"}
+INT_FIELDS = {"frontier_reached", "labels", "unstable", "latch", "previous_component", "forcing",
+              "activation_count"}
 
 
 class B200BackendUnavailable(RuntimeError):
@@ -177,6 +185,30 @@ class DepositionStats(C.Structure):
     ]
 
 
+class MobilizeStats(C.Structure):
+    _fields_ = [
+        ("transferred_volume_m3", C.c_double), ("newly_activated_volume_m3", C.c_double),
+        ("reactivated_volume_m3", C.c_double), ("newly_activated_area_m2", C.c_double),
+        ("reactivated_area_step_m2", C.c_double), ("transferred_w6_quanta", C.c_int64),
+        ("cells", C.c_int), ("pad", C.c_int),
+    ]
+
+
+class PersistenceStats(C.Structure):
+    _fields_ = [
+        ("unique_cells_ever_activated", C.c_int), ("cells_activated_more_than_once", C.c_int),
+        ("current_mobile_cell_count", C.c_int), ("retired_candidate_cell_count", C.c_int),
+        ("active_tile_count", C.c_int), ("pad", C.c_int),
+        ("cumulative_r2m_m3", C.c_double), ("cumulative_m2r_m3", C.c_double),
+        ("unique_activated_area_m2", C.c_double), ("reactivated_area_m2", C.c_double),
+        ("current_mobile_volume_m3", C.c_double), ("maximum_mobile_speed_m_s", C.c_double),
+        ("net_terrain_volume_change_m3", C.c_double), ("net_spatial_transfer_m3", C.c_double),
+        ("activated_slope_sum_rad", C.c_double), ("activated_slope_max_rad", C.c_double),
+        ("slope_minus_stop_sum_rad", C.c_double), ("start_minus_slope_sum_rad", C.c_double),
+        ("retired_candidate_area_m2", C.c_double), ("moving_mobile_volume_m3", C.c_double),
+    ]
+
+
 class PatchDesc(C.Structure):
     _fields_ = [
         ("ny", C.c_int), ("nx", C.c_int), ("dx_m", C.c_double), ("dy_m", C.c_double),
@@ -225,6 +257,11 @@ _PROTOTYPES = {
                              C.c_void_p]),
     "sb_deposition_step": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(DepositionParams),
                                      C.POINTER(DepositionStats)]),
+    "sb_avalanche_set_initial_resting": (C.c_int, [C.c_void_p]),
+    "sb_avalanche_mobilize": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                        C.POINTER(MobilizeStats)]),
+    "sb_avalanche_persistence": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, C.POINTER(PersistenceStats)]),
     "sb_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(PatchDesc),
                                   C.POINTER(C.c_void_p)]),
     "sb_batch_destroy": (C.c_int, [C.c_void_p]),
@@ -271,6 +308,8 @@ ABI_STRUCTS = {
     "sb_patch_desc": PatchDesc,
     "sb_deposition_params": DepositionParams,
     "sb_deposition_stats": DepositionStats,
+    "sb_mobilize_stats": MobilizeStats,
+    "sb_persistence_stats": PersistenceStats,
 }
 
 

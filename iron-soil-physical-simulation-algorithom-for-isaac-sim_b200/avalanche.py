@@ -121,6 +121,50 @@ class LabelDiagnosis:
     union_iterations: int
 
 
+@dataclass(frozen=True)
+class DeviceLargeAvalancheResult:
+    """Field set of the reference's DeviceLargeAvalancheResult
+    (runtime/gpu_large_avalanche.py:469-507)."""
+
+    classification: str
+    transitioned: bool
+    unstable_cell_count: int
+    connected_region_count: int
+    largest_connected_cell_count: int
+    largest_connected_area_m2: float
+    largest_connected_mobilizable_volume_m3: float
+    mean_excess_start_deg: float
+    maximum_excess_start_deg: float
+    persistence_s: float
+    transferred_volume_m3: float
+    gravity_initiation_impulse_kg_m_s: np.ndarray
+    residual_seed_tile_ids: np.ndarray
+    union_iterations: int
+    parameter_basis: str
+    sensitivity_case: str
+    newly_activated_volume_m3: float
+    reactivated_volume_m3: float
+    newly_activated_area_m2: float
+    reactivated_area_step_m2: float
+    cumulative_resting_to_mobile_m3: float
+    cumulative_mobile_to_resting_m3: float
+    unique_cells_ever_activated: int
+    cells_activated_more_than_once: int
+    unique_activated_area_m2: float
+    reactivated_area_m2: float
+    retired_candidate_area_m2: float
+    current_mobile_volume_m3: float
+    moving_mobile_volume_m3: float
+    maximum_mobile_speed_m_s: float
+    active_tile_count: int
+    net_terrain_volume_change_m3: float
+    net_spatial_transfer_m3: float
+    mean_activated_slope_deg: float
+    maximum_activated_slope_deg: float
+    mean_slope_minus_theta_stop_deg: float
+    mean_theta_start_minus_slope_deg: float
+
+
 class B200LargeAvalancheBridge:
     NO_LARGE_EVENT = "NO_LARGE_EVENT"
     LOCAL_STATIC_INSTABILITY = "LOCAL_STATIC_INSTABILITY"
@@ -129,7 +173,9 @@ class B200LargeAvalancheBridge:
 
     def __init__(self, grid: DeviceGrid, material: MaterialScenario,
                  config: LargeAvalancheTransitionConfig | None = None, *,
-                 gravity_m_s2: float = 9.81) -> None:
+                 gravity_m_s2: float = 9.81, state=None) -> None:
+        self.state = state
+        self._clock_s = 0.0
         self.grid = grid
         self.material = material
         self.config = config or LargeAvalancheTransitionConfig()
@@ -201,6 +247,79 @@ class B200LargeAvalancheBridge:
             volume, mean_start, float(np.rad2deg(st.excess_start_max_rad)), mean_stop,
             float(np.rad2deg(st.excess_stop_max_rad)), self._persistence_s, candidate, ready,
             int(st.winner_root), int(st.union_passes))
+
+
+def _observe_and_maybe_mobilize(self, dt_s: float, *, release_settled_latches: bool = True
+                                ) -> DeviceLargeAvalancheResult:
+    """Diagnosis, then (when the transition is ready) activation of the selected
+    component, and the lifecycle summary (reference
+    runtime/gpu_large_avalanche.py:541-676, :785-840)."""
+    diag = self.observe(dt_s, release_settled_latches=release_settled_latches)
+    lib = _lib.load()
+    cfg = self.config
+    self._clock_s += float(dt_s)
+    now = float(getattr(self.state, "timestamp_device_s", self._clock_s)) if self.state else self._clock_s
+    mob = _lib.MobilizeStats()
+    if diag.transition_ready:
+        _lib.check(self.grid.ctx, lib.sb_avalanche_mobilize(
+            self.grid.ctx, now, float(cfg.mobilization_depth_m), float(cfg.dry_tolerance_m), mob),
+            "mobilize")
+    start = float(np.deg2rad(self.material.start_angle_deg))
+    stop = float(np.deg2rad(self.material.stop_angle_deg))
+    per = _lib.PersistenceStats()
+    _lib.check(self.grid.ctx, lib.sb_avalanche_persistence(
+        self.grid.ctx, start, stop, float(cfg.dry_tolerance_m),
+        float(cfg.mobile_activity_speed_m_s), per), "persistence")
+    ntiles = int(lib.sb_frontier_tile_count(self.grid.ctx))
+    flags = np.zeros(max(ntiles, 1), dtype=np.int32)
+    _lib.check(self.grid.ctx, lib.sb_frontier_active_tiles(self.grid.ctx, flags.ctypes.data,
+                                                           int(ntiles)), "seed tiles")
+    seeds = np.flatnonzero(flags[:ntiles])
+    unique = int(per.unique_cells_ever_activated)
+
+    def mean_deg(x):
+        return float(np.rad2deg(x / unique)) if unique else 0.0
+
+    return DeviceLargeAvalancheResult(
+        classification=diag.classification, transitioned=float(mob.transferred_volume_m3) > 0.0,
+        unstable_cell_count=diag.unstable_cell_count,
+        connected_region_count=diag.connected_region_count,
+        largest_connected_cell_count=diag.largest_connected_cell_count,
+        largest_connected_area_m2=diag.largest_connected_area_m2,
+        largest_connected_mobilizable_volume_m3=diag.largest_connected_mobilizable_volume_m3,
+        mean_excess_start_deg=diag.mean_excess_start_deg,
+        maximum_excess_start_deg=diag.maximum_excess_start_deg,
+        persistence_s=diag.persistence_s, transferred_volume_m3=float(mob.transferred_volume_m3),
+        gravity_initiation_impulse_kg_m_s=np.zeros(2),
+        residual_seed_tile_ids=np.asarray(seeds, dtype=np.int32),
+        union_iterations=diag.union_iterations,
+        parameter_basis=getattr(cfg, "parameter_basis", ""),
+        sensitivity_case=getattr(cfg, "sensitivity_case", ""),
+        newly_activated_volume_m3=float(mob.newly_activated_volume_m3),
+        reactivated_volume_m3=float(mob.reactivated_volume_m3),
+        newly_activated_area_m2=float(mob.newly_activated_area_m2),
+        reactivated_area_step_m2=float(mob.reactivated_area_step_m2),
+        cumulative_resting_to_mobile_m3=float(per.cumulative_r2m_m3),
+        cumulative_mobile_to_resting_m3=float(per.cumulative_m2r_m3),
+        unique_cells_ever_activated=unique,
+        cells_activated_more_than_once=int(per.cells_activated_more_than_once),
+        unique_activated_area_m2=float(per.unique_activated_area_m2),
+        reactivated_area_m2=float(per.reactivated_area_m2),
+        retired_candidate_area_m2=float(per.retired_candidate_area_m2),
+        current_mobile_volume_m3=float(per.current_mobile_volume_m3),
+        moving_mobile_volume_m3=float(per.moving_mobile_volume_m3),
+        maximum_mobile_speed_m_s=float(per.maximum_mobile_speed_m_s),
+        active_tile_count=int(per.active_tile_count),
+        net_terrain_volume_change_m3=float(per.net_terrain_volume_change_m3),
+        net_spatial_transfer_m3=float(per.net_spatial_transfer_m3),
+        mean_activated_slope_deg=mean_deg(per.activated_slope_sum_rad),
+        maximum_activated_slope_deg=float(np.rad2deg(per.activated_slope_max_rad)),
+        mean_slope_minus_theta_stop_deg=mean_deg(per.slope_minus_stop_sum_rad),
+        mean_theta_start_minus_slope_deg=mean_deg(per.start_minus_slope_sum_rad),
+    )
+
+
+B200LargeAvalancheBridge.observe_and_maybe_mobilize = _observe_and_maybe_mobilize
 
 
 def label_mask(grid: DeviceGrid, mask: np.ndarray, connectivity: int = 8):

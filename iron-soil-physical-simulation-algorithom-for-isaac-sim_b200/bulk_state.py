@@ -57,6 +57,9 @@ class B200BulkState:
         self.grid.upload("mobile", np.zeros(initial.shape))
         self.grid.upload("momentum_x", np.zeros(initial.shape))
         self.grid.upload("momentum_y", np.zeros(initial.shape))
+        # reference for the large-avalanche net terrain change (initial_resting)
+        _lib.check(self.grid.ctx, _lib.load().sb_avalanche_set_initial_resting(self.grid.ctx),
+                   "initial resting")
 
     # ------------------------------------------------------------------ time
     @property

@@ -30,6 +30,7 @@
 #include "sb_relax.cuh"
 #include "sb_exchange.cuh"
 #include "sb_deposition.cuh"
+#include "sb_avalanche.cuh"
 #include "sb_path.cuh"
 #include "sb_batch.cuh"
 #include "sb_learned.cuh"
@@ -163,6 +164,18 @@ struct sb_ctx {
   double* m2r = nullptr;
   DepositionOut* dep_out = nullptr;
   DepositionOut* dep_out_host = nullptr;
+  // large-avalanche activation history (flat) and lifecycle sums
+  double* owned_surface = nullptr;
+  int* act_count = nullptr;
+  double* act_first = nullptr;
+  double* act_last = nullptr;
+  double* r2m = nullptr;
+  void* initial_b = nullptr;   // b_eff at sb_avalanche_set_initial_resting (pitched)
+  int* ptiles = nullptr;       // activity tile flags (tile_size tiles)
+  MobilizeOut* mob_out = nullptr;
+  MobilizeOut* mob_out_host = nullptr;
+  double* pers_out = nullptr;
+  double* pers_out_host = nullptr;
   long long launches = 0;
   char err[1024] = {0};
 };
@@ -231,6 +244,7 @@ void* field_ptr(sb_ctx* c, int field, int* is_int, int* is_height, int* is_suppo
     case SB_FIELD_EXTERNAL_Y: return c->ext_y;
     case SB_FIELD_FRONTIER_REACHED: *is_int = 1; return c->reached;
     case SB_FIELD_FORCING: *is_int = 1; if (is_flat) *is_flat = 1; return c->forcing;
+    case SB_FIELD_ACTIVATION_COUNT: *is_int = 1; if (is_flat) *is_flat = 1; return c->act_count;
     default: return nullptr;
   }
 }
@@ -521,6 +535,8 @@ size_t sb_sizeof(const char* type_name) {
       {"sb_patch_desc", sizeof(sb_patch_desc)},
       {"sb_deposition_params", sizeof(sb_deposition_params)},
       {"sb_deposition_stats", sizeof(sb_deposition_stats)},
+      {"sb_mobilize_stats", sizeof(sb_mobilize_stats)},
+      {"sb_persistence_stats", sizeof(sb_persistence_stats)},
   };
   for (const Entry& e : table)
     if (std::strcmp(e.name, type_name) == 0) return e.size;
@@ -637,6 +653,22 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMalloc(&ctx->m2r, n * 8));
   SB_CUDA(ctx, cudaMemsetAsync(ctx->forcing, 0, n * 4, ctx->stream));
   SB_CUDA(ctx, cudaMemsetAsync(ctx->m2r, 0, n * 8, ctx->stream));
+  SB_CUDA(ctx, cudaMalloc(&ctx->owned_surface, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->act_count, n * 4));
+  SB_CUDA(ctx, cudaMalloc(&ctx->act_first, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->act_last, n * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->r2m, n * 8));
+  {
+    void* hist[] = {ctx->owned_surface, ctx->act_first, ctx->act_last, ctx->r2m};
+    for (void* p : hist) SB_CUDA(ctx, cudaMemsetAsync(p, 0, n * 8, ctx->stream));
+    SB_CUDA(ctx, cudaMemsetAsync(ctx->act_count, 0, n * 4, ctx->stream));
+  }
+  SB_CUDA(ctx, cudaMalloc(&ctx->initial_b, (size_t)ctx->pitch * d.ny * ctx->esize));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->initial_b, 0, (size_t)ctx->pitch * d.ny * ctx->esize, ctx->stream));
+  SB_CUDA(ctx, cudaMalloc(&ctx->mob_out, sizeof(MobilizeOut)));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->mob_out_host, sizeof(MobilizeOut)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->pers_out, kPersistSlots * sizeof(double)));
+  SB_CUDA(ctx, cudaMallocHost(&ctx->pers_out_host, kPersistSlots * sizeof(double)));
   SB_CUDA(ctx, cudaMalloc(&ctx->dep_out, sizeof(DepositionOut)));
   SB_CUDA(ctx, cudaMallocHost(&ctx->dep_out_host, sizeof(DepositionOut)));
   void* zero_init[] = {ctx->parent, ctx->latch, ctx->previous, ctx->export_cum, ctx->export_base};
@@ -648,6 +680,7 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   ctx->ftiles0 = (d.ny + d.tile_size - 1) / d.tile_size;
   ctx->ftiles1 = (d.nx + d.tile_size - 1) / d.tile_size;
   const size_t nt = (size_t)ctx->ftiles0 * ctx->ftiles1;
+  SB_CUDA(ctx, cudaMalloc(&ctx->ptiles, nt * sizeof(int)));
   SB_CUDA(ctx, cudaMalloc(&ctx->ftile_next, nt * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->phase[0], nt * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->phase[1], nt * 4));
@@ -732,7 +765,9 @@ int sb_ctx_destroy(sb_ctx* ctx) {
                   ctx->roots.max_exc_start, ctx->roots.max_exc_stop, ctx->roots.prev_overlap,
                   ctx->root_list, ctx->lout, ctx->b_alt, ctx->ftile_next, ctx->phase[0],
                   ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout, ctx->pstate,
-                  ctx->path_count, ctx->forcing, ctx->m2r, ctx->dep_out};
+                  ctx->path_count, ctx->forcing, ctx->m2r, ctx->dep_out, ctx->owned_surface,
+                  ctx->act_count, ctx->act_first, ctx->act_last, ctx->r2m, ctx->initial_b,
+                  ctx->ptiles, ctx->mob_out, ctx->pers_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
@@ -741,6 +776,8 @@ int sb_ctx_destroy(sb_ctx* ctx) {
     if (e) cudaEventDestroy(e);
   if (ctx->xout_host) cudaFreeHost(ctx->xout_host);
   if (ctx->dep_out_host) cudaFreeHost(ctx->dep_out_host);
+  if (ctx->mob_out_host) cudaFreeHost(ctx->mob_out_host);
+  if (ctx->pers_out_host) cudaFreeHost(ctx->pers_out_host);
   if (ctx->pstate_host) cudaFreeHost(ctx->pstate_host);
   if (ctx->path_count_host) cudaFreeHost(ctx->path_count_host);
   if (ctx->path_exec) cudaGraphExecDestroy(ctx->path_exec);
@@ -759,8 +796,32 @@ int sb_synchronize(sb_ctx* ctx) {
   return SB_OK;
 }
 
+}  // extern "C"
+
+// Per-cell float64 records (flat ny*nx, float64 in both precisions).
+static double* flat_f64_field(sb_ctx* ctx, int field) {
+  switch (field) {
+    case SB_FIELD_M2R_CUMULATIVE: return ctx->m2r;
+    case SB_FIELD_R2M_CUMULATIVE: return ctx->r2m;
+    case SB_FIELD_FIRST_ACTIVATION_TIME: return ctx->act_first;
+    case SB_FIELD_LAST_ACTIVATION_TIME: return ctx->act_last;
+    case SB_FIELD_OWNED_SURFACE: return ctx->owned_surface;
+    case SB_FIELD_OWNED_EXPORT_BASELINE: return ctx->export_base;
+    case SB_FIELD_EXPORT_CUMULATIVE: return ctx->export_cum;
+    default: return nullptr;
+  }
+}
+
+extern "C" {
+
 int sb_upload(sb_ctx* ctx, int field, const double* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
+  if (double* rec = flat_f64_field(ctx, field)) {  // checkpoint restore of a record
+    SB_CUDA(ctx, cudaMemcpyAsync(rec, host, (size_t)ctx->d.ny * ctx->d.nx * 8,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return SB_OK;
+  }
   int is_int, is_h, is_s, is_flat;
   void* dst = field_ptr(ctx, field, &is_int, &is_h, &is_s, &is_flat);
   if (!dst || is_int) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] field %d is not a float field", field);
@@ -802,8 +863,8 @@ int sb_upload(sb_ctx* ctx, int field, const double* host) {
 
 int sb_download(sb_ctx* ctx, int field, double* host) {
   if (!ctx || !host) return SB_ERR_BAD_ARG;
-  if (field == SB_FIELD_M2R_CUMULATIVE) {  // flat double in both precisions
-    SB_CUDA(ctx, cudaMemcpyAsync(host, ctx->m2r, (size_t)ctx->d.ny * ctx->d.nx * 8,
+  if (double* rec = flat_f64_field(ctx, field)) {
+    SB_CUDA(ctx, cudaMemcpyAsync(host, rec, (size_t)ctx->d.ny * ctx->d.nx * 8,
                                  cudaMemcpyDeviceToHost, ctx->stream));
     SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return SB_OK;
@@ -1602,6 +1663,111 @@ extern "C" int sb_deposition_step(sb_ctx* ctx, double dt_s, const sb_deposition_
   out->deposited_w6_quanta = fx(ctx) ? o.volume_w6_quanta : 0;
   out->cells = o.cells;
   out->pad = 0;
+  return SB_OK;
+}
+
+extern "C" int sb_avalanche_set_initial_resting(sb_ctx* ctx) {
+  if (!ctx) return SB_ERR_BAD_ARG;
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->initial_b, ctx->b, (size_t)ctx->pitch * ctx->d.ny * ctx->esize,
+                               cudaMemcpyDeviceToDevice, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+extern "C" int sb_avalanche_mobilize(sb_ctx* ctx, double activation_time_s,
+                                     double mobilization_depth_m, double dry_tolerance_m,
+                                     sb_mobilize_stats* out) {
+  if (!ctx || !out) return SB_ERR_BAD_ARG;
+  if (!std::isfinite(activation_time_s) || !(mobilization_depth_m > 0.0) ||
+      !(dry_tolerance_m >= 0.0))
+    return fail(ctx, SB_ERR_BAD_ARG, "[GpuLargeAvalanche] invalid mobilization parameters");
+  MobilizeConst c{ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m,
+                  ctx->d.dx_m * ctx->d.dy_m / 6.0, mobilization_depth_m, dry_tolerance_m,
+                  activation_time_s};
+  const int P = ctx->parity_host;
+  const int grid = ctx->ledger_blocks;
+  if (fx(ctx))
+    mobilize_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (const int32_t*)ctx->z, (int32_t*)ctx->b, (int32_t*)ctx->h[P], ctx->parent, ctx->latch,
+        (const float*)ctx->severity, ctx->owned_surface, ctx->export_base, ctx->export_cum,
+        ctx->act_count, ctx->act_first, ctx->act_last, ctx->r2m, ctx->lout, ctx->partials,
+        ctx->arrive, ctx->mob_out);
+  else
+    mobilize_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (const double*)ctx->z, (double*)ctx->b, (double*)ctx->h[P], ctx->parent, ctx->latch,
+        (const double*)ctx->severity, ctx->owned_surface, ctx->export_base, ctx->export_cum,
+        ctx->act_count, ctx->act_first, ctx->act_last, ctx->r2m, ctx->lout, ctx->partials,
+        ctx->arrive, ctx->mob_out);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->mob_out_host, ctx->mob_out, sizeof(MobilizeOut),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const MobilizeOut& o = *ctx->mob_out_host;
+  const double f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
+  out->transferred_volume_m3 = fx(ctx) ? (double)o.transferred_w6_quanta * ctx->quantum * f : o.v[0];
+  out->newly_activated_volume_m3 = o.v[1];
+  out->reactivated_volume_m3 = o.v[2];
+  out->newly_activated_area_m2 = o.v[3];
+  out->reactivated_area_step_m2 = o.v[4];
+  out->transferred_w6_quanta = fx(ctx) ? o.transferred_w6_quanta : 0;
+  out->cells = (int)o.v[5];
+  out->pad = 0;
+  return SB_OK;
+}
+
+extern "C" int sb_avalanche_persistence(sb_ctx* ctx, double start_angle_rad, double stop_angle_rad,
+                                        double dry_tolerance_m, double activity_speed_m_s,
+                                        sb_persistence_stats* out) {
+  if (!ctx || !out) return SB_ERR_BAD_ARG;
+  PersistConst c{ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->d.tile_size, ctx->ftiles1, ctx->quantum,
+                 ctx->d.datum_m, ctx->d.dx_m * ctx->d.dy_m / 6.0, start_angle_rad, stop_angle_rad,
+                 dry_tolerance_m, activity_speed_m_s};
+  const size_t nt = (size_t)ctx->ftiles0 * ctx->ftiles1;
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->ptiles, 0, nt * sizeof(int), ctx->stream));
+  const int P = ctx->parity_host;
+  const int grid = ctx->ledger_blocks;
+  if (fx(ctx))
+    persistence_kernel<true><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (const int32_t*)ctx->initial_b, (const int32_t*)ctx->b, (const int32_t*)ctx->h[P],
+        (const float*)ctx->qx[P], (const float*)ctx->qy[P], (const float*)ctx->slope, ctx->parent,
+        ctx->latch, ctx->act_count, ctx->r2m, ctx->m2r, ctx->ptiles, ctx->partials, ctx->arrive,
+        ctx->pers_out);
+  else
+    persistence_kernel<false><<<grid, kThreads, 0, ctx->stream>>>(
+        c, (const double*)ctx->initial_b, (const double*)ctx->b, (const double*)ctx->h[P],
+        (const double*)ctx->qx[P], (const double*)ctx->qy[P], (const double*)ctx->slope,
+        ctx->parent, ctx->latch, ctx->act_count, ctx->r2m, ctx->m2r, ctx->ptiles, ctx->partials,
+        ctx->arrive, ctx->pers_out);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  std::vector<int> flags(nt);
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->pers_out_host, ctx->pers_out, kPersistSlots * sizeof(double),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(flags.data(), ctx->ptiles, nt * sizeof(int), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const double* v = ctx->pers_out_host;
+  out->unique_cells_ever_activated = (int)v[14];
+  out->cells_activated_more_than_once = (int)v[15];
+  out->current_mobile_cell_count = (int)v[16];
+  out->retired_candidate_cell_count = (int)v[17];
+  out->active_tile_count = (int)std::count_if(flags.begin(), flags.end(), [](int f) { return f != 0; });
+  out->pad = 0;
+  out->cumulative_r2m_m3 = v[0];
+  out->cumulative_m2r_m3 = v[1];
+  out->unique_activated_area_m2 = v[2];
+  out->reactivated_area_m2 = v[3];
+  out->current_mobile_volume_m3 = v[4];
+  out->maximum_mobile_speed_m_s = v[5];
+  out->net_terrain_volume_change_m3 = v[6];
+  out->net_spatial_transfer_m3 = v[7];
+  out->activated_slope_sum_rad = v[8];
+  out->activated_slope_max_rad = v[9];
+  out->slope_minus_stop_sum_rad = v[10];
+  out->start_minus_slope_sum_rad = v[11];
+  out->retired_candidate_area_m2 = v[12];
+  out->moving_mobile_volume_m3 = v[13];
   return SB_OK;
 }
 
