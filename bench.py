@@ -193,7 +193,20 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     from soilb200.pipeline import PlainPath
 
     torch.cuda.set_device(local_rank)
-    cfg = workloads.config1(N, seed=1, dx=DX)
+    site = args.workload == "site_c4_4096"
+    if site:
+        n = 4096
+        cfg = workloads.config4(n, seed=4, dx=DX)
+
+        class _Cuts:  # the 64 cuts' union as one per-step command
+            @staticmethod
+            def footprint(t):
+                return workloads.merged_footprint(cfg["cuts"], t)
+        cut = _Cuts()
+    else:
+        n = N
+        cfg = workloads.config1(N, seed=1, dx=DX)
+        cut = cfg["cut"]
     # one CUDA graph per step; with SOILB200_NO_GRAPH=1 (profilers) the same
     # kernels are launched operator by operator instead
     fused = os.environ.get("SOILB200_NO_GRAPH") != "1"
@@ -201,7 +214,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                      device=local_rank, residual="gated", fused=fused)
     grid = path.grid
     total_steps = args.warmup + args.steps
-    sched = cut_schedule(cfg["cut"], total_steps, pinned=True)
+    sched = cut_schedule(cut, total_steps, pinned=True)
     stream = torch.cuda.ExternalStream(grid.stream_handle(), device=local_rank)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
 
@@ -240,7 +253,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             d2h += stats_bytes
     launches = grid.kernel_launches() - launches0
     dev_s = sum(step_ms) / 1000.0
-    cells = N * N
+    cells = n * n
     cell_substeps = cells * sum(substeps)
     if world > 1:
         import torch.distributed as dist
@@ -259,12 +272,15 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     result = None
     if rank == 0:
         result = {
-            "metric": METRIC, "value": cell_substeps / dev_s if dev_s > 0 else 0.0, "unit": UNIT,
+            "metric": ("Mobile V2 cell-substeps/s at 4096^2 (config-4 site, 64 cuts)" if site
+                       else METRIC),
+            "value": cell_substeps / dev_s if dev_s > 0 else 0.0, "unit": UNIT,
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": dev_s * 1000.0 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32-quanta+f32 (f64/i64 ledger)",
-            "data": "synthetic (seeded config-1 value-noise pile + bucket cut)",
-            "config": {"workload": "config1_plain_path_701", "grid": [N, N], "dx_m": DX,
+            "data": ("synthetic (seeded config-4 value-noise site + 64 bucket cuts)" if site
+                     else "synthetic (seeded config-1 value-noise pile + bucket cut)"),
+            "config": {"workload": args.workload, "grid": [n, n], "dx_m": DX,
                        "dt_s": DT, "steps_simulated_before_timing": args.warmup,
                        "step": "cut entrain -> Mobile V2 (all substeps) -> labelling -> "
                                "gated residual frontier",
@@ -282,7 +298,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "mean_launch_ms": per_launch_ms,
-                         "traffic": NCU_TRAFFIC_BYTES["config1_plain_path_701"],
+                         "traffic": NCU_TRAFFIC_BYTES.get(args.workload),
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
@@ -458,23 +474,29 @@ def run_repose(args, rounds: int = 4, eps_slope: float = 1e-4):
     tol = eps_slope * DX
     q = 2.0 ** k
 
-    def one(r):
+    # one resident grid per arm (buffers, graphs and the network's workspace are
+    # reused across trials); each trial re-uploads the post-cut surface untimed
+    grids = {}
+    for r in (0, rounds):
         g = soilb200.DeviceGrid(b.shape, DX, DX, precision="fx32", height_exponent=k, datum_m=datum)
-        g.upload("b_eff", b)
         g.upload("z_base", np.zeros_like(b))
-        lr = learned.LearnedRelaxation(g, net, 35.0)
+        grids[r] = (g, learned.LearnedRelaxation(g, net, 35.0))
+
+    def one(r):
+        g, lr = grids[r]
+        g.upload("b_eff", b)
         s0 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
         stream = torch.cuda.ExternalStream(g.stream_handle())
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        launches0 = g.kernel_launches()
         e0.record(stream)
         st = lr.relax(tol, max_iterations=400000, rounds=r)
         e1.record(stream)
         e1.synchronize()
         s1 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
-        launches = g.kernel_launches()
-        g.close()
-        return e0.elapsed_time(e1), int(st.iterations), bool(st.converged), s0 == s1, launches
+        return (e0.elapsed_time(e1), int(st.iterations), bool(st.converged), s0 == s1,
+                g.kernel_launches() - launches0)
 
     for _ in range(args.warmup):
         one(0)
@@ -484,6 +506,8 @@ def run_repose(args, rounds: int = 4, eps_slope: float = 1e-4):
         for _ in range(args.steps):
             plain.append(one(0))
             learn.append(one(rounds))
+    for g, _ in grids.values():
+        g.close()
     pm = statistics.median(p[0] for p in plain)
     lm = statistics.median(p[0] for p in learn)
     return {"metric": "ms to repose at 701^2 after the cut, learned proposal + plain sweeps (35 deg, eps 1e-4)",
@@ -577,8 +601,9 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el * 1000.0 / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded config-1 value-noise pile + bucket cut)",
-            "config": {"workload": "config1_plain_path_701", "grid": [N, N], "dx_m": DX,
+            "data": ("synthetic (seeded config-4 value-noise site + 64 bucket cuts)" if site
+                     else "synthetic (seeded config-1 value-noise pile + bucket cut)"),
+            "config": {"workload": args.workload, "grid": [n, n], "dx_m": DX,
                        "dt_s": DT},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                              "sample": f"{args.steps} physics steps ({subs} substeps) after "
@@ -596,7 +621,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="config1_plain_path_701",
                     choices=["config1_plain_path_701", "mobile_v2_4096", "batched_c2_512",
-                             "repose_701"])
+                             "repose_701", "site_c4_4096"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

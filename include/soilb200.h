@@ -462,7 +462,8 @@ void* sb_batch_stream(sb_batch* batch);
  * the tensor cores; weights prepacked per row offset dy in the canonical
  * K-major layout (n = dx*cout + co rows, k = ci).  Device pointers, 16-byte
  * aligned; work is queued on `stream`; d_status (device int, may be null)
- * becomes 1 if a bounded device wait gave up. */
+ * becomes 1 if a bounded device wait gave up.  out_f32 = 0 writes BF16 (all
+ * cout channels); out_f32 = k (multiple of 4) writes FP32, first k channels. */
 const char* sb_learned_last_error(void);
 int sb_learned_conv(const void* in, void* out, const void* wpk, const void* mask, int batch, int h,
                     int w, int cin, int cout, int relu, int out_f32, int rows_per_cta,
@@ -474,7 +475,8 @@ int sb_learned_wgrad(const void* in, const void* grad, float* partial, size_t pa
                      int* d_status, void* stream);
 /* Features (bf16 [batch][h][w][16]: channels 0..3 = height drop along the
  * east, north, north-east, north-west edges over L*tan_crit) of float64
- * heights; training loss of f32 fluxes against target height changes. */
+ * heights; training loss of f32 fluxes [pixel][4] against target height
+ * changes. */
 int sb_learned_features_f64(const double* heights, void* feat, int batch, int h, int w, double dx,
                             double dy, double tan_crit, void* stream);
 int sb_learned_loss(const float* flux, const float* target_dh, float* resid, void* dflux,
@@ -482,7 +484,8 @@ int sb_learned_loss(const float* flux, const float* target_dh, float* resid, voi
                     double tan_crit, float inv_scale2_n, void* stream);
 int sb_learned_loss_blocks(int batch, int h, int w);
 /* On a context's resident b_eff (SB_FX32): features, then the network's
- * fluxes applied in whole height quanta (tq: int32 [ny][nx][4] scratch). */
+ * fluxes (f32 [ny][nx][4]) applied in whole height quanta (tq: int32
+ * [ny][nx][4] scratch). */
 int sb_learned_features(sb_ctx* ctx, void* feat, double tan_crit);
 int sb_learned_apply(sb_ctx* ctx, const float* flux, int32_t* tq, double tan_crit);
 

@@ -110,13 +110,13 @@ __device__ __forceinline__ uint32_t core_off(int r, int k, int kdim) {
 
 struct ConvArgs {
   const __nv_bfloat16* in;      // [batch][h][w][cin]
-  void* out;                    // [batch][h][w][cout], bf16 or f32 (out_f32)
+  void* out;                    // bf16 [batch][h][w][cout], or f32 [batch][h][w][out_f32]
   const __nv_bfloat16* wpk;     // 3 row offsets x canonical B (n = dx*cout + co, k = ci)
   const __nv_bfloat16* mask;    // optional [batch][h][w][cout]: out *= (mask > 0)
   int batch, h, w;
   int rows_per_cta;
   int relu;
-  int out_f32;
+  int out_f32;                  // 0: bf16, all channels; k (multiple of 4): f32, first k channels
   int* status;                  // set to 1 if a bounded wait gave up
 };
 
@@ -243,9 +243,10 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
             if (!(__bfloat162float(mk[j]) > 0.f)) o[j] = 0.f;
         }
         if (a.out_f32) {
-          float* op = reinterpret_cast<float*>(a.out) + pix * COUT + c8;
-#pragma unroll
-          for (int j = 0; j < 8; ++j) op[j] = o[j];
+          float* op = reinterpret_cast<float*>(a.out) + pix * a.out_f32 + c8;
+          if (c8 < a.out_f32) *reinterpret_cast<float4*>(op) = make_float4(o[0], o[1], o[2], o[3]);
+          if (c8 + 4 < a.out_f32)
+            *reinterpret_cast<float4*>(op + 4) = make_float4(o[4], o[5], o[6], o[7]);
         } else {
           __align__(16) __nv_bfloat16 ob[8];
 #pragma unroll
@@ -477,7 +478,7 @@ __device__ __forceinline__ double learned_transfer(const LearnedGeom& g, double 
 // Fixed point: transfers rounded to whole quanta per edge (int32 [pixel][4]),
 // then gathered -- every quantum leaves one cell and enters one neighbour.
 __global__ void learned_quantize_kernel(const LearnedGeom g, const int32_t* __restrict__ hq,
-                                        const float* __restrict__ flux /*[pixel][16]*/,
+                                        const float* __restrict__ flux /*[pixel][4]*/,
                                         int32_t* __restrict__ tq /*[pixel][4]*/) {
   const long long n = (long long)g.batch * g.h * g.w;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -495,7 +496,7 @@ __global__ void learned_quantize_kernel(const LearnedGeom g, const int32_t* __re
       int q = 0;
       if (rn < g.h && cn >= 0 && cn < g.w) {
         const double hn = (double)H[(size_t)rn * g.pitch + cn] * g.Q;
-        const double t = learned_transfer(g, (double)flux[i * 16 + k], hc, hn);
+        const double t = learned_transfer(g, (double)flux[i * 4 + k], hc, hn);
         q = (int)trunc(t / g.Q);  // toward zero: stays within the half-difference limit
       }
       tq[i * 4 + k] = q;
@@ -546,10 +547,10 @@ __global__ void learned_loss_kernel(const LearnedGeom g, const float* __restrict
     for (int k = 0; k < 4; ++k) {
       int dr, dc;
       edge_of(k, dr, dc);
-      if (r + dr < g.h && c + dc >= 0 && c + dc < g.w) dh -= flux[i * 16 + k] * s;
+      if (r + dr < g.h && c + dc >= 0 && c + dc < g.w) dh -= flux[i * 4 + k] * s;
       const int rs = r - dr, cs = c - dc;
       if (rs >= 0 && cs >= 0 && cs < g.w)
-        dh += flux[(((long long)bb * g.h + rs) * g.w + cs) * 16 + k] * s;
+        dh += flux[(((long long)bb * g.h + rs) * g.w + cs) * 4 + k] * s;
     }
     const float e = dh - target_dh[i];
     resid[i] = e;

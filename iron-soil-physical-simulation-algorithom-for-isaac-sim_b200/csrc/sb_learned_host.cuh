@@ -71,6 +71,8 @@ int sb_learned_conv(const void* in, void* out, const void* wpk, const void* mask
   if (!in || !out || !wpk || batch <= 0 || h <= 0 || w <= 0 || !conv_shape_ok(cin, cout) ||
       rows_per_cta <= 0)
     return lfail(SB_ERR_BAD_ARG, "[soilb200] conv: bad arguments (cin, cout in {16, 32})");
+  if (out_f32 < 0 || out_f32 > cout || (out_f32 & 3))
+    return lfail(SB_ERR_BAD_ARG, "[soilb200] conv: out_f32 must be 0 or a multiple of 4 <= cout");
   if (((uintptr_t)in | (uintptr_t)out | (uintptr_t)wpk | (uintptr_t)mask) & 15)
     return lfail(SB_ERR_BAD_ARG, "[soilb200] conv: buffers must be 16-byte aligned");
   ConvArgs a{(const __nv_bfloat16*)in, out, (const __nv_bfloat16*)wpk,
@@ -118,7 +120,7 @@ int sb_learned_features_f64(const double* heights, void* feat, int batch, int h,
   return lcuda(cudaGetLastError());
 }
 
-// Training loss of predicted fluxes (f32 [pixel][16]) against target height
+// Training loss of predicted fluxes (f32 [pixel][4]) against target height
 // changes (f32 [pixel]); resid (f32 [pixel]) and dflux (bf16 [pixel][16]) are
 // outputs; loss_part holds one double per block (grid_for blocks).
 int sb_learned_loss(const float* flux, const float* target_dh, float* resid, void* dflux,
@@ -141,7 +143,7 @@ int sb_learned_loss_blocks(int batch, int h, int w) {
 
 // Proposal on a context's resident b_eff (SB_FX32): features into feat
 // (bf16 [ny][nx][16]); after the caller's network has produced flux (f32
-// [ny][nx][16]), sb_learned_apply moves the proposed transfers in whole
+// [ny][nx][4]), sb_learned_apply moves the proposed transfers in whole
 // quanta (tq: int32 [ny][nx][4] scratch), exactly conserving sum(b_eff).
 int sb_learned_features(sb_ctx* ctx, void* feat, double tan_crit) {
   if (!ctx || !feat || !(tan_crit > 0.0)) return SB_ERR_BAD_ARG;

@@ -113,20 +113,24 @@ def conv_rows(b: int, h: int, w: int) -> int:
     return int(min(32, max(4, -(-b * h * tiles // (148 * 4)))))
 
 
-def conv(x, wpk, cin: int, cout: int, *, relu: bool, out_f32: bool = False, mask=None,
+def conv(x, wpk, cin: int, cout: int, *, relu: bool, out_f32: bool | int = False, mask=None,
          status=None, stream=None, rows: int | None = None):
-    """One tensor-core 3x3 convolution of a BF16 NHWC tensor [B, H, W, cin]."""
+    """One tensor-core 3x3 convolution of a BF16 NHWC tensor [B, H, W, cin].
+
+    ``out_f32``: False -> BF16 output of all channels; True -> FP32, all
+    channels; an int k -> FP32, the first k channels only."""
     torch = _torch()
     b, h, w, c = x.shape
     rows = conv_rows(b, h, w) if rows is None else int(rows)
     if c != cin:
         raise ValueError(f"[soilb200] conv input has {c} channels, expected {cin}")
-    out = torch.empty(b, h, w, cout, dtype=torch.float32 if out_f32 else torch.bfloat16,
-                      device=x.device)
+    nf = (cout if out_f32 is True else int(out_f32)) if out_f32 is not False else 0
+    out = torch.empty(b, h, w, nf if nf else cout,
+                      dtype=torch.float32 if nf else torch.bfloat16, device=x.device)
     st = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
     _ok(_lib.load().sb_learned_conv(x.data_ptr(), out.data_ptr(), wpk.data_ptr(),
                                     mask.data_ptr() if mask is not None else None, b, h, w, cin,
-                                    cout, int(relu), int(out_f32), rows,
+                                    cout, int(relu), nf, rows,
                                     status.data_ptr() if status is not None else None, st),
         "conv")
     return out
@@ -148,7 +152,7 @@ def wgrad(x, g, cin: int, cout: int, *, status=None, stream=None, rows: int = 16
 
 
 def network_forward(net: ReposeNet, feat, packed=None, stream=None):
-    """Activations (inputs of layers 1..3) and the f32 fluxes [B, H, W, 16]."""
+    """Activations (inputs of layers 1..3) and the f32 fluxes [B, H, W, 4]."""
     packed = packed or net.packed()
     acts = []
     a = feat
@@ -156,8 +160,8 @@ def network_forward(net: ReposeNet, feat, packed=None, stream=None):
         last = li == len(LAYERS) - 1
         if li > 0:
             acts.append(a)
-        a = conv(a, packed[li], ci, co, relu=not last, out_f32=last, status=net.status,
-                 stream=stream)
+        a = conv(a, packed[li], ci, co, relu=not last, out_f32=4 if last else False,
+                 status=net.status, stream=stream)
     return acts, a
 
 

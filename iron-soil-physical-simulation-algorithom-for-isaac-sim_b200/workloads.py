@@ -182,3 +182,63 @@ def config3_patch(i: int, n: int = 128, dx: float = 0.05) -> np.ndarray:
             np.abs(h[1:, 1:] - h[:-1, :-1]).max() / diag, np.abs(h[1:, :-1] - h[:-1, 1:]).max() / diag)
     return (h - h.min()) * (target / s)
 
+
+class SiteCut:
+    """A config-1 bucket cut evaluated on a local window of a large grid
+    (same footprint rule as ``BucketCut``; cost proportional to the window)."""
+
+    def __init__(self, shape, dx: float, initial_surface: np.ndarray, start, heading,
+                 width: float = 1.8, length: float = 0.3, travel: float = 6.0,
+                 speed: float = 0.5, depth: float = 0.4) -> None:
+        ny, nx = shape
+        self.nx = nx
+        self.speed, self.travel, self.length, self.width = speed, travel, length, width
+        self.start = (float(start[0]), float(start[1]))
+        hx, hy = heading
+        norm = float(np.hypot(hx, hy))
+        self._h = (hx / norm, hy / norm)
+        reach = travel + width + length
+        c0 = max(0, int((self.start[0] - reach) / dx) - 1)
+        c1 = min(nx, int((self.start[0] + reach) / dx) + 2)
+        r0 = max(0, int((self.start[1] - reach) / dx) - 1)
+        r1 = min(ny, int((self.start[1] + reach) / dx) + 2)
+        rows, cols = np.indices((r1 - r0, c1 - c0))
+        rows, cols = rows + r0, cols + c0
+        self._flat = (rows * nx + cols).ravel().astype(np.int64)
+        px = cols.ravel() * dx - self.start[0]
+        py = rows.ravel() * dx - self.start[1]
+        self._along = px * self._h[0] + py * self._h[1]
+        self._across = -px * self._h[1] + py * self._h[0]
+        self._target = np.asarray(initial_surface, np.float64).ravel()[self._flat] - depth
+
+    def footprint(self, t_s: float):
+        s = min(self.speed * max(t_s, 0.0), self.travel)
+        inside = ((self._along <= s) & (self._along >= s - self.length)
+                  & (np.abs(self._across) <= 0.5 * self.width))
+        return self._flat[inside], self._target[inside]
+
+
+def merged_footprint(cuts, t_s: float):
+    """Union of several cuts' footprints: each cell once, at its lowest target."""
+    parts = [c.footprint(t_s) for c in cuts]
+    idx = np.concatenate([p[0] for p in parts]) if parts else np.zeros(0, np.int64)
+    tgt = np.concatenate([p[1] for p in parts]) if parts else np.zeros(0)
+    if idx.size == 0:
+        return idx.astype(np.int32), tgt
+    order = np.lexsort((tgt, idx))
+    idx, tgt = idx[order], tgt[order]
+    first = np.ones(idx.size, bool)
+    first[1:] = idx[1:] != idx[:-1]
+    return idx[first].astype(np.int32), tgt[first]
+
+
+def config4(n: int = 4096, seed: int = 4, dx: float = 0.05, n_cuts: int = 64):
+    b = noise_pile(n, seed, dx, base_cells=max(12, round(12 * n / 701)))
+    rng = np.random.default_rng(seed + 1)
+    cuts = []
+    for _ in range(n_cuts):
+        x, y = rng.uniform(0.15, 0.85, size=2) * (n - 1) * dx
+        ang = rng.uniform(0.0, 2.0 * np.pi)
+        cuts.append(SiteCut((n, n), dx, b, (x, y), (np.cos(ang), np.sin(ang))))
+    return {"b_eff": b, "z_base": np.zeros((n, n)), "cuts": cuts}
+
