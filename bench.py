@@ -457,7 +457,7 @@ def c1_after_cut(n: int = N):
     return b
 
 
-def run_repose(args, rounds: int = 4, eps_slope: float = 1e-4):
+def run_repose(args, rounds: int = 8, plain_between: int = 5, eps_slope: float = 1e-4):
     """Second headline metric: ms to repose at 701^2 after the cut, the learned
     proposal (tensor-core conv net, flux form, exact quanta) + plain sweeps
     against plain sweeps alone, same tolerance (eps * dx m), same start."""
@@ -491,7 +491,8 @@ def run_repose(args, rounds: int = 4, eps_slope: float = 1e-4):
         torch.cuda.synchronize()
         launches0 = g.kernel_launches()
         e0.record(stream)
-        st = lr.relax(tol, max_iterations=400000, rounds=r)
+        st = lr.relax(tol, max_iterations=400000, rounds=r,
+                      plain_between=plain_between if r else 0)
         e1.record(stream)
         e1.synchronize()
         s1 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
@@ -514,7 +515,8 @@ def run_repose(args, rounds: int = 4, eps_slope: float = 1e-4):
             "value": lm, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": lm, "higher_is_better": False, "dtype": "int32-quanta (bf16 net, f32 accumulate)",
             "data": "synthetic (config-1 pile after the full straight cut)",
-            "config": {"workload": "repose_701", "proposal_rounds": rounds, "tolerance_m": tol,
+            "config": {"workload": "repose_701", "proposal_rounds": rounds,
+                       "plain_sweeps_between_proposals": plain_between, "tolerance_m": tol,
                        "plain_ms": pm, "speedup_vs_plain": pm / lm,
                        "plain_iterations": plain[0][1], "learned_iterations": learn[0][1],
                        "converged": all(p[2] for p in plain + learn),

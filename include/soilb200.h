@@ -381,6 +381,21 @@ int sb_avalanche_persistence(sb_ctx* ctx, double start_angle_rad, double stop_an
                              double dry_tolerance_m, double activity_speed_m_s,
                              sb_persistence_stats* out);
 
+/* ---- Surface publication (runtime/bulk_state_authority.py: dirty tracking
+ *      :733-781 with kernels :156-192, tile downloads :1280-1328, batched
+ *      bilinear queries :1138-1183 with kernel :195-231) ---------------------
+ * Free surface = b_eff + mobile.  sb_surface_capture snapshots it;
+ * sb_surface_dirty_tiles flags every tile (tile_size of the context, row-major
+ * tile ids) holding a cell whose surface moved by more than tolerance_m since
+ * the snapshot (flags: ceil(ny/tile) * ceil(nx/tile) int32).
+ * sb_surface_region downloads rows [r0, r1) x cols [c0, c1).
+ * sb_surface_sample_bilinear samples at fractional (row, col), clamped. */
+int sb_surface_capture(sb_ctx* ctx);
+int sb_surface_dirty_tiles(sb_ctx* ctx, double tolerance_m, int32_t* flags, int ntiles);
+int sb_surface_region(sb_ctx* ctx, int r0, int r1, int c0, int c1, double* out);
+int sb_surface_sample_bilinear(sb_ctx* ctx, const double* rows, const double* cols, int count,
+                               double* out);
+
 /* ---- Mobile -> Resting deposition (bulk_interaction/warp_deposition.py:23-130,
  *      WarpDepositionOperator.step_resident :183-238) -------------------------
  * Every cell with mobile material, no tool forcing (SB_FIELD_FORCING) and

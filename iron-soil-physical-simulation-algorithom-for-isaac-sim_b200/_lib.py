@@ -262,6 +262,11 @@ _PROTOTYPES = {
                                         C.POINTER(MobilizeStats)]),
     "sb_avalanche_persistence": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double,
                                            C.c_double, C.POINTER(PersistenceStats)]),
+    "sb_surface_capture": (C.c_int, [C.c_void_p]),
+    "sb_surface_dirty_tiles": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_int]),
+    "sb_surface_region": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "sb_surface_sample_bilinear": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                             C.c_void_p]),
     "sb_batch_create": (C.c_int, [C.c_int, C.c_int, C.POINTER(PatchDesc),
                                   C.POINTER(C.c_void_p)]),
     "sb_batch_destroy": (C.c_int, [C.c_void_p]),

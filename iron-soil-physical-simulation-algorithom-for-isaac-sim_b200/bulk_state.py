@@ -52,6 +52,7 @@ class B200BulkState:
         self.tile_size = int(tile_size)
         self.precision = precision
         self._timestamp_device_s = 0.0
+        self._dirty_tile_ids: set[int] = set()
         self.grid.upload("z_base", z)
         self.grid.upload("b_eff", initial)
         self.grid.upload("mobile", np.zeros(initial.shape))
@@ -84,6 +85,81 @@ class B200BulkState:
 
     def close(self) -> None:
         self.grid.close()
+
+    # ------------------------------------------------------ surface publication
+    def mark_dirty_tiles(self, tile_ids) -> None:
+        for tile_id in np.asarray(tuple(tile_ids), dtype=np.int64).ravel():
+            if tile_id < 0 or tile_id >= self.tile_count:
+                raise ValueError("[DeviceBulkState] dirty tile ID outside grid")
+            self._dirty_tile_ids.add(int(tile_id))
+
+    def mark_dirty_bbox(self, bbox_yx) -> None:
+        row0, row1, col0, col1 = (int(v) for v in bbox_yx)
+        if row1 <= row0 or col1 <= col0:
+            return
+        tiles_y, tiles_x = self.tile_shape
+        fy, ly = max(0, row0 // self.tile_size), min(tiles_y - 1, (row1 - 1) // self.tile_size)
+        fx, lx = max(0, col0 // self.tile_size), min(tiles_x - 1, (col1 - 1) // self.tile_size)
+        self.mark_dirty_tiles(r * tiles_x + c for r in range(fy, ly + 1) for c in range(fx, lx + 1))
+
+    def capture_surface_for_dirty_tracking(self) -> None:
+        """Snapshot the resident free surface before a mutating device operator."""
+        _lib.check(self.grid.ctx, _lib.load().sb_surface_capture(self.grid.ctx), "capture")
+
+    def collect_surface_dirty_tiles(self, *, tolerance_m: float = 1.0e-10) -> np.ndarray:
+        """Tiles whose surface moved since the snapshot (compact flags only)."""
+        tol = float(tolerance_m)
+        if not np.isfinite(tol) or tol < 0.0:
+            raise ValueError("[DeviceBulkState] dirty tolerance must be finite/non-negative")
+        flags = np.zeros(self.tile_count, dtype=np.int32)
+        _lib.check(self.grid.ctx, _lib.load().sb_surface_dirty_tiles(
+            self.grid.ctx, tol, flags.ctypes.data, int(flags.size)), "dirty tiles")
+        ids = np.flatnonzero(flags).astype(np.int32)
+        self.mark_dirty_tiles(ids)
+        return ids
+
+    def consume_dirty_tile_ids(self) -> np.ndarray:
+        out = np.asarray(sorted(self._dirty_tile_ids), dtype=np.int32)
+        self._dirty_tile_ids.clear()
+        return out
+
+    def download_dirty_tiles(self, tile_ids=None) -> dict:
+        """Current free surface of the selected (default: all dirty) tiles, each
+        with its one-cell overlap to the next tile, as the reference publishes."""
+        selected = (np.asarray(tuple(tile_ids), dtype=np.int32) if tile_ids is not None
+                    else self.consume_dirty_tile_ids())
+        tiles_y, tiles_x = self.tile_shape
+        out = {}
+        for tile in selected:
+            t = int(tile)
+            if t < 0 or t >= tiles_y * tiles_x:
+                raise ValueError("[DeviceBulkState] dirty tile ID outside grid")
+            row, col = divmod(t, tiles_x)
+            r0, c0 = row * self.tile_size, col * self.tile_size
+            r1 = min(r0 + self.tile_size + 1, self.shape[0])
+            c1 = min(c0 + self.tile_size + 1, self.shape[1])
+            buf = np.empty((r1 - r0, c1 - c0), dtype=np.float64)
+            _lib.check(self.grid.ctx, _lib.load().sb_surface_region(
+                self.grid.ctx, r0, r1, c0, c1, buf.ctypes.data), "tile download")
+            out[t] = buf
+        return out
+
+    def sample_surface_bilinear(self, row_col, *, source: str) -> np.ndarray:
+        """Batched bilinear free-surface heights at fractional (row, col)."""
+        if not source:
+            raise ValueError("[DeviceBulkState] terrain query source must be non-empty")
+        q = np.asarray(row_col, dtype=np.float64)
+        if q.ndim != 2 or q.shape[1] != 2 or not np.all(np.isfinite(q)):
+            raise ValueError("[DeviceBulkState] terrain queries must be finite [N,2]")
+        if q.shape[0] == 0:
+            return np.empty(0, dtype=np.float64)
+        rows = np.ascontiguousarray(q[:, 0])
+        cols = np.ascontiguousarray(q[:, 1])
+        out = np.empty(q.shape[0], dtype=np.float64)
+        _lib.check(self.grid.ctx, _lib.load().sb_surface_sample_bilinear(
+            self.grid.ctx, rows.ctypes.data, cols.ctypes.data, int(q.shape[0]), out.ctypes.data),
+            "surface query")
+        return out
 
     # ---------------------------------------------------------------- ledger
     def reservoir_reduction(self, density_kg_m3: float) -> dict:

@@ -631,6 +631,8 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
   const float dtf = (float)sub_dt;
   const float dec = (float)(c.mu_g * sub_dt);
   if (y0 >= c.ny) return;  // warp-uniform
+  float fa[kFvDiag] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  float fwave = 0.f;
   FxCell cur, nxt, nn;
   fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0, gx, colok, cur);
   fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 + 1, gx, colok, nxt);
@@ -710,19 +712,20 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
       hdst[gi] = hq;
       qxdst[gi] = qxo;
       qydst[gi] = qyo;
-      const double h64 = (double)hn;
-      acc[0] += (double)qxn - (double)cur.qx;
-      acc[1] += (double)qyn - (double)cur.qy;
-      acc[2] += (double)qex - (double)qxn;
-      acc[3] += (double)qey - (double)qyn;
-      acc[4] += (double)qxo - (double)qex;
-      acc[5] += (double)qyo - (double)qey;
-      acc[6] += 0.5 * h64 *
-                ((double)spd * (double)spd - ((double)vax * (double)vax + (double)vay * (double)vay));
-      acc[7] += h64 * ((0.5 * ((double)vbx + (double)vex)) * (double)ax +
-                       (0.5 * ((double)vby + (double)vey)) * (double)ay) * sub_dt;
+      // per-lane diagnostics in float over this strip (at most rows_per_warp
+      // cells), folded into the double sums once at the end
+      fa[0] += qxn - cur.qx;
+      fa[1] += qyn - cur.qy;
+      fa[2] += qex - qxn;
+      fa[3] += qey - qyn;
+      fa[4] += qxo - qex;
+      fa[5] += qyo - qey;
+      // friction dissipation 0.5 h (|v|^2 - |v fac|^2) = 0.5 h |v|^2 (1 - fac)(1 + fac)
+      fa[6] += ((0.5f * hn) * (spd * spd)) * ((1.f - fac) * (1.f + fac));
+      if (c.has_external)
+        fa[7] += (hn * ((0.5f * (vbx + vex)) * ax + (0.5f * (vby + vey)) * ay)) * dtf;
       const float wv = spd * fac + sqrtf(c.KGf * hn);  // |new velocity| + celerity
-      wave = fmax(wave, (double)wv);
+      fwave = fmaxf(fwave, wv);
     }
     ms = mn;
     nts = nt;
@@ -731,6 +734,9 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
     nxt = nn;
     fx_prepare(c, nxt);
   }
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) acc[k] += (double)fa[k];
+  wave = fmax(wave, (double)fwave);
 }
 
 __global__ void __launch_bounds__(kThreads, 4)

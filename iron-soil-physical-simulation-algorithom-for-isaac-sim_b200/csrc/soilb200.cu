@@ -31,6 +31,7 @@
 #include "sb_exchange.cuh"
 #include "sb_deposition.cuh"
 #include "sb_avalanche.cuh"
+#include "sb_surface.cuh"
 #include "sb_path.cuh"
 #include "sb_batch.cuh"
 #include "sb_learned.cuh"
@@ -176,6 +177,14 @@ struct sb_ctx {
   MobilizeOut* mob_out_host = nullptr;
   double* pers_out = nullptr;
   double* pers_out_host = nullptr;
+  // surface publication: captured free surface (flat double), dirty tile
+  // flags, batched query buffers (grown on demand)
+  double* surf_before = nullptr;
+  int* dtiles = nullptr;
+  double* q_rows = nullptr;
+  double* q_cols = nullptr;
+  double* q_out = nullptr;
+  int q_cap = 0;
   long long launches = 0;
   char err[1024] = {0};
 };
@@ -653,6 +662,8 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMalloc(&ctx->m2r, n * 8));
   SB_CUDA(ctx, cudaMemsetAsync(ctx->forcing, 0, n * 4, ctx->stream));
   SB_CUDA(ctx, cudaMemsetAsync(ctx->m2r, 0, n * 8, ctx->stream));
+  SB_CUDA(ctx, cudaMalloc(&ctx->surf_before, n * 8));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->surf_before, 0, n * 8, ctx->stream));
   SB_CUDA(ctx, cudaMalloc(&ctx->owned_surface, n * 8));
   SB_CUDA(ctx, cudaMalloc(&ctx->act_count, n * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->act_first, n * 8));
@@ -681,6 +692,7 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   ctx->ftiles1 = (d.nx + d.tile_size - 1) / d.tile_size;
   const size_t nt = (size_t)ctx->ftiles0 * ctx->ftiles1;
   SB_CUDA(ctx, cudaMalloc(&ctx->ptiles, nt * sizeof(int)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->dtiles, nt * sizeof(int)));
   SB_CUDA(ctx, cudaMalloc(&ctx->ftile_next, nt * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->phase[0], nt * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->phase[1], nt * 4));
@@ -767,7 +779,8 @@ int sb_ctx_destroy(sb_ctx* ctx) {
                   ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout, ctx->pstate,
                   ctx->path_count, ctx->forcing, ctx->m2r, ctx->dep_out, ctx->owned_surface,
                   ctx->act_count, ctx->act_first, ctx->act_last, ctx->r2m, ctx->initial_b,
-                  ctx->ptiles, ctx->mob_out, ctx->pers_out};
+                  ctx->ptiles, ctx->mob_out, ctx->pers_out, ctx->surf_before, ctx->dtiles,
+                  ctx->q_rows, ctx->q_cols, ctx->q_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
@@ -1768,6 +1781,110 @@ extern "C" int sb_avalanche_persistence(sb_ctx* ctx, double start_angle_rad, dou
   out->start_minus_slope_sum_rad = v[11];
   out->retired_candidate_area_m2 = v[12];
   out->moving_mobile_volume_m3 = v[13];
+  return SB_OK;
+}
+
+extern "C" int sb_surface_capture(sb_ctx* ctx) {
+  if (!ctx) return SB_ERR_BAD_ARG;
+  const int P = ctx->parity_host;
+  const int g = grid_for((long long)ctx->d.ny * ctx->d.nx);
+  if (fx(ctx))
+    surface_capture_kernel<true><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, (const int32_t*)ctx->b,
+        (const int32_t*)ctx->h[P], ctx->surf_before);
+  else
+    surface_capture_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, 0.0, 0.0, (const double*)ctx->b, (const double*)ctx->h[P],
+        ctx->surf_before);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+extern "C" int sb_surface_dirty_tiles(sb_ctx* ctx, double tolerance_m, int32_t* flags, int ntiles) {
+  if (!ctx || !flags) return SB_ERR_BAD_ARG;
+  if (!std::isfinite(tolerance_m) || tolerance_m < 0.0)
+    return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] dirty tolerance must be finite/non-negative");
+  const size_t nt = (size_t)ctx->ftiles0 * ctx->ftiles1;
+  if ((size_t)ntiles < nt) return fail(ctx, SB_ERR_CAPACITY, "[soilb200] tile flag buffer too small");
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->dtiles, 0, nt * sizeof(int), ctx->stream));
+  const int P = ctx->parity_host;
+  const int g = grid_for((long long)ctx->d.ny * ctx->d.nx);
+  if (fx(ctx))
+    surface_flag_kernel<true><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, (const int32_t*)ctx->b,
+        (const int32_t*)ctx->h[P], ctx->surf_before, ctx->d.tile_size, ctx->ftiles1, tolerance_m,
+        ctx->dtiles);
+  else
+    surface_flag_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, 0.0, 0.0, (const double*)ctx->b, (const double*)ctx->h[P],
+        ctx->surf_before, ctx->d.tile_size, ctx->ftiles1, tolerance_m, ctx->dtiles);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(flags, ctx->dtiles, nt * sizeof(int), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+extern "C" int sb_surface_region(sb_ctx* ctx, int r0, int r1, int c0, int c1, double* out) {
+  if (!ctx || !out) return SB_ERR_BAD_ARG;
+  if (r0 < 0 || c0 < 0 || r1 > ctx->d.ny || c1 > ctx->d.nx || r1 <= r0 || c1 <= c0)
+    return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] region outside grid");
+  const int count = (r1 - r0) * (c1 - c0);
+  const int P = ctx->parity_host;
+  const int g = grid_for(count);
+  if (fx(ctx))
+    surface_region_kernel<true><<<g, kThreads, 0, ctx->stream>>>(
+        c1 - c0, count, r0, c0, ctx->pitch, ctx->quantum, ctx->d.datum_m, (const int32_t*)ctx->b,
+        (const int32_t*)ctx->h[P], ctx->staging);
+  else
+    surface_region_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
+        c1 - c0, count, r0, c0, ctx->pitch, 0.0, 0.0, (const double*)ctx->b,
+        (const double*)ctx->h[P], ctx->staging);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(out, ctx->staging, (size_t)count * 8, cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return SB_OK;
+}
+
+extern "C" int sb_surface_sample_bilinear(sb_ctx* ctx, const double* rows, const double* cols,
+                                          int count, double* out) {
+  if (!ctx || count < 0 || (count > 0 && (!rows || !cols || !out))) return SB_ERR_BAD_ARG;
+  if (count == 0) return SB_OK;
+  for (int i = 0; i < count; ++i)
+    if (!std::isfinite(rows[i]) || !std::isfinite(cols[i]))
+      return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] terrain queries must be finite [N,2]");
+  if (count > ctx->q_cap) {
+    cudaFree(ctx->q_rows);
+    cudaFree(ctx->q_cols);
+    cudaFree(ctx->q_out);
+    ctx->q_rows = ctx->q_cols = ctx->q_out = nullptr;
+    ctx->q_cap = 0;
+    SB_CUDA(ctx, cudaMalloc(&ctx->q_rows, (size_t)count * 8));
+    SB_CUDA(ctx, cudaMalloc(&ctx->q_cols, (size_t)count * 8));
+    SB_CUDA(ctx, cudaMalloc(&ctx->q_out, (size_t)count * 8));
+    ctx->q_cap = count;
+  }
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->q_rows, rows, (size_t)count * 8, cudaMemcpyHostToDevice, ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->q_cols, cols, (size_t)count * 8, cudaMemcpyHostToDevice, ctx->stream));
+  const int P = ctx->parity_host;
+  const int g = grid_for(count);
+  if (fx(ctx))
+    surface_bilinear_kernel<true><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, (const int32_t*)ctx->b,
+        (const int32_t*)ctx->h[P], ctx->q_rows, ctx->q_cols, count, ctx->q_out);
+  else
+    surface_bilinear_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
+        ctx->d.ny, ctx->d.nx, ctx->pitch, 0.0, 0.0, (const double*)ctx->b, (const double*)ctx->h[P],
+        ctx->q_rows, ctx->q_cols, count, ctx->q_out);
+  ctx->launches++;
+  SB_CUDA(ctx, cudaGetLastError());
+  SB_CUDA(ctx, cudaMemcpyAsync(out, ctx->q_out, (size_t)count * 8, cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return SB_OK;
 }
 

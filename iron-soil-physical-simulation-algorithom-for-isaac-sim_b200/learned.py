@@ -291,13 +291,31 @@ class LearnedRelaxation:
                                                                self.tan_crit), "apply")
 
     def relax(self, tolerance_m: float, max_iterations: int = 20000, rounds: int = 1,
-              spacing=None):
-        """Proposal rounds, then relax_critical_slope sweeps; returns RelaxStats."""
+              spacing=None, plain_between: int = 0):
+        """Learned rounds, then relax_critical_slope sweeps to the tolerance.
+
+        With ``plain_between`` > 0 each proposal is followed by that many plain
+        sweeps (the proposal moves material over the network's receptive field,
+        the sweeps resolve what it left); the schedule stops early once the
+        sweeps converge.  Returns the final sweep's RelaxStats, with
+        ``iterations`` counting every plain sweep that ran."""
         s0, s1 = spacing if spacing is not None else (self.grid.dy, self.grid.dx)
-        if rounds > 0:
-            self.propose(rounds)
+        lib = _lib.load()
+        done = 0
+        for _ in range(max(0, rounds)):
+            self.propose(1)
+            if plain_between > 0:
+                p = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
+                                     int(plain_between), 0)
+                st = _lib.RelaxStats()
+                _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, p, st), "relax")
+                done += int(st.iterations)
+                if st.converged:
+                    st.iterations = done
+                    return st
         params = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
                                   int(max_iterations), 0)
         st = _lib.RelaxStats()
-        _lib.check(self.grid.ctx, _lib.load().sb_relax_full(self.grid.ctx, params, st), "relax")
+        _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, params, st), "relax")
+        st.iterations = int(st.iterations) + done
         return st
