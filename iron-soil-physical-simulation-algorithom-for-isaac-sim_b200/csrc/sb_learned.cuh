@@ -125,43 +125,73 @@ struct ConvSmem {
   static constexpr int N = 3 * COUT;
   static constexpr int W_BYTES = 3 * N * CIN * 2;   // packed weights, three row offsets
   static constexpr int ROW_BYTES = 128 * CIN * 2;  // one input row of the tile
+  static constexpr int SLOTS = 4;                  // rows y-1..y+1 in use + one in flight
   static constexpr int XCH_FLOATS = 4 * 2 * COUT;  // warp-boundary partial sums
-  static constexpr int BYTES = W_BYTES + 3 * ROW_BYTES + XCH_FLOATS * 4 + 64;
+  static constexpr int BYTES = W_BYTES + SLOTS * ROW_BYTES + XCH_FLOATS * 4 + 64;
   static constexpr uint32_t TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
 };
 
-// Loads input row r of the tile (pixels x0 .. x0+127) into ring slot dst in
-// canonical A layout; zeros outside the image.
+// Starts the asynchronous copy of input row r of the tile (pixels x0 .. x0+127)
+// into a ring slot in canonical A layout; 16-byte cp.async chunks, zero-filled
+// outside the image.  Completed by conv_row_wait.
 template <int CIN>
-__device__ __forceinline__ void conv_load_row(const __nv_bfloat16* __restrict__ in, int b, int h,
-                                              int w, int r, int x0, unsigned char* dst) {
+__device__ __forceinline__ void conv_row_async(const __nv_bfloat16* __restrict__ in, int b, int h,
+                                               int w, int r, int x0, unsigned char* dst) {
   const int m = threadIdx.x;
   const int x = x0 + m;
   const bool ok = r >= 0 && r < h && x >= 0 && x < w;
-  const uint4* src = reinterpret_cast<const uint4*>(in + (((size_t)b * h + (ok ? r : 0)) * w +
-                                                          (ok ? x : 0)) * CIN);
+  const __nv_bfloat16* src = in + (((size_t)b * h + (ok ? r : 0)) * w + (ok ? x : 0)) * CIN;
+  const unsigned bytes = ok ? 16u : 0u;
 #pragma unroll
-  for (int kb = 0; kb < CIN / 8; ++kb) {
-    const uint4 v = ok ? src[kb] : make_uint4(0, 0, 0, 0);
-    *reinterpret_cast<uint4*>(dst + core_off(m, kb * 8, CIN)) = v;
+  for (int kb = 0; kb < CIN / 8; ++kb)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                     smem_u32(dst + core_off(m, kb * 8, CIN))),
+                 "l"(src + kb * 8), "r"(bytes)
+                 : "memory");
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void conv_row_wait() {
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  fence_async_smem();  // the rows are read by the tensor core (async proxy)
+}
+
+template <int CIN, int COUT>
+__device__ __forceinline__ void conv_issue_row(uint32_t tmem, uint32_t ring_base,
+                                               uint32_t w_base, int y, uint32_t idesc) {
+  using S = ConvSmem<CIN, COUT>;
+  const uint32_t lbo = 128, sbo = (CIN / 8) * 128;
+#pragma unroll
+  for (int dy = 0; dy < 3; ++dy) {
+    const uint32_t a_row = ring_base + ((y - 1 + dy + S::SLOTS) % S::SLOTS) * S::ROW_BYTES;
+    const uint32_t b_off = w_base + dy * (S::N * CIN * 2);
+#pragma unroll
+    for (int kk = 0; kk < CIN / 16; ++kk)
+      umma_bf16(tmem, umma_desc(a_row + kk * 256, lbo, sbo), umma_desc(b_off + kk * 256, lbo, sbo),
+                idesc, (dy | kk) != 0);
   }
 }
 
+// Per CTA: one 128-pixel tile (126 output columns) of rows [y0, y1).  Row y's
+// MMAs are issued as soon as row y-1's accumulator has been read, so they run
+// while row y-1's epilogue exchanges and stores; input rows arrive by cp.async
+// two rows ahead.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs a) {
   using S = ConvSmem<CIN, COUT>;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* wsm = smem;
   unsigned char* ring = smem + S::W_BYTES;
-  float* xch = reinterpret_cast<float*>(ring + 3 * S::ROW_BYTES);
+  float* xch = reinterpret_cast<float*>(ring + S::SLOTS * S::ROW_BYTES);
   uint64_t* bar = reinterpret_cast<uint64_t*>(xch + S::XCH_FLOATS);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
 
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int x0 = blockIdx.x * kConvTileOut - 1;
   const int y0 = blockIdx.y * a.rows_per_cta;
   const int y1 = min(y0 + a.rows_per_cta, a.h);
   const int b = blockIdx.z;
+  auto slot = [&](int r) { return ring + ((r + S::SLOTS) % S::SLOTS) * S::ROW_BYTES; };
 
   // weights -> shared memory (already in canonical layout)
   {
@@ -171,53 +201,52 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
   }
   if (tid == 0) mbar_init(bar, 1);
   if (warp == 0) tmem_alloc(tslot, S::TMEM_COLS);
-  conv_load_row<CIN>(a.in, b, a.h, a.w, y0 - 1, x0, ring + ((y0 - 1 + 3) % 3) * S::ROW_BYTES);
-  conv_load_row<CIN>(a.in, b, a.h, a.w, y0, x0, ring + (y0 % 3) * S::ROW_BYTES);
-  fence_async_smem();
+  conv_row_async<CIN>(a.in, b, a.h, a.w, y0 - 1, x0, slot(y0 - 1));
+  conv_row_async<CIN>(a.in, b, a.h, a.w, y0, x0, slot(y0));
+  conv_row_async<CIN>(a.in, b, a.h, a.w, y0 + 1, x0, slot(y0 + 1));
+  conv_row_wait();
+  fence_async_smem();  // the weights too
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t idesc = umma_idesc_bf16(128, S::N);
-  const uint32_t lbo = 128, sbo = (CIN / 8) * 128;
   const uint32_t w_base = smem_u32(wsm), ring_base = smem_u32(ring);
   unsigned phase = 0;
   bool ok = true;
-
-  for (int y = y0; y < y1; ++y) {
-    conv_load_row<CIN>(a.in, b, a.h, a.w, y + 1, x0, ring + ((y + 1) % 3) * S::ROW_BYTES);
-    fence_async_smem();
-    __syncthreads();
+  if (y0 < y1) {
     if (tid == 0) {
-      tc_fence_after();
-#pragma unroll
-      for (int dy = 0; dy < 3; ++dy) {
-        const uint32_t a_row = ring_base + ((y - 1 + dy + 3) % 3) * S::ROW_BYTES;
-        const uint32_t b_off = w_base + dy * (S::N * CIN * 2);
-#pragma unroll
-        for (int kk = 0; kk < CIN / 16; ++kk)
-          umma_bf16(tmem, umma_desc(a_row + kk * 256, lbo, sbo), umma_desc(b_off + kk * 256, lbo, sbo),
-                    idesc, (dy | kk) != 0);
-      }
+      conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y0, idesc);
       umma_commit(bar);
     }
+    if (y0 + 1 < y1) conv_row_async<CIN>(a.in, b, a.h, a.w, y0 + 2, x0, slot(y0 + 2));
+  }
+
+  for (int y = y0; y < y1; ++y) {
     ok = mbar_wait(bar, phase) && ok;
     phase ^= 1;
     tc_fence_after();
-    // this thread's row of D: columns (dx, co)
-    float d[S::N];
+    float d[S::N];  // this thread's row of D: columns (dx, co)
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
 #pragma unroll
     for (int c = 0; c < S::N; c += 16) tmem_ld16(lane_addr + c, d + c);
     tc_fence_before();
-    // neighbours' dx = 0 / dx = 2 partial sums: shuffles inside a warp, shared
-    // memory across the three warp boundaries
-    const int lane = tid & 31;
+    if (y + 1 < y1) conv_row_wait();  // row y+2 has landed
     if (lane == 31)
       for (int co = 0; co < COUT; ++co) xch[(warp * 2) * COUT + co] = d[co];
     if (lane == 0)
       for (int co = 0; co < COUT; ++co) xch[(warp * 2 + 1) * COUT + co] = d[2 * COUT + co];
     __syncthreads();
+    // the accumulator is free again: the next row's MMAs overlap this epilogue
+    if (y + 1 < y1) {
+      if (tid == 0) {
+        tc_fence_after();
+        conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y + 1, idesc);
+        umma_commit(bar);
+      }
+      // slot of row y-1 is free (row y's MMAs have completed)
+      if (y + 2 < y1) conv_row_async<CIN>(a.in, b, a.h, a.w, y + 3, x0, slot(y + 3));
+    }
     const int xo = x0 + tid;
     const bool store = tid >= 1 && tid <= kConvTileOut && xo < a.w;
     const size_t pix = ((size_t)b * a.h + y) * a.w + (store ? xo : 0);
@@ -256,8 +285,9 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
         }
       }
     }
-    __syncthreads();
+    __syncthreads();  // xch is rewritten by the next row
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (!ok && tid == 0 && a.status) atomicExch(a.status, 1);
   tc_fence_before();
   __syncthreads();

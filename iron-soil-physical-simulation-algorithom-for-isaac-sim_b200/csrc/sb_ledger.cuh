@@ -192,7 +192,7 @@ __device__ __forceinline__ void ledger_prologue(const FvConst& c, const LedgerOu
 }
 
 template <bool FX>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 3)
     ledger_kernel(const FvConst c, const typename FvTypes<FX>::B* __restrict__ b,
                   const typename FvTypes<FX>::B* __restrict__ z,
                   const typename FvTypes<FX>::H* __restrict__ h0,

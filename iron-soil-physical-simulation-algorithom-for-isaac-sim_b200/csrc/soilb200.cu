@@ -624,8 +624,9 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
     const long long warps = (long long)ctx->fv_strips * ((d.ny + rows - 1) / rows);
     ctx->fv_stream_blocks = (int)((warps + kThreads / 32 - 1) / (kThreads / 32));
   }
-  // grid-stride reductions: two CTAs per SM keep the final fold short
-  ctx->ledger_blocks = std::min(grid_for((long long)d.ny * d.nx), 2 * 148);
+  // grid-stride reductions: three CTAs per SM (the ledger kernel's register
+  // bound) keep the final fold short
+  ctx->ledger_blocks = std::min(grid_for((long long)d.ny * d.nx), 3 * 148);
   const size_t np = (size_t)std::max({tiles, ctx->ledger_blocks, ctx->fv_stream_blocks}) *
                     (kFvPartial > L_NP ? kFvPartial : L_NP);
   SB_CUDA(ctx, cudaMalloc(&ctx->partials, np * sizeof(double)));
@@ -1086,7 +1087,7 @@ static int run_label(sb_ctx* ctx, const LabelConst& c) {
       c, ctx->parent, (const typename T::B*)ctx->b, (const typename T::B*)ctx->z,
       (const typename T::R*)ctx->slope, (const typename T::R*)ctx->severity, ctx->latch,
       ctx->previous, ctx->roots, ctx->root_list, ctx->lout, 0);
-  label_reduce_kernel<<<148, kThreads, 0, ctx->stream>>>(ctx->roots, ctx->root_list, ctx->lout,
+  label_reduce_kernel<<<32, kThreads, 0, ctx->stream>>>(ctx->roots, ctx->root_list, ctx->lout,
                                                          ctx->arrive);
   ctx->launches += 4;
   SB_CUDA(ctx, cudaGetLastError());
@@ -1155,7 +1156,7 @@ extern "C" int sb_label_mask(sb_ctx* ctx, const int32_t* mask, int connectivity,
     label_compress_kernel<false><<<g, kThreads, 0, ctx->stream>>>(
         c, ctx->parent, nullptr, nullptr, nullptr, nullptr, ctx->latch, ctx->previous, ctx->roots,
         ctx->root_list, ctx->lout, 1);
-  label_reduce_kernel<<<148, kThreads, 0, ctx->stream>>>(ctx->roots, ctx->root_list, ctx->lout,
+  label_reduce_kernel<<<32, kThreads, 0, ctx->stream>>>(ctx->roots, ctx->root_list, ctx->lout,
                                                          ctx->arrive);
   ctx->launches += 4;
   SB_CUDA(ctx, cudaGetLastError());
@@ -2014,7 +2015,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   }
   {
     void* args[] = {&ctx->roots, &ctx->root_list, &ctx->lout, &ctx->arrive};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_reduce_kernel, dim3(148), 0, args)))
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_reduce_kernel, dim3(32), 0, args)))
       return rc;
     prev = node;
   }
