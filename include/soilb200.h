@@ -237,6 +237,10 @@ typedef struct sb_relax_stats {
 
 /* relax_critical_slope on SB_FIELD_B_EFF (slope_model.py:273-343). */
 int sb_relax_full(sb_ctx* ctx, const sb_relax_params* params, sb_relax_stats* out);
+/* The same sweeps queued on the context's stream without waiting for them or
+ * reading statistics back (at most max_iterations; for interleaving with other
+ * device work, e.g. learned proposals). */
+int sb_relax_sweeps(sb_ctx* ctx, const sb_relax_params* params);
 /* Frontier seeds: reached := 1 at the cells and their 3x3-stencil tiles become
  * active (_seed_gpu_residual_frontier, v2_physics_core.py:1153-1170). */
 int sb_frontier_seed_cells(sb_ctx* ctx, const int32_t* flat_indices, int count);

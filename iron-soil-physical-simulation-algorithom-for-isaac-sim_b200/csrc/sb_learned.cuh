@@ -9,13 +9,14 @@
 // Convolutions are implicit GEMMs on the 5th-generation tensor cores
 // (tcgen05.mma, kind::f16, operands in shared memory, accumulator in TMEM):
 //
-//   forward / data gradient: per output row of a 126-pixel tile, the input
-//     rows y-1, y, y+1 (128 pixels each, K = input channels) are multiplied
-//     by the weights of that row offset with N = (dx, out channel) = 3*COUT,
-//     accumulating D[pixel, (dx, co)] over the three rows; the epilogue adds
-//     the dx = 0 / 2 partial sums of the neighbouring pixels (exchanged in
-//     shared memory).  The data gradient is the same kernel run with the
-//     flipped, transposed weights and the ReLU mask of the layer's input.
+//   forward / data gradient: per output row of a 128-pixel tile, the nine
+//     taps (dy, dx) are nine K-major operands (M = 128 pixels, K = input
+//     channels) read straight out of the staged input rows -- a column
+//     offset is a 16-byte start offset in the pixel-major staging layout --
+//     against the tap's weights (N = output channels), accumulated in one
+//     TMEM tile that is the output row.  The data gradient is the same kernel
+//     run with the flipped, transposed weights and the ReLU mask of the
+//     layer's input.
 //   weight gradient: per input row, A = the row shifted by dx (M = (dx, ci),
 //     K = 128 pixels) times B = output-gradient rows (N = co), accumulated in
 //     TMEM over the CTA's band for the three row offsets; per-CTA partials
@@ -32,7 +33,7 @@
 namespace sb {
 
 constexpr int kConvThreads = 128;   // 4 warps: TMEM lanes 0..127 = tile pixels
-constexpr int kConvTileOut = 126;   // output pixels per 128-pixel input tile
+constexpr int kConvTileOut = 128;   // output pixels per CTA row tile
 
 // ---------------------------------------------------------------- tcgen05
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
@@ -120,34 +121,41 @@ struct ConvArgs {
   int* status;                  // set to 1 if a bounded wait gave up
 };
 
+// Input rows are staged pixel-major: 130 pixels (x0-1 .. x0+128) of 16 bytes
+// (8 channels) per K chunk, chunks kRowLbo bytes apart.  In the canonical
+// K-major layout that is SBO = 128 B (8 consecutive pixels per core matrix,
+// core matrices contiguous) and LBO = kRowLbo, so the operand for column
+// offset dx is the same rows starting dx * 16 bytes later: no copies.
+constexpr int kRowPixels = 130;
+constexpr uint32_t kRowLbo = kRowPixels * 16;
+
 template <int CIN, int COUT>
 struct ConvSmem {
-  static constexpr int N = 3 * COUT;
-  static constexpr int W_BYTES = 3 * N * CIN * 2;   // packed weights, three row offsets
-  static constexpr int ROW_BYTES = 128 * CIN * 2;  // one input row of the tile
-  static constexpr int SLOTS = 4;                  // rows y-1..y+1 in use + one in flight
-  static constexpr int XCH_FLOATS = 4 * 2 * COUT;  // warp-boundary partial sums
-  static constexpr int BYTES = W_BYTES + SLOTS * ROW_BYTES + XCH_FLOATS * 4 + 64;
-  static constexpr uint32_t TMEM_COLS = N <= 32 ? 32 : (N <= 64 ? 64 : 128);
+  static constexpr int W_BLOCK = COUT * CIN * 2;         // one tap's weights (canonical B)
+  static constexpr int W_BYTES = 9 * W_BLOCK;
+  static constexpr int ROW_BYTES = (CIN / 8) * kRowLbo;  // one staged input row
+  static constexpr int SLOTS = 4;                        // rows y-1..y+1 in use + one in flight
+  static constexpr int BYTES = W_BYTES + SLOTS * ROW_BYTES + 64;
+  static constexpr uint32_t TMEM_COLS = 32;              // N = COUT <= 32 f32 columns
 };
 
-// Starts the asynchronous copy of input row r of the tile (pixels x0 .. x0+127)
-// into a ring slot in canonical A layout; 16-byte cp.async chunks, zero-filled
-// outside the image.  Completed by conv_row_wait.
+// Starts the asynchronous copy of input row r (pixels x0-1 .. x0+128) into
+// a ring slot; 16-byte cp.async chunks, zero-filled outside the image.
 template <int CIN>
 __device__ __forceinline__ void conv_row_async(const __nv_bfloat16* __restrict__ in, int b, int h,
-                                               int w, int r, int x0, unsigned char* dst) {
-  const int m = threadIdx.x;
-  const int x = x0 + m;
-  const bool ok = r >= 0 && r < h && x >= 0 && x < w;
-  const __nv_bfloat16* src = in + (((size_t)b * h + (ok ? r : 0)) * w + (ok ? x : 0)) * CIN;
-  const unsigned bytes = ok ? 16u : 0u;
+                                               int w, int r, int x0, unsigned char* slot) {
+  for (int j = threadIdx.x; j < kRowPixels; j += kConvThreads) {
+    const int x = x0 - 1 + j;
+    const bool ok = r >= 0 && r < h && x >= 0 && x < w;
+    const __nv_bfloat16* src = in + (((size_t)b * h + (ok ? r : 0)) * w + (ok ? x : 0)) * CIN;
+    const unsigned bytes = ok ? 16u : 0u;
 #pragma unroll
-  for (int kb = 0; kb < CIN / 8; ++kb)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
-                     smem_u32(dst + core_off(m, kb * 8, CIN))),
-                 "l"(src + kb * 8), "r"(bytes)
-                 : "memory");
+    for (int kb = 0; kb < CIN / 8; ++kb)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                       smem_u32(slot + kb * kRowLbo + j * 16)),
+                   "l"(src + kb * 8), "r"(bytes)
+                   : "memory");
+  }
   asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
@@ -156,38 +164,41 @@ __device__ __forceinline__ void conv_row_wait() {
   fence_async_smem();  // the rows are read by the tensor core (async proxy)
 }
 
+// D[pixel, co] for output row y: nine taps (dy, dx), each M = 128 pixels x
+// K = CIN against the tap's weights (N = COUT), accumulated in TMEM.
 template <int CIN, int COUT>
 __device__ __forceinline__ void conv_issue_row(uint32_t tmem, uint32_t ring_base,
                                                uint32_t w_base, int y, uint32_t idesc) {
   using S = ConvSmem<CIN, COUT>;
-  const uint32_t lbo = 128, sbo = (CIN / 8) * 128;
 #pragma unroll
   for (int dy = 0; dy < 3; ++dy) {
-    const uint32_t a_row = ring_base + ((y - 1 + dy + S::SLOTS) % S::SLOTS) * S::ROW_BYTES;
-    const uint32_t b_off = w_base + dy * (S::N * CIN * 2);
+    const uint32_t slot = ring_base + ((y - 1 + dy + S::SLOTS) % S::SLOTS) * S::ROW_BYTES;
 #pragma unroll
-    for (int kk = 0; kk < CIN / 16; ++kk)
-      umma_bf16(tmem, umma_desc(a_row + kk * 256, lbo, sbo), umma_desc(b_off + kk * 256, lbo, sbo),
-                idesc, (dy | kk) != 0);
+    for (int dx = 0; dx < 3; ++dx) {
+      const uint32_t b_base = w_base + (dy * 3 + dx) * S::W_BLOCK;
+#pragma unroll
+      for (int kk = 0; kk < CIN / 16; ++kk)
+        umma_bf16(tmem, umma_desc(slot + kk * 2 * kRowLbo + dx * 16, kRowLbo, 128),
+                  umma_desc(b_base + kk * 256, 128, (CIN / 8) * 128), idesc,
+                  (dy | dx | kk) != 0);
+    }
   }
 }
 
-// Per CTA: one 128-pixel tile (126 output columns) of rows [y0, y1).  Row y's
-// MMAs are issued as soon as row y-1's accumulator has been read, so they run
-// while row y-1's epilogue exchanges and stores; input rows arrive by cp.async
-// two rows ahead.
+// Per CTA: one 128-pixel tile of rows [y0, y1).  Row y+1's MMAs are issued as
+// soon as row y's accumulator has been read, so they run while row y's
+// epilogue converts and stores; input rows arrive by cp.async two rows ahead.
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs a) {
   using S = ConvSmem<CIN, COUT>;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* wsm = smem;
   unsigned char* ring = smem + S::W_BYTES;
-  float* xch = reinterpret_cast<float*>(ring + S::SLOTS * S::ROW_BYTES);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(xch + S::XCH_FLOATS);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ring + S::SLOTS * S::ROW_BYTES);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int x0 = blockIdx.x * kConvTileOut - 1;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int x0 = blockIdx.x * kConvTileOut;
   const int y0 = blockIdx.y * a.rows_per_cta;
   const int y1 = min(y0 + a.rows_per_cta, a.h);
   const int b = blockIdx.z;
@@ -205,13 +216,14 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
   conv_row_async<CIN>(a.in, b, a.h, a.w, y0, x0, slot(y0));
   conv_row_async<CIN>(a.in, b, a.h, a.w, y0 + 1, x0, slot(y0 + 1));
   conv_row_wait();
-  fence_async_smem();  // the weights too
+  fence_async_smem();  // the weights (generic stores) too
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t idesc = umma_idesc_bf16(128, S::N);
+  const uint32_t idesc = umma_idesc_bf16(128, COUT);
   const uint32_t w_base = smem_u32(wsm), ring_base = smem_u32(ring);
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
   unsigned phase = 0;
   bool ok = true;
   if (y0 < y1) {
@@ -226,47 +238,32 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
     ok = mbar_wait(bar, phase) && ok;
     phase ^= 1;
     tc_fence_after();
-    float d[S::N];  // this thread's row of D: columns (dx, co)
-    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    float d[COUT];  // this thread's pixel of the output row
 #pragma unroll
-    for (int c = 0; c < S::N; c += 16) tmem_ld16(lane_addr + c, d + c);
+    for (int c = 0; c < COUT; c += 16) tmem_ld16(lane_addr + c, d + c);
     tc_fence_before();
     if (y + 1 < y1) conv_row_wait();  // row y+2 has landed
-    if (lane == 31)
-      for (int co = 0; co < COUT; ++co) xch[(warp * 2) * COUT + co] = d[co];
-    if (lane == 0)
-      for (int co = 0; co < COUT; ++co) xch[(warp * 2 + 1) * COUT + co] = d[2 * COUT + co];
-    __syncthreads();
-    // the accumulator is free again: the next row's MMAs overlap this epilogue
+    __syncthreads();                  // everyone has read the accumulator
     if (y + 1 < y1) {
       if (tid == 0) {
         tc_fence_after();
         conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y + 1, idesc);
         umma_commit(bar);
       }
-      // slot of row y-1 is free (row y's MMAs have completed)
+      // the slot of row y-1 is free: row y's MMAs have completed
       if (y + 2 < y1) conv_row_async<CIN>(a.in, b, a.h, a.w, y + 3, x0, slot(y + 3));
     }
     const int xo = x0 + tid;
-    const bool store = tid >= 1 && tid <= kConvTileOut && xo < a.w;
-    const size_t pix = ((size_t)b * a.h + y) * a.w + (store ? xo : 0);
+    if (xo < a.w) {
+      const size_t pix = ((size_t)b * a.h + y) * a.w + xo;
 #pragma unroll
-    for (int c8 = 0; c8 < COUT; c8 += 8) {
-      float o[8];
+      for (int c8 = 0; c8 < COUT; c8 += 8) {
+        float o[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int co = c8 + j;
-        float left = __shfl_up_sync(0xffffffffu, d[co], 1);
-        float right = __shfl_down_sync(0xffffffffu, d[2 * COUT + co], 1);
-        if (lane == 0 && warp > 0) left = xch[((warp - 1) * 2) * COUT + co];
-        if (lane == 31 && warp < 3) right = xch[((warp + 1) * 2 + 1) * COUT + co];
-        float v = (left + d[COUT + co]) + right;
-        if (a.relu) v = fmaxf(v, 0.f);
-        o[j] = v;
-      }
-      if (store) {
+        for (int j = 0; j < 8; ++j) o[j] = a.relu ? fmaxf(d[c8 + j], 0.f) : d[c8 + j];
         if (a.mask) {
-          const __nv_bfloat16* mk = a.mask + pix * COUT + c8;
+          const uint4 mv = *reinterpret_cast<const uint4*>(a.mask + pix * COUT + c8);
+          const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&mv);
 #pragma unroll
           for (int j = 0; j < 8; ++j)
             if (!(__bfloat162float(mk[j]) > 0.f)) o[j] = 0.f;
@@ -277,15 +274,14 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
           if (c8 + 4 < a.out_f32)
             *reinterpret_cast<float4*>(op + 4) = make_float4(o[4], o[5], o[6], o[7]);
         } else {
-          __align__(16) __nv_bfloat16 ob[8];
+          __align__(16) __nv_bfloat162 ob[4];
 #pragma unroll
-          for (int j = 0; j < 8; ++j) ob[j] = __float2bfloat16_rn(o[j]);
+          for (int j = 0; j < 4; ++j) ob[j] = __floats2bfloat162_rn(o[2 * j], o[2 * j + 1]);
           *reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(a.out) + pix * COUT + c8) =
               *reinterpret_cast<const uint4*>(ob);
         }
       }
     }
-    __syncthreads();  // xch is rewritten by the next row
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (!ok && tid == 0 && a.status) atomicExch(a.status, 1);

@@ -464,4 +464,20 @@ __global__ void __launch_bounds__(kThreads)
   out[3] = (double)ia;
 }
 
+// The ping-pong relaxation may end in the alternate buffer: copy it back
+// (every block reads the same flag), then clear the flag in a second launch.
+template <bool FX>
+__global__ void relax_copyback_kernel(const typename FvTypes<FX>::B* __restrict__ src,
+                                      typename FvTypes<FX>::B* __restrict__ dst, long long count,
+                                      const RelaxControl* ctl) {
+  if (!ctl->parity) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+__global__ void relax_parity_clear_kernel(RelaxControl* ctl) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) ctl->parity = 0;
+}
+
 }  // namespace sb

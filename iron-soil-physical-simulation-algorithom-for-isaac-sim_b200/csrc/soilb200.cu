@@ -144,6 +144,8 @@ struct sb_ctx {
   RelaxControl* rctl = nullptr;
   RelaxControl* rctl_host = nullptr;
   LoopGraph relax_full;
+  LoopGraph relax_full2;  // second cached relaxation graph (e.g. short sweeps vs. to tolerance)
+  int relax_lru = 0;
   LoopGraph frontier;
   // fused plain-path step
   PathState* pstate = nullptr;
@@ -768,6 +770,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   if (ctx->mobile.exec) cudaGraphExecDestroy(ctx->mobile.exec);
   if (ctx->mobile.graph) cudaGraphDestroy(ctx->mobile.graph);
   ctx->relax_full.reset();
+  ctx->relax_full2.reset();
   ctx->frontier.reset();
   void* ptrs[] = {ctx->b, ctx->z, ctx->h[0], ctx->h[1], ctx->qx[0], ctx->qx[1], ctx->qy[0],
                   ctx->qy[1], ctx->ext_x, ctx->ext_y, ctx->reached, ctx->staging,
@@ -1252,8 +1255,7 @@ __global__ void relax_reset_kernel(RelaxControl* ctl) {
 }
 
 template <bool FX>
-static int build_relax_full(sb_ctx* ctx, const RelaxConst& c) {
-  LoopGraph& lg = ctx->relax_full;
+static int build_relax_full(sb_ctx* ctx, const RelaxConst& c, LoopGraph& lg) {
   lg.reset();
   cudaGraph_t g;
   SB_CUDA(ctx, cudaGraphCreate(&g, 0));
@@ -1285,9 +1287,54 @@ static int build_relax_full(sb_ctx* ctx, const RelaxConst& c) {
   int rc = add_kernel(ctx, body, &n_body, nullptr, 0, (void*)relax_full_kernel<FX>,
                       dim3(tiles0 * tiles1), 0, args);
   if (rc) return rc;
+  // leave the result in b_eff whichever ping-pong buffer it ended in
+  cudaGraphNode_t n_copy, n_par;
+  {
+    long long count = (long long)ctx->pitch * ctx->d.ny;
+    void* cargs[] = {(void*)&ctx->b_alt, (void*)&ctx->b, (void*)&count, (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_copy, &n_loop, 1, (void*)relax_copyback_kernel<FX>,
+                         dim3(grid_for(count)), 0, cargs)))
+      return rc;
+    void* pargs[] = {(void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_par, &n_copy, 1, (void*)relax_parity_clear_kernel, dim3(1), 0,
+                         pargs)))
+      return rc;
+  }
   SB_CUDA(ctx, cudaGraphInstantiate(&lg.exec, g, 0));
   lg.key = c;
   lg.valid = true;
+  return SB_OK;
+}
+
+// Cached graph for these parameters (two slots, least recently used replaced).
+static int relax_graph_for(sb_ctx* ctx, const RelaxConst& c, LoopGraph** out) {
+  LoopGraph* slots[2] = {&ctx->relax_full, &ctx->relax_full2};
+  for (int i = 0; i < 2; ++i)
+    if (slots[i]->valid && std::memcmp(&slots[i]->key, &c, sizeof(RelaxConst)) == 0) {
+      ctx->relax_lru = i ^ 1;
+      *out = slots[i];
+      return SB_OK;
+    }
+  const int victim = ctx->relax_lru;
+  const int rc = fx(ctx) ? build_relax_full<true>(ctx, c, *slots[victim])
+                         : build_relax_full<false>(ctx, c, *slots[victim]);
+  if (rc) return rc;
+  ctx->relax_lru = victim ^ 1;
+  *out = slots[victim];
+  return SB_OK;
+}
+
+// Queues max_iterations (or fewer, if converged) sweeps without waiting for
+// them or reading their statistics back.
+extern "C" int sb_relax_sweeps(sb_ctx* ctx, const sb_relax_params* p) {
+  if (!ctx || !p) return SB_ERR_BAD_ARG;
+  RelaxConst c;
+  int rc = relax_const(ctx, p, &c, kRelaxTile);
+  if (rc) return rc;
+  LoopGraph* lg = nullptr;
+  if ((rc = relax_graph_for(ctx, c, &lg))) return rc;
+  SB_CUDA(ctx, cudaGraphLaunch(lg->exec, ctx->stream));
+  ctx->launches += 3;
   return SB_OK;
 }
 
@@ -1296,22 +1343,14 @@ extern "C" int sb_relax_full(sb_ctx* ctx, const sb_relax_params* p, sb_relax_sta
   RelaxConst c;
   int rc = relax_const(ctx, p, &c, kRelaxTile);
   if (rc) return rc;
-  LoopGraph& lg = ctx->relax_full;
-  if (!lg.valid || std::memcmp(&lg.key, &c, sizeof(RelaxConst)) != 0) {
-    rc = fx(ctx) ? build_relax_full<true>(ctx, c) : build_relax_full<false>(ctx, c);
-    if (rc) return rc;
-  }
-  SB_CUDA(ctx, cudaGraphLaunch(lg.exec, ctx->stream));
+  LoopGraph* lg = nullptr;
+  if ((rc = relax_graph_for(ctx, c, &lg))) return rc;
+  SB_CUDA(ctx, cudaGraphLaunch(lg->exec, ctx->stream));
   SB_CUDA(ctx, cudaMemcpyAsync(ctx->rctl_host, ctx->rctl, sizeof(RelaxControl),
                                cudaMemcpyDeviceToHost, ctx->stream));
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const RelaxControl& k = *ctx->rctl_host;
-  ctx->launches += 1 + k.iterations;
-  if (k.parity) {  // result lives in the alternate buffer: copy it back
-    SB_CUDA(ctx, cudaMemcpyAsync(ctx->b, ctx->b_alt, (size_t)ctx->pitch * ctx->d.ny * ctx->esize,
-                                 cudaMemcpyDeviceToDevice, ctx->stream));
-    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  }
+  ctx->launches += 3 + k.iterations;
   std::memset(out, 0, sizeof(*out));
   out->iterations = k.iterations;
   out->converged = k.converged;

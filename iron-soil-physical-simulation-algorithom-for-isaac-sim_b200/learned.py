@@ -44,17 +44,16 @@ def _ok(rc: int, what: str) -> None:
 
 
 def pack_index(cin: int, cout: int) -> np.ndarray:
-    """Packed position -> flat index of W[3, 3, cin, cout]: per row offset dy
-    the canonical K-major operand with rows n = dx * cout + co and k = ci
+    """Packed position -> flat index of W[3, 3, cin, cout]: one block per tap
+    (dy, dx), each the canonical K-major operand with rows n = co and k = ci
     (8 x 16-byte core matrices, (n/8, k/8) blocks of 128 bytes)."""
-    n_rows = 3 * cout
-    idx = np.empty(3 * n_rows * cin, dtype=np.int64)
-    n = np.arange(n_rows)[:, None]
+    block = cout * cin
+    idx = np.empty(9 * block, dtype=np.int64)
+    n = np.arange(cout)[:, None]
     k = np.arange(cin)[None, :]
     off = ((n >> 3) * (cin >> 3) + (k >> 3)) * 64 + (n & 7) * 8 + (k & 7)  # in elements
-    dx, co = n // cout, n % cout
-    for dy in range(3):
-        idx[dy * n_rows * cin + off] = ((dy * 3 + dx) * cin + k) * cout + co
+    for tap in range(9):
+        idx[tap * block + off] = (tap * cin + k) * cout + n
     return idx
 
 
@@ -109,7 +108,7 @@ class ReposeNet:
 
 def conv_rows(b: int, h: int, w: int) -> int:
     """Rows per CTA: about one wave of 4 resident CTAs on each of 148 SMs."""
-    tiles = (w + 125) // 126
+    tiles = (w + 127) // 128
     return int(min(32, max(4, -(-b * h * tiles // (148 * 4)))))
 
 
@@ -295,27 +294,23 @@ class LearnedRelaxation:
         """Learned rounds, then relax_critical_slope sweeps to the tolerance.
 
         With ``plain_between`` > 0 each proposal is followed by that many plain
-        sweeps (the proposal moves material over the network's receptive field,
-        the sweeps resolve what it left); the schedule stops early once the
-        sweeps converge.  Returns the final sweep's RelaxStats, with
-        ``iterations`` counting every plain sweep that ran."""
+        sweeps (the proposal moves material over the network's receptive
+        field, the sweeps resolve what it left); the whole schedule is queued
+        on the grid's stream without host round trips, and only the final
+        sweeps to the tolerance report back.  Returns that RelaxStats, with
+        ``iterations`` including the interleaved sweeps (as an upper bound:
+        the interleaved calls stop early when already converged)."""
         s0, s1 = spacing if spacing is not None else (self.grid.dy, self.grid.dx)
         lib = _lib.load()
-        done = 0
+        between = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
+                                   int(max(plain_between, 1)), 0)
         for _ in range(max(0, rounds)):
             self.propose(1)
             if plain_between > 0:
-                p = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
-                                     int(plain_between), 0)
-                st = _lib.RelaxStats()
-                _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, p, st), "relax")
-                done += int(st.iterations)
-                if st.converged:
-                    st.iterations = done
-                    return st
+                _lib.check(self.grid.ctx, lib.sb_relax_sweeps(self.grid.ctx, between), "relax")
         params = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
                                   int(max_iterations), 0)
         st = _lib.RelaxStats()
         _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, params, st), "relax")
-        st.iterations = int(st.iterations) + done
+        st.iterations = int(st.iterations) + max(0, rounds) * max(plain_between, 0)
         return st
