@@ -244,7 +244,10 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             e1.record(stream)
             e1.synchronize()
             wall += time.perf_counter() - t0
-            step_ms.append(e0.elapsed_time(e1))
+            # device time of the step: the step graph's own first/last event
+            # nodes (the host-side events also see the host's launch and
+            # return latency around the synchronous call)
+            step_ms.append(path.last_stats.device_ms if fused else e0.elapsed_time(e1))
             substeps.append(st.substeps)
             ls = path.mobile.last_stats
             if ls is not None and ls.substeps:
@@ -288,6 +291,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                        "l2": "flushed (256 MiB write) between timed steps",
                        "parallelism": f"replicas x{world}",
                        "launch": "one CUDA graph per step" if fused else "operator by operator",
+                       "device_time": ("event nodes at the step graph's first and last node"
+                                       if fused else "CUDA events around each step"),
                        "substeps_total": int(sum(substeps))},
             "e2e": {"value": cell_substeps / wall if wall > 0 else 0.0, "unit": UNIT,
                     "h2d_bytes_per_step": h2d // max(args.steps, 1),

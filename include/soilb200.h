@@ -305,6 +305,7 @@ typedef struct sb_path_stats {
   int candidate;
   int transition_ready;
   int residual_ran;
+  double device_ms;            /* device time of the step graph (first to last node) */
 } sb_path_stats;
 
 int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_flat_indices,

@@ -166,6 +166,7 @@ class PathStats(C.Structure):
         ("entrained_m3", C.c_double), ("persistence_s", C.c_double),
         ("mean_excess_start_deg", C.c_double), ("classification", C.c_int),
         ("candidate", C.c_int), ("transition_ready", C.c_int), ("residual_ran", C.c_int),
+        ("device_ms", C.c_double),
     ]
 
 

@@ -187,9 +187,11 @@ __device__ __forceinline__ void face_fp64(const FvConst& c, double bl, double br
 // Finalisation of one substep by the last block: fixed-order reduction of the
 // block partials, loop control, next dt.
 // --------------------------------------------------------------------------
-template <int NP>
+// Slots [0, NSUM) are sums, [NSUM, NP) maxima; both known at compile time so
+// the NP warp reductions are independent and interleave.
+template <int NP, int NSUM>
 __device__ void reduce_partials(const double* partials, int nblocks, double* out,
-                                double* scratch, const bool* is_max) {
+                                double* scratch) {
   double v[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) v[k] = 0.0;
@@ -197,25 +199,25 @@ __device__ void reduce_partials(const double* partials, int nblocks, double* out
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
       const double x = __ldcg(partials + (size_t)b * NP + k);
-      v[k] = is_max[k] ? fmax(v[k], x) : v[k] + x;
+      v[k] = k >= NSUM ? fmax(v[k], x) : v[k] + x;
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int k = 0; k < NP; ++k) v[k] = is_max[k] ? warp_max(v[k]) : warp_sum(v[k]);
+  for (int k = 0; k < NP; ++k) v[k] = k >= NSUM ? warp_max(v[k]) : warp_sum(v[k]);
   if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < NP; ++k) scratch[warp * NP + k] = v[k];
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < NP) {  // one thread per slot, warps folded in order
+    const int k = threadIdx.x;
+    const bool mx = k >= NSUM;
+    double s = 0.0;
 #pragma unroll
-    for (int k = 0; k < NP; ++k) {
-      double s = 0.0;
-      for (int w = 0; w < kThreads / 32; ++w)
-        s = is_max[k] ? fmax(s, scratch[w * NP + k]) : s + scratch[w * NP + k];
-      out[k] = s;
-    }
+    for (int w = 0; w < kThreads / 32; ++w)
+      s = mx ? fmax(s, scratch[w * NP + k]) : s + scratch[w * NP + k];
+    out[k] = s;
   }
   __syncthreads();
 }
@@ -270,10 +272,7 @@ __device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, doub
 
   __threadfence();
   __shared__ double tot[kFvPartial];
-  __shared__ bool is_max[kFvPartial];
-  if (threadIdx.x < kFvPartial) is_max[threadIdx.x] = threadIdx.x >= kFvDiag;
-  __syncthreads();
-  reduce_partials<kFvPartial>(partials, c.nblocks, tot, red, is_max);
+  reduce_partials<kFvPartial, kFvDiag>(partials, c.nblocks, tot, red);
   if (threadIdx.x == 0) {
     for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] += tot[k];
     ctl->substeps += 1;

@@ -216,11 +216,27 @@ __global__ void __launch_bounds__(kThreads, 3)
   for (int k = 0; k < L_NP; ++k) v[k] = 0.0;
   v[L_NEGMINH] = -1.0e300;
   long long iq0 = 0, iq1 = 0, iq2 = 0;
-  const long long ncell = (long long)c.ny * c.nx;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ncell;
-       i += (long long)gridDim.x * blockDim.x)
-    ledger_cell<FX>(c, b, z, h, qx, qy, ext_x, ext_y, datum, (int)(i / c.nx), (int)(i % c.nx), v,
-                    iq0, iq1, iq2);
+  {
+    // warp items = 32-column segments of one row; a lane owns one column
+    const int strips = (c.nx + 31) >> 5;
+    const int items = strips * c.ny;
+    const int nwarps = gridDim.x * (kThreads / 32);
+    const int lane = threadIdx.x & 31;
+    int it = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+    int r = it / strips, s = it - r * strips;
+    const int dr = nwarps / strips, ds = nwarps - dr * strips;
+    for (; it < items; it += nwarps) {
+      const int col = (s << 5) + lane;
+      if (col < c.nx)
+        ledger_cell<FX>(c, b, z, h, qx, qy, ext_x, ext_y, datum, r, col, v, iq0, iq1, iq2);
+      r += dr;
+      s += ds;
+      if (s >= strips) {
+        s -= strips;
+        ++r;
+      }
+    }
+  }
   __shared__ double red[kThreads / 32 * L_NP];
   __shared__ long long ired[kThreads / 32 * kLedgerI64];
   __shared__ int last;
@@ -236,11 +252,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   // fixed-order final reduction: every thread folds a strided subset of the
   // block partials, then a fixed shuffle/shared-memory tree combines them
   LedgerOut* out = mode == 0 ? &io->before : &io->after;
-  __shared__ bool is_max[L_NP];
   __shared__ double tot[L_NP];
-  if (threadIdx.x < L_NP) is_max[threadIdx.x] = threadIdx.x >= L_NSUM;
-  __syncthreads();
-  reduce_partials<L_NP>(partials, gridDim.x, tot, red, is_max);
+  reduce_partials<L_NP, L_NSUM>(partials, gridDim.x, tot, red);
   {
     long long a[kLedgerI64] = {0, 0, 0};
     for (unsigned bk = threadIdx.x; bk < gridDim.x; bk += kThreads)
@@ -270,9 +283,9 @@ __global__ void __launch_bounds__(kThreads, 3)
   }
 }
 
-// Resets the loop control block for a new physics step of dt seconds.
-__global__ void fv_begin_kernel(FvControl* ctl, const double* dt) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
+// Resets the loop control block for a new physics step of dt seconds (one thread).
+__device__ __forceinline__ void fv_begin_body(FvControl* ctl, const double* dt) {
+  {
     ctl->remaining = *dt;
     ctl->sub_dt = 0.0;
     ctl->max_cfl = 0.0;
@@ -286,6 +299,10 @@ __global__ void fv_begin_kernel(FvControl* ctl, const double* dt) {
     ctl->arrive = 0;
     ctl->wait_fail = 0;
   }
+}
+
+__global__ void fv_begin_kernel(FvControl* ctl, const double* dt) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) fv_begin_body(ctl, dt);
 }
 
 // ---------------------------------------------------------------------------

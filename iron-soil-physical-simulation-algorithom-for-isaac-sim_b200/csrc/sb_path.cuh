@@ -44,6 +44,17 @@ struct PathState {
   int pad;
 };
 
+// Step start: the Mobile V2 loop control for dt (fv_begin) and cleared
+// exchange and labelling records.  One block.
+__global__ void path_begin_kernel(FvControl* ctl, const double* dt, ExchangeOut* xout,
+                                  LabelOut* lout) {
+  if (threadIdx.x == 0) fv_begin_body(ctl, dt);
+  unsigned* xw = reinterpret_cast<unsigned*>(xout);
+  unsigned* lw = reinterpret_cast<unsigned*>(lout);
+  for (int k = threadIdx.x; k < (int)(sizeof(ExchangeOut) / 4); k += blockDim.x) xw[k] = 0u;
+  for (int k = threadIdx.x; k < (int)(sizeof(LabelOut) / 4); k += blockDim.x) lw[k] = 0u;
+}
+
 // Bucket-cut entrainment to target surfaces; the command length is read on
 // the device so the graph is independent of it (mode 1 of entrain_kernel).
 template <bool FX>
@@ -96,7 +107,8 @@ __global__ void __launch_bounds__(kThreads)
 // Classification, persistence and gating (reference gpu_large_avalanche.py
 // :620-676 and the residual gate of v2_physics_core.py:930-1003).
 __global__ void path_classify_kernel(const PathConst c, const LabelOut* lo, const StepIO* io,
-                                     const ExchangeOut* xo, PathState* ps, const double* dt_dev) {
+                                     const ExchangeOut* xo, PathState* ps, const double* dt_dev,
+                                     RelaxControl* rctl) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double dt = *dt_dev;
   const int largest = lo->winner >= 0 ? lo->largest : 0;
@@ -134,13 +146,30 @@ __global__ void path_classify_kernel(const PathConst c, const LabelOut* lo, cons
   const bool quiet = mobile_volume <= c.settled_volume && a.v[L_MAXSPEED] <= c.settled_speed;
   const bool yield_present = lo->total_unstable > 0 && volume > c.dry_tol * c.dx * c.dy;
   ps->residual_enable = c.residual_mode == 2 || (c.residual_mode == 1 && quiet && !yield_present);
+  // frontier loop control for this step: a disabled residual leaves the
+  // pending tile flags untouched for a later step (the reference keeps them queued)
+  rctl->iterations = 0;
+  rctl->done = ps->residual_enable ? 0 : 1;
+  rctl->converged = 0;
+  rctl->status = 0;
+  rctl->max_excess_bits = 0;
+  rctl->arrive = 0;
+  rctl->parity = 0;
+  rctl->n_active = 0;
+  rctl->rounds = 0;
+  rctl->moved_edges = 0;
 }
 
+// Previous-candidate mask and frontier seeds of the winner; the last block
+// to finish then opens the residual frontier loop (frontier_begin).
 __global__ void __launch_bounds__(kThreads)
     path_update_previous_kernel(const LabelConst c, const int* __restrict__ parent,
                                 int* __restrict__ previous, int* __restrict__ reached,
                                 int* __restrict__ tile_flags, const LabelOut* out,
-                                const PathState* ps) {
+                                const PathState* ps, const RelaxConst rc, int* __restrict__ phase0,
+                                int* __restrict__ phase1, RelaxControl* rctl,
+                                cudaGraphConditionalHandle handle) {
+  __shared__ int last;
   const int n = c.ny * c.nx;
   const int winner = out->winner;
   const int keep = ps->keep_candidate, seed = ps->seed_frontier;
@@ -153,23 +182,41 @@ __global__ void __launch_bounds__(kThreads)
       tile_flags[(r / c.tile_size) * c.frontier_tiles_x + col / c.tile_size] = 1;
     }
   }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&rctl->arrive, 1u) == gridDim.x - 1) ? 1 : 0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) rctl->arrive = 0;
+  frontier_begin_body(rc, tile_flags, phase0, phase1, rctl, handle);
 }
 
-// Frontier reset for the step graph: a disabled residual leaves the pending
-// tile flags untouched for a later step (the reference keeps them queued).
-__global__ void path_frontier_reset_kernel(RelaxControl* ctl, const PathState* ps) {
-  if (threadIdx.x == 0) {
-    ctl->iterations = 0;
-    ctl->done = ps->residual_enable ? 0 : 1;
-    ctl->converged = 0;
-    ctl->status = 0;
-    ctl->max_excess_bits = 0;
-    ctl->arrive = 0;
-    ctl->parity = 0;
-    ctl->n_active = 0;
-    ctl->rounds = 0;
-    ctl->moved_edges = 0;
+// Step end: the step's records into the caller-visible pinned host copies
+// (device-mapped pointers, one launch instead of one copy per record), and the
+// reached mask cleared after a converged residual (frontier_finish).
+struct PathRecordPtrs {
+  const void* src[6];
+  void* dst[6];
+  int bytes[6];
+};
+
+__global__ void __launch_bounds__(kThreads)
+    path_records_kernel(const PathRecordPtrs p, const RelaxConst rc, int* __restrict__ reached,
+                        const RelaxControl* rctl) {
+  if (blockIdx.x == 0) {
+    for (int k = 0; k < 6; ++k) {
+      const unsigned* s = static_cast<const unsigned*>(p.src[k]);
+      unsigned* d = static_cast<unsigned*>(p.dst[k]);
+      for (int w = threadIdx.x; w < p.bytes[k] / 4; w += blockDim.x) d[w] = __ldcg(s + w);
+    }
+    __threadfence_system();
   }
+  if (!rctl->converged) return;
+  const long long n = (long long)rc.n0 * rc.pitch;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    reached[i] = 0;
 }
 
 }  // namespace sb

@@ -204,9 +204,11 @@ __device__ __forceinline__ long long gcd_ll(long long a, long long b) {
 }
 
 // Round start: next-active flags -> phase buffer 0; decides termination.
-__global__ void frontier_begin_kernel(const RelaxConst c, int* __restrict__ unstable,
-                                      int* __restrict__ phase0, int* __restrict__ phase1,
-                                      RelaxControl* ctl, cudaGraphConditionalHandle handle) {
+// Body for one block of kThreads threads.
+__device__ __forceinline__ void frontier_begin_body(const RelaxConst& c, int* __restrict__ unstable,
+                                                    int* __restrict__ phase0,
+                                                    int* __restrict__ phase1, RelaxControl* ctl,
+                                                    cudaGraphConditionalHandle handle) {
   __shared__ int cnt[kThreads / 32];
   if (*(volatile int*)&ctl->done) {  // loop disabled before it started: keep the flags
     if (threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
@@ -239,6 +241,12 @@ __global__ void frontier_begin_kernel(const RelaxConst c, int* __restrict__ unst
     __threadfence();
     cudaGraphSetConditional(handle, ctl->done ? 0u : 1u);
   }
+}
+
+__global__ void frontier_begin_kernel(const RelaxConst c, int* __restrict__ unstable,
+                                      int* __restrict__ phase0, int* __restrict__ phase1,
+                                      RelaxControl* ctl, cudaGraphConditionalHandle handle) {
+  frontier_begin_body(c, unstable, phase0, phase1, ctl, handle);
 }
 
 template <bool FX>

@@ -121,6 +121,7 @@ struct sb_ctx {
   int ledger_blocks = 0;
   MobileGraph mobile;
   cudaEvent_t ev_loop[2] = {nullptr, nullptr};  // around the substep WHILE node
+  cudaEvent_t ev_path[2] = {nullptr, nullptr};  // first and last node of the step graph
   bool use_graphs = true;  // false: host-driven launches (profilers that cannot see
                            // kernels inside conditional graphs)
   // labelling (flat ny*nx arrays)
@@ -641,6 +642,8 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMallocHost(&ctx->io_host, sizeof(StepIO)));
   SB_CUDA(ctx, cudaEventCreate(&ctx->ev_loop[0]));
   SB_CUDA(ctx, cudaEventCreate(&ctx->ev_loop[1]));
+  SB_CUDA(ctx, cudaEventCreate(&ctx->ev_path[0]));
+  SB_CUDA(ctx, cudaEventCreate(&ctx->ev_path[1]));
   // labelling buffers (flat ny*nx)
   const size_t n = (size_t)d.ny * d.nx;
   SB_CUDA(ctx, cudaMalloc(&ctx->parent, n * 4));
@@ -790,6 +793,8 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
   if (ctx->rctl_host) cudaFreeHost(ctx->rctl_host);
   for (cudaEvent_t e : ctx->ev_loop)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->ev_path)
     if (e) cudaEventDestroy(e);
   if (ctx->xout_host) cudaFreeHost(ctx->xout_host);
   if (ctx->dep_out_host) cudaFreeHost(ctx->dep_out_host);
@@ -1933,19 +1938,6 @@ extern "C" int sb_surface_sample_bilinear(sb_ctx* ctx, const double* rows, const
 // ---------------------------------------------------------------------------
 namespace {
 
-int add_memset(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps,
-               size_t ndeps, void* dst, size_t bytes) {
-  cudaMemsetParams mp{};
-  mp.dst = dst;
-  mp.value = 0;
-  mp.elementSize = 4;
-  mp.width = bytes / 4;
-  mp.height = 1;
-  mp.pitch = 0;
-  SB_CUDA(ctx, cudaGraphAddMemsetNode(node, g, deps, ndeps, &mp));
-  return SB_OK;
-}
-
 template <bool FX>
 int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   using T = FvTypes<FX>;
@@ -1964,8 +1956,14 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   const int ny = ctx->d.ny, nx = ctx->d.nx;
   double Q = ctx->quantum, datum = ctx->d.datum_m, f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
   cudaGraphNode_t prev, node;
-  // 1. cut entrainment
-  if ((rc = add_memset(ctx, g, &prev, nullptr, 0, ctx->xout, sizeof(ExchangeOut)))) return rc;
+  SB_CUDA(ctx, cudaGraphAddEventRecordNode(&prev, g, nullptr, 0, ctx->ev_path[0]));
+  // 1. step start (loop control, cleared records), cut entrainment
+  {
+    void* args[] = {(void*)&ctx->ctl, (void*)&ctx->dt_dev, (void*)&ctx->xout, (void*)&ctx->lout};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_begin_kernel, dim3(1), 0, args)))
+      return rc;
+    prev = node;
+  }
   {
     int pitch = ctx->pitch;
     int nyv = ny, nxv = nx;
@@ -1982,11 +1980,6 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   static_limit = std::tan(p->mobile.start_angle_deg * (M_PI / 180.0)) + 1.0e-14;
   dat = ctx->d.datum_m;
   static int mode0 = 0, mode1 = 1, use_h = 1, no_h = 0;
-  {
-    void* args[] = {(void*)&ctx->ctl, (void*)&ctx->dt_dev};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)fv_begin_kernel, dim3(1), 0, args))) return rc;
-    prev = node;
-  }
   {
     std::vector<void*> args;
     ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode0, &h_mob, &use_h, args);
@@ -2026,8 +2019,6 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   static LabelConst lc;
   lc = make_label_const(ctx, &p->label);
   const int ltiles = lc.tiles_x * ((ny + kLabelTile - 1) / kLabelTile);
-  if ((rc = add_memset(ctx, g, &node, &prev, 1, ctx->lout, sizeof(LabelOut)))) return rc;
-  prev = node;
   {
     void* args[] = {&lc, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1], &ctx->qx[0], &ctx->qx[1],
                     &ctx->qy[0], &ctx->qy[1], &ctx->ctl, &ctx->parent, &ctx->slope, &ctx->severity,
@@ -2075,36 +2066,26 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   pc.dry_tol = p->label.dry_tolerance_m;
   pc.residual_mode = p->residual_mode;
   pc.fx = FX ? 1 : 0;
+  static RelaxConst rcn;
+  if ((rc = relax_const(ctx, &p->relax, &rcn, ctx->d.tile_size))) return rc;
   {
-    void* args[] = {&pc, &ctx->lout, &ctx->io, &ctx->xout, &ctx->pstate, &ctx->dt_dev};
+    void* args[] = {&pc, &ctx->lout, &ctx->io, &ctx->xout, &ctx->pstate, &ctx->dt_dev, &ctx->rctl};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_classify_kernel, dim3(1), 0, args)))
       return rc;
     prev = node;
   }
+  // 5. previous mask + frontier seeds; its last block opens the gated
+  // residual frontier loop (same kernels as sb_frontier_run)
+  void* begin_args[] = {&rcn, &ctx->ftile_next, &ctx->phase[0], &ctx->phase[1], &ctx->rctl,
+                        &h_front};
   {
     void* args[] = {&lc, &ctx->parent, &ctx->previous, &ctx->reached, &ctx->ftile_next, &ctx->lout,
-                    &ctx->pstate};
+                    &ctx->pstate, &rcn, &ctx->phase[0], &ctx->phase[1], &ctx->rctl, &h_front};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_update_previous_kernel,
                          dim3(grid_for((long long)ny * nx)), 0, args)))
       return rc;
     prev = node;
   }
-  // 5. gated residual frontier (same kernels as sb_frontier_run)
-  static RelaxConst rcn;
-  if ((rc = relax_const(ctx, &p->relax, &rcn, ctx->d.tile_size))) return rc;
-  {
-    void* args[] = {&ctx->rctl, &ctx->pstate};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_frontier_reset_kernel, dim3(1), 0,
-                         args)))
-      return rc;
-    prev = node;
-  }
-  void* begin_args[] = {&rcn, &ctx->ftile_next, &ctx->phase[0], &ctx->phase[1], &ctx->rctl,
-                        &h_front};
-  if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)frontier_begin_kernel, dim3(1), 0,
-                       begin_args)))
-    return rc;
-  prev = node;
   {
     cudaGraphNodeParams cp{};
     cp.type = cudaGraphNodeTypeConditional;
@@ -2137,26 +2118,33 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          begin_args)))
       return rc;
   }
+  // 6. records to the pinned host copies (+ frontier_finish)
   {
-    void* args[] = {&rcn, &ctx->reached, &ctx->rctl};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)frontier_finish_kernel,
-                         dim3(grid_for((long long)rcn.n0 * rcn.pitch)), 0, args)))
+    static PathRecordPtrs rp;
+    const void* srcs[6] = {ctx->ctl, ctx->io, ctx->lout, ctx->rctl, ctx->pstate, ctx->xout};
+    void* hosts[6] = {ctx->ctl_host, ctx->io_host, ctx->lout_host, ctx->rctl_host,
+                      ctx->pstate_host, ctx->xout_host};
+    const int sizes[6] = {(int)sizeof(FvControl), (int)sizeof(StepIO), (int)sizeof(LabelOut),
+                          (int)sizeof(RelaxControl), (int)sizeof(PathState),
+                          (int)sizeof(ExchangeOut)};
+    for (int k = 0; k < 6; ++k) {
+      static_assert(sizeof(FvControl) % 4 == 0 && sizeof(StepIO) % 4 == 0 &&
+                        sizeof(LabelOut) % 4 == 0 && sizeof(RelaxControl) % 4 == 0 &&
+                        sizeof(PathState) % 4 == 0 && sizeof(ExchangeOut) % 4 == 0,
+                    "records are copied as 32-bit words");
+      void* dptr = nullptr;
+      SB_CUDA(ctx, cudaHostGetDevicePointer(&dptr, hosts[k], 0));
+      rp.src[k] = srcs[k];
+      rp.dst[k] = dptr;
+      rp.bytes[k] = sizes[k];
+    }
+    void* args[] = {&rp, &rcn, &ctx->reached, &ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_records_kernel,
+                         dim3(std::min(grid_for((long long)rcn.n0 * rcn.pitch), 2 * 148)), 0, args)))
       return rc;
     prev = node;
   }
-  // 6. records back to pinned host memory
-  struct Copy { void* dst; const void* src; size_t n; };
-  const Copy copies[] = {{ctx->ctl_host, ctx->ctl, sizeof(FvControl)},
-                         {ctx->io_host, ctx->io, sizeof(StepIO)},
-                         {ctx->lout_host, ctx->lout, sizeof(LabelOut)},
-                         {ctx->rctl_host, ctx->rctl, sizeof(RelaxControl)},
-                         {ctx->pstate_host, ctx->pstate, sizeof(PathState)},
-                         {ctx->xout_host, ctx->xout, sizeof(ExchangeOut)}};
-  for (const Copy& cpy : copies) {
-    SB_CUDA(ctx, cudaGraphAddMemcpyNode1D(&node, g, &prev, 1, cpy.dst, cpy.src, cpy.n,
-                                          cudaMemcpyDeviceToHost));
-    prev = node;
-  }
+  SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_path[1]));
   (void)one;
   (void)zero;
   SB_CUDA(ctx, cudaGraphInstantiate(&ctx->path_exec, g, 0));
@@ -2241,6 +2229,9 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
   out->candidate = ps.candidate;
   out->transition_ready = ps.ready;
   out->residual_ran = ps.residual_enable;
+  float step_ms = 0.f;
+  SB_CUDA(ctx, cudaEventElapsedTime(&step_ms, ctx->ev_path[0], ctx->ev_path[1]));
+  out->device_ms = step_ms;
   const FvControl& k = *ctx->ctl_host;
   ctx->launches += 12 + k.substeps + 10LL * r.rounds;
   if (ctx->xout_host->bad_index)
