@@ -75,8 +75,7 @@ __global__ void __launch_bounds__(kThreads)
     batch_ledger_kernel(const BatchPatch* __restrict__ patches, const int* __restrict__ band_patch,
                         int nbands, BatchArena a, const BatchCtl* __restrict__ ctl,
                         double* __restrict__ partials, long long* __restrict__ ipartials) {
-  __shared__ double red[kThreads / 32 * L_NP];
-  __shared__ long long ired[kThreads / 32 * kLedgerI64];
+  __shared__ double fold[fold_words(L_NP)];
   const int band = blockIdx.x;
   if (band >= nbands) return;
   const int p = band_patch[band];
@@ -96,8 +95,8 @@ __global__ void __launch_bounds__(kThreads)
     ledger_cell<true>(c, a.b + base, a.z + base, a.h[parity] + base, a.qx[parity] + base,
                       a.qy[parity] + base, nullptr, nullptr, P.datum, r0 + i / c.nx, i % c.nx, v,
                       iq0, iq1, iq2);
-  ledger_block_store(v, iq0, iq1, iq2, red, ired, partials + (size_t)band * L_NP,
-                     ipartials + (size_t)band * kLedgerI64);
+  ledger_block_store(v, iq0, iq1, iq2, fold, partials + (size_t)band * L_NP,
+                     ipartials + (size_t)band * kLedgerI64, 1);
 }
 
 // One warp per patch: fixed-order fold of the patch's band partials into its

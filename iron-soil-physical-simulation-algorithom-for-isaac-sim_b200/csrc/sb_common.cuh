@@ -68,6 +68,56 @@ __device__ __forceinline__ void block_sum(double (&v)[N], double* scratch) {
   __syncthreads();
 }
 
+// Fixed-order block reduction of NV values per thread through shared memory.
+// A shuffle tree over NV doubles costs 10*NV shuffles per warp and the SM
+// issues about one warp-shuffle per clock, so with many values per thread the
+// shuffles, not the arithmetic, bound a block reduction; here each value is
+// stored once and folded by NV*8 threads.  Slots [0, NSUM) are summed, slots
+// [NSUM, NV) take the maximum.  Order: 32 consecutive threads in order, then
+// the 8 groups in order.  ``scratch`` holds fold_words(NV) values of type T;
+// the result is returned as a pointer to NV values in ``scratch``, valid for
+// every thread of the block until the scratch is reused.
+constexpr int kFoldStride = kThreads + kThreads / 32;  // one pad slot per 32 threads
+__host__ __device__ constexpr int fold_words(int nv) { return nv * kFoldStride + nv * 8 + nv; }
+
+__device__ __forceinline__ double fold_max(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ long long fold_max(long long a, long long b) { return a > b ? a : b; }
+
+template <typename T, int NV, int NSUM>
+__device__ __forceinline__ const T* block_fold(const T* v, T* scratch) {
+  static_assert(NV * 8 <= kThreads, "one pass of chunk folds");
+  const int t = threadIdx.x;
+  const int pos = t + (t >> 5);
+#pragma unroll
+  for (int k = 0; k < NV; ++k) scratch[k * kFoldStride + pos] = v[k];
+  __syncthreads();
+  T* part = scratch + NV * kFoldStride;
+  T* out = part + NV * 8;
+  if (t < NV * 8) {
+    const int k = t >> 3, ch = t & 7;
+    const T* src = scratch + k * kFoldStride + ch * 33;
+    T s = src[0];
+    if (k >= NSUM) {
+#pragma unroll 8
+      for (int j = 1; j < 32; ++j) s = fold_max(s, src[j]);
+    } else {
+#pragma unroll 8
+      for (int j = 1; j < 32; ++j) s += src[j];
+    }
+    part[t] = s;
+  }
+  __syncthreads();
+  if (t < NV) {
+    const T* p = part + t * 8;
+    T s = p[0];
+#pragma unroll
+    for (int ch = 1; ch < 8; ++ch) s = t >= NSUM ? fold_max(s, p[ch]) : s + p[ch];
+    out[t] = s;
+  }
+  __syncthreads();
+  return out;
+}
+
 __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

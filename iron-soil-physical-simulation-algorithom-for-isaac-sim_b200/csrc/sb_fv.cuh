@@ -101,7 +101,6 @@ struct FvSmem {
   typename T::R enm[kEastFaces], enp[kEastFaces], et[kEastFaces];
   M nm[kNorthFaces];
   typename T::R nnm[kNorthFaces], nnp[kNorthFaces], nt[kNorthFaces];
-  double red[kThreads / 32 * kFvPartial];
   uint64_t bar;
   int flag;
 };
@@ -113,8 +112,11 @@ struct FvSmem {
 // --------------------------------------------------------------------------
 // FX face: un/ut are the cells' velocity components q/h (0 for empty cells), cl/cr
 // their celerities sqrt(K g h).  The hydrostatic depth only differs from h on
-// the lower side of a face (d > 0), so only that side needs a square root.
-// Reconstructed discharge is u * hs (= q * hs / h of the reference).
+// the lower side of a face (d > 0): it and its celerity are computed once, for
+// whichever side is lower, and selected (on a flat face the same expressions
+// reproduce h and the prepared celerity exactly), so the face has no branch.
+// Reconstructed discharge is u * hs (= q * hs / h of the reference).  The
+// reciprocals are IEEE round-to-nearest (__frcp_rn == 1.0f / x).
 __device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int br, int hlq,
                                         int hrq, float unl, float utl, float unr, float utr,
                                         float cl, float cr, int& m, float& fnm, float& fnp,
@@ -124,17 +126,14 @@ __device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int
   const int dr = bface - br;
   const float hl = (float)hlq * c.Qf;
   const float hr = (float)hrq * c.Qf;
-  float hsl = hl, hsr = hr, csl = cl, csr = cr, corl = 0.f, corr = 0.f;
-  if (dl != 0) {
-    hsl = fmaxf(hl - (float)dl * c.QKf, 0.f);
-    csl = sqrtf(c.KGf * hsl);
-    corl = (c.HKGf * hl) * hl - (c.HKGf * hsl) * hsl;
-  }
-  if (dr != 0) {
-    hsr = fmaxf(hr - (float)dr * c.QKf, 0.f);
-    csr = sqrtf(c.KGf * hsr);
-    corr = (c.HKGf * hr) * hr - (c.HKGf * hsr) * hsr;
-  }
+  // only the lower side of a face can have a hydrostatic depth below h
+  const bool llow = dl != 0;
+  const float hlow = llow ? hl : hr;
+  const float hs_low = fmaxf(hlow - (float)(dl + dr) * c.QKf, 0.f);
+  const float cs_low = sqrtf(c.KGf * hs_low);
+  const float cor_low = (c.HKGf * hlow) * hlow - (c.HKGf * hs_low) * hs_low;
+  const float hsl = llow ? hs_low : hl, csl = llow ? cs_low : cl, corl = llow ? cor_low : 0.f;
+  const float hsr = llow ? hr : hs_low, csr = llow ? cr : cs_low, corr = llow ? 0.f : cor_low;
   const float qnsl = unl * hsl, qtsl = utl * hsl;
   const float qnsr = unr * hsr, qtsr = utr * hsr;
   const bool wl = hsl > c.dryf, wr = hsr > c.dryf;
@@ -187,39 +186,25 @@ __device__ __forceinline__ void face_fp64(const FvConst& c, double bl, double br
 // Finalisation of one substep by the last block: fixed-order reduction of the
 // block partials, loop control, next dt.
 // --------------------------------------------------------------------------
-// Slots [0, NSUM) are sums, [NSUM, NP) maxima; both known at compile time so
-// the NP warp reductions are independent and interleave.
+// Grid reduction of block partials stored slot-major (partials[k * nblocks +
+// block]): thread t folds blocks t, t + kThreads, ... in order (coalesced
+// loads), then the block folds the threads in a fixed order.  Slots [0, NSUM)
+// are sums, [NSUM, NP) maxima (0 is the identity of both: every maximum here is
+// of non-negative values or only tested against 0).  Returns a pointer into
+// scratch (fold_words(NP) doubles).
 template <int NP, int NSUM>
-__device__ void reduce_partials(const double* partials, int nblocks, double* out,
-                                double* scratch) {
+__device__ const double* reduce_partials(const double* partials, int nblocks, double* scratch) {
   double v[NP];
 #pragma unroll
   for (int k = 0; k < NP; ++k) v[k] = 0.0;
   for (int b = threadIdx.x; b < nblocks; b += kThreads) {
 #pragma unroll
     for (int k = 0; k < NP; ++k) {
-      const double x = __ldcg(partials + (size_t)b * NP + k);
+      const double x = __ldcg(partials + (size_t)k * nblocks + b);
       v[k] = k >= NSUM ? fmax(v[k], x) : v[k] + x;
     }
   }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < NP; ++k) v[k] = k >= NSUM ? warp_max(v[k]) : warp_sum(v[k]);
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < NP; ++k) scratch[warp * NP + k] = v[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < NP) {  // one thread per slot, warps folded in order
-    const int k = threadIdx.x;
-    const bool mx = k >= NSUM;
-    double s = 0.0;
-#pragma unroll
-    for (int w = 0; w < kThreads / 32; ++w)
-      s = mx ? fmax(s, scratch[w * NP + k]) : s + scratch[w * NP + k];
-    out[k] = s;
-  }
-  __syncthreads();
+  return block_fold<double, NP, NSUM>(v, scratch);
 }
 
 // Computes sub_dt/max_cfl for the next substep from ctl->wave (CPU: reference
@@ -240,27 +225,17 @@ __device__ __forceinline__ void plan_substep(const FvConst& c, FvControl* ctl) {
 // error status and the next substep's dt; the graph's while-condition is set
 // from here.
 __device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, double* partials,
-                                          const double* acc, double wave, int neg, double* red,
-                                          int* flag, double sub_dt, int parity,
+                                          const double* acc, double wave, int neg, int* flag,
+                                          double sub_dt, int parity,
                                           cudaGraphConditionalHandle loop_handle, int use_handle) {
+  __shared__ double fold[fold_words(kFvPartial)];
   double v[kFvPartial];
 #pragma unroll
-  for (int k = 0; k < kFvDiag; ++k) v[k] = warp_sum(acc[k]);
-  v[kFvDiag] = warp_max(wave);
-  v[kFvDiag + 1] = (double)__reduce_or_sync(0xffffffffu, (unsigned)neg);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < kFvPartial; ++k) red[warp * kFvPartial + k] = v[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < kFvPartial) {
-    const int k = threadIdx.x;
-    double a = 0.0;
-    for (int w2 = 0; w2 < kThreads / 32; ++w2)
-      a = k >= kFvDiag ? fmax(a, red[w2 * kFvPartial + k]) : a + red[w2 * kFvPartial + k];
-    partials[(size_t)blockIdx.x * kFvPartial + k] = a;
-  }
+  for (int k = 0; k < kFvDiag; ++k) v[k] = acc[k];
+  v[kFvDiag] = wave;
+  v[kFvDiag + 1] = neg ? 1.0 : 0.0;
+  const double* bt = block_fold<double, kFvPartial, kFvDiag>(v, fold);
+  if (threadIdx.x < kFvPartial) partials[(size_t)threadIdx.x * c.nblocks + blockIdx.x] = bt[threadIdx.x];
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -271,8 +246,7 @@ __device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, doub
   if (!*flag) return;
 
   __threadfence();
-  __shared__ double tot[kFvPartial];
-  reduce_partials<kFvPartial, kFvDiag>(partials, c.nblocks, tot, red);
+  const double* tot = reduce_partials<kFvPartial, kFvDiag>(partials, c.nblocks, fold);
   if (threadIdx.x == 0) {
     for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] += tot[k];
     ctl->substeps += 1;
@@ -358,7 +332,7 @@ __global__ void __launch_bounds__(kThreads)
     // per-cell velocity and celerity of the whole halo box
     for (int j = threadIdx.x; j < Tl::BOX; j += kThreads) {
       const float hf = (float)s.h[j] * c.Qf;
-      const float inv = s.h[j] > 0 ? 1.0f / hf : 0.f;
+      const float inv = s.h[j] > 0 ? __frcp_rn(hf) : 0.f;
       s.u[j] = s.qx[j] * inv;
       s.v[j] = s.qy[j] * inv;
       s.cel[j] = sqrtf(c.KGf * hf);
@@ -467,7 +441,7 @@ __global__ void __launch_bounds__(kThreads)
       const float qyn = wet ? qy_old + dqy : 0.f;
       float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
       if (wet) {
-        const float inv = 1.0f / hn;
+        const float inv = __frcp_rn(hn);
         vbx = qxn * inv;
         vby = qyn * inv;
         if (c.has_external) {
@@ -552,7 +526,7 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
 
-  fv_finish(c, ctl, partials, acc, wave, neg, s.red, &s.flag, sub_dt, parity, loop_handle,
+  fv_finish(c, ctl, partials, acc, wave, neg, &s.flag, sub_dt, parity, loop_handle,
             use_handle);
 }
 
@@ -600,7 +574,7 @@ __device__ __forceinline__ void fx_load(const FvConst& c, const int32_t* __restr
 // Per-cell velocity q/h (0 for an empty cell) and celerity sqrt(K g h).
 __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
   const float hf = (float)x.h * c.Qf;
-  const float inv = x.h > 0 ? 1.0f / hf : 0.f;
+  const float inv = x.h > 0 ? __frcp_rn(hf) : 0.f;
   x.u = x.qx * inv;
   x.v = x.qy * inv;
   x.cel = sqrtf(c.KGf * hf);
@@ -650,6 +624,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
     }
   }
   fx_prepare(c, nxt);
+#pragma unroll 2
   for (int r = y0; r < y1; ++r) {
     fx_load(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
     // east face: this column and the next lane's
@@ -691,7 +666,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
       const float qyn = wet ? cur.qy + dqy : 0.f;
       float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
       if (wet) {
-        const float inv = 1.0f / hn;
+        const float inv = __frcp_rn(hn);
         vbx = qxn * inv;
         vby = qyn * inv;
         if (c.has_external) {
@@ -745,7 +720,6 @@ __global__ void __launch_bounds__(kThreads, 4)
                      const float* __restrict__ ext_x, const float* __restrict__ ext_y,
                      FvControl* ctl, double* __restrict__ partials,
                      cudaGraphConditionalHandle loop_handle, int use_handle) {
-  __shared__ double red[kThreads / 32 * kFvPartial];
   __shared__ int flag;
   if (*(volatile int*)&ctl->done) return;  // uniform across the grid
   const double sub_dt = ctl->sub_dt;
@@ -758,7 +732,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   fx_strip_run(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
                parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x, ext_y,
                gw % c.tiles_x, (gw / c.tiles_x) * c.rows_per_warp, sub_dt, acc, wave);
-  fv_finish(c, ctl, partials, acc, wave, 0, red, &flag, sub_dt, parity, loop_handle, use_handle);
+  fv_finish(c, ctl, partials, acc, wave, 0, &flag, sub_dt, parity, loop_handle, use_handle);
 }
 
 }  // namespace sb

@@ -29,6 +29,10 @@
 namespace sb {
 
 constexpr int kLabelTile = 32;
+// Threads of the yield/labelling tile kernel: 12 warps per 32x32 tile and 4
+// tiles per SM keep ~40 warps resident on the one-wave grid of a 701^2 step
+// (its FP64 yield arithmetic is latency bound; 8 warps per tile left ~26).
+constexpr int kLabelInitThreads = 384;
 // Fixed-point units of the per-root sums.  2^32 keeps the int64 sums free of
 // overflow up to 2^24 cells with slopes < pi/2 rad and failure depths < 8 m
 // (1.7e7 * 8 * 6 * 2^32 < 2^63), at a resolution of 2.3e-10.
@@ -110,7 +114,7 @@ __device__ __forceinline__ void local_ccl(int* lab, int connectivity, int gy0, i
                                           int* __restrict__ parent) {
   __syncthreads();
   // block-local union over the backward neighbours W, N (and NW, NE for 8-conn)
-  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kThreads) {
+  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += blockDim.x) {
     if (lab[li] < 0) continue;
     const int ly = li / kLabelTile, lx = li % kLabelTile;
     if (lx > 0 && lab[li - 1] >= 0) lunion(lab, li, li - 1);
@@ -124,7 +128,7 @@ __device__ __forceinline__ void local_ccl(int* lab, int connectivity, int gy0, i
     }
   }
   __syncthreads();
-  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kThreads) {
+  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += blockDim.x) {
     if (lab[li] < 0) continue;
     const int root = lfind(lab, li);
     const int ly = li / kLabelTile, lx = li % kLabelTile;
@@ -135,7 +139,7 @@ __device__ __forceinline__ void local_ccl(int* lab, int connectivity, int gy0, i
 
 
 template <bool FX>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kLabelInitThreads, 4)
     label_init_local_kernel(const LabelConst c, const typename FvTypes<FX>::B* __restrict__ b,
                             const typename FvTypes<FX>::B* __restrict__ z,
                             const typename FvTypes<FX>::H* __restrict__ h0,
@@ -155,7 +159,7 @@ __global__ void __launch_bounds__(kThreads)
   const typename FvTypes<FX>::H* h = P ? h1 : h0;
   const typename FvTypes<FX>::R* qx = P ? qx1 : qx0;
   const typename FvTypes<FX>::R* qy = P ? qy1 : qy0;
-  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kThreads) {
+  for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kLabelInitThreads) {
     const int ly = li / kLabelTile, lx = li % kLabelTile;
     const int r = gy0 + ly, col = gx0 + lx;
     int u = 0;

@@ -130,37 +130,20 @@ __device__ __forceinline__ void ledger_cell(const FvConst& c,
     v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
 }
 
-// Block reduction of per-thread ledger values into one block's partials
-// (L_NP doubles at part, kLedgerI64 integers at ipart), in a fixed order.
-__device__ __forceinline__ void ledger_block_store(double* v, long long iq0, long long iq1,
-                                                   long long iq2, double* red, long long* ired,
-                                                   double* part, long long* ipart) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < L_NP; ++k) v[k] = k < L_NSUM ? warp_sum(v[k]) : warp_max(v[k]);
-  iq0 = (long long)warp_sum_u64((unsigned long long)iq0);
-  iq1 = (long long)warp_sum_u64((unsigned long long)iq1);
-  iq2 = (long long)warp_sum_u64((unsigned long long)iq2);
-  if (lane == 0) {
-#pragma unroll
-    for (int k = 0; k < L_NP; ++k) red[warp * L_NP + k] = v[k];
-    ired[warp * kLedgerI64] = iq0;
-    ired[warp * kLedgerI64 + 1] = iq1;
-    ired[warp * kLedgerI64 + 2] = iq2;
-  }
-  __syncthreads();
-  if (threadIdx.x < L_NP) {
-    const int k = threadIdx.x;
-    double a = k == L_NEGMINH ? -1.0e300 : 0.0;
-    for (int w = 0; w < kThreads / 32; ++w)
-      a = k < L_NSUM ? a + red[w * L_NP + k] : fmax(a, red[w * L_NP + k]);
-    part[k] = a;
-  } else if (threadIdx.x < L_NP + kLedgerI64) {
-    const int k = threadIdx.x - L_NP;
-    long long a = 0;
-    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + k];
-    ipart[k] = a;
-  }
+// Block reduction of per-thread ledger values into one block's partials, in a
+// fixed order: slot k to part[k * stride], integer slot k to ipart[k * stride].
+// fold: fold_words(L_NP) doubles of shared memory.
+__device__ __forceinline__ void ledger_block_store(const double* v, long long iq0, long long iq1,
+                                                   long long iq2, double* fold, double* part,
+                                                   long long* ipart, int stride) {
+  const double* bt = block_fold<double, L_NP, L_NSUM>(v, fold);
+  const double mine = threadIdx.x < L_NP ? bt[threadIdx.x] : 0.0;
+  __syncthreads();  // the integer fold reuses the scratch
+  const long long iv[kLedgerI64] = {iq0, iq1, iq2};
+  const long long* it =
+      block_fold<long long, kLedgerI64, kLedgerI64>(iv, reinterpret_cast<long long*>(fold));
+  if (threadIdx.x < L_NP) part[(size_t)threadIdx.x * stride] = mine;
+  if (threadIdx.x < kLedgerI64) ipart[(size_t)threadIdx.x * stride] = it[threadIdx.x];
 }
 
 // Final value of ledger slot k: the FX path accumulates squared gradient and
@@ -237,40 +220,30 @@ __global__ void __launch_bounds__(kThreads, 3)
       }
     }
   }
-  __shared__ double red[kThreads / 32 * L_NP];
-  __shared__ long long ired[kThreads / 32 * kLedgerI64];
+  __shared__ double fold[fold_words(L_NP)];
   __shared__ int last;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  ledger_block_store(v, iq0, iq1, iq2, red, ired, partials + (size_t)blockIdx.x * L_NP,
-                     ipartials + (size_t)blockIdx.x * kLedgerI64);
+  // block partials slot-major: partials[k * gridDim.x + block]
+  ledger_block_store(v, iq0, iq1, iq2, fold, partials + blockIdx.x, ipartials + blockIdx.x,
+                     gridDim.x);
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = (atomicAdd(arrive, 1u) == gridDim.x - 1) ? 1 : 0;
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // fixed-order final reduction: every thread folds a strided subset of the
-  // block partials, then a fixed shuffle/shared-memory tree combines them
+  // fixed-order final reduction over the block partials
   LedgerOut* out = mode == 0 ? &io->before : &io->after;
-  __shared__ double tot[L_NP];
-  reduce_partials<L_NP, L_NSUM>(partials, gridDim.x, tot, red);
-  {
-    long long a[kLedgerI64] = {0, 0, 0};
-    for (unsigned bk = threadIdx.x; bk < gridDim.x; bk += kThreads)
-      for (int k = 0; k < kLedgerI64; ++k) a[k] += __ldcg(ipartials + (size_t)bk * kLedgerI64 + k);
-    for (int k = 0; k < kLedgerI64; ++k) a[k] = (long long)warp_sum_u64((unsigned long long)a[k]);
-    if (lane == 0)
-      for (int k = 0; k < kLedgerI64; ++k) ired[warp * kLedgerI64 + k] = a[k];
-  }
-  __syncthreads();
-  if (threadIdx.x < L_NP) {
-    out->v[threadIdx.x] = ledger_final_value<FX>(threadIdx.x, tot[threadIdx.x]);
-  }
-  if (threadIdx.x < kLedgerI64) {
-    long long a = 0;
-    for (int w = 0; w < kThreads / 32; ++w) a += ired[w * kLedgerI64 + threadIdx.x];
-    out->iq[threadIdx.x] = a;
-  }
+  const double* tot = reduce_partials<L_NP, L_NSUM>(partials, gridDim.x, fold);
+  const double mine = threadIdx.x < L_NP ? tot[threadIdx.x] : 0.0;
+  __syncthreads();  // the integer fold reuses the scratch
+  long long a[kLedgerI64] = {0, 0, 0};
+  for (unsigned bk = threadIdx.x; bk < gridDim.x; bk += kThreads)
+#pragma unroll
+    for (int k = 0; k < kLedgerI64; ++k) a[k] += __ldcg(ipartials + (size_t)k * gridDim.x + bk);
+  const long long* itot =
+      block_fold<long long, kLedgerI64, kLedgerI64>(a, reinterpret_cast<long long*>(fold));
+  if (threadIdx.x < L_NP) out->v[threadIdx.x] = ledger_final_value<FX>(threadIdx.x, mine);
+  if (threadIdx.x < kLedgerI64) out->iq[threadIdx.x] = itot[threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
     *arrive = 0;

@@ -342,11 +342,12 @@ void ledger_args(sb_ctx* ctx, const FvConst& c, double* datum, double* static_li
 }
 
 int add_kernel(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps,
-               size_t ndeps, void* func, dim3 grid, size_t smem, void** args) {
+               size_t ndeps, void* func, dim3 grid, size_t smem, void** args,
+               unsigned threads = kThreads) {
   cudaKernelNodeParams kp{};
   kp.func = func;
   kp.gridDim = grid;
-  kp.blockDim = dim3(kThreads);
+  kp.blockDim = dim3(threads);
   kp.sharedMemBytes = (unsigned)smem;
   kp.kernelParams = args;
   SB_CUDA(ctx, cudaGraphAddKernelNode(node, g, deps, ndeps, &kp));
@@ -613,10 +614,10 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   ctx->fv_blocks = tiles;
   if (d.precision == SB_FX32) {
     const char* tile_env = std::getenv("SOILB200_FV_TILE");
-    ctx->fv_stream = !(tile_env && tile_env[0] == '1');
+    ctx->fv_stream = (tile_env && tile_env[0] == '1') ? 0 : 1;
     ctx->fv_strips = (d.nx + kStripOut - 1) / kStripOut;
-    // rows per warp: enough warps for ~48 resident per SM, 4..64 rows each
-    const long long want_warps = 148LL * 48;
+    const long long want_warps = 148LL * 32;  // 4 CTAs of 8 warps per SM
+    // rows per warp: about one wave of resident warps, 4..64 rows each
     long long rows = ((long long)d.ny * ctx->fv_strips + want_warps - 1) / want_warps;
     rows = rows < 4 ? 4 : (rows > 64 ? 64 : rows);
     if (const char* rows_env = std::getenv("SOILB200_FV_ROWS")) {
@@ -1082,7 +1083,7 @@ static int run_label(sb_ctx* ctx, const LabelConst& c) {
   using T = FvTypes<FX>;
   const int tiles = c.tiles_x * ((c.ny + kLabelTile - 1) / kLabelTile);
   SB_CUDA(ctx, cudaMemsetAsync(ctx->lout, 0, sizeof(LabelOut), ctx->stream));
-  label_init_local_kernel<FX><<<tiles, kThreads, 0, ctx->stream>>>(
+  label_init_local_kernel<FX><<<tiles, kLabelInitThreads, 0, ctx->stream>>>(
       c, (const typename T::B*)ctx->b, (const typename T::B*)ctx->z,
       (const typename T::H*)ctx->h[0], (const typename T::H*)ctx->h[1],
       (const typename T::R*)ctx->qx[0], (const typename T::R*)ctx->qx[1],
@@ -2007,13 +2008,16 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   }
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[1]));
   prev = node;
+  // The after-step ledger and the labelling chain both only read the final
+  // state: they run as two branches of the graph (the ledger's final fold on
+  // one SM overlaps the labelling) and join at the component reduction.
+  cudaGraphNode_t n_after;
   {
     std::vector<void*> args;
     ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode1, &h_mob, &no_h, args);
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks),
-                         0, args.data())))
+    if ((rc = add_kernel(ctx, g, &n_after, &prev, 1, (void*)ledger_kernel<FX>,
+                         dim3(ctx->ledger_blocks), 0, args.data())))
       return rc;
-    prev = node;
   }
   // 3. labelling
   static LabelConst lc;
@@ -2024,7 +2028,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                     &ctx->qy[0], &ctx->qy[1], &ctx->ctl, &ctx->parent, &ctx->slope, &ctx->severity,
                     &ctx->latch, &ctx->export_cum, &ctx->export_base, &ctx->roots};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_init_local_kernel<FX>, dim3(ltiles),
-                         0, args)))
+                         0, args, kLabelInitThreads)))
       return rc;
     prev = node;
   }
@@ -2045,7 +2049,8 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   }
   {
     void* args[] = {&ctx->roots, &ctx->root_list, &ctx->lout, &ctx->arrive};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_reduce_kernel, dim3(32), 0, args)))
+    const cudaGraphNode_t deps[2] = {prev, n_after};
+    if ((rc = add_kernel(ctx, g, &node, deps, 2, (void*)label_reduce_kernel, dim3(32), 0, args)))
       return rc;
     prev = node;
   }
