@@ -59,6 +59,9 @@ struct FvControl {
   int static_skip;
   unsigned int arrive;
   int wait_fail;
+  unsigned long long wave_bits;  // this substep's wave-speed maximum (atomicMax of the bits)
+  int neg_flag;                  // this substep's positivity failure (atomicOr)
+  int pad;
 };
 
 template <bool FX>
@@ -219,12 +222,15 @@ __device__ __forceinline__ void plan_substep(const FvConst& c, FvControl* ctl) {
   ctl->sub_dt = sub;
 }
 
-// Block partials of one substep (impulse/energy sums, wave maximum,
-// positivity flag) and, in the last block to arrive, the fixed-order grid
-// reduction and loop control: substep count, remaining time, ping-pong parity,
-// error status and the next substep's dt; the graph's while-condition is set
-// from here.
-__device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, double* partials,
+// End of one substep.  Every block folds its impulse/energy sums, wave
+// maximum and positivity flag (fixed order); the sums are added to the block's
+// own accumulators (diag_acc[k * nblocks + block], summed over the step's
+// substeps and folded by the after-step ledger), the maximum and the flag go
+// to the control block by atomicMax / atomicOr (order-free, so deterministic).
+// The last block to arrive then only reads those two words: substep count,
+// remaining time, ping-pong parity, error status and the next substep's dt;
+// the graph's while-condition is set from here.
+__device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, double* diag_acc,
                                           const double* acc, double wave, int neg, int* flag,
                                           double sub_dt, int parity,
                                           cudaGraphConditionalHandle loop_handle, int use_handle) {
@@ -235,7 +241,14 @@ __device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, doub
   v[kFvDiag] = wave;
   v[kFvDiag + 1] = neg ? 1.0 : 0.0;
   const double* bt = block_fold<double, kFvPartial, kFvDiag>(v, fold);
-  if (threadIdx.x < kFvPartial) partials[(size_t)threadIdx.x * c.nblocks + blockIdx.x] = bt[threadIdx.x];
+  if (threadIdx.x < kFvDiag) {
+    double* a = diag_acc + (size_t)threadIdx.x * c.nblocks + blockIdx.x;
+    *a = *a + bt[threadIdx.x];
+  } else if (threadIdx.x == kFvDiag) {  // wave >= 0: its bits order like the values
+    atomicMax(&ctl->wave_bits, (unsigned long long)__double_as_longlong(bt[kFvDiag]));
+  } else if (threadIdx.x == kFvDiag + 1 && bt[kFvDiag + 1] != 0.0) {
+    atomicOr(&ctl->neg_flag, 1);
+  }
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -243,34 +256,31 @@ __device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, doub
     *flag = (prev == (unsigned)c.nblocks - 1) ? 1 : 0;
   }
   __syncthreads();
-  if (!*flag) return;
-
+  if (!*flag || threadIdx.x != 0) return;
   __threadfence();
-  const double* tot = reduce_partials<kFvPartial, kFvDiag>(partials, c.nblocks, fold);
-  if (threadIdx.x == 0) {
-    for (int k = 0; k < kFvDiag; ++k) ctl->diag[k] += tot[k];
-    ctl->substeps += 1;
-    ctl->remaining -= sub_dt;
-    ctl->parity = parity ^ 1;
-    ctl->wave = tot[kFvDiag];
-    ctl->arrive = 0;
-    if (ctl->wait_fail) {
-      ctl->status = 6;  // SB_ERR_WAIT_LIMIT
-      ctl->done = 1;
-    } else if (tot[kFvDiag + 1] != 0.0) {
-      ctl->status = 3;  // SB_ERR_POSITIVITY
-      ctl->done = 1;
-    } else if (!(ctl->remaining > 1.0e-14)) {
-      ctl->done = 1;
-    } else if (ctl->substeps >= c.max_substeps) {
-      ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
-      ctl->done = 1;
-    } else {
-      plan_substep(c, ctl);
-    }
-    __threadfence();
-    if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
+  const double w = __longlong_as_double((long long)atomicExch(&ctl->wave_bits, 0ull));
+  const int failed = atomicExch(&ctl->neg_flag, 0);
+  ctl->substeps += 1;
+  ctl->remaining -= sub_dt;
+  ctl->parity = parity ^ 1;
+  ctl->wave = w;
+  ctl->arrive = 0;
+  if (ctl->wait_fail) {
+    ctl->status = 6;  // SB_ERR_WAIT_LIMIT
+    ctl->done = 1;
+  } else if (failed) {
+    ctl->status = 3;  // SB_ERR_POSITIVITY
+    ctl->done = 1;
+  } else if (!(ctl->remaining > 1.0e-14)) {
+    ctl->done = 1;
+  } else if (ctl->substeps >= c.max_substeps) {
+    ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
+    ctl->done = 1;
+  } else {
+    plan_substep(c, ctl);
   }
+  __threadfence();
+  if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
 }
 
 template <bool FX>
@@ -290,7 +300,7 @@ __global__ void __launch_bounds__(kThreads)
                       typename FvTypes<FX>::R* __restrict__ qy1,
                       const typename FvTypes<FX>::R* __restrict__ ext_x,
                       const typename FvTypes<FX>::R* __restrict__ ext_y, FvControl* ctl,
-                      double* __restrict__ partials, cudaGraphConditionalHandle loop_handle,
+                      double* __restrict__ diag_acc, cudaGraphConditionalHandle loop_handle,
                       int use_handle) {
   using T = FvTypes<FX>;
   using Tl = FvTile<FX>;
@@ -526,7 +536,7 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
 
-  fv_finish(c, ctl, partials, acc, wave, neg, &s.flag, sub_dt, parity, loop_handle,
+  fv_finish(c, ctl, diag_acc, acc, wave, neg, &s.flag, sub_dt, parity, loop_handle,
             use_handle);
 }
 
@@ -718,7 +728,7 @@ __global__ void __launch_bounds__(kThreads, 4)
                      int32_t* __restrict__ h1, float* __restrict__ qx0, float* __restrict__ qx1,
                      float* __restrict__ qy0, float* __restrict__ qy1,
                      const float* __restrict__ ext_x, const float* __restrict__ ext_y,
-                     FvControl* ctl, double* __restrict__ partials,
+                     FvControl* ctl, double* __restrict__ diag_acc,
                      cudaGraphConditionalHandle loop_handle, int use_handle) {
   __shared__ int flag;
   if (*(volatile int*)&ctl->done) return;  // uniform across the grid
@@ -732,7 +742,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   fx_strip_run(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
                parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x, ext_y,
                gw % c.tiles_x, (gw / c.tiles_x) * c.rows_per_warp, sub_dt, acc, wave);
-  fv_finish(c, ctl, partials, acc, wave, 0, &flag, sub_dt, parity, loop_handle, use_handle);
+  fv_finish(c, ctl, diag_acc, acc, wave, 0, &flag, sub_dt, parity, loop_handle, use_handle);
 }
 
 }  // namespace sb

@@ -174,6 +174,10 @@ __device__ __forceinline__ void ledger_prologue(const FvConst& c, const LedgerOu
   }
 }
 
+// mode 0: "before" ledger of a step + prologue (static short-circuit, first
+// dt, loop condition); mode 1: "after" ledger; mode 2: "after" ledger plus the
+// fold of the step's substep impulse/energy sums (diag_acc, c.nblocks FV
+// blocks) into the control block.
 template <bool FX>
 __global__ void __launch_bounds__(kThreads, 3)
     ledger_kernel(const FvConst c, const typename FvTypes<FX>::B* __restrict__ b,
@@ -188,7 +192,8 @@ __global__ void __launch_bounds__(kThreads, 3)
                   const typename FvTypes<FX>::R* __restrict__ ext_y, double datum,
                   double static_limit, int mode, FvControl* ctl, StepIO* io,
                   double* __restrict__ partials, long long* __restrict__ ipartials,
-                  unsigned int* arrive, cudaGraphConditionalHandle loop_handle, int use_handle) {
+                  unsigned int* arrive, double* __restrict__ diag_acc,
+                  cudaGraphConditionalHandle loop_handle, int use_handle) {
   using T = FvTypes<FX>;
   const int parity = ctl->parity;
   const typename T::H* h = parity ? h1 : h0;
@@ -232,7 +237,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   if (!last) return;
   __threadfence();
   // fixed-order final reduction over the block partials
-  LedgerOut* out = mode == 0 ? &io->before : &io->after;
+  LedgerOut* out = mode == 0 ? &io->before : &io->after;  // mode 1, 2: after
   const double* tot = reduce_partials<L_NP, L_NSUM>(partials, gridDim.x, fold);
   const double mine = threadIdx.x < L_NP ? tot[threadIdx.x] : 0.0;
   __syncthreads();  // the integer fold reuses the scratch
@@ -245,6 +250,25 @@ __global__ void __launch_bounds__(kThreads, 3)
   if (threadIdx.x < L_NP) out->v[threadIdx.x] = ledger_final_value<FX>(threadIdx.x, mine);
   if (threadIdx.x < kLedgerI64) out->iq[threadIdx.x] = itot[threadIdx.x];
   __syncthreads();
+  if (mode == 2) {
+    // the step's impulse/energy sums: fold the FV blocks' accumulators in a
+    // fixed order and clear them for the next step
+    const int nb = c.nblocks;
+    double d[kFvDiag];
+#pragma unroll
+    for (int k = 0; k < kFvDiag; ++k) d[k] = 0.0;
+    for (int bk = threadIdx.x; bk < nb; bk += kThreads) {
+#pragma unroll
+      for (int k = 0; k < kFvDiag; ++k) {
+        double* a = diag_acc + (size_t)k * nb + bk;
+        d[k] += __ldcg(a);
+        *a = 0.0;
+      }
+    }
+    const double* dt = block_fold<double, kFvDiag, kFvDiag>(d, fold);
+    if (threadIdx.x < kFvDiag) ctl->diag[threadIdx.x] = dt[threadIdx.x];
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     *arrive = 0;
     if (mode == 0) {

@@ -104,6 +104,7 @@ struct sb_ctx {
   StepIO* io = nullptr;
   double* partials = nullptr;
   long long* ipartials = nullptr;
+  double* fv_diag = nullptr;  // per-FV-block impulse/energy sums of the current step
   unsigned int* arrive = nullptr;
   double* dt_dev = nullptr;
   double* dt_host = nullptr;      // pinned
@@ -317,7 +318,7 @@ void fv_launch(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle
     L.smem = 0;
     L.args = {(void*)&c,         (void*)&ctx->b,     (void*)&ctx->h[0],  (void*)&ctx->h[1],
               (void*)&ctx->qx[0], (void*)&ctx->qx[1], (void*)&ctx->qy[0], (void*)&ctx->qy[1],
-              (void*)&ctx->ext_x, (void*)&ctx->ext_y, (void*)&ctx->ctl,   (void*)&ctx->partials,
+              (void*)&ctx->ext_x, (void*)&ctx->ext_y, (void*)&ctx->ctl,   (void*)&ctx->fv_diag,
               (void*)handle,      (void*)use_handle};
   } else {
     L.func = (void*)fv_substep_kernel<FX>;
@@ -326,7 +327,7 @@ void fv_launch(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle
               (void*)&ctx->tm_qx[0], (void*)&ctx->tm_qx[1], (void*)&ctx->tm_qy[0], (void*)&ctx->tm_qy[1],
               (void*)&ctx->h[0],   (void*)&ctx->h[1],     (void*)&ctx->qx[0],   (void*)&ctx->qx[1],
               (void*)&ctx->qy[0],  (void*)&ctx->qy[1],    (void*)&ctx->ext_x,   (void*)&ctx->ext_y,
-              (void*)&ctx->ctl,    (void*)&ctx->partials, (void*)handle,        (void*)use_handle};
+              (void*)&ctx->ctl,    (void*)&ctx->fv_diag,  (void*)handle,        (void*)use_handle};
   }
   L.grid = dim3(c.nblocks);
 }
@@ -338,7 +339,8 @@ void ledger_args(sb_ctx* ctx, const FvConst& c, double* datum, double* static_li
           (void*)&ctx->qx[0], (void*)&ctx->qx[1],   (void*)&ctx->qy[0],     (void*)&ctx->qy[1],
           (void*)&ctx->ext_x, (void*)&ctx->ext_y,   (void*)datum,           (void*)static_limit,
           (void*)mode,        (void*)&ctx->ctl,     (void*)&ctx->io,        (void*)&ctx->partials,
-          (void*)&ctx->ipartials, (void*)&ctx->arrive, (void*)handle,       (void*)use_handle};
+          (void*)&ctx->ipartials, (void*)&ctx->arrive, (void*)&ctx->fv_diag, (void*)handle,
+          (void*)use_handle};
 }
 
 int add_kernel(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps,
@@ -374,7 +376,7 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
   int use_handle = 1;
   double datum = ctx->d.datum_m;
   double limit = static_limit;
-  int mode0 = 0, mode1 = 1;
+  int mode0 = 0, mode1 = 2;  // 2: after-step ledger + substep diagnostics fold
   FvConst cc = c;
 
   cudaGraphNode_t n_begin, n_pro, n_loop, n_after, n_body;
@@ -469,7 +471,7 @@ static int mobile_step_host_loop(sb_ctx* ctx, const FvConst& c, double static_li
   // Same kernels as the graph, launched from the host; the loop flag is read
   // back after every substep (one synchronisation per substep).
   double datum = ctx->d.datum_m, limit = static_limit;
-  int mode0 = 0, mode1 = 1, no_handle = 0;
+  int mode0 = 0, mode1 = 2, no_handle = 0;  // 2: after-step ledger + diagnostics fold
   cudaGraphConditionalHandle handle{};
   FvConst cc = c;
   {
@@ -635,6 +637,11 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
                     (kFvPartial > L_NP ? kFvPartial : L_NP);
   SB_CUDA(ctx, cudaMalloc(&ctx->partials, np * sizeof(double)));
   SB_CUDA(ctx, cudaMalloc(&ctx->ipartials, (size_t)ctx->ledger_blocks * kLedgerI64 * 8));
+  {
+    const size_t nd = (size_t)kFvDiag * std::max(tiles, ctx->fv_stream_blocks);
+    SB_CUDA(ctx, cudaMalloc(&ctx->fv_diag, nd * sizeof(double)));
+    SB_CUDA(ctx, cudaMemsetAsync(ctx->fv_diag, 0, nd * sizeof(double), ctx->stream));
+  }
   SB_CUDA(ctx, cudaMalloc(&ctx->arrive, sizeof(unsigned)));
   SB_CUDA(ctx, cudaMemsetAsync(ctx->arrive, 0, sizeof(unsigned), ctx->stream));
   SB_CUDA(ctx, cudaMalloc(&ctx->dt_dev, sizeof(double)));
@@ -778,7 +785,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   ctx->frontier.reset();
   void* ptrs[] = {ctx->b, ctx->z, ctx->h[0], ctx->h[1], ctx->qx[0], ctx->qx[1], ctx->qy[0],
                   ctx->qy[1], ctx->ext_x, ctx->ext_y, ctx->reached, ctx->staging,
-                  ctx->range_error, ctx->ctl, ctx->io, ctx->partials, ctx->ipartials,
+                  ctx->range_error, ctx->ctl, ctx->io, ctx->partials, ctx->ipartials, ctx->fv_diag,
                   ctx->arrive, ctx->dt_dev, ctx->parent, ctx->slope, ctx->severity, ctx->latch,
                   ctx->previous, ctx->export_cum, ctx->export_base, ctx->roots.count,
                   ctx->roots.area6, ctx->roots.volume, ctx->roots.exc_start, ctx->roots.exc_stop,
@@ -1980,7 +1987,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   static double static_limit, dat;
   static_limit = std::tan(p->mobile.start_angle_deg * (M_PI / 180.0)) + 1.0e-14;
   dat = ctx->d.datum_m;
-  static int mode0 = 0, mode1 = 1, use_h = 1, no_h = 0;
+  static int mode0 = 0, mode1 = 2, use_h = 1, no_h = 0;  // 2: after + diagnostics fold
   {
     std::vector<void*> args;
     ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode0, &h_mob, &use_h, args);
