@@ -175,8 +175,8 @@ __global__ void __launch_bounds__(kThreads, 3)
   double wave = 0.0;
   fx_strip_run(c, a.b + base, a.h[parity] + base, a.qx[parity] + base, a.qy[parity] + base,
                a.h[parity ^ 1] + base, a.qx[parity ^ 1] + base, a.qy[parity ^ 1] + base, nullptr,
-               nullptr, local % c.tiles_x, (local / c.tiles_x) * c.rows_per_warp, sub_dt, acc,
-               wave);
+               nullptr, local % c.tiles_x, (local / c.tiles_x) * c.rows_per_warp,
+               min((local / c.tiles_x + 1) * c.rows_per_warp, c.ny), sub_dt, acc, wave);
 #pragma unroll
   for (int k = 0; k < kFvDiag; ++k) acc[k] = warp_sum(acc[k]);
   wave = warp_max(wave);

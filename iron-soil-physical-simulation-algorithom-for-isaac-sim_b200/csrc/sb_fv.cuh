@@ -35,7 +35,8 @@ constexpr int kFvPartial = 10;  // kFvDiag + wave max + positivity flag
 
 struct FvConst {
   int ny, nx, pitch, tiles_x, nblocks;  // FX: tiles_x = column strips, nblocks = launch grid
-  int rows_per_warp;                    // FX streaming kernel: rows of one warp's strip
+  int rows_per_warp;                    // batched strips: rows of one warp's strip
+  int row_chunks;                       // FX streaming kernel: row chunks per strip
   double dx, dy, K, g, cfl, dry, mu_g, c_half, kg, min_spacing;
   // fixed-point constants
   double Q;
@@ -62,6 +63,7 @@ struct FvControl {
   unsigned long long wave_bits;  // this substep's wave-speed maximum (atomicMax of the bits)
   int neg_flag;                  // this substep's positivity failure (atomicOr)
   int pad;
+  unsigned long long pmax[4];    // "before" ledger maxima for the prologue: external, |q|, grad, wave
 };
 
 template <bool FX>
@@ -544,7 +546,7 @@ __global__ void __launch_bounds__(kThreads)
 // FX32 substep as a register-streaming stencil.
 //
 // A warp owns a strip of 32 columns (lanes 1..30 are output columns, lanes 0
-// and 31 their west/east neighbours) and walks down rows_per_warp rows.  Per
+// and 31 their west/east neighbours) and walks down a chunk of rows.  Per
 // row every lane evaluates the east face of its column (the east neighbour's
 // state arrives by shuffle) and the north face (the next row is already in
 // registers); the west face is the previous lane's east face (one more
@@ -590,7 +592,7 @@ __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
   x.cel = sqrtf(c.KGf * hf);
 }
 
-// One warp's strip: columns strip*30-1 .. strip*30+30, rows y0 .. y0+rows-1
+// One warp's strip: columns strip*30-1 .. strip*30+30, rows y0 .. y1-1
 // of a grid whose row 0 starts at the given field pointers (row pitch
 // c.pitch).  Accumulates the impulse/energy sums into acc and the largest
 // next-substep wave speed into wave.  Every lane of the warp must call it.
@@ -602,9 +604,8 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
                                              float* __restrict__ qydst,
                                              const float* __restrict__ ext_x,
                                              const float* __restrict__ ext_y, int strip, int y0,
-                                             double sub_dt, double* acc, double& wave) {
+                                             int y1, double sub_dt, double* acc, double& wave) {
   const int lane = threadIdx.x & 31;
-  const int y1 = min(y0 + c.rows_per_warp, c.ny);
   const int gx = strip * kStripOut - 1 + lane;
   const bool colok = gx >= 0 && gx < c.nx;
   const bool out_lane = lane >= 1 && lane <= kStripOut && colok;
@@ -696,8 +697,8 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
       hdst[gi] = hq;
       qxdst[gi] = qxo;
       qydst[gi] = qyo;
-      // per-lane diagnostics in float over this strip (at most rows_per_warp
-      // cells), folded into the double sums once at the end
+      // per-lane diagnostics in float over this strip (one cell per row of
+      // the chunk), folded into the double sums once at the end
       fa[0] += qxn - cur.qx;
       fa[1] += qyn - cur.qy;
       fa[2] += qex - qxn;
@@ -739,9 +740,13 @@ __global__ void __launch_bounds__(kThreads, 4)
 #pragma unroll
   for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
   double wave = 0.0;
+  // row chunk j of the strip: rows [j*ny/J, (j+1)*ny/J), balanced to within one row
+  const int j = gw / c.tiles_x, nchunk = c.row_chunks;
+  const int y0 = j < nchunk ? (int)((long long)j * c.ny / nchunk) : c.ny;
+  const int y1 = j < nchunk ? (int)((long long)(j + 1) * c.ny / nchunk) : c.ny;
   fx_strip_run(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
                parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x, ext_y,
-               gw % c.tiles_x, (gw / c.tiles_x) * c.rows_per_warp, sub_dt, acc, wave);
+               gw % c.tiles_x, y0, y1, sub_dt, acc, wave);
   fv_finish(c, ctl, diag_acc, acc, wave, 0, &flag, sub_dt, parity, loop_handle, use_handle);
 }
 

@@ -154,6 +154,25 @@ __device__ __forceinline__ double ledger_final_value(int k, double val) {
   return val;
 }
 
+// Fixed-order fold of a ledger's slot-major block partials (nb blocks) into
+// out.  Every thread of the block calls it; scratch: fold_words(L_NP) doubles.
+template <bool FX>
+__device__ void ledger_final_fold(const double* partials, const long long* ipartials, int nb,
+                                  double* fold, LedgerOut* out) {
+  const double* tot = reduce_partials<L_NP, L_NSUM>(partials, nb, fold);
+  const double mine = threadIdx.x < L_NP ? tot[threadIdx.x] : 0.0;
+  __syncthreads();  // the integer fold reuses the scratch
+  long long a[kLedgerI64] = {0, 0, 0};
+  for (int bk = threadIdx.x; bk < nb; bk += kThreads)
+#pragma unroll
+    for (int k = 0; k < kLedgerI64; ++k) a[k] += __ldcg(ipartials + (size_t)k * nb + bk);
+  const long long* itot =
+      block_fold<long long, kLedgerI64, kLedgerI64>(a, reinterpret_cast<long long*>(fold));
+  if (threadIdx.x < L_NP) out->v[threadIdx.x] = ledger_final_value<FX>(threadIdx.x, mine);
+  if (threadIdx.x < kLedgerI64) out->iq[threadIdx.x] = itot[threadIdx.x];
+  __syncthreads();
+}
+
 // Static short-circuit and the first substep's dt from a "before" ledger
 // (reference step :199-205, :239-253).  One thread.
 __device__ __forceinline__ void ledger_prologue(const FvConst& c, const LedgerOut* out,
@@ -175,9 +194,12 @@ __device__ __forceinline__ void ledger_prologue(const FvConst& c, const LedgerOu
 }
 
 // mode 0: "before" ledger of a step + prologue (static short-circuit, first
-// dt, loop condition); mode 1: "after" ledger; mode 2: "after" ledger plus the
-// fold of the step's substep impulse/energy sums (diag_acc, c.nblocks FV
-// blocks) into the control block.
+// dt, loop condition).  The prologue only needs four maxima, which the blocks
+// send by atomicMax (order-free), so the last block plans the first substep
+// at once; the before ledger's sums stay as block partials (part_before).
+// mode 1: "after" ledger.  mode 2: "after" ledger, then the folds that the
+// step deferred: the before ledger's partials into io->before and the step's
+// substep impulse/energy sums (diag_acc, c.nblocks FV blocks) into ctl->diag.
 template <bool FX>
 __global__ void __launch_bounds__(kThreads, 3)
     ledger_kernel(const FvConst c, const typename FvTypes<FX>::B* __restrict__ b,
@@ -193,6 +215,7 @@ __global__ void __launch_bounds__(kThreads, 3)
                   double static_limit, int mode, FvControl* ctl, StepIO* io,
                   double* __restrict__ partials, long long* __restrict__ ipartials,
                   unsigned int* arrive, double* __restrict__ diag_acc,
+                  double* __restrict__ part_before, long long* __restrict__ ipart_before,
                   cudaGraphConditionalHandle loop_handle, int use_handle) {
   using T = FvTypes<FX>;
   const int parity = ctl->parity;
@@ -228,29 +251,43 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ double fold[fold_words(L_NP)];
   __shared__ int last;
   // block partials slot-major: partials[k * gridDim.x + block]
-  ledger_block_store(v, iq0, iq1, iq2, fold, partials + blockIdx.x, ipartials + blockIdx.x,
-                     gridDim.x);
+  double* part = mode == 0 ? part_before : partials;
+  long long* ipart = mode == 0 ? ipart_before : ipartials;
+  ledger_block_store(v, iq0, iq1, iq2, fold, part + blockIdx.x, ipart + blockIdx.x, gridDim.x);
+  __syncthreads();
+  if (mode == 0 && threadIdx.x < 4) {  // the prologue's maxima (all >= 0: bits order like values)
+    const int slot = threadIdx.x == 0 ? L_MAXEXT
+                     : threadIdx.x == 1 ? L_MAXQ
+                     : threadIdx.x == 2 ? L_MAXGRAD
+                                        : L_MAXWAVE;
+    const double m = part[(size_t)slot * gridDim.x + blockIdx.x];
+    atomicMax(&ctl->pmax[threadIdx.x], (unsigned long long)__double_as_longlong(m));
+  }
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = (atomicAdd(arrive, 1u) == gridDim.x - 1) ? 1 : 0;
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // fixed-order final reduction over the block partials
-  LedgerOut* out = mode == 0 ? &io->before : &io->after;  // mode 1, 2: after
-  const double* tot = reduce_partials<L_NP, L_NSUM>(partials, gridDim.x, fold);
-  const double mine = threadIdx.x < L_NP ? tot[threadIdx.x] : 0.0;
-  __syncthreads();  // the integer fold reuses the scratch
-  long long a[kLedgerI64] = {0, 0, 0};
-  for (unsigned bk = threadIdx.x; bk < gridDim.x; bk += kThreads)
-#pragma unroll
-    for (int k = 0; k < kLedgerI64; ++k) a[k] += __ldcg(ipartials + (size_t)k * gridDim.x + bk);
-  const long long* itot =
-      block_fold<long long, kLedgerI64, kLedgerI64>(a, reinterpret_cast<long long*>(fold));
-  if (threadIdx.x < L_NP) out->v[threadIdx.x] = ledger_final_value<FX>(threadIdx.x, mine);
-  if (threadIdx.x < kLedgerI64) out->iq[threadIdx.x] = itot[threadIdx.x];
-  __syncthreads();
+  if (mode == 0) {
+    if (threadIdx.x == 0) {
+      // prologue: static short-circuit and the first substep's dt
+      LedgerOut pro;
+      pro.v[L_MAXEXT] = __longlong_as_double((long long)atomicExch(&ctl->pmax[0], 0ull));
+      pro.v[L_MAXQ] = __longlong_as_double((long long)atomicExch(&ctl->pmax[1], 0ull));
+      pro.v[L_MAXGRAD] = ledger_final_value<FX>(
+          L_MAXGRAD, __longlong_as_double((long long)atomicExch(&ctl->pmax[2], 0ull)));
+      pro.v[L_MAXWAVE] = __longlong_as_double((long long)atomicExch(&ctl->pmax[3], 0ull));
+      *arrive = 0;
+      ledger_prologue(c, &pro, static_limit, ctl);
+      __threadfence();
+      if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
+    }
+    return;
+  }
+  ledger_final_fold<FX>(partials, ipartials, gridDim.x, fold, &io->after);
   if (mode == 2) {
+    ledger_final_fold<FX>(part_before, ipart_before, gridDim.x, fold, &io->before);
     // the step's impulse/energy sums: fold the FV blocks' accumulators in a
     // fixed order and clear them for the next step
     const int nb = c.nblocks;
@@ -269,15 +306,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (threadIdx.x < kFvDiag) ctl->diag[threadIdx.x] = dt[threadIdx.x];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    *arrive = 0;
-    if (mode == 0) {
-      // prologue: static short-circuit and the first substep's dt
-      ledger_prologue(c, out, static_limit, ctl);
-      __threadfence();
-      if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
-    }
-  }
+  if (threadIdx.x == 0) *arrive = 0;
 }
 
 // Resets the loop control block for a new physics step of dt seconds (one thread).

@@ -105,6 +105,8 @@ struct sb_ctx {
   double* partials = nullptr;
   long long* ipartials = nullptr;
   double* fv_diag = nullptr;  // per-FV-block impulse/energy sums of the current step
+  double* lpart_before = nullptr;       // "before" ledger block partials (folded at step end)
+  long long* lipart_before = nullptr;
   unsigned int* arrive = nullptr;
   double* dt_dev = nullptr;
   double* dt_host = nullptr;      // pinned
@@ -114,9 +116,10 @@ struct sb_ctx {
   CUtensorMap tm_b, tm_h[2], tm_qx[2], tm_qy[2];
   int fv_blocks = 0;
   // FX32 substep kernel: register-streaming strips (default) or the TMA tile
-  // kernel (SOILB200_FV_TILE=1); strips of 30 output columns x fv_rows rows
+  // kernel (SOILB200_FV_TILE=1); strips of 30 output columns, fv_rows row
+  // chunks per strip
   int fv_stream = 0;
-  int fv_rows = 0;
+  int fv_rows = 0;  // FX streaming kernel: row chunks per strip
   int fv_strips = 0;
   int fv_stream_blocks = 0;
   int ledger_blocks = 0;
@@ -272,7 +275,7 @@ FvConst make_const(const sb_ctx* ctx, const sb_mobile_params* p) {
   if (ctx->fv_stream) {
     c.tiles_x = ctx->fv_strips;
     c.nblocks = ctx->fv_stream_blocks;
-    c.rows_per_warp = ctx->fv_rows;
+    c.row_chunks = ctx->fv_rows;
   }
   c.dx = ctx->d.dx_m;
   c.dy = ctx->d.dy_m;
@@ -339,7 +342,8 @@ void ledger_args(sb_ctx* ctx, const FvConst& c, double* datum, double* static_li
           (void*)&ctx->qx[0], (void*)&ctx->qx[1],   (void*)&ctx->qy[0],     (void*)&ctx->qy[1],
           (void*)&ctx->ext_x, (void*)&ctx->ext_y,   (void*)datum,           (void*)static_limit,
           (void*)mode,        (void*)&ctx->ctl,     (void*)&ctx->io,        (void*)&ctx->partials,
-          (void*)&ctx->ipartials, (void*)&ctx->arrive, (void*)&ctx->fv_diag, (void*)handle,
+          (void*)&ctx->ipartials, (void*)&ctx->arrive, (void*)&ctx->fv_diag,
+          (void*)&ctx->lpart_before, (void*)&ctx->lipart_before, (void*)handle,
           (void*)use_handle};
 }
 
@@ -618,16 +622,19 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
     const char* tile_env = std::getenv("SOILB200_FV_TILE");
     ctx->fv_stream = (tile_env && tile_env[0] == '1') ? 0 : 1;
     ctx->fv_strips = (d.nx + kStripOut - 1) / kStripOut;
-    const long long want_warps = 148LL * 32;  // 4 CTAs of 8 warps per SM
-    // rows per warp: about one wave of resident warps, 4..64 rows each
-    long long rows = ((long long)d.ny * ctx->fv_strips + want_warps - 1) / want_warps;
-    rows = rows < 4 ? 4 : (rows > 64 ? 64 : rows);
+    // row chunks per strip: one wave of warps (4 CTAs of 8 warps on each of
+    // the 148 SMs), at least 3 rows per chunk; the chunks split the rows
+    // evenly (sizes differ by at most one row), so every SM gets the same work
+    const long long want_warps = 148LL * 32;
+    long long chunks = want_warps / ctx->fv_strips;
+    chunks = std::min<long long>(chunks, d.ny / 3);
+    chunks = std::max<long long>(chunks, 1);
     if (const char* rows_env = std::getenv("SOILB200_FV_ROWS")) {
       const long long r = std::atoll(rows_env);
-      if (r >= 1 && r <= 4096) rows = r;
+      if (r >= 1 && r <= 4096) chunks = (d.ny + r - 1) / r;
     }
-    ctx->fv_rows = (int)rows;
-    const long long warps = (long long)ctx->fv_strips * ((d.ny + rows - 1) / rows);
+    ctx->fv_rows = (int)chunks;
+    const long long warps = (long long)ctx->fv_strips * chunks;
     ctx->fv_stream_blocks = (int)((warps + kThreads / 32 - 1) / (kThreads / 32));
   }
   // grid-stride reductions: three CTAs per SM (the ledger kernel's register
@@ -637,6 +644,8 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
                     (kFvPartial > L_NP ? kFvPartial : L_NP);
   SB_CUDA(ctx, cudaMalloc(&ctx->partials, np * sizeof(double)));
   SB_CUDA(ctx, cudaMalloc(&ctx->ipartials, (size_t)ctx->ledger_blocks * kLedgerI64 * 8));
+  SB_CUDA(ctx, cudaMalloc(&ctx->lpart_before, (size_t)ctx->ledger_blocks * L_NP * sizeof(double)));
+  SB_CUDA(ctx, cudaMalloc(&ctx->lipart_before, (size_t)ctx->ledger_blocks * kLedgerI64 * 8));
   {
     const size_t nd = (size_t)kFvDiag * std::max(tiles, ctx->fv_stream_blocks);
     SB_CUDA(ctx, cudaMalloc(&ctx->fv_diag, nd * sizeof(double)));
@@ -786,6 +795,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   void* ptrs[] = {ctx->b, ctx->z, ctx->h[0], ctx->h[1], ctx->qx[0], ctx->qx[1], ctx->qy[0],
                   ctx->qy[1], ctx->ext_x, ctx->ext_y, ctx->reached, ctx->staging,
                   ctx->range_error, ctx->ctl, ctx->io, ctx->partials, ctx->ipartials, ctx->fv_diag,
+                  ctx->lpart_before, ctx->lipart_before,
                   ctx->arrive, ctx->dt_dev, ctx->parent, ctx->slope, ctx->severity, ctx->latch,
                   ctx->previous, ctx->export_cum, ctx->export_base, ctx->roots.count,
                   ctx->roots.area6, ctx->roots.volume, ctx->roots.exc_start, ctx->roots.exc_stop,

@@ -4,7 +4,8 @@ The streaming kernel (warps walk down 30-column strips, faces in registers)
 and the TMA tile kernel (SOILB200_FV_TILE=1) must produce identical int32
 heights and float32 momentum, and both must equal the CPU mirror
 (oracle/fixed_point.py), across strip edges (nx around multiples of 30) and
-row-chunk edges (SOILB200_FV_ROWS forces 1, 3 and 64 rows per warp).
+row-chunk edges (SOILB200_FV_ROWS=r splits every strip into ceil(ny/r)
+balanced row chunks: r = 1, 3 and 64).
 """
 
 import numpy as np
