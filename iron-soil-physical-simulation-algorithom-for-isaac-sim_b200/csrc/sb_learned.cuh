@@ -134,7 +134,7 @@ struct ConvSmem {
   static constexpr int W_BLOCK = COUT * CIN * 2;         // one tap's weights (canonical B)
   static constexpr int W_BYTES = 9 * W_BLOCK;
   static constexpr int ROW_BYTES = (CIN / 8) * kRowLbo;  // one staged input row
-  static constexpr int SLOTS = 4;                        // rows y-1..y+1 in use + one in flight
+  static constexpr int SLOTS = 4;                        // rows y..y+2 in use + one in flight
   static constexpr int BYTES = W_BYTES + SLOTS * ROW_BYTES + 64;
   static constexpr uint32_t TMEM_COLS = 32;              // N = COUT <= 32 f32 columns
 };
@@ -164,22 +164,38 @@ __device__ __forceinline__ void conv_row_wait() {
   fence_async_smem();  // the rows are read by the tensor core (async proxy)
 }
 
+// Waits until at most `pending` (0..2) of this thread's most recent row copies
+// are still in flight.
+__device__ __forceinline__ void conv_row_wait_pending(int pending) {
+  if (pending >= 2)
+    asm volatile("cp.async.wait_group 2;" ::: "memory");
+  else if (pending == 1)
+    asm volatile("cp.async.wait_group 1;" ::: "memory");
+  else
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
+  fence_async_smem();
+}
+
 // D[pixel, co] for output row y: nine taps (dy, dx), each M = 128 pixels x
 // K = CIN against the tap's weights (N = COUT), accumulated in TMEM.
 template <int CIN, int COUT>
 __device__ __forceinline__ void conv_issue_row(uint32_t tmem, uint32_t ring_base,
                                                uint32_t w_base, int y, uint32_t idesc) {
   using S = ConvSmem<CIN, COUT>;
+  // descriptors are built once per row; a tap's operand is the same descriptor
+  // with a 16-byte-multiple start offset added to its address field (bits
+  // 0-13 hold addr >> 4; shared-memory offsets stay below 2^18, so no carry)
+  const uint64_t bdesc0 = umma_desc(w_base, 128, (CIN / 8) * 128);
 #pragma unroll
   for (int dy = 0; dy < 3; ++dy) {
     const uint32_t slot = ring_base + ((y - 1 + dy + S::SLOTS) % S::SLOTS) * S::ROW_BYTES;
+    const uint64_t adesc0 = umma_desc(slot, kRowLbo, 128);
 #pragma unroll
     for (int dx = 0; dx < 3; ++dx) {
-      const uint32_t b_base = w_base + (dy * 3 + dx) * S::W_BLOCK;
 #pragma unroll
       for (int kk = 0; kk < CIN / 16; ++kk)
-        umma_bf16(tmem, umma_desc(slot + kk * 2 * kRowLbo + dx * 16, kRowLbo, 128),
-                  umma_desc(b_base + kk * 256, 128, (CIN / 8) * 128), idesc,
+        umma_bf16(tmem, adesc0 + (uint64_t)((kk * 2 * kRowLbo + dx * 16) >> 4),
+                  bdesc0 + (uint64_t)(((dy * 3 + dx) * S::W_BLOCK + kk * 256) >> 4), idesc,
                   (dy | dx | kk) != 0);
     }
   }
@@ -187,7 +203,12 @@ __device__ __forceinline__ void conv_issue_row(uint32_t tmem, uint32_t ring_base
 
 // Per CTA: one 128-pixel tile of rows [y0, y1).  Row y+1's MMAs are issued as
 // soon as row y's accumulator has been read, so they run while row y's
-// epilogue converts and stores; input rows arrive by cp.async two rows ahead.
+// epilogue converts and stores; input rows are fetched by cp.async into a
+// ring of SLOTS rows, SLOTS - 3 rows ahead of the rows the next MMA batch
+// reads.  (Six slots measured slower than four: the extra 16 KB per CTA of
+// the 32-channel layers cost a CTA per SM, and the per-row time is set by the
+// tensor core's shared-memory operand reads -- 40 wavefronts per
+// M128 x N32 x K16 MMA -- not by the copies.)
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs a) {
   using S = ConvSmem<CIN, COUT>;
@@ -226,12 +247,17 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
   const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
   unsigned phase = 0;
   bool ok = true;
+  int issued = y0 + 1;  // last input row whose copy has been started
   if (y0 < y1) {
     if (tid == 0) {
       conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y0, idesc);
       umma_commit(bar);
     }
-    if (y0 + 1 < y1) conv_row_async<CIN>(a.in, b, a.h, a.w, y0 + 2, x0, slot(y0 + 2));
+    // rows up to y1 are read (the last MMA batch, row y1-1, reads y1)
+    for (int r = y0 + 2; r <= y0 + S::SLOTS - 2 && r <= y1; ++r) {
+      conv_row_async<CIN>(a.in, b, a.h, a.w, r, x0, slot(r));
+      issued = r;
+    }
   }
 
   for (int y = y0; y < y1; ++y) {
@@ -242,16 +268,19 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
 #pragma unroll
     for (int c = 0; c < COUT; c += 16) tmem_ld16(lane_addr + c, d + c);
     tc_fence_before();
-    if (y + 1 < y1) conv_row_wait();  // row y+2 has landed
-    __syncthreads();                  // everyone has read the accumulator
+    if (y + 1 < y1) conv_row_wait_pending(issued - (y + 2));  // row y+2 has landed
+    __syncthreads();                                         // everyone has read the accumulator
     if (y + 1 < y1) {
       if (tid == 0) {
         tc_fence_after();
         conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y + 1, idesc);
         umma_commit(bar);
       }
-      // the slot of row y-1 is free: row y's MMAs have completed
-      if (y + 2 < y1) conv_row_async<CIN>(a.in, b, a.h, a.w, y + 3, x0, slot(y + 3));
+      // the slot of row y-1 (= row y-1+SLOTS) is free: row y's MMAs have completed
+      if (issued + 1 <= y1 && issued + 1 <= y + S::SLOTS - 1) {
+        conv_row_async<CIN>(a.in, b, a.h, a.w, issued + 1, x0, slot(issued + 1));
+        ++issued;
+      }
     }
     const int xo = x0 + tid;
     if (xo < a.w) {
@@ -456,38 +485,39 @@ struct LearnedGeom {
   double datum;
 };
 
+// The per-pixel kernels below take one image row per block iteration
+// (blockIdx.x strides over batch * h rows, threads over the row's columns), so
+// no pixel index is divided into (batch, row, column).
+
 // Features: per edge k, (H[c] - H[n_k]) / (L_k tan_crit) as BF16 channels
 // 0..3 of a 16-channel pixel (12 zero channels); 0 for edges leaving the grid.
 template <typename HT>
 __global__ void learned_features_kernel(const LearnedGeom g, const HT* __restrict__ hgt,
                                         __nv_bfloat16* __restrict__ feat) {
-  const long long n = (long long)g.batch * g.h * g.w;
   const double diag = sqrt(g.dx * g.dx + g.dy * g.dy);
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % g.w);
-    const int r = (int)((i / g.w) % g.h);
-    const int bb = (int)(i / ((long long)g.w * g.h));
+  const double scale = g.Q > 0.0 ? g.Q : 1.0;
+  const double inv_l[4] = {scale / (g.dx * g.tan_crit), scale / (g.dy * g.tan_crit),
+                           scale / (diag * g.tan_crit), scale / (diag * g.tan_crit)};
+  for (int row = blockIdx.x; row < g.batch * g.h; row += gridDim.x) {
+    const int bb = row / g.h, r = row - bb * g.h;
     const HT* H = hgt + (size_t)bb * g.h * g.pitch;
-    const double hc = (double)H[(size_t)r * g.pitch + c];
-    __align__(16) __nv_bfloat16 f[16];
+    for (int c = threadIdx.x; c < g.w; c += blockDim.x) {
+      const double hc = (double)H[(size_t)r * g.pitch + c];
+      __align__(16) __nv_bfloat16 f[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) f[k] = __float2bfloat16_rn(0.f);
+      for (int k = 0; k < 16; ++k) f[k] = __float2bfloat16_rn(0.f);
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      int dr, dc;
-      edge_of(k, dr, dc);
-      const int rn = r + dr, cn = c + dc;
-      if (rn < g.h && cn >= 0 && cn < g.w) {
-        const double L = k == 0 ? g.dx : (k == 1 ? g.dy : diag);
-        const double scale = g.Q > 0.0 ? g.Q : 1.0;
-        const double d = (hc - (double)H[(size_t)rn * g.pitch + cn]) * scale / (L * g.tan_crit);
-        f[k] = __float2bfloat16_rn((float)d);
+      for (int k = 0; k < 4; ++k) {
+        int dr, dc;
+        edge_of(k, dr, dc);
+        const int rn = r + dr, cn = c + dc;
+        if (rn < g.h && cn >= 0 && cn < g.w)
+          f[k] = __float2bfloat16_rn((float)((hc - (double)H[(size_t)rn * g.pitch + cn]) * inv_l[k]));
       }
+      uint4* dst = reinterpret_cast<uint4*>(feat + ((size_t)row * g.w + c) * 16);
+      dst[0] = reinterpret_cast<const uint4*>(f)[0];
+      dst[1] = reinterpret_cast<const uint4*>(f)[1];
     }
-    uint4* dst = reinterpret_cast<uint4*>(feat + i * 16);
-    dst[0] = reinterpret_cast<const uint4*>(f)[0];
-    dst[1] = reinterpret_cast<const uint4*>(f)[1];
   }
 }
 
@@ -503,53 +533,56 @@ __device__ __forceinline__ double learned_transfer(const LearnedGeom& g, double 
 
 // Fixed point: transfers rounded to whole quanta per edge (int32 [pixel][4]),
 // then gathered -- every quantum leaves one cell and enters one neighbour.
+// Q is a power of two, so t / Q == t * (1 / Q) exactly.
 __global__ void learned_quantize_kernel(const LearnedGeom g, const int32_t* __restrict__ hq,
                                         const float* __restrict__ flux /*[pixel][4]*/,
                                         int32_t* __restrict__ tq /*[pixel][4]*/) {
-  const long long n = (long long)g.batch * g.h * g.w;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % g.w);
-    const int r = (int)((i / g.w) % g.h);
-    const int bb = (int)(i / ((long long)g.w * g.h));
+  const double inv_q = 1.0 / g.Q;
+  for (int row = blockIdx.x; row < g.batch * g.h; row += gridDim.x) {
+    const int bb = row / g.h, r = row - bb * g.h;
     const int32_t* H = hq + (size_t)bb * g.h * g.pitch;
-    const double hc = (double)H[(size_t)r * g.pitch + c] * g.Q;
+    for (int c = threadIdx.x; c < g.w; c += blockDim.x) {
+      const size_t i = (size_t)row * g.w + c;
+      const double hc = (double)H[(size_t)r * g.pitch + c] * g.Q;
+      const float4 fl = *reinterpret_cast<const float4*>(flux + i * 4);
+      const float fk[4] = {fl.x, fl.y, fl.z, fl.w};
+      int q[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      int dr, dc;
-      edge_of(k, dr, dc);
-      const int rn = r + dr, cn = c + dc;
-      int q = 0;
-      if (rn < g.h && cn >= 0 && cn < g.w) {
-        const double hn = (double)H[(size_t)rn * g.pitch + cn] * g.Q;
-        const double t = learned_transfer(g, (double)flux[i * 4 + k], hc, hn);
-        q = (int)trunc(t / g.Q);  // toward zero: stays within the half-difference limit
+      for (int k = 0; k < 4; ++k) {
+        int dr, dc;
+        edge_of(k, dr, dc);
+        const int rn = r + dr, cn = c + dc;
+        q[k] = 0;
+        if (rn < g.h && cn >= 0 && cn < g.w) {
+          const double hn = (double)H[(size_t)rn * g.pitch + cn] * g.Q;
+          const double t = learned_transfer(g, (double)fk[k], hc, hn);
+          q[k] = (int)trunc(t * inv_q);  // toward zero: stays within the half-difference limit
+        }
       }
-      tq[i * 4 + k] = q;
+      *reinterpret_cast<int4*>(tq + i * 4) = make_int4(q[0], q[1], q[2], q[3]);
     }
   }
 }
 
 __global__ void learned_apply_fx_kernel(const LearnedGeom g, int32_t* __restrict__ hq,
                                         const int32_t* __restrict__ tq) {
-  const long long n = (long long)g.batch * g.h * g.w;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % g.w);
-    const int r = (int)((i / g.w) % g.h);
-    const int bb = (int)(i / ((long long)g.w * g.h));
-    long long d = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      d -= tq[i * 4 + k];
-      int dr, dc;
-      edge_of(k, dr, dc);
-      const int rs = r - dr, cs = c - dc;  // the cell whose edge k ends here
-      if (rs >= 0 && cs >= 0 && cs < g.w)
-        d += tq[(((long long)bb * g.h + rs) * g.w + cs) * 4 + k];
-    }
+  for (int row = blockIdx.x; row < g.batch * g.h; row += gridDim.x) {
+    const int bb = row / g.h, r = row - bb * g.h;
     int32_t* H = hq + (size_t)bb * g.h * g.pitch;
-    H[(size_t)r * g.pitch + c] = (int32_t)((long long)H[(size_t)r * g.pitch + c] + d);
+    for (int c = threadIdx.x; c < g.w; c += blockDim.x) {
+      const size_t i = (size_t)row * g.w + c;
+      const int4 own = *reinterpret_cast<const int4*>(tq + i * 4);
+      long long d = -(long long)own.x - own.y - own.z - own.w;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        int dr, dc;
+        edge_of(k, dr, dc);
+        const int rs = r - dr, cs = c - dc;  // the cell whose edge k ends here
+        if (rs >= 0 && cs >= 0 && cs < g.w)
+          d += tq[(((size_t)bb * g.h + rs) * g.w + cs) * 4 + k];
+      }
+      H[(size_t)r * g.pitch + c] = (int32_t)((long long)H[(size_t)r * g.pitch + c] + d);
+    }
   }
 }
 

@@ -53,6 +53,13 @@ int lfail(int code, const char* msg) {
   return code;
 }
 
+// Blocks for the row-per-block pixel kernels: one per image row, at most
+// 8 CTAs on each of the 148 SMs (the rest loop).
+int learned_row_grid(int batch, int h) {
+  const long long rows = (long long)batch * h;
+  return (int)(rows < 148LL * 8 ? rows : 148LL * 8);
+}
+
 int lcuda(cudaError_t e) {
   if (e == cudaSuccess) return SB_OK;
   std::snprintf(g_learned_err, sizeof(g_learned_err), "CUDA error %s", cudaGetErrorString(e));
@@ -115,7 +122,7 @@ int sb_learned_features_f64(const double* heights, void* feat, int batch, int h,
   if (!heights || !feat || batch <= 0 || h <= 0 || w <= 0 || !(tan_crit > 0.0))
     return lfail(SB_ERR_BAD_ARG, "[soilb200] features: bad arguments");
   LearnedGeom g{batch, h, w, w, dx, dy, tan_crit, 0.0, 0.0};
-  learned_features_kernel<double><<<grid_for((long long)batch * h * w), kThreads, 0,
+  learned_features_kernel<double><<<learned_row_grid(batch, h), kThreads, 0,
                                     (cudaStream_t)stream>>>(g, heights, (__nv_bfloat16*)feat);
   return lcuda(cudaGetLastError());
 }
@@ -150,8 +157,8 @@ int sb_learned_features(sb_ctx* ctx, void* feat, double tan_crit) {
   if (!fx(ctx)) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] the learned proposal runs on SB_FX32 grids");
   LearnedGeom g{1, ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->d.dx_m, ctx->d.dy_m, tan_crit,
                 ctx->quantum, ctx->d.datum_m};
-  learned_features_kernel<int32_t><<<grid_for((long long)ctx->d.ny * ctx->d.nx), kThreads, 0,
-                                     ctx->stream>>>(g, (const int32_t*)ctx->b, (__nv_bfloat16*)feat);
+  learned_features_kernel<int32_t><<<learned_row_grid(1, ctx->d.ny), kThreads, 0, ctx->stream>>>(
+      g, (const int32_t*)ctx->b, (__nv_bfloat16*)feat);
   ctx->launches++;
   SB_CUDA(ctx, cudaGetLastError());
   return SB_OK;
@@ -159,10 +166,12 @@ int sb_learned_features(sb_ctx* ctx, void* feat, double tan_crit) {
 
 int sb_learned_apply(sb_ctx* ctx, const float* flux, int32_t* tq, double tan_crit) {
   if (!ctx || !flux || !tq || !(tan_crit > 0.0)) return SB_ERR_BAD_ARG;
+  if (((uintptr_t)flux | (uintptr_t)tq) & 15)
+    return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] learned apply: flux and tq must be 16-byte aligned");
   if (!fx(ctx)) return fail(ctx, SB_ERR_BAD_ARG, "[soilb200] the learned proposal runs on SB_FX32 grids");
   LearnedGeom g{1, ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->d.dx_m, ctx->d.dy_m, tan_crit,
                 ctx->quantum, ctx->d.datum_m};
-  const int blocks = grid_for((long long)ctx->d.ny * ctx->d.nx);
+  const int blocks = learned_row_grid(1, ctx->d.ny);
   learned_quantize_kernel<<<blocks, kThreads, 0, ctx->stream>>>(g, (const int32_t*)ctx->b, flux, tq);
   learned_apply_fx_kernel<<<blocks, kThreads, 0, ctx->stream>>>(g, (int32_t*)ctx->b, tq);
   ctx->launches += 2;
