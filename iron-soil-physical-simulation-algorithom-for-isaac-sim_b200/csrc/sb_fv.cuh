@@ -119,13 +119,22 @@ struct FvSmem {
 // their celerities sqrt(K g h).  The hydrostatic depth only differs from h on
 // the lower side of a face (d > 0): it and its celerity are computed once, for
 // whichever side is lower, and selected (on a flat face the same expressions
-// reproduce h and the prepared celerity exactly), so the face has no branch.
+// reproduce h and the prepared celerity exactly), so the face has no branch
+// other than the early return for a face between two empty cells (all of a
+// terrain away from the mobile layer), whose fluxes are all zero.
 // Reconstructed discharge is u * hs (= q * hs / h of the reference).  The
 // reciprocals are IEEE round-to-nearest (__frcp_rn == 1.0f / x).
 __device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int br, int hlq,
                                         int hrq, float unl, float utl, float unr, float utr,
                                         float cl, float cr, int& m, float& fnm, float& fnp,
                                         float& ft) {
+  if ((hlq | hrq) == 0) {
+    // both cells empty: every flux below is a (signed) zero; return +0 (the
+    // sign of a zero flux never changes a field value)
+    m = 0;
+    fnm = fnp = ft = 0.f;
+    return;
+  }
   const int bface = max(bl, br);
   const int dl = bface - bl;
   const int dr = bface - br;
@@ -585,11 +594,17 @@ __device__ __forceinline__ void fx_load(const FvConst& c, const int32_t* __restr
 
 // Per-cell velocity q/h (0 for an empty cell) and celerity sqrt(K g h).
 __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
-  const float hf = (float)x.h * c.Qf;
-  const float inv = x.h > 0 ? __frcp_rn(hf) : 0.f;
-  x.u = x.qx * inv;
-  x.v = x.qy * inv;
-  x.cel = sqrtf(c.KGf * hf);
+  if (x.h > 0) {
+    const float hf = (float)x.h * c.Qf;
+    const float inv = __frcp_rn(hf);
+    x.u = x.qx * inv;
+    x.v = x.qy * inv;
+    x.cel = sqrtf(c.KGf * hf);
+  } else {  // empty cell (the same values: q * 0 and sqrt(0)); no reciprocal or root
+    x.u = x.qx * 0.f;
+    x.v = x.qy * 0.f;
+    x.cel = 0.f;
+  }
 }
 
 // One warp's strip: columns strip*30-1 .. strip*30+30, rows y0 .. y1-1
