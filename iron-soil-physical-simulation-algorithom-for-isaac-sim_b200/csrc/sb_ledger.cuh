@@ -84,14 +84,18 @@ __device__ __forceinline__ void ledger_cell(const FvConst& c,
   const bool wet = hv > c.dry;
   double s2 = 0.0, spd = 0.0, e = 0.0, wave;
   if constexpr (FX) {
-    const float hn = (float)h[gi] * c.Qf;
-    float vx = 0.f, vy = 0.f;
-    if (hn > c.dryf) {
-      const float inv = 1.0f / hn;
-      vx = qx[gi] * inv;
-      vy = qy[gi] * inv;
+    if (h[gi] == 0) {
+      wave = 0.0;  // empty cell: no velocity, no celerity (the expression below gives 0)
+    } else {
+      const float hn = (float)h[gi] * c.Qf;
+      float vx = 0.f, vy = 0.f;
+      if (hn > c.dryf) {
+        const float inv = 1.0f / hn;
+        vx = qx[gi] * inv;
+        vy = qy[gi] * inv;
+      }
+      wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
     }
-    wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
     if (wet) {  // one reciprocal: e = |q|^2 / h (= h |u|^2), s2 = e / h
       const double inv = 1.0 / hv;
       e = (qxv * qxv + qyv * qyv) * inv;
