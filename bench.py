@@ -167,11 +167,11 @@ class ClockSampler:
 # the same workload (dram__bytes_read.sum + dram__bytes_write.sum); the
 # captures and their commands are summarised in profiles/.
 NCU_TRAFFIC_BYTES = {
-    # profiles/plain_path_step_701_launches.md: 8.504320 MB read + 256 B write
+    # fv_stream_kernel at 701^2, ncu --set full of one launch: 7.987712 MB read
     # (cold L2 under ncu; the state fits in L2, so writes stay there)
-    "config1_plain_path_701": 8_504_576,
-    # profiles/fv_stream_kernel_mobile_v2_4096.md: 282.211584 MB + 167.329280 MB
-    "mobile_v2_4096": 449_540_864,
+    "config1_plain_path_701": 7_987_712,
+    # profiles/fv_stream_kernel_mobile_v2_4096.md: 275.369216 MB + 164.824064 MB
+    "mobile_v2_4096": 440_193_280,
 }
 
 
