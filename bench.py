@@ -236,18 +236,25 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             flush.zero_()
             torch.cuda.synchronize()
             idx, tgt = sched[k]
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            t0 = time.perf_counter()
-            e0.record(stream)
-            st = path.step(DT, idx, tgt)
-            e1.record(stream)
-            e1.synchronize()
-            wall += time.perf_counter() - t0
-            # device time of the step: the step graph's own first/last event
-            # nodes (the host-side events also see the host's launch and
-            # return latency around the synchronous call)
-            step_ms.append(path.last_stats.device_ms if fused else e0.elapsed_time(e1))
+            if fused:
+                # the step call is synchronous (its records are read back before
+                # it returns): the wall clock around it is the end-to-end time,
+                # and its device time comes from the step graph's own first and
+                # last event nodes
+                t0 = time.perf_counter()
+                st = path.step(DT, idx, tgt)
+                wall += time.perf_counter() - t0
+                step_ms.append(path.last_stats.device_ms)
+            else:
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                t0 = time.perf_counter()
+                e0.record(stream)
+                st = path.step(DT, idx, tgt)
+                e1.record(stream)
+                e1.synchronize()
+                wall += time.perf_counter() - t0
+                step_ms.append(e0.elapsed_time(e1))
             substeps.append(st.substeps)
             ls = path.mobile.last_stats
             if ls is not None and ls.substeps:

@@ -381,9 +381,11 @@ __global__ void __launch_bounds__(kThreads)
 
 // Region count, total, largest (ties -> smallest root) in one pass over roots;
 // the last block copies the winner's accumulators into the output record.
-__global__ void __launch_bounds__(kThreads)
-    label_reduce_kernel(LabelRoots roots, const int* __restrict__ root_list, LabelOut* out,
-                        unsigned int* arrive) {
+// Returns true in the one thread (thread 0 of the last block) that wrote the
+// final record.
+__device__ __forceinline__ bool label_reduce_body(const LabelRoots& roots,
+                                                  const int* __restrict__ root_list, LabelOut* out,
+                                                  unsigned int* arrive) {
   const int nroots = out->root_count;
   unsigned long long best = 0;
   int total = 0;
@@ -406,7 +408,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ int last;
   if (threadIdx.x == 0) last = atomicAdd(arrive, 1u) == gridDim.x - 1;
   __syncthreads();
-  if (!last || threadIdx.x != 0) return;
+  if (!last || threadIdx.x != 0) return false;
   __threadfence();
   *arrive = 0;
   out->regions = nroots;
@@ -414,7 +416,7 @@ __global__ void __launch_bounds__(kThreads)
   if (key == 0) {
     out->largest = 0;
     out->winner = -1;
-    return;
+    return true;
   }
   const int winner = (int)(0x7fffffffu - (unsigned)(key & 0xffffffffu));
   out->largest = (int)(key >> 32);
@@ -426,6 +428,13 @@ __global__ void __launch_bounds__(kThreads)
   out->max_exc_start = roots.max_exc_start[winner];
   out->max_exc_stop = roots.max_exc_stop[winner];
   out->prev_overlap = roots.prev_overlap[winner];
+  return true;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    label_reduce_kernel(LabelRoots roots, const int* __restrict__ root_list, LabelOut* out,
+                        unsigned int* arrive) {
+  label_reduce_body(roots, root_list, out, arrive);
 }
 
 // previous-component mask and residual frontier seeding (reference :277-306).

@@ -106,10 +106,11 @@ __global__ void __launch_bounds__(kThreads)
 
 // Classification, persistence and gating (reference gpu_large_avalanche.py
 // :620-676 and the residual gate of v2_physics_core.py:930-1003).
-__global__ void path_classify_kernel(const PathConst c, const LabelOut* lo, const StepIO* io,
-                                     const ExchangeOut* xo, PathState* ps, const double* dt_dev,
-                                     RelaxControl* rctl) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One thread.
+__device__ __forceinline__ void path_classify_body(const PathConst& c, const LabelOut* lo,
+                                                   const StepIO* io, const ExchangeOut* xo,
+                                                   PathState* ps, const double* dt_dev,
+                                                   RelaxControl* rctl) {
   const double dt = *dt_dev;
   const int largest = lo->winner >= 0 ? lo->largest : 0;
   const double area = (double)lo->area6 * c.f;
@@ -158,6 +159,19 @@ __global__ void path_classify_kernel(const PathConst c, const LabelOut* lo, cons
   rctl->n_active = 0;
   rctl->rounds = 0;
   rctl->moved_edges = 0;
+}
+
+// The component reduction and, in the thread that finishes it, the
+// classification: one node of the step graph instead of two.
+__global__ void __launch_bounds__(kThreads)
+    path_reduce_classify_kernel(LabelRoots roots, const int* __restrict__ root_list, LabelOut* lo,
+                                unsigned int* arrive, const PathConst c, const StepIO* io,
+                                const ExchangeOut* xo, PathState* ps, const double* dt_dev,
+                                RelaxControl* rctl) {
+  if (label_reduce_body(roots, root_list, lo, arrive)) {
+    __threadfence();
+    path_classify_body(c, lo, io, xo, ps, dt_dev, rctl);
+  }
 }
 
 // Previous-candidate mask and frontier seeds of the winner; the last block

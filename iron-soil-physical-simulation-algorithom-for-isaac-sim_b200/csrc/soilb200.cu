@@ -408,7 +408,12 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     FvLaunch L;
     fv_launch<FX>(ctx, cc, &handle, &use_handle, L);
+    // two substeps per loop iteration (the second returns at once when the
+    // first ended the step): half the conditional-node relaunches
     int rc = add_kernel(ctx, body, &n_body, nullptr, 0, L.func, L.grid, L.smem, L.args.data());
+    if (rc) return rc;
+    cudaGraphNode_t n_body2;
+    rc = add_kernel(ctx, body, &n_body2, &n_body, 1, L.func, L.grid, L.smem, L.args.data());
     if (rc) return rc;
   }
   {
@@ -1027,7 +1032,8 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
                                ctx->stream));
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const FvControl& k = *ctx->ctl_host;
-  ctx->launches += 3 + k.substeps;
+  // graph: two substep launches per loop iteration; host loop: one per substep
+  ctx->launches += 3 + (ctx->use_graphs ? (k.substeps + 1) / 2 * 2 : k.substeps);
   rc = fill_mobile_stats(ctx, params, out);
   if (rc) return rc;
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
@@ -2018,8 +2024,13 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     prev = node;
     FvLaunch L;
     fv_launch<FX>(ctx, fc, &h_mob, &use_h, L);
-    cudaGraphNode_t body_node;
+    // two substeps per loop iteration (the second returns at once when the
+    // first ended the step): half the conditional-node relaunches
+    cudaGraphNode_t body_node, body_node2;
     if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node, nullptr, 0, L.func,
+                         L.grid, L.smem, L.args.data())))
+      return rc;
+    if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node2, &body_node, 1, L.func,
                          L.grid, L.smem, L.args.data())))
       return rc;
   }
@@ -2064,14 +2075,8 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
       return rc;
     prev = node;
   }
-  {
-    void* args[] = {&ctx->roots, &ctx->root_list, &ctx->lout, &ctx->arrive};
-    const cudaGraphNode_t deps[2] = {prev, n_after};
-    if ((rc = add_kernel(ctx, g, &node, deps, 2, (void*)label_reduce_kernel, dim3(32), 0, args)))
-      return rc;
-    prev = node;
-  }
-  // 4. classification / persistence / gate, then previous mask + seeding
+  // 4. component reduction + classification / persistence / gate, then
+  // previous mask + seeding
   static PathConst pc;
   pc = PathConst{};
   pc.f = f;
@@ -2091,8 +2096,11 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   static RelaxConst rcn;
   if ((rc = relax_const(ctx, &p->relax, &rcn, ctx->d.tile_size))) return rc;
   {
-    void* args[] = {&pc, &ctx->lout, &ctx->io, &ctx->xout, &ctx->pstate, &ctx->dt_dev, &ctx->rctl};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_classify_kernel, dim3(1), 0, args)))
+    void* args[] = {&ctx->roots, &ctx->root_list, &ctx->lout, &ctx->arrive, &pc,
+                    &ctx->io,    &ctx->xout,      &ctx->pstate, &ctx->dt_dev, &ctx->rctl};
+    const cudaGraphNode_t deps[2] = {prev, n_after};
+    if ((rc = add_kernel(ctx, g, &node, deps, 2, (void*)path_reduce_classify_kernel, dim3(32), 0,
+                         args)))
       return rc;
     prev = node;
   }
@@ -2255,7 +2263,9 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
   SB_CUDA(ctx, cudaEventElapsedTime(&step_ms, ctx->ev_path[0], ctx->ev_path[1]));
   out->device_ms = step_ms;
   const FvControl& k = *ctx->ctl_host;
-  ctx->launches += 12 + k.substeps + 10LL * r.rounds;
+  // ten kernels outside the loops, two substep launches per loop iteration,
+  // ten kernels per residual round
+  ctx->launches += 10 + (k.substeps + 1) / 2 * 2 + 10LL * r.rounds;
   if (ctx->xout_host->bad_index)
     return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] entrainment index outside state");
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");

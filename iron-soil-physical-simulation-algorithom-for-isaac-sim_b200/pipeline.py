@@ -72,6 +72,7 @@ class PlainPath:
         self.max_rounds = int(max_rounds)
         self.last_stats: _lib.PathStats | None = None
         self._params = self._path_params()
+        self._sb_path_step = _lib.load().sb_path_step
 
     def _path_params(self) -> _lib.PathParams:
         cfg = self.avalanche.config
@@ -105,19 +106,20 @@ class PlainPath:
                 raise ValueError("[DeviceBulkState] invalid entrainment request")
         st = _lib.PathStats()
         g = self.grid
-        _lib.check(g.ctx, _lib.load().sb_path_step(
+        _lib.check(g.ctx, self._sb_path_step(
             g.ctx, float(dt_s), idx.ctypes.data if n else None, tgt.ctypes.data if n else None,
             n, self._params, st), "sb_path_step")
         self.last_stats = st
-        self.mobile.last_stats = st.mobile
+        mob, lab = st.mobile, st.label
+        self.mobile.last_stats = mob
         self.state.advance_time(dt_s)
-        return PathStepStats(int(st.mobile.substeps), float(st.entrained_m3),
-                             CLASSIFICATIONS[st.classification], int(st.label.unstable_cell_count),
-                             int(st.label.connected_region_count),
-                             int(st.label.largest_connected_cell_count),
+        after = mob.after
+        return PathStepStats(int(mob.substeps), float(st.entrained_m3),
+                             CLASSIFICATIONS[st.classification], int(lab.unstable_cell_count),
+                             int(lab.connected_region_count),
+                             int(lab.largest_connected_cell_count),
                              int(st.relax.iterations) if st.residual_ran else 0,
-                             float(st.mobile.after.volume_w_m3),
-                             float(st.mobile.after.max_speed_m_s))
+                             float(after.volume_w_m3), float(after.max_speed_m_s))
 
     def _step_operators(self, dt_s, cut_cells, cut_targets) -> PathStepStats:
         entrained = 0.0
