@@ -186,6 +186,19 @@ def measured_peak():
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def combine_over_ranks(dev_s: float, wall_s: float, work: float, device: str):
+    """Replicas: the job's time is the slowest rank's (device and wall clock),
+    its work the sum over ranks.  Every rank calls this with the same
+    collectives in the same order."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([dev_s, wall_s], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([float(work)], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1]), float(c[0])
+
+
 def run_gpu(args, rank: int, world: int, local_rank: int):
     import torch
     import soilb200
@@ -266,13 +279,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     cells = n * n
     cell_substeps = cells * sum(substeps)
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([dev_s, wall], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        c = torch.tensor([float(cell_substeps)], dtype=torch.float64, device=f"cuda:{local_rank}")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        dev_s, wall = float(t[0]), float(t[1])
-        cell_substeps = float(c[0])
+        dev_s, wall, cell_substeps = combine_over_ranks(dev_s, wall, cell_substeps,
+                                                        f"cuda:{local_rank}")
     peak, peak_kind = measured_peak()
     tot_loop = sum(m for m, _ in loop_ms)
     tot_launch = sum(n for _, n in loop_ms)

@@ -76,3 +76,34 @@ def test_fx32_path_conserves_total_volume_exactly():
     assert moved > 0.0
     assert path.state.reservoir_reduction(1600.0)["mobile_quanta_w6"] > 0
     path.close()
+
+
+def test_host_driven_substep_loop_equals_graph(monkeypatch):
+    """SOILB200_NO_GRAPH=1 (host-driven launches of the same kernels, one
+    synchronisation per substep) gives the step graph's fields and records."""
+    n = 96
+    b, cut = _setup(n, seed=2)
+    z = np.zeros_like(b)
+    graph = PlainPath(b, z, dx=0.05, material=_material(), tile_size=32, residual="gated",
+                      fused=False)
+    monkeypatch.setenv("SOILB200_NO_GRAPH", "1")
+    host = PlainPath(b, z, dx=0.05, material=_material(), tile_size=32, residual="gated",
+                     fused=False)
+    monkeypatch.delenv("SOILB200_NO_GRAPH")
+    for k in range(12):
+        idx, tgt = cut.footprint((k + 1) * DT)
+        a = graph.step(DT, idx, tgt)
+        o = host.step(DT, idx, tgt)
+        assert a.substeps == o.substeps, k
+        assert (a.unstable_cells, a.regions, a.largest) == (o.unstable_cells, o.regions, o.largest)
+        sa, so = graph.mobile.last_stats, host.mobile.last_stats
+        assert sa.friction_dissipation == pytest.approx(so.friction_dissipation, rel=1e-12, abs=1e-30)
+        for j in range(2):
+            assert sa.conservative_impulse_m4_s[j] == pytest.approx(
+                so.conservative_impulse_m4_s[j], rel=1e-12, abs=1e-30)
+        assert sa.before.mass_m3 == so.before.mass_m3
+        assert sa.after.mass_m3 == so.after.mass_m3
+        for fa, fo in zip(_fields(graph), _fields(host)):
+            assert np.array_equal(fa, fo), k
+    graph.close()
+    host.close()
