@@ -1487,7 +1487,7 @@ static int build_frontier(sb_ctx* ctx, const RelaxConst& c) {
   lg.graph = g;
   cudaGraphConditionalHandle handle;
   SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
-  static RelaxConst cc;  // copied into the node parameters at add time
+  RelaxConst cc;  // copied into the node parameters at add time
   cc = c;
   cudaGraphNode_t n_reset, n_begin0, n_loop, n_finish;
   int rc;
@@ -1998,12 +1998,12 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     prev = node;
   }
   // 2. Mobile V2 (same kernels as the standalone step graph)
-  static FvConst fc;
+  FvConst fc;
   fc = make_const(ctx, &p->mobile);
-  static double static_limit, dat;
+  double static_limit, dat;
   static_limit = std::tan(p->mobile.start_angle_deg * (M_PI / 180.0)) + 1.0e-14;
   dat = ctx->d.datum_m;
-  static int mode0 = 0, mode1 = 2, use_h = 1, no_h = 0;  // 2: after + diagnostics fold
+  int mode0 = 0, mode1 = 2, use_h = 1, no_h = 0;  // 2: after + diagnostics fold
   {
     std::vector<void*> args;
     ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode0, &h_mob, &use_h, args);
@@ -2048,7 +2048,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
       return rc;
   }
   // 3. labelling
-  static LabelConst lc;
+  LabelConst lc;
   lc = make_label_const(ctx, &p->label);
   const int ltiles = lc.tiles_x * ((ny + kLabelTile - 1) / kLabelTile);
   {
@@ -2067,7 +2067,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     prev = node;
   }
   {
-    static int mask_only = 0;
+    int mask_only = 0;
     void* args[] = {&lc, &ctx->parent, &ctx->b, &ctx->z, &ctx->slope, &ctx->severity, &ctx->latch,
                     &ctx->previous, &ctx->roots, &ctx->root_list, &ctx->lout, &mask_only};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_compress_kernel<FX>,
@@ -2077,7 +2077,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   }
   // 4. component reduction + classification / persistence / gate, then
   // previous mask + seeding
-  static PathConst pc;
+  PathConst pc;
   pc = PathConst{};
   pc.f = f;
   pc.Q = ctx->quantum;
@@ -2093,7 +2093,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   pc.dry_tol = p->label.dry_tolerance_m;
   pc.residual_mode = p->residual_mode;
   pc.fx = FX ? 1 : 0;
-  static RelaxConst rcn;
+  RelaxConst rcn;
   if ((rc = relax_const(ctx, &p->relax, &rcn, ctx->d.tile_size))) return rc;
   {
     void* args[] = {&ctx->roots, &ctx->root_list, &ctx->lout, &ctx->arrive, &pc,
@@ -2125,8 +2125,8 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     SB_CUDA(ctx, cudaGraphAddNode(&node, g, &prev, 1, &cp));
     prev = node;
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    static int dirs[8], pars[8];
-    static typename T::H* hf;
+    int dirs[8], pars[8];
+    typename T::H* hf;
     hf = (typename T::H*)ctx->b;
     cudaGraphNode_t bprev = nullptr, bnode;
     for (int k = 0; k < 8; ++k) {
@@ -2150,7 +2150,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   }
   // 6. records to the pinned host copies (+ frontier_finish)
   {
-    static PathRecordPtrs rp;
+    PathRecordPtrs rp;
     const void* srcs[6] = {ctx->ctl, ctx->io, ctx->lout, ctx->rctl, ctx->pstate, ctx->xout};
     void* hosts[6] = {ctx->ctl_host, ctx->io_host, ctx->lout_host, ctx->rctl_host,
                       ctx->pstate_host, ctx->xout_host};
