@@ -477,10 +477,15 @@ def c1_after_cut(n: int = N):
     return b
 
 
-def run_repose(args, rounds: int = 8, plain_between: int = 5, eps_slope: float = 1e-4):
+REPOSE_SCALES = (1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5)
+
+
+def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: float = 1e-4):
     """Second headline metric: ms to repose at 701^2 after the cut, the learned
     proposal (tensor-core conv net, flux form, exact quanta) + plain sweeps
-    against plain sweeps alone, same tolerance (eps * dx m), same start."""
+    against plain sweeps alone, same tolerance (eps * dx m), same start.  The
+    proposal runs len(scales) rounds, round i moving scales[i] of the
+    network's transfer (full-size rounds first, then damped ones)."""
     import torch
     import soilb200
     from soilb200 import learned
@@ -496,6 +501,7 @@ def run_repose(args, rounds: int = 8, plain_between: int = 5, eps_slope: float =
 
     # one resident grid per arm (buffers, graphs and the network's workspace are
     # reused across trials); each trial re-uploads the post-cut surface untimed
+    rounds = len(scales)
     grids = {}
     for r in (0, rounds):
         g = soilb200.DeviceGrid(b.shape, DX, DX, precision="fx32", height_exponent=k, datum_m=datum)
@@ -512,7 +518,7 @@ def run_repose(args, rounds: int = 8, plain_between: int = 5, eps_slope: float =
         launches0 = g.kernel_launches()
         e0.record(stream)
         st = lr.relax(tol, max_iterations=400000, rounds=r,
-                      plain_between=plain_between if r else 0)
+                      plain_between=plain_between if r else 0, scales=scales[:r])
         e1.record(stream)
         e1.synchronize()
         s1 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
@@ -536,6 +542,7 @@ def run_repose(args, rounds: int = 8, plain_between: int = 5, eps_slope: float =
             "ms_per_step": lm, "higher_is_better": False, "dtype": "int32-quanta (bf16 net, f32 accumulate)",
             "data": "synthetic (config-1 pile after the full straight cut)",
             "config": {"workload": "repose_701", "proposal_rounds": rounds,
+                       "proposal_scales": list(scales),
                        "plain_sweeps_between_proposals": plain_between, "tolerance_m": tol,
                        "plain_ms": pm, "speedup_vs_plain": pm / lm,
                        "plain_iterations": plain[0][1], "learned_iterations": learn[0][1],

@@ -275,9 +275,14 @@ class LearnedRelaxation:
         self._torch_stream = torch.cuda.ExternalStream(self._stream, device=dev)
         torch.cuda.current_stream(dev).synchronize()
 
-    def propose(self, rounds: int = 1) -> None:
+    def propose(self, rounds: int = 1, scale: float = 1.0) -> None:
+        """``rounds`` proposals; each moves ``scale`` times the network's
+        transfer (flux * tan_crit * dx * scale per edge, still limited to half
+        the height difference and rounded toward zero to whole quanta)."""
         torch = _torch()
         lib = _lib.load()
+        if not scale > 0.0:
+            raise ValueError("[soilb200] the proposal scale must be positive")
         with torch.cuda.stream(self._torch_stream):
             for _ in range(rounds):
                 _lib.check(self.grid.ctx, lib.sb_learned_features(self.grid.ctx,
@@ -285,32 +290,39 @@ class LearnedRelaxation:
                                                                   self.tan_crit), "features")
                 _, flux = network_forward(self.net, self._feat, self._packed,
                                           stream=self._stream)
+                # the transfer is flux * tan * dx, so the scale rides on tan
                 _lib.check(self.grid.ctx, lib.sb_learned_apply(self.grid.ctx, flux.data_ptr(),
                                                                self._tq.data_ptr(),
-                                                               self.tan_crit), "apply")
+                                                               self.tan_crit * scale), "apply")
 
     def relax(self, tolerance_m: float, max_iterations: int = 20000, rounds: int = 1,
-              spacing=None, plain_between: int = 0):
+              spacing=None, plain_between: int = 0, scales=None):
         """Learned rounds, then relax_critical_slope sweeps to the tolerance.
 
         With ``plain_between`` > 0 each proposal is followed by that many plain
         sweeps (the proposal moves material over the network's receptive
         field, the sweeps resolve what it left); the whole schedule is queued
         on the grid's stream without host round trips, and only the final
-        sweeps to the tolerance report back.  Returns that RelaxStats, with
-        ``iterations`` including the interleaved sweeps (as an upper bound:
-        the interleaved calls stop early when already converged)."""
+        sweeps to the tolerance report back.  ``scales`` (one positive factor
+        per round, default 1.0 each) damps later proposals, whose full-size
+        transfers overshoot once the surface is near repose.  Returns that
+        RelaxStats, with ``iterations`` including the interleaved sweeps (as an
+        upper bound: the interleaved calls stop early when already converged)."""
+        rounds = max(0, int(rounds))
+        scales = [1.0] * rounds if scales is None else [float(x) for x in scales]
+        if len(scales) != rounds:
+            raise ValueError("[soilb200] scales needs one factor per proposal round")
         s0, s1 = spacing if spacing is not None else (self.grid.dy, self.grid.dx)
         lib = _lib.load()
         between = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
                                    int(max(plain_between, 1)), 0)
-        for _ in range(max(0, rounds)):
-            self.propose(1)
+        for sc in scales:
+            self.propose(1, sc)
             if plain_between > 0:
                 _lib.check(self.grid.ctx, lib.sb_relax_sweeps(self.grid.ctx, between), "relax")
         params = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
                                   int(max_iterations), 0)
         st = _lib.RelaxStats()
         _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, params, st), "relax")
-        st.iterations = int(st.iterations) + max(0, rounds) * max(plain_between, 0)
+        st.iterations = int(st.iterations) + rounds * max(plain_between, 0)
         return st

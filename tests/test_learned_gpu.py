@@ -161,3 +161,32 @@ def test_fixed_point_proposal_conserves_volume_and_relaxes():
     sum2 = int(np.rint((out - datum) * q).astype(np.int64).sum())
     assert sum2 == sum0
     grid.close()
+
+
+def test_scaled_proposal_schedule():
+    """A vanishing scale rounds every transfer to zero quanta (nothing moves);
+    a damped schedule keeps the exact volume and still reaches the tolerance."""
+    ln = _learned()
+    from soilb200 import workloads
+    b = workloads.config3_patch(5, n=96)
+    k, datum = soilb200.choose_quantization(b)
+    grid = soilb200.DeviceGrid(b.shape, 0.05, 0.05, precision="fx32", height_exponent=k,
+                               datum_m=datum)
+    grid.upload("b_eff", b)
+    grid.upload("z_base", np.zeros_like(b))
+    q = 2.0 ** k
+    before = grid.download("b_eff")
+    net = ln.ReposeNet(seed=2)
+    relax = ln.LearnedRelaxation(grid, net, 35.0)
+    relax.propose(rounds=1, scale=1e-30)
+    assert np.array_equal(grid.download("b_eff"), before)
+    with pytest.raises(ValueError):
+        relax.propose(rounds=1, scale=0.0)
+    with pytest.raises(ValueError):
+        relax.relax(1e-6, rounds=2, scales=[1.0])
+    sum0 = int(np.rint((before - datum) * q).astype(np.int64).sum())
+    st = relax.relax(1e-6, rounds=4, plain_between=3, scales=[1.0, 1.0, 0.5, 0.5])
+    assert st.converged
+    sum1 = int(np.rint((grid.download("b_eff") - datum) * q).astype(np.int64).sum())
+    assert sum1 == sum0
+    grid.close()
