@@ -44,11 +44,25 @@ struct PathState {
   int pad;
 };
 
-// Step start: the Mobile V2 loop control for dt (fv_begin) and cleared
+// Per-step inputs of the fused step, written by the host into mapped pinned
+// memory before each graph launch and read by the graph's first kernels over
+// the host link (no copy-engine operations between steps).
+struct PathInput {
+  double dt;
+  int count;  // cut command length
+  int pad;
+};
+
+// Step start: dt and the cut command length from the host-mapped inputs into
+// device copies, the Mobile V2 loop control for dt (fv_begin) and cleared
 // exchange and labelling records.  One block.
-__global__ void path_begin_kernel(FvControl* ctl, const double* dt, ExchangeOut* xout,
-                                  LabelOut* lout) {
-  if (threadIdx.x == 0) fv_begin_body(ctl, dt);
+__global__ void path_begin_kernel(FvControl* ctl, const PathInput* in, double* dt_dev,
+                                  int* count_dev, ExchangeOut* xout, LabelOut* lout) {
+  if (threadIdx.x == 0) {
+    *dt_dev = __ldcv(&in->dt);
+    *count_dev = __ldcv(&in->count);
+    fv_begin_body(ctl, dt_dev);
+  }
   unsigned* xw = reinterpret_cast<unsigned*>(xout);
   unsigned* lw = reinterpret_cast<unsigned*>(lout);
   for (int k = threadIdx.x; k < (int)(sizeof(ExchangeOut) / 4); k += blockDim.x) xw[k] = 0u;
@@ -57,6 +71,7 @@ __global__ void path_begin_kernel(FvControl* ctl, const double* dt, ExchangeOut*
 
 // Bucket-cut entrainment to target surfaces; the command length is read on
 // the device so the graph is independent of it (mode 1 of entrain_kernel).
+// idx / target are the host-mapped command (read once each, uncached).
 template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     path_entrain_kernel(int ny, int nx, int pitch, double Q, double datum, double f,
@@ -72,7 +87,8 @@ __global__ void __launch_bounds__(kThreads)
   long long vq = 0;
   double vs = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-    const int i = idx[k];
+    const int i = __ldcv(idx + k);
+    const double tk = __ldcv(target + k);
     if (i < 0 || i >= ny * nx) {
       atomicExch(&out->bad_index, 1);
       continue;
@@ -82,7 +98,7 @@ __global__ void __launch_bounds__(kThreads)
     const int w6 = vertex_weight6(r, c, ny, nx);
     if constexpr (FX) {
       const long long avail = (long long)b[gi] - (long long)z[gi];
-      const long long req = (long long)b[gi] - (long long)rint((target[k] - datum) / Q);
+      const long long req = (long long)b[gi] - (long long)rint((tk - datum) / Q);
       long long d = req < avail ? req : avail;
       if (d < 0) d = 0;
       b[gi] = (int32_t)(b[gi] - d);
@@ -90,7 +106,7 @@ __global__ void __launch_bounds__(kThreads)
       vq += d * w6;
     } else {
       const double avail = fmax(b[gi] - z[gi], 0.0);
-      const double d = fmin(fmax(b[gi] - target[k], 0.0), avail);
+      const double d = fmin(fmax(b[gi] - tk, 0.0), avail);
       b[gi] = b[gi] - d;
       h[gi] = h[gi] + d;
       vs += d * ((double)w6 * f);

@@ -155,8 +155,11 @@ struct sb_ctx {
   // fused plain-path step
   PathState* pstate = nullptr;
   PathState* pstate_host = nullptr;
-  int* path_count = nullptr;
-  int* path_count_host = nullptr;
+  int* path_count = nullptr;       // device copy of the cut length (written by path_begin)
+  PathInput* path_in = nullptr;     // pinned, mapped: dt + cut length of the next step
+  int32_t* path_idx = nullptr;      // pinned, mapped: cut command of the next step
+  double* path_val = nullptr;
+  int path_cap = 0;                 // cells path_idx / path_val hold
   cudaGraphExec_t path_exec = nullptr;
   cudaGraph_t path_graph = nullptr;
   unsigned char path_key[512] = {0};
@@ -736,7 +739,7 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMemsetAsync(ctx->pstate, 0, sizeof(PathState), ctx->stream));
   SB_CUDA(ctx, cudaMallocHost(&ctx->pstate_host, sizeof(PathState)));
   SB_CUDA(ctx, cudaMalloc(&ctx->path_count, sizeof(int)));
-  SB_CUDA(ctx, cudaMallocHost(&ctx->path_count_host, sizeof(int)));
+  SB_CUDA(ctx, cudaHostAlloc(&ctx->path_in, sizeof(PathInput), cudaHostAllocMapped));
   // TMA descriptors (box = halo tile of the FV kernel)
   int rc;
   {
@@ -824,7 +827,9 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   if (ctx->mob_out_host) cudaFreeHost(ctx->mob_out_host);
   if (ctx->pers_out_host) cudaFreeHost(ctx->pers_out_host);
   if (ctx->pstate_host) cudaFreeHost(ctx->pstate_host);
-  if (ctx->path_count_host) cudaFreeHost(ctx->path_count_host);
+  if (ctx->path_in) cudaFreeHost(ctx->path_in);
+  if (ctx->path_idx) cudaFreeHost(ctx->path_idx);
+  if (ctx->path_val) cudaFreeHost(ctx->path_val);
   if (ctx->path_exec) cudaGraphExecDestroy(ctx->path_exec);
   if (ctx->path_graph) cudaGraphDestroy(ctx->path_graph);
   if (ctx->dt_host) cudaFreeHost(ctx->dt_host);
@@ -1983,7 +1988,10 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&prev, g, nullptr, 0, ctx->ev_path[0]));
   // 1. step start (loop control, cleared records), cut entrainment
   {
-    void* args[] = {(void*)&ctx->ctl, (void*)&ctx->dt_dev, (void*)&ctx->xout, (void*)&ctx->lout};
+    void* in_dev = nullptr;
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
+    void* args[] = {(void*)&ctx->ctl, &in_dev, (void*)&ctx->dt_dev, (void*)&ctx->path_count,
+                    (void*)&ctx->xout, (void*)&ctx->lout};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_begin_kernel, dim3(1), 0, args)))
       return rc;
     prev = node;
@@ -1991,8 +1999,11 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   {
     int pitch = ctx->pitch;
     int nyv = ny, nxv = nx;
+    void *idx_dev = nullptr, *val_dev = nullptr;
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&idx_dev, ctx->path_idx, 0));
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&val_dev, ctx->path_val, 0));
     void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
-                    &ctx->ctl, &ctx->xidx, &ctx->xval, &ctx->path_count, &ctx->xout};
+                    &ctx->ctl, &idx_dev, &val_dev, &ctx->path_count, &ctx->xout};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_entrain_kernel<FX>, dim3(64), 0, args)))
       return rc;
     prev = node;
@@ -2205,6 +2216,23 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
   if (rc) return rc;
   if (!ctx->use_graphs)
     return fail(ctx, SB_ERR_STATE, "[soilb200] the fused step needs CUDA graphs (unset SOILB200_NO_GRAPH)");
+  if (cut_count > ctx->path_cap || !ctx->path_idx) {
+    // the graph reads the command from these buffers: grow them (rare; the
+    // cut footprint changes little between steps) and rebuild the graph
+    const long long cells = (long long)ctx->d.ny * ctx->d.nx;
+    const int cap = (int)std::min<long long>(
+        cells, std::max<long long>({(long long)cut_count, 2LL * ctx->path_cap, 4096LL}));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->path_idx) cudaFreeHost(ctx->path_idx);
+    if (ctx->path_val) cudaFreeHost(ctx->path_val);
+    ctx->path_idx = nullptr;
+    ctx->path_val = nullptr;
+    ctx->path_cap = 0;
+    ctx->path_valid = false;
+    SB_CUDA(ctx, cudaHostAlloc(&ctx->path_idx, (size_t)cap * 4, cudaHostAllocMapped));
+    SB_CUDA(ctx, cudaHostAlloc(&ctx->path_val, (size_t)cap * 8, cudaHostAllocMapped));
+    ctx->path_cap = cap;
+  }
   if (!ctx->path_valid || std::memcmp(ctx->path_key, p, sizeof(*p)) != 0) {
     static_assert(sizeof(sb_path_params) <= sizeof(((sb_ctx*)nullptr)->path_key), "key size");
     rc = fx(ctx) ? build_path_graph<true>(ctx, p) : build_path_graph<false>(ctx, p);
@@ -2213,17 +2241,13 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
     // the standalone Mobile graph shares the control block; force its rebuild check
     ctx->mobile.valid = false;
   }
-  *ctx->dt_host = dt_s;
-  *ctx->path_count_host = cut_count;
-  SB_CUDA(ctx, cudaMemcpyAsync(ctx->dt_dev, ctx->dt_host, sizeof(double), cudaMemcpyHostToDevice,
-                               ctx->stream));
-  SB_CUDA(ctx, cudaMemcpyAsync(ctx->path_count, ctx->path_count_host, sizeof(int),
-                               cudaMemcpyHostToDevice, ctx->stream));
+  // the previous step's graph has finished (every call ends synchronised), so
+  // the mapped inputs are free to overwrite; the launch publishes them
+  ctx->path_in->dt = dt_s;
+  ctx->path_in->count = cut_count;
   if (cut_count > 0) {
-    SB_CUDA(ctx, cudaMemcpyAsync(ctx->xidx, cut_idx, (size_t)cut_count * 4, cudaMemcpyHostToDevice,
-                                 ctx->stream));
-    SB_CUDA(ctx, cudaMemcpyAsync(ctx->xval, cut_target, (size_t)cut_count * 8,
-                                 cudaMemcpyHostToDevice, ctx->stream));
+    std::memcpy(ctx->path_idx, cut_idx, (size_t)cut_count * 4);
+    std::memcpy(ctx->path_val, cut_target, (size_t)cut_count * 8);
   }
   SB_CUDA(ctx, cudaGraphLaunch(ctx->path_exec, ctx->stream));
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -107,3 +107,31 @@ def test_host_driven_substep_loop_equals_graph(monkeypatch):
             assert np.array_equal(fa, fo), k
     graph.close()
     host.close()
+
+
+@pytest.mark.parametrize("precision", ["fx32", "fp64"])
+def test_fused_step_cut_command_growth(precision):
+    """Cut commands of varying length, one larger than the fused step's first
+    command buffer (4096 cells), an empty one and a repeated one: the fused
+    step still equals the operator path field for field."""
+    n = 160
+    b, _ = _setup(n, seed=3)
+    z = np.zeros_like(b)
+    fused = PlainPath(b, z, dx=0.05, material=_material(), precision=precision, tile_size=32,
+                      residual="always", fused=True)
+    ops = PlainPath(b, z, dx=0.05, material=_material(), precision=precision, tile_size=32,
+                    residual="always", fused=False)
+    rng = np.random.default_rng(7)
+    sizes = [200, 0, 6000, 6000, 50, 9000, 0, 300]
+    for k, m in enumerate(sizes):
+        idx = rng.choice(n * n, size=m, replace=False).astype(np.int32)
+        tgt = b.ravel()[idx] - rng.uniform(0.0, 0.05, size=m)
+        a = fused.step(DT, idx, tgt)
+        o = ops.step(DT, idx, tgt)
+        assert a.substeps == o.substeps, k
+        assert a.entrained_m3 == pytest.approx(o.entrained_m3, rel=1e-12, abs=1e-15), k
+        assert a.residual_rounds == o.residual_rounds, k
+        for fa, fo in zip(_fields(fused), _fields(ops)):
+            assert np.array_equal(fa, fo), k
+    fused.close()
+    ops.close()
