@@ -278,7 +278,10 @@ int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double* requested
  * (gpu_large_avalanche.py:541-676) -> frontier seeding for local
  * instabilities -> residual MiniSlope frontier rounds, gated as the
  * reference gates them (quiet mobile layer, no mobilizable yield).  The whole
- * step is one CUDA graph launch with one host synchronisation. */
+ * step is one CUDA graph launch with one host synchronisation.  The cut
+ * command is copied on the host into the context's mapped pinned buffers
+ * (read by the graph over the host link), so the caller's arrays may be
+ * pageable and are not referenced after the call. */
 typedef struct sb_path_params {
   sb_mobile_params mobile;
   sb_label_params label;
