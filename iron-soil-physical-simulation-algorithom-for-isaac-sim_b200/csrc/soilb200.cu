@@ -2246,6 +2246,9 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
   ctx->path_in->dt = dt_s;
   ctx->path_in->count = cut_count;
   if (cut_count > 0) {
+    for (int k = 0; k < cut_count; ++k)
+      if (!std::isfinite(cut_target[k]))
+        return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] invalid entrainment request");
     std::memcpy(ctx->path_idx, cut_idx, (size_t)cut_count * 4);
     std::memcpy(ctx->path_val, cut_target, (size_t)cut_count * 8);
   }

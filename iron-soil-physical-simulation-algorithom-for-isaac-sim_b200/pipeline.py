@@ -102,7 +102,7 @@ class PlainPath:
         if n:
             idx = np.ascontiguousarray(cut_cells, dtype=np.int32)
             tgt = np.ascontiguousarray(cut_targets, dtype=np.float64)
-            if tgt.shape != idx.shape or not np.all(np.isfinite(tgt)):
+            if tgt.shape != idx.shape:  # finiteness is checked by sb_path_step
                 raise ValueError("[DeviceBulkState] invalid entrainment request")
         st = _lib.PathStats()
         g = self.grid

@@ -135,3 +135,22 @@ def test_fused_step_cut_command_growth(precision):
             assert np.array_equal(fa, fo), k
     fused.close()
     ops.close()
+
+
+def test_fused_step_rejects_invalid_cut_commands():
+    """A non-finite target, an index outside the grid and mismatched lengths
+    raise ValueError with the reference's message; a later valid step works."""
+    n = 64
+    b, _ = _setup(n, seed=2)
+    path = PlainPath(b, np.zeros_like(b), dx=0.05, material=_material(), tile_size=32,
+                     fused=True)
+    idx = np.array([n * n // 2 + n // 2 + k for k in range(3)], dtype=np.int32)  # on the pile
+    with pytest.raises(ValueError, match="invalid entrainment request"):
+        path.step(DT, idx, np.array([0.1, np.nan, 0.1]))
+    with pytest.raises(ValueError, match="invalid entrainment request"):
+        path.step(DT, idx, np.array([0.1, 0.1]))
+    with pytest.raises(ValueError, match="entrainment index outside state"):
+        path.step(DT, np.array([5, n * n], dtype=np.int32), np.array([0.1, 0.1]))
+    st = path.step(DT, idx, b.ravel()[idx] - 0.01)
+    assert st.entrained_m3 > 0.0
+    path.close()
