@@ -29,10 +29,11 @@
 namespace sb {
 
 constexpr int kLabelTile = 32;
-// Threads of the yield/labelling tile kernel: 12 warps per 32x32 tile and 4
-// tiles per SM keep ~40 warps resident on the one-wave grid of a 701^2 step
-// (its FP64 yield arithmetic is latency bound; 8 warps per tile left ~26).
-constexpr int kLabelInitThreads = 384;
+// Threads of the yield/labelling tile kernel: 16 warps per 32x32 tile (two
+// cells per thread) and 3 tiles per SM; its FP64 yield arithmetic is latency
+// bound, and 12 warps per tile (4 tiles per SM) measured 1.3 % slower on the
+// whole 701^2 step, 8 warps 0.1 % slower still.
+constexpr int kLabelInitThreads = 512;
 // Fixed-point units of the per-root sums.  2^32 keeps the int64 sums free of
 // overflow up to 2^24 cells with slopes < pi/2 rad and failure depths < 8 m
 // (1.7e7 * 8 * 6 * 2^32 < 2^63), at a resolution of 2.3e-10.
@@ -139,7 +140,7 @@ __device__ __forceinline__ void local_ccl(int* lab, int connectivity, int gy0, i
 
 
 template <bool FX>
-__global__ void __launch_bounds__(kLabelInitThreads, 4)
+__global__ void __launch_bounds__(kLabelInitThreads, 3)
     label_init_local_kernel(const LabelConst c, const typename FvTypes<FX>::B* __restrict__ b,
                             const typename FvTypes<FX>::B* __restrict__ z,
                             const typename FvTypes<FX>::H* __restrict__ h0,
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(kLabelInitThreads, 4)
       const double gy = free_surface_diff<FX>(b, h, (size_t)ru * c.pitch + col,
                                               (size_t)rd * c.pitch + col, c.Q) / deny;
       const double mag = sqrt(gx * gx + gy * gy);
-      double layer, mob, qxv = (double)qx[gi], qyv = (double)qy[gi];
+      double layer, mob;
       if constexpr (FX) {
         const long long dq = (long long)b[gi] - (long long)z[gi];
         layer = fmin((double)(dq > 0 ? dq : 0) * c.Q, c.mob_depth);
@@ -204,10 +205,12 @@ __global__ void __launch_bounds__(kLabelInitThreads, 4)
         roots.max_exc_stop[flat] = 0;
         roots.prev_overlap[flat] = 0;
       }
-      if (c.release_latches) {
+      // a latch that is already released stays released: only set latches
+      // need the speed and export test
+      if (c.release_latches && latch[flat] != 0) {
         double speed = 0.0;
         if (mob > c.dry) {
-          const double vx = qxv / mob, vy = qyv / mob;
+          const double vx = (double)qx[gi] / mob, vy = (double)qy[gi] / mob;
           speed = sqrt(vx * vx + vy * vy);
         }
         const double w = (double)vertex_weight6(r, col, c.ny, c.nx) * (c.dx * c.dy / 6.0);
