@@ -18,8 +18,30 @@ struct ExchangeOut {
   double volume_w_fp64;        // FP64: sum depth * w
   double momentum_w[2];        // deposition: sum removed q * w
   int bad_index;
-  int pad;
+  unsigned int arrive;         // blocks done with their partials (exchange_fold)
 };
+
+// Floating-point exchange sums in a fixed order: block partials (slot-major,
+// NV x gridDim.x in part), folded by the last block into out[0..NV).  The
+// result depends only on the grid and the command order, not on which block
+// finishes first.  Every thread of a kThreads block calls it.
+template <int NV>
+__device__ __forceinline__ void exchange_fold(const double (&v)[NV], double* __restrict__ part,
+                                              unsigned int* arrive, double* out) {
+  __shared__ double fold[fold_words(NV)];
+  __shared__ int last;
+  const double* bt = block_fold<double, NV, NV>(v, fold);
+  if (threadIdx.x < NV) part[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = bt[threadIdx.x];
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(arrive, 1u) == gridDim.x - 1 ? 1 : 0;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* tot = reduce_partials<NV, NV>(part, (int)gridDim.x, fold);
+  if (threadIdx.x < NV) out[threadIdx.x] = tot[threadIdx.x];
+  if (threadIdx.x == 0) *arrive = 0u;
+}
 
 // mode 0: requested depth; mode 1: requested target surface (depth = b - target).
 template <bool FX>
@@ -27,7 +49,8 @@ __global__ void __launch_bounds__(kThreads)
     entrain_kernel(int ny, int nx, int pitch, double Q, double datum, double f,
                    typename FvTypes<FX>::B* __restrict__ b, const typename FvTypes<FX>::B* __restrict__ z,
                    typename FvTypes<FX>::H* __restrict__ h, const int32_t* __restrict__ idx,
-                   const double* __restrict__ value, int count, int mode, ExchangeOut* out) {
+                   const double* __restrict__ value, int count, int mode, ExchangeOut* out,
+                   double* __restrict__ part) {
   long long vq = 0;
   double vs = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
@@ -62,11 +85,13 @@ __global__ void __launch_bounds__(kThreads)
       vs += d * ((double)w6 * f);
     }
   }
-  vq = (long long)warp_sum_u64((unsigned long long)vq);
-  vs = warp_sum(vs);
-  if ((threadIdx.x & 31) == 0) {
-    if (vq) atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
-    if (vs != 0.0) atomicAdd(&out->volume_w_fp64, vs);
+  if constexpr (FX) {
+    vq = (long long)warp_sum_u64((unsigned long long)vq);
+    if ((threadIdx.x & 31) == 0 && vq)
+      atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
+  } else {
+    const double v[1] = {vs};
+    exchange_fold<1>(v, part, &out->arrive, &out->volume_w_fp64);
   }
 }
 
@@ -76,7 +101,7 @@ __global__ void __launch_bounds__(kThreads)
                    typename FvTypes<FX>::B* __restrict__ b, typename FvTypes<FX>::H* __restrict__ h,
                    typename FvTypes<FX>::R* __restrict__ qx, typename FvTypes<FX>::R* __restrict__ qy,
                    const int32_t* __restrict__ idx, const double* __restrict__ depth, int count,
-                   ExchangeOut* out) {
+                   ExchangeOut* out, double* __restrict__ part) {
   long long vq = 0;
   double vs = 0.0, mx = 0.0, my = 0.0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
@@ -115,15 +140,16 @@ __global__ void __launch_bounds__(kThreads)
       my += ry * w;
     }
   }
-  vq = (long long)warp_sum_u64((unsigned long long)vq);
-  vs = warp_sum(vs);
-  mx = warp_sum(mx);
-  my = warp_sum(my);
-  if ((threadIdx.x & 31) == 0) {
-    if (vq) atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
-    if (vs != 0.0) atomicAdd(&out->volume_w_fp64, vs);
-    if (mx != 0.0) atomicAdd(&out->momentum_w[0], mx);
-    if (my != 0.0) atomicAdd(&out->momentum_w[1], my);
+  if constexpr (FX) {
+    vq = (long long)warp_sum_u64((unsigned long long)vq);
+    if ((threadIdx.x & 31) == 0 && vq)
+      atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
+    const double v[2] = {mx, my};
+    exchange_fold<2>(v, part, &out->arrive, out->momentum_w);
+  } else {
+    // volume_w_fp64 and momentum_w[0..1] are consecutive
+    const double v[3] = {vs, mx, my};
+    exchange_fold<3>(v, part, &out->arrive, &out->volume_w_fp64);
   }
 }
 

@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(kThreads)
                         typename FvTypes<FX>::H* __restrict__ h1,
                         const FvControl* ctl, const int32_t* __restrict__ idx,
                         const double* __restrict__ target, const int* count_dev,
-                        ExchangeOut* out) {
+                        ExchangeOut* out, double* __restrict__ part) {
   const int count = *count_dev;
   typename FvTypes<FX>::H* h = ctl->parity ? h1 : h0;
   long long vq = 0;
@@ -112,11 +112,13 @@ __global__ void __launch_bounds__(kThreads)
       vs += d * ((double)w6 * f);
     }
   }
-  vq = (long long)warp_sum_u64((unsigned long long)vq);
-  vs = warp_sum(vs);
-  if ((threadIdx.x & 31) == 0) {
-    if (vq) atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
-    if (vs != 0.0) atomicAdd(&out->volume_w_fp64, vs);
+  if constexpr (FX) {
+    vq = (long long)warp_sum_u64((unsigned long long)vq);
+    if ((threadIdx.x & 31) == 0 && vq)
+      atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
+  } else {
+    const double v[1] = {vs};
+    exchange_fold<1>(v, part, &out->arrive, &out->volume_w_fp64);
   }
 }
 

@@ -17,6 +17,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -169,6 +170,7 @@ struct sb_ctx {
   double* xval = nullptr;
   ExchangeOut* xout = nullptr;
   ExchangeOut* xout_host = nullptr;
+  double* xpart = nullptr;  // exchange kernels' block partials (3 x grid_for max)
   // deposition: tool-forcing mask (int32, flat), per-cell settled volume
   // record (double m^3, flat), device/host result records
   int32_t* forcing = nullptr;
@@ -734,6 +736,9 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMalloc(&ctx->xidx, n * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->xval, n * 8));
   SB_CUDA(ctx, cudaMalloc(&ctx->xout, sizeof(ExchangeOut)));
+  static_assert(offsetof(ExchangeOut, momentum_w) == offsetof(ExchangeOut, volume_w_fp64) + 8,
+                "exchange_fold writes volume and momentum sums as one array");
+  SB_CUDA(ctx, cudaMalloc(&ctx->xpart, 3 * 148 * 8 * sizeof(double)));
   SB_CUDA(ctx, cudaMallocHost(&ctx->xout_host, sizeof(ExchangeOut)));
   SB_CUDA(ctx, cudaMalloc(&ctx->pstate, sizeof(PathState)));
   SB_CUDA(ctx, cudaMemsetAsync(ctx->pstate, 0, sizeof(PathState), ctx->stream));
@@ -809,7 +814,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
                   ctx->roots.area6, ctx->roots.volume, ctx->roots.exc_start, ctx->roots.exc_stop,
                   ctx->roots.max_exc_start, ctx->roots.max_exc_stop, ctx->roots.prev_overlap,
                   ctx->root_list, ctx->lout, ctx->b_alt, ctx->ftile_next, ctx->phase[0],
-                  ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout, ctx->pstate,
+                  ctx->phase[1], ctx->rctl, ctx->xidx, ctx->xval, ctx->xout, ctx->xpart, ctx->pstate,
                   ctx->path_count, ctx->forcing, ctx->m2r, ctx->dep_out, ctx->owned_surface,
                   ctx->act_count, ctx->act_first, ctx->act_last, ctx->r2m, ctx->initial_b,
                   ctx->ptiles, ctx->mob_out, ctx->pers_out, ctx->surf_before, ctx->dtiles,
@@ -1641,11 +1646,13 @@ static int entrain_common(sb_ctx* ctx, const int32_t* idx, const double* val, in
   if (fx(ctx))
     entrain_kernel<true><<<grid_for(count), kThreads, 0, ctx->stream>>>(
         ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, f, (int32_t*)ctx->b,
-        (const int32_t*)ctx->z, (int32_t*)ctx->h[P], ctx->xidx, ctx->xval, count, mode, ctx->xout);
+        (const int32_t*)ctx->z, (int32_t*)ctx->h[P], ctx->xidx, ctx->xval, count, mode, ctx->xout,
+        ctx->xpart);
   else
     entrain_kernel<false><<<grid_for(count), kThreads, 0, ctx->stream>>>(
         ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, ctx->d.datum_m, f, (double*)ctx->b,
-        (const double*)ctx->z, (double*)ctx->h[P], ctx->xidx, ctx->xval, count, mode, ctx->xout);
+        (const double*)ctx->z, (double*)ctx->h[P], ctx->xidx, ctx->xval, count, mode, ctx->xout,
+        ctx->xpart);
   ctx->launches++;
   if ((rc = exchange_finish(ctx))) return rc;
   if (volume_m3)
@@ -1677,11 +1684,13 @@ extern "C" int sb_deposit(sb_ctx* ctx, const int32_t* flat_indices, const double
   if (fx(ctx))
     deposit_kernel<true><<<grid_for(count), kThreads, 0, ctx->stream>>>(
         ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, f, (int32_t*)ctx->b, (int32_t*)ctx->h[P],
-        (float*)ctx->qx[P], (float*)ctx->qy[P], ctx->xidx, ctx->xval, count, ctx->xout);
+        (float*)ctx->qx[P], (float*)ctx->qy[P], ctx->xidx, ctx->xval, count, ctx->xout,
+        ctx->xpart);
   else
     deposit_kernel<false><<<grid_for(count), kThreads, 0, ctx->stream>>>(
         ctx->d.ny, ctx->d.nx, ctx->pitch, ctx->quantum, f, (double*)ctx->b, (double*)ctx->h[P],
-        (double*)ctx->qx[P], (double*)ctx->qy[P], ctx->xidx, ctx->xval, count, ctx->xout);
+        (double*)ctx->qx[P], (double*)ctx->qy[P], ctx->xidx, ctx->xval, count, ctx->xout,
+        ctx->xpart);
   ctx->launches++;
   if ((rc = exchange_finish(ctx))) return rc;
   const ExchangeOut& o = *ctx->xout_host;
@@ -2003,7 +2012,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     SB_CUDA(ctx, cudaHostGetDevicePointer(&idx_dev, ctx->path_idx, 0));
     SB_CUDA(ctx, cudaHostGetDevicePointer(&val_dev, ctx->path_val, 0));
     void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
-                    &ctx->ctl, &idx_dev, &val_dev, &ctx->path_count, &ctx->xout};
+                    &ctx->ctl, &idx_dev, &val_dev, &ctx->path_count, &ctx->xout, &ctx->xpart};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_entrain_kernel<FX>, dim3(64), 0, args)))
       return rc;
     prev = node;
