@@ -630,10 +630,9 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": el * 1000.0 / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": ("synthetic (seeded config-4 value-noise site + 64 bucket cuts)" if site
-                     else "synthetic (seeded config-1 value-noise pile + bucket cut)"),
-            "config": {"workload": args.workload, "grid": [n, n], "dx_m": DX,
-                       "dt_s": DT},
+            "data": "synthetic (seeded config-1 value-noise pile + bucket cut)",
+            "config": {"workload": "config1_plain_path_701", "grid": [N, N], "dx_m": DX,
+                       "dt_s": DT, "steps_simulated_before_timing": args.warmup},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
                              "sample": f"{args.steps} physics steps ({subs} substeps) after "
                                        f"{args.warmup} warm-up steps, NumPy oracle, 1 core"},

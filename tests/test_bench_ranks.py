@@ -51,3 +51,25 @@ def test_replicas_combine_max_time_and_sum_work():
             assert dev_s == pytest.approx(2e-3)
             assert wall_s == pytest.approx(3e-3)
             assert work == 21.0
+
+
+def test_reference_arm_prints_one_json_line():
+    """``bench.py --impl reference`` runs the CPU restatement of the path on
+    the default workload and prints the contract's JSON line (no GPU)."""
+    import json
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    out = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference",
+                          "--steps", "1", "--warmup", "3"], cwd=root, capture_output=True,
+                         text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference"
+    assert d["value"] > 0 and d["unit"] == "cell-substeps/s"
+    assert d["config"]["workload"] == "config1_plain_path_701"
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
