@@ -251,4 +251,23 @@ __global__ void __launch_bounds__(kThreads)
     reached[i] = 0;
 }
 
+// The standalone Mobile V2 step graph's ends: dt from the host-mapped input
+// into the device copy + loop control (one thread), and the step records to
+// mapped host memory (one block), so a step issues no copy-engine operation.
+__global__ void fv_begin_mapped_kernel(FvControl* ctl, const double* dt_mapped, double* dt_dev) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    *dt_dev = __ldcv(dt_mapped);
+    fv_begin_body(ctl, dt_dev);
+  }
+}
+
+__global__ void records_copy_kernel(const PathRecordPtrs p, int n) {
+  for (int k = 0; k < n; ++k) {
+    const unsigned* s = static_cast<const unsigned*>(p.src[k]);
+    unsigned* d = static_cast<unsigned*>(p.dst[k]);
+    for (int w = threadIdx.x; w < p.bytes[k] / 4; w += blockDim.x) d[w] = __ldcg(s + w);
+  }
+  __threadfence_system();
+}
+
 }  // namespace sb

@@ -390,8 +390,11 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
 
   cudaGraphNode_t n_begin, n_pro, n_loop, n_after, n_body;
   {
-    void* args[] = {(void*)&ctx->ctl, (void*)&ctx->dt_dev};
-    int rc = add_kernel(ctx, g, &n_begin, nullptr, 0, (void*)fv_begin_kernel, dim3(1), 0, args);
+    void* dt_mapped = nullptr;
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&dt_mapped, ctx->dt_host, 0));
+    void* args[] = {(void*)&ctx->ctl, &dt_mapped, (void*)&ctx->dt_dev};
+    int rc = add_kernel(ctx, g, &n_begin, nullptr, 0, (void*)fv_begin_mapped_kernel, dim3(1), 0,
+                        args);
     if (rc) return rc;
   }
   {
@@ -428,6 +431,24 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
     SB_CUDA(ctx, cudaGraphAddEventRecordNode(&n_ev1, g, &n_loop, 1, ctx->ev_loop[1]));
     int rc = add_kernel(ctx, g, &n_after, &n_ev1, 1, (void*)ledger_kernel<FX>,
                         dim3(ctx->ledger_blocks), 0, args.data());
+    if (rc) return rc;
+  }
+  {
+    // loop control and step ledgers straight into the pinned host copies
+    PathRecordPtrs rp{};
+    void *ctl_dst = nullptr, *io_dst = nullptr;
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&ctl_dst, ctx->ctl_host, 0));
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&io_dst, ctx->io_host, 0));
+    rp.src[0] = ctx->ctl;
+    rp.dst[0] = ctl_dst;
+    rp.bytes[0] = (int)sizeof(FvControl);
+    rp.src[1] = ctx->io;
+    rp.dst[1] = io_dst;
+    rp.bytes[1] = (int)sizeof(StepIO);
+    int nrec = 2;
+    void* args[] = {&rp, &nrec};
+    cudaGraphNode_t n_rec;
+    int rc = add_kernel(ctx, g, &n_rec, &n_after, 1, (void*)records_copy_kernel, dim3(1), 0, args);
     if (rc) return rc;
   }
   SB_CUDA(ctx, cudaGraphInstantiate(&mg.exec, g, 0));
@@ -1026,24 +1047,28 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
                  : build_mobile_graph<false>(ctx, c, static_limit);
     if (rc) return rc;
   }
+  // the previous call ended synchronised, so the mapped dt is free to rewrite
   *ctx->dt_host = dt_s;
-  SB_CUDA(ctx, cudaMemcpyAsync(ctx->dt_dev, ctx->dt_host, sizeof(double), cudaMemcpyHostToDevice,
-                               ctx->stream));
   if (ctx->use_graphs) {
+    // the graph reads dt from the mapped pinned copy and writes its records
+    // back into mapped pinned memory: no copy-engine operations per step
     SB_CUDA(ctx, cudaGraphLaunch(mg.exec, ctx->stream));
   } else {
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->dt_dev, ctx->dt_host, sizeof(double),
+                                 cudaMemcpyHostToDevice, ctx->stream));
     rc = fx(ctx) ? mobile_step_host_loop<true>(ctx, c, static_limit)
                  : mobile_step_host_loop<false>(ctx, c, static_limit);
     if (rc) return rc;
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(FvControl),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->io_host, ctx->io, sizeof(StepIO), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
   }
-  SB_CUDA(ctx, cudaMemcpyAsync(ctx->ctl_host, ctx->ctl, sizeof(FvControl), cudaMemcpyDeviceToHost,
-                               ctx->stream));
-  SB_CUDA(ctx, cudaMemcpyAsync(ctx->io_host, ctx->io, sizeof(StepIO), cudaMemcpyDeviceToHost,
-                               ctx->stream));
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const FvControl& k = *ctx->ctl_host;
-  // graph: two substep launches per loop iteration; host loop: one per substep
-  ctx->launches += 3 + (ctx->use_graphs ? (k.substeps + 1) / 2 * 2 : k.substeps);
+  // graph: begin, two ledgers, records + two substep launches per loop
+  // iteration; host loop: begin, two ledgers + one launch per substep
+  ctx->launches += ctx->use_graphs ? 4 + (k.substeps + 1) / 2 * 2 : 3 + k.substeps;
   rc = fill_mobile_stats(ctx, params, out);
   if (rc) return rc;
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
