@@ -90,7 +90,6 @@ __global__ void __launch_bounds__(kThreads)
   }
   const bool loaded = mbar_wait(&bar, 0);
   double worst = 0.0;
-  const int npairs = kRelaxBox * kRelaxBox;
   for (int d = 0; d < 4; ++d) {
     int d0, d1;
     dir_of(d, d0, d1);
@@ -111,17 +110,27 @@ __global__ void __launch_bounds__(kThreads)
         worst = fmax(worst, ex);
       }
       __syncthreads();
-      // (2) Jacobi update of the active-parity pairs inside the box
+      // (2) Jacobi update of the active-parity pairs inside the box: only the
+      // rows (d0 != 0) or columns (d0 == 0) whose global index has parity
+      // par hold an active endpoint a -- half the box, kRelaxBox/2 lines
       if (loaded) {
-        for (int k = threadIdx.x; k < npairs; k += kThreads) {
-          const int la0 = k / kRelaxBox, la1 = k % kRelaxBox;
+        constexpr int kHalf = kRelaxBox / 2;
+        const int first = d0 ? ((par - g0) & 1) : ((par - g1) & 1);
+        for (int k = threadIdx.x; k < kHalf * kRelaxBox; k += kThreads) {
+          int la0, la1;
+          if (d0) {
+            la0 = first + 2 * (k / kRelaxBox);
+            la1 = k % kRelaxBox;
+          } else {
+            la0 = k / kHalf;
+            la1 = first + 2 * (k % kHalf);
+          }
           const int lb0 = la0 + d0, lb1 = la1 + d1;
           if (lb0 >= kRelaxBox || lb1 < 0 || lb1 >= kRelaxBox) continue;
           const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
           if (a0 < 0 || a1 < 0 || a0 >= c.n0 || a1 >= c.n1) continue;
           if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
-          if ((((d0 ? a0 : a1) & 1)) != par) continue;
-          const int ia = k, ib = lb0 * kRelaxBox + lb1;
+          const int ia = la0 * kRelaxBox + la1, ib = lb0 * kRelaxBox + lb1;
           if constexpr (FX) {
             const long long df = (long long)s[ia] - (long long)s[ib];
             const double ex = (double)(df < 0 ? -df : df) - c.crit_q[d];
