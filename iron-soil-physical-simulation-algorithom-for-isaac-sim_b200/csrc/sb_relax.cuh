@@ -280,11 +280,22 @@ __global__ void __launch_bounds__(kThreads)
   int d0, d1;
   dir_of(dir, d0, d1);
   int moved = 0;
-  for (int k = threadIdx.x; k < T * T; k += kThreads) {
-    const int a0 = tr * T + k / T, a1 = tc * T + k % T;
+  // only the tile's rows (d0 != 0) or columns (d0 == 0) of parity par hold an
+  // active endpoint a: enumerate those lines alone
+  const int first = d0 ? ((par - tr * T) & 1) : ((par - tc * T) & 1);
+  const int half = (T - first + 1) / 2;
+  for (int k = threadIdx.x; k < half * T; k += kThreads) {
+    int la0, la1;
+    if (d0) {
+      la0 = first + 2 * (k / T);
+      la1 = k % T;
+    } else {
+      la0 = k / half;
+      la1 = first + 2 * (k % half);
+    }
+    const int a0 = tr * T + la0, a1 = tc * T + la1;
     const int b0 = a0 + d0, b1 = a1 + d1;
     if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
-    if (((d0 ? a0 : a1) & 1) != par) continue;
     const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
     if (!reached[ia] && !reached[ib]) continue;
     bool did = false;
