@@ -94,9 +94,14 @@ __global__ void __launch_bounds__(kThreads)
     int d0, d1;
     dir_of(d, d0, d1);
     for (int par = 0; par < 2; ++par) {
-      // (1) max excess over pairs owned by the interior, both parities, pre-update
-      for (int k = threadIdx.x; k < kRelaxTile * kRelaxTile; k += kThreads) {
-        const int la0 = kRelaxHalo + k / kRelaxTile, la1 = kRelaxHalo + k % kRelaxTile;
+      // (1) max excess, before this sub-phase's update, over the pairs owned by
+      // the interior whose endpoint a has the inactive parity (those of the
+      // active parity are taken in (2) as they are read, before their update)
+      constexpr int kHalfTile = kRelaxTile / 2;
+      const int ifirst = d0 ? ((1 - par - g0) & 1) : ((1 - par - g1) & 1);
+      for (int k = threadIdx.x; k < kHalfTile * kRelaxTile; k += kThreads) {
+        const int la0 = kRelaxHalo + (d0 ? ifirst + 2 * (k / kRelaxTile) : k / kHalfTile);
+        const int la1 = kRelaxHalo + (d0 ? k % kRelaxTile : ifirst + 2 * (k % kHalfTile));
         const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
         if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
         const int ia = la0 * kRelaxBox + la1, ib = (la0 + d0) * kRelaxBox + la1 + d1;
@@ -131,9 +136,12 @@ __global__ void __launch_bounds__(kThreads)
           if (a0 < 0 || a1 < 0 || a0 >= c.n0 || a1 >= c.n1) continue;
           if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
           const int ia = la0 * kRelaxBox + la1, ib = lb0 * kRelaxBox + lb1;
+          const bool owned = la0 >= kRelaxHalo && la0 < kRelaxHalo + kRelaxTile &&
+                             la1 >= kRelaxHalo && la1 < kRelaxHalo + kRelaxTile;
           if constexpr (FX) {
             const long long df = (long long)s[ia] - (long long)s[ib];
             const double ex = (double)(df < 0 ? -df : df) - c.crit_q[d];
+            if (owned) worst = fmax(worst, ex);
             if (ex > 0.0) {
               const long long t = (long long)ceil(ex * 0.5);
               const long long st = df < 0 ? -t : t;
@@ -143,6 +151,7 @@ __global__ void __launch_bounds__(kThreads)
           } else {
             const double diff = s[ia] - s[ib];
             const double ex = fmax(fabs(diff) - c.crit[d], 0.0);
+            if (owned) worst = fmax(worst, ex);
             const double sg = diff > 0.0 ? 1.0 : (diff < 0.0 ? -1.0 : 0.0);
             const double t = 0.5 * ex * sg;
             s[ia] = s[ia] - t;
