@@ -321,8 +321,8 @@ int sb_path_reset(sb_ctx* ctx);
  * No counterpart in the reference.  For callers that must not allocate device
  * memory once running -- e.g. a simulator plugin whose frame callbacks forbid
  * cudaMalloc (it can block, synchronise the device and break real-time step
- * budgets), or code issuing work into a CUDA stream capture it does not own,
- * where allocation calls are not permitted.  The caller passes device
+ * budgets), or a host that hands the plugin a fixed device-memory budget at
+ * start-up and owns every allocation after that.  The caller passes device
  * pointers for the int32 mask (nonzero = member) and the int32 output labels
  * (canonical: -1 outside the mask, else the component's minimum flat index),
  * both ny*nx row-major, plus the stream to run on.  Scratch (per-root counters
@@ -330,7 +330,9 @@ int sb_path_reset(sb_ctx* ctx);
  * GPU that loads the library until process exit; it is never allocated by
  * this call.  Limit: ny*nx <= 524288 cells (SB_ERR_CAPACITY beyond).  The
  * first call on a device looks up the scratch address with the device
- * current, so make that first call before any stream capture.  Every call
+ * current and keeps it for the process (after cudaDeviceReset the module is
+ * reloaded at a new address, so do not call this across a device reset);
+ * make that first call before any stream capture.  Every call
  * shares the one scratch array (its contents persist; each call clears what
  * must start at zero), so calls that overlap on the GPU race: serialise them
  * (one stream, or wait between calls).  Blocks until the stats are read.

@@ -361,8 +361,8 @@ def label_mask_preallocated(mask_ptr: int, labels_ptr: int, shape, connectivity:
     """Connected components with no device allocation by this library.
 
     For callers that cannot allocate device memory while they run (a plugin
-    frame callback with a fixed memory budget, or work recorded into a CUDA
-    stream capture owned by someone else).  ``mask_ptr`` / ``labels_ptr`` are
+    frame callback with a fixed memory budget handed over at start-up, where
+    cudaMalloc may block or synchronise the device).  ``mask_ptr`` / ``labels_ptr`` are
     device addresses of int32 row-major ``shape`` arrays (e.g. from
     ``tensor.data_ptr()``); the scratch is a fixed static device array, so
     ``shape`` may hold at most 524288 cells and concurrent calls must not

@@ -17,14 +17,22 @@ CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 LIB_NAME = "libsoilb200.so"
 
-# -fmad=false: every float/double operation is a separately rounded IEEE op,
-# which the parity instantiation and the fixed-point CPU mirror rely on.
-NVCC_FLAGS = [
+# soilb200.cu: -fmad=false -- every float/double operation is a separately
+# rounded IEEE op, which the FP64 parity instantiations and the fixed-point CPU
+# mirror rely on.  sb_fv_fast.cu (the production FX32 substep kernel) is
+# compiled with FMA contraction.  Each translation unit becomes an object file
+# under _build/, then both are linked into the shared library.
+COMMON_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
-    "-lineinfo", "-O3", "-std=c++17", "-fmad=false",
+    "-lineinfo", "-O3", "-std=c++17",
     "--expt-relaxed-constexpr",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
 ]
+UNITS = {
+    "soilb200.cu": ["-fmad=false"],
+    "sb_fv_fast.cu": ["-fmad=true"],
+}
+NVCC_FLAGS = COMMON_FLAGS  # kept for callers that print the flags
 
 
 def nvcc_path() -> str:
@@ -35,20 +43,32 @@ def nvcc_path() -> str:
 
 
 def sources() -> list[Path]:
-    return [CSRC / "soilb200.cu"]
+    return [CSRC / name for name in UNITS]
 
 
 def build_library(verbose: bool = False, extra_flags: list[str] | None = None) -> Path:
     out = HERE / LIB_NAME
     deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    deps.append(Path(__file__))
     if out.exists() and all(out.stat().st_mtime >= d.stat().st_mtime for d in deps):
         return out
+    objdir = HERE.parent / "_build"
+    objdir.mkdir(exist_ok=True)
+    nvcc = nvcc_path()
+    env = dict(os.environ)
+    objs = []
+    for name, flags in UNITS.items():
+        obj = objdir / (Path(name).stem + ".o")
+        cmd = [nvcc, *COMMON_FLAGS, *flags, *(extra_flags or []), f"-I{INCLUDE}", "-c",
+               str(CSRC / name), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True, env=env)
+        objs.append(str(obj))
     tmp = out.with_suffix(".so.tmp")
-    cmd = [nvcc_path(), *NVCC_FLAGS, *(extra_flags or []), f"-I{INCLUDE}",
-           *[str(s) for s in sources()], "-o", str(tmp)]
+    cmd = [nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", *objs, "-o", str(tmp)]
     if verbose:
         print(" ".join(cmd))
-    env = dict(os.environ)
     subprocess.run(cmd, check=True, env=env)
     os.replace(tmp, out)
     return out

@@ -18,39 +18,10 @@
 // are identical to stepping it alone.
 #pragma once
 
+#include "sb_batch_fv.cuh"
 #include "sb_ledger.cuh"
 
 namespace sb {
-
-constexpr int kBandRows = 32;  // ledger band height (one CTA per band)
-
-struct BatchPatch {
-  FvConst c;          // geometry (ny, nx, pitch, strips in tiles_x, rows_per_warp) + constants
-  long long base;     // element offset of the patch's row 0 in the field arenas
-  double datum;       // support datum of the patch's b / z quanta
-  double static_limit;
-  int first_item, n_items;  // FV warps
-  int first_band, n_bands;  // ledger CTAs
-};
-
-struct BatchCtl {  // per patch, device resident
-  FvControl k;
-  LedgerOut before;
-  LedgerOut after;
-};
-
-struct BatchGlobal {
-  unsigned arrive;
-  int active;
-};
-
-struct BatchArena {
-  const int32_t* b;
-  const int32_t* z;
-  int32_t* h[2];
-  float* qx[2];
-  float* qy[2];
-};
 
 __global__ void batch_begin_kernel(int npatch, BatchCtl* ctl, const double* dt) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -151,39 +122,6 @@ __global__ void __launch_bounds__(kThreads)
     g->active = 0;
     __threadfence();
     if (use_handle) cudaGraphSetConditional(handle, active > 0 ? 1u : 0u);
-  }
-}
-
-// One substep of every active patch; a warp per work item.
-__global__ void __launch_bounds__(kThreads, 3)
-    batch_fv_kernel(const BatchPatch* __restrict__ patches, const int* __restrict__ item_patch,
-                    int nitems, BatchArena a, const BatchCtl* __restrict__ ctl,
-                    double* __restrict__ item_partials) {
-  const int gw = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
-  if (gw >= nitems) return;  // warp-uniform
-  const int p = item_patch[gw];
-  if (ctl[p].k.done) return;
-  const BatchPatch& P = patches[p];
-  const FvConst& c = P.c;  // read through the read-only cache, not copied
-  const long long base = P.base;
-  const double sub_dt = ctl[p].k.sub_dt;
-  const int parity = ctl[p].k.parity;
-  const int local = gw - P.first_item;
-  double acc[kFvDiag];
-#pragma unroll
-  for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
-  double wave = 0.0;
-  fx_strip_run(c, a.b + base, a.h[parity] + base, a.qx[parity] + base, a.qy[parity] + base,
-               a.h[parity ^ 1] + base, a.qx[parity ^ 1] + base, a.qy[parity ^ 1] + base, nullptr,
-               nullptr, local % c.tiles_x, (local / c.tiles_x) * c.rows_per_warp,
-               min((local / c.tiles_x + 1) * c.rows_per_warp, c.ny), sub_dt, acc, wave);
-#pragma unroll
-  for (int k = 0; k < kFvDiag; ++k) acc[k] = warp_sum(acc[k]);
-  wave = warp_max(wave);
-  if ((threadIdx.x & 31) == 0) {
-    double* out = item_partials + (size_t)gw * (kFvDiag + 1);
-    for (int k = 0; k < kFvDiag; ++k) out[k] = acc[k];
-    out[kFvDiag] = wave;
   }
 }
 

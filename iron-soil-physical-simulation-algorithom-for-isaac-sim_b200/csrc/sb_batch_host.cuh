@@ -208,7 +208,12 @@ int batch_build_graph(sb_batch* bt) {
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     void* fargs[] = {&bt->d_patches, &bt->d_item_patch, &nitems, &a, &bt->d_ctl,
                      &bt->d_item_partials};
-    if ((rc = badd_kernel(bt, body, &nb1, nullptr, 0, (void*)batch_fv_kernel, gi, fargs))) return rc;
+    // production: the FMA-contracted fast kernel; SOILB200_FV_EXACT=1 selects
+    // the CPU mirror's IEEE arithmetic (as for the single-grid kernel)
+    const char* exact_env = std::getenv("SOILB200_FV_EXACT");
+    void* fv = (exact_env && exact_env[0] == '1') ? (void*)batch_fv_kernel<false>
+                                                  : const_cast<void*>(batch_fv_fast_kernel());
+    if ((rc = badd_kernel(bt, body, &nb1, nullptr, 0, fv, gi, fargs))) return rc;
     void* rargs[] = {&npatch, &bt->d_patches, &bt->d_ctl, &bt->d_item_partials, &bt->d_g,
                      &handle, &use1};
     if ((rc = badd_kernel(bt, body, &nb2, &nb1, 1, (void*)batch_round_kernel, gw, rargs))) return rc;

@@ -66,6 +66,26 @@ struct FvControl {
   unsigned long long pmax[4];    // "before" ledger maxima for the prologue: external, |q|, grad, wave
 };
 
+// Ledger record layout (filled by the ledger kernels of sb_ledger.cuh).
+enum LedgerSlot {
+  L_HSUM = 0, L_HSUM_W, L_QX, L_QY, L_QX_W, L_QY_W, L_HS2, L_HS2_W, L_HB, L_HB_W, L_HH, L_HH_W,
+  L_REST_W,  // FP64: sum max(b - z, 0) * w6
+  L_NSUM,
+  L_MAXSPEED = L_NSUM, L_NEGMINH, L_MAXQ, L_MAXGRAD, L_MAXWAVE, L_MAXEXT,
+  L_NP
+};
+constexpr int kLedgerI64 = 3;  // h quanta, h quanta * w6, max(b - z, 0) quanta * w6
+
+struct LedgerOut {
+  double v[L_NP];
+  long long iq[kLedgerI64];
+};
+
+struct StepIO {  // per-step device record: ledgers before/after + loop control
+  LedgerOut before;
+  LedgerOut after;
+};
+
 template <bool FX>
 struct FvTypes;
 template <>
@@ -111,6 +131,47 @@ struct FvSmem {
 };
 
 // --------------------------------------------------------------------------
+// Float arithmetic of the FX32 kernels.  FAST = false: IEEE round-to-nearest
+// reciprocal, square root and division (the CPU mirror's arithmetic, bit for
+// bit, in a translation unit compiled without FMA contraction).  FAST = true
+// (production): the PTX approximate instructions rcp.approx.ftz.f32 and
+// sqrt.approx.ftz.f32 (relative error ~2^-23) in a translation unit compiled
+// with FMA contraction.  Mass stays exact either way: every face mass flux is
+// rounded to whole quanta and applied with opposite signs to its two cells.
+// --------------------------------------------------------------------------
+template <bool FAST>
+__device__ __forceinline__ float fx_rcp(float x) {
+  if constexpr (FAST) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  } else {
+    return __frcp_rn(x);
+  }
+}
+
+template <bool FAST>
+__device__ __forceinline__ float fx_sqrt(float x) {
+  if constexpr (FAST) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+  } else {
+    return sqrtf(x);
+  }
+}
+
+// Coulomb friction factor max(0, 1 - dec / max(spd, 1e-15)).
+template <bool FAST>
+__device__ __forceinline__ float fx_friction(float dec, float spd) {
+  if constexpr (FAST) {
+    return fmaxf(0.f, 1.f - dec * fx_rcp<true>(fmaxf(spd, 1.0e-15f)));
+  } else {
+    return fmaxf(0.f, 1.f - dec / fmaxf(spd, 1.0e-15f));
+  }
+}
+
+// --------------------------------------------------------------------------
 // Face fluxes.  (L, R) = (west, east) or (south, north) cell; n/t = normal and
 // tangential momentum components.  Outputs: mass flux (quanta or raw),
 // normal-momentum flux seen by L (minus) and by R (plus), tangential flux.
@@ -122,8 +183,9 @@ struct FvSmem {
 // reproduce h and the prepared celerity exactly), so the face has no branch
 // other than the early return for a face between two empty cells (all of a
 // terrain away from the mobile layer), whose fluxes are all zero.
-// Reconstructed discharge is u * hs (= q * hs / h of the reference).  The
-// reciprocals are IEEE round-to-nearest (__frcp_rn == 1.0f / x).
+// Reconstructed discharge is u * hs (= q * hs / h of the reference).  Roots
+// and reciprocals go through fx_sqrt / fx_rcp (IEEE when FAST is false).
+template <bool FAST = false>
 __device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int br, int hlq,
                                         int hrq, float unl, float utl, float unr, float utr,
                                         float cl, float cr, int& m, float& fnm, float& fnp,
@@ -144,7 +206,7 @@ __device__ __forceinline__ void face_fx(const FvConst& c, float lam, int bl, int
   const bool llow = dl != 0;
   const float hlow = llow ? hl : hr;
   const float hs_low = fmaxf(hlow - (float)(dl + dr) * c.QKf, 0.f);
-  const float cs_low = sqrtf(c.KGf * hs_low);
+  const float cs_low = fx_sqrt<FAST>(c.KGf * hs_low);
   const float cor_low = (c.HKGf * hlow) * hlow - (c.HKGf * hs_low) * hs_low;
   const float hsl = llow ? hs_low : hl, csl = llow ? cs_low : cl, corl = llow ? cor_low : 0.f;
   const float hsr = llow ? hr : hs_low, csr = llow ? cr : cs_low, corr = llow ? 0.f : cor_low;
@@ -567,6 +629,7 @@ __global__ void __launch_bounds__(kThreads)
 // so both produce identical fields.
 // --------------------------------------------------------------------------
 constexpr int kStripOut = 30;
+constexpr int kMinChunkRows = 3;  // shortest row chunk of one strip warp
 
 struct FxCell {
   int b, h;
@@ -593,13 +656,14 @@ __device__ __forceinline__ void fx_load(const FvConst& c, const int32_t* __restr
 }
 
 // Per-cell velocity q/h (0 for an empty cell) and celerity sqrt(K g h).
+template <bool FAST>
 __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
   if (x.h > 0) {
     const float hf = (float)x.h * c.Qf;
-    const float inv = __frcp_rn(hf);
+    const float inv = fx_rcp<FAST>(hf);
     x.u = x.qx * inv;
     x.v = x.qy * inv;
-    x.cel = sqrtf(c.KGf * hf);
+    x.cel = fx_sqrt<FAST>(c.KGf * hf);
   } else {  // empty cell (the same values: q * 0 and sqrt(0)); no reciprocal or root
     x.u = x.qx * 0.f;
     x.v = x.qy * 0.f;
@@ -611,6 +675,7 @@ __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
 // of a grid whose row 0 starts at the given field pointers (row pitch
 // c.pitch).  Accumulates the impulse/energy sums into acc and the largest
 // next-substep wave speed into wave.  Every lane of the warp must call it.
+template <bool FAST = false>
 __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __restrict__ bsrc,
                                              const int32_t* __restrict__ hsrc,
                                              const float* __restrict__ qxsrc,
@@ -641,15 +706,15 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
   {
     FxCell prv;
     fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 - 1, gx, colok, prv);
-    fx_prepare(c, prv);
-    fx_prepare(c, cur);
+    fx_prepare<FAST>(c, prv);
+    fx_prepare<FAST>(c, cur);
     if (y0 > 0 && colok) {
       float fnm;
-      face_fx(c, lamy_f, prv.b, cur.b, prv.h, cur.h, prv.v, prv.u, cur.v, cur.u, prv.cel,
+      face_fx<FAST>(c, lamy_f, prv.b, cur.b, prv.h, cur.h, prv.v, prv.u, cur.v, cur.u, prv.cel,
               cur.cel, ms, fnm, nnps, nts);
     }
   }
-  fx_prepare(c, nxt);
+  fx_prepare<FAST>(c, nxt);
 #pragma unroll 2
   for (int r = y0; r < y1; ++r) {
     fx_load(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
@@ -662,7 +727,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
     int me = 0;
     float enm = 0.f, enp = 0.f, et = 0.f;
     if (east_ok)
-      face_fx(c, lamx_f, cur.b, eb, cur.h, eh, cur.u, cur.v, eu, ev, cur.cel, ec, me, enm, enp,
+      face_fx<FAST>(c, lamx_f, cur.b, eb, cur.h, eh, cur.u, cur.v, eu, ev, cur.cel, ec, me, enm, enp,
               et);
     // west face = the previous lane's east face
     const int mw = __shfl_up_sync(0xffffffffu, me, 1);
@@ -672,7 +737,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
     int mn = 0;
     float nnm = 0.f, nnp = 0.f, nt = 0.f;
     if (colok && r + 1 < c.ny)
-      face_fx(c, lamy_f, cur.b, nxt.b, cur.h, nxt.h, cur.v, cur.u, nxt.v, nxt.u, cur.cel,
+      face_fx<FAST>(c, lamy_f, cur.b, nxt.b, cur.h, nxt.h, cur.v, cur.u, nxt.v, nxt.u, cur.cel,
               nxt.cel, mn, nnm, nnp, nt);
     if (out_lane) {
       const size_t gi = (size_t)r * c.pitch + gx;
@@ -692,7 +757,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
       const float qyn = wet ? cur.qy + dqy : 0.f;
       float vbx = 0.f, vby = 0.f, qex = qxn, qey = qyn, vex = 0.f, vey = 0.f;
       if (wet) {
-        const float inv = __frcp_rn(hn);
+        const float inv = fx_rcp<FAST>(hn);
         vbx = qxn * inv;
         vby = qyn * inv;
         if (c.has_external) {
@@ -705,8 +770,8 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
           vey = vby;
         }
       }
-      const float spd = sqrtf(vex * vex + vey * vey);
-      const float fac = fmaxf(0.f, 1.f - dec / fmaxf(spd, 1.0e-15f));
+      const float spd = fx_sqrt<FAST>(vex * vex + vey * vey);
+      const float fac = fx_friction<FAST>(dec, spd);
       const float vax = vex * fac, vay = vey * fac;
       const float qxo = hn * vax, qyo = hn * vay;
       hdst[gi] = hq;
@@ -724,7 +789,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
       fa[6] += ((0.5f * hn) * (spd * spd)) * ((1.f - fac) * (1.f + fac));
       if (c.has_external)
         fa[7] += (hn * ((0.5f * (vbx + vex)) * ax + (0.5f * (vby + vey)) * ay)) * dtf;
-      const float wv = spd * fac + sqrtf(c.KGf * hn);  // |new velocity| + celerity
+      const float wv = spd * fac + fx_sqrt<FAST>(c.KGf * hn);  // |new velocity| + celerity
       fwave = fmaxf(fwave, wv);
     }
     ms = mn;
@@ -732,13 +797,14 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
     nnps = nnp;
     cur = nxt;
     nxt = nn;
-    fx_prepare(c, nxt);
+    fx_prepare<FAST>(c, nxt);
   }
 #pragma unroll
   for (int k = 0; k < kFvDiag; ++k) acc[k] += (double)fa[k];
   wave = fmax(wave, (double)fwave);
 }
 
+template <bool FAST>
 __global__ void __launch_bounds__(kThreads, 4)
     fv_stream_kernel(const FvConst c, const int32_t* __restrict__ bsrc, int32_t* __restrict__ h0,
                      int32_t* __restrict__ h1, float* __restrict__ qx0, float* __restrict__ qx1,
@@ -759,7 +825,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   const int j = gw / c.tiles_x, nchunk = c.row_chunks;
   const int y0 = j < nchunk ? (int)((long long)j * c.ny / nchunk) : c.ny;
   const int y1 = j < nchunk ? (int)((long long)(j + 1) * c.ny / nchunk) : c.ny;
-  fx_strip_run(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
+  fx_strip_run<FAST>(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
                parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x, ext_y,
                gw % c.tiles_x, y0, y1, sub_dt, acc, wave);
   fv_finish(c, ctl, diag_acc, acc, wave, 0, &flag, sub_dt, parity, loop_handle, use_handle);

@@ -13,25 +13,6 @@
 
 namespace sb {
 
-enum LedgerSlot {
-  L_HSUM = 0, L_HSUM_W, L_QX, L_QY, L_QX_W, L_QY_W, L_HS2, L_HS2_W, L_HB, L_HB_W, L_HH, L_HH_W,
-  L_REST_W,  // FP64: sum max(b - z, 0) * w6
-  L_NSUM,
-  L_MAXSPEED = L_NSUM, L_NEGMINH, L_MAXQ, L_MAXGRAD, L_MAXWAVE, L_MAXEXT,
-  L_NP
-};
-constexpr int kLedgerI64 = 3;  // h quanta, h quanta * w6, max(b - z, 0) quanta * w6
-
-struct LedgerOut {
-  double v[L_NP];
-  long long iq[kLedgerI64];
-};
-
-struct StepIO {  // per-step device record: ledgers before/after + loop control
-  LedgerOut before;
-  LedgerOut after;
-};
-
 // Ledger contributions of cell (r, col): sums into v[0 .. L_NSUM), maxima
 // into v[L_NSUM .. L_NP), exact quanta sums into iq0..iq2 (FX).
 template <bool FX>

@@ -21,6 +21,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/soilb200.h"
@@ -38,6 +39,13 @@
 #include "sb_learned.cuh"
 
 using namespace sb;
+
+namespace sb {
+// Address of fv_stream_kernel<true>, instantiated in sb_fv_fast.cu (compiled
+// with FMA contraction); this file only ever instantiates the exact variant.
+const void* fv_stream_fast_kernel();
+const void* batch_fv_fast_kernel();  // batch_fv_kernel<true>, same translation unit
+}  // namespace sb
 
 namespace {
 
@@ -120,6 +128,7 @@ struct sb_ctx {
   // kernel (SOILB200_FV_TILE=1); strips of 30 output columns, fv_rows row
   // chunks per strip
   int fv_stream = 0;
+  int fv_exact = 0;  // 1: FX32 strip kernel with the CPU mirror's IEEE arithmetic
   int fv_rows = 0;  // FX streaming kernel: row chunks per strip
   int fv_strips = 0;
   int fv_stream_blocks = 0;
@@ -322,7 +331,8 @@ template <bool FX>
 void fv_launch(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle, int* use_handle,
                FvLaunch& L) {
   if (FX && ctx->fv_stream) {
-    L.func = (void*)fv_stream_kernel;
+    L.func = ctx->fv_exact ? (void*)fv_stream_kernel<false>
+                           : const_cast<void*>(fv_stream_fast_kernel());
     L.smem = 0;
     L.args = {(void*)&c,         (void*)&ctx->b,     (void*)&ctx->h[0],  (void*)&ctx->h[1],
               (void*)&ctx->qx[0], (void*)&ctx->qx[1], (void*)&ctx->qy[0], (void*)&ctx->qy[1],
@@ -652,13 +662,18 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   if (d.precision == SB_FX32) {
     const char* tile_env = std::getenv("SOILB200_FV_TILE");
     ctx->fv_stream = (tile_env && tile_env[0] == '1') ? 0 : 1;
+    const char* exact_env = std::getenv("SOILB200_FV_EXACT");
+    ctx->fv_exact = (exact_env && exact_env[0] == '1') ? 1 : 0;
     ctx->fv_strips = (d.nx + kStripOut - 1) / kStripOut;
-    // row chunks per strip: one wave of warps (4 CTAs of 8 warps on each of
-    // the 148 SMs), at least 3 rows per chunk; the chunks split the rows
-    // evenly (sizes differ by at most one row), so every SM gets the same work
-    const long long want_warps = 148LL * 32;
+    // row chunks per strip: at most one wave of warps (4 CTAs of 8 warps on
+    // each SM of this device) and at least kMinChunkRows rows per chunk (every
+    // chunk pays one extra row of loads, two cell preparations and one face);
+    // the chunks split the rows evenly (sizes differ by at most one row)
+    int sms = 0;
+    SB_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device));
+    const long long want_warps = (long long)std::max(sms, 1) * 32;
     long long chunks = want_warps / ctx->fv_strips;
-    chunks = std::min<long long>(chunks, d.ny / 3);
+    chunks = std::min<long long>(chunks, d.ny / kMinChunkRows);
     chunks = std::max<long long>(chunks, 1);
     if (const char* rows_env = std::getenv("SOILB200_FV_ROWS")) {
       const long long r = std::atoll(rows_env);
@@ -2363,7 +2378,10 @@ static_assert(sizeof(LabelOut) + sizeof(unsigned int) <= kStaticHeaderBytes, "he
 static __device__ __align__(256) unsigned char g_label_scratch[kStaticScratchBytes];
 
 constexpr int kMaxDevices = 64;
+// Device address of g_label_scratch per device ordinal, looked up once; the
+// mutex makes a first call from two host threads at once safe.
 unsigned char* g_label_scratch_ptr[kMaxDevices] = {nullptr};
+std::mutex g_label_scratch_mutex;
 
 // Per-cell init of the static variant: only the counters it uses are cleared.
 __global__ void __launch_bounds__(kThreads)
@@ -2444,14 +2462,18 @@ extern "C" int sb_label_mask_static(const int32_t* d_mask, int32_t* d_labels, in
   if ((long long)ny * nx > kStaticLabelMaxCells) return SB_ERR_CAPACITY;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return SB_ERR_CUDA;
-  if (!g_label_scratch_ptr[dev]) {
-    // one-time set-up on this device (the device is current): the host-side
-    // symbol is only a stand-in, the kernels need its device address
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_label_scratch) != cudaSuccess || !p) return SB_ERR_CUDA;
-    g_label_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_label_scratch_mutex);
+    if (!g_label_scratch_ptr[dev]) {
+      // one-time set-up on this device (the device is current): the host-side
+      // symbol is only a stand-in, the kernels need its device address
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_label_scratch) != cudaSuccess || !p) return SB_ERR_CUDA;
+      g_label_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    base = g_label_scratch_ptr[dev];
   }
-  unsigned char* base = g_label_scratch_ptr[dev];
   LabelOut* lout = reinterpret_cast<LabelOut*>(base);
   unsigned int* arrive = reinterpret_cast<unsigned int*>(base + sizeof(LabelOut));
   int* count = reinterpret_cast<int*>(base + kStaticCountOffset);

@@ -16,6 +16,9 @@ No public dataset is involved: every terrain is generated from
   {64, 96, 128, 192, 256, 384, 512} and aspect <= 2:1, each a config-0-style
   terrain (10 deg tilt + 8 bumps) with a mound of mobile material at a seeded
   position; every patch takes its own CFL substeps.
+* config 3 -- 128^2 training patches (seed i): the reference's fractal
+  gradient noise (``fractal_perlin_noise``) steepened to a maximum neighbour
+  slope of U[45, 60] deg, relaxed to 35 deg by the plain sweep.
 """
 
 from __future__ import annotations
@@ -165,17 +168,68 @@ def config2(n_patches: int = 512, dx: float = 0.05):
     return [config2_patch(i, dx) for i in range(n_patches)]
 
 
+def fractal_perlin_noise(nx: int, ny: int, seed=None, *, base_cells: int = 3, octaves: int = 5,
+                         persistence: float = 0.52, lacunarity: float = 2.0) -> np.ndarray:
+    """Seeded fractal gradient (Perlin) noise: the generator of the reference's
+    training patches (``slope_model.fractal_perlin_noise``, slope_model.py:77-129).
+
+    Same parameters and the same random draws (one ``(m+1, m+1)`` array of
+    gradient angles per octave from ``default_rng(seed)``, m = round(cells of
+    that octave)), so a seed gives the reference's field: per octave, unit
+    gradients on an m x m lattice over [0, 1]^2, the dot products with the
+    offsets to the four lattice corners blended by the quintic fade
+    6t^5 - 15t^4 + 10t^3, octave weights normalised, then the field scaled to
+    max |value| = 1.  Indexed [x, y] with shape (nx, ny), as the reference.
+    """
+    if nx < 2 or ny < 2:
+        raise ValueError("noise dimensions must be at least 2")
+    if base_cells < 1 or octaves < 1:
+        raise ValueError("base_cells and octaves must be positive")
+    rng = np.random.default_rng(seed)
+    px = np.linspace(0.0, 1.0, nx)
+    py = np.linspace(0.0, 1.0, ny)
+    field = np.zeros((nx, ny))
+    total = 0.0
+    amp = 1.0
+    freq = float(base_cells)
+
+    def fade(t):
+        return t * t * t * (t * (t * 6.0 - 15.0) + 10.0)
+
+    for _ in range(octaves):
+        m = max(1, int(round(freq)))
+        theta = rng.uniform(0.0, 2.0 * np.pi, (m + 1, m + 1))
+        gcos, gsin = np.cos(theta), np.sin(theta)
+        cx = np.minimum((px * m).astype(int), m - 1)
+        cy = np.minimum((py * m).astype(int), m - 1)
+        ox = px * m - cx
+        oy = py * m - cy
+        ox[-1] = 1.0
+        oy[-1] = 1.0
+        X, Y = cx[:, None], cy[None, :]
+        U, V = ox[:, None], oy[None, :]
+        corner = {}
+        for di in (0, 1):
+            for dj in (0, 1):
+                corner[di, dj] = gcos[X + di, Y + dj] * (U - di) + gsin[X + di, Y + dj] * (V - dj)
+        fu, fv = fade(U), fade(V)
+        lo = corner[0, 0] + fu * (corner[1, 0] - corner[0, 0])
+        hi = corner[0, 1] + fu * (corner[1, 1] - corner[0, 1])
+        field += amp * (lo + fv * (hi - lo))
+        total += amp
+        amp *= persistence
+        freq *= lacunarity
+    field /= max(total, 1e-12)
+    peak = float(np.abs(field).max())
+    return field / peak if peak > 0.0 else field
+
+
 def config3_patch(i: int, n: int = 128, dx: float = 0.05) -> np.ndarray:
-    """Training patch i of config 3: steepened fractal noise (non-negative heights)."""
-    rng = np.random.default_rng(i)
-    acc = np.zeros((n, n))
-    weight, amp = 0.0, 1.0
-    for o in range(5):
-        acc += amp * value_noise((n, n), 4 * 2 ** o, rng)
-        weight += amp
-        amp *= 0.5
-    h = acc / weight
-    target = np.tan(np.deg2rad(rng.uniform(45.0, 60.0)))
+    """Training patch i of config 3: the reference generator's fractal noise
+    (seed i) steepened to a seeded 45-60 deg maximum neighbour slope and
+    shifted to non-negative heights."""
+    h = fractal_perlin_noise(n, n, seed=i)
+    target = np.tan(np.deg2rad(np.random.default_rng([i, 3]).uniform(45.0, 60.0)))
     # steepest of the four neighbour directions (slope_model.max_neighbor_slope's measure)
     diag = np.hypot(dx, dx)
     s = max(np.abs(np.diff(h, axis=0)).max() / dx, np.abs(np.diff(h, axis=1)).max() / dx,

@@ -11,6 +11,9 @@ grid_spacing)`` convention, ``slope_model.py:273-343``):
   (Jacobi inside a sub-phase, Gauss-Seidel across the 8 sub-phases).  The
   iteration's max excess is taken over *all* pairs of each sub-phase before
   its update; convergence when it is <= tolerance.
+* ``reached_relax`` -- the event-driven reached-bbox backend: the same
+  sub-phase schedule gated by a growing reached mask, with a confirming scan
+  before it stops (``solvers/event_driven_slope.py:166-302``).
 * ``frontier_relax`` -- the production compact-frontier round schedule
   (``runtime/v2_physics_core.py:1172-1254`` over
   ``solvers/warp_compact_frontier.py:56-130`` and the edge ownership of
@@ -136,6 +139,70 @@ def relax_critical_slope_fixed(hq, grid_spacing, crit_tan: float, quantum: float
             converged = True
             break
     return h, it, converged
+
+
+# ---------------------------------------------------------------------------
+# Reached-gated sweep (event-driven reached-bbox backend)
+# ---------------------------------------------------------------------------
+def reached_relax(height, seeds, spacing, crit_tan: float, tolerance: float,
+                  max_iterations: int = 1_000_000):
+    """``EventDrivenMinimumSlopeAdapter._relax_dynamic_frontier``
+    (solvers/event_driven_slope.py:166-302), closed boundary, on a generic
+    [axis 0, axis 1] array (the reference's H[x, y]).
+
+    The reference crops every sub-phase to the reached-tile envelope plus one
+    cell; every edge with a reached endpoint lies inside that window, so the
+    crop only saves work and is left out here.  Per iteration and sub-phase
+    (direction, parity): excess = max(|a - b| - crit * L, 0) over all pairs;
+    the iteration maximum takes the reachable pairs (a or b reached) before
+    the sub-phase's update; pairs of the active parity that are reachable move
+    half their excess (0.5 * excess * sign(a - b)) and both endpoints of a
+    moved pair become reached.  When the iteration's maximum is <= tolerance
+    the post-iteration state is scanned once more (all reachable pairs) and
+    the solve ends if that is <= tolerance too.  Returns (h, reached,
+    iterations).
+    """
+    h = np.array(height, dtype=np.float64, copy=True)
+    reached = np.array(seeds, dtype=bool, copy=True)
+    pairs = neighbor_pairs(*spacing)
+    iterations = 0
+    while True:
+        iterations += 1
+        if iterations > max_iterations:
+            raise RuntimeError("NUMERICAL_NONCONVERGENCE: reached-bbox MiniSlope exceeded the "
+                               "numerical safety limit")
+        worst = 0.0
+        for d0, d1, dist in pairs:
+            crit = crit_tan * dist
+            for parity in (0, 1):
+                a, b = paired_views(h, d0, d1)
+                ra, rb = paired_views(reached, d0, d1)
+                diff = a - b
+                excess = np.maximum(np.abs(diff) - crit, 0.0)
+                reach = ra | rb
+                if np.any(reach):
+                    worst = max(worst, float(excess[reach].max()))
+                if d0:
+                    coord = np.arange(a.shape[0])[:, None]
+                else:
+                    coord = np.arange(a.shape[1])[None, :]
+                go = ((coord & 1) == parity) & reach & (excess > 0.0)
+                t = np.where(go, 0.5 * excess * np.sign(diff), 0.0)
+                a -= t
+                b += t
+                ra |= go
+                rb |= go
+        if worst <= tolerance:
+            remaining = 0.0
+            for d0, d1, dist in pairs:
+                a, b = paired_views(h, d0, d1)
+                ra, rb = paired_views(reached, d0, d1)
+                reach = ra | rb
+                if np.any(reach):
+                    remaining = max(remaining,
+                                    float((np.abs(a - b) - crit_tan * dist)[reach].max()))
+            if remaining <= tolerance:
+                return h, reached, iterations
 
 
 # ---------------------------------------------------------------------------

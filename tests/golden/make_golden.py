@@ -3,7 +3,7 @@
 
 Run in a container that has the reference checked out (read-only is fine)::
 
-    REFERENCE_ROOT=/root/reference python tests/golden/make_golden.py
+    REFERENCE_ROOT=<path of the reference checkout> python tests/golden/make_golden.py
 
 The fixtures (small compressed ``.npz`` files next to this script) hold the
 inputs and the reference's outputs, so the GPU tests and the oracle pins never
@@ -25,6 +25,12 @@ need the reference at run time.  Cases:
   (bulk_interaction/deposition.py:67-160) on the three scenarios of the
   reference's device-deposition tests (tests/test_device_bulk_state.py:150-230)
   and a seeded static blanket below the stop angle.
+* ``event.npz``         -- ``EventDrivenMinimumSlopeAdapter.solve`` (the
+  reached-bbox MiniSlope backend) on the reference's three acceptance
+  scenarios and two seeded events (``--event``).
+* ``fractal.npz``       -- ``slope_model.fractal_perlin_noise`` (the
+  generator of the config-3 training patches) on four seeds/parameter sets
+  (``--fractal``).
 * ``gate0.npz``         -- the 5 s config-0 gate: 256x256, seed 0, 300 steps of
   1/60 s at CFL 0.4 and mu = tan 35 deg, each followed by
   ``relax_critical_slope`` of ``b_eff`` at 35 deg (row-major array, spacing
@@ -41,7 +47,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+if not os.environ.get("REFERENCE_ROOT"):
+    raise SystemExit("set REFERENCE_ROOT to the reference project's checkout")
+REF = Path(os.environ["REFERENCE_ROOT"])
 sys.path[:0] = [str(REF / "src"), str(REF)]
 sys.dont_write_bytecode = True
 
@@ -385,7 +393,97 @@ def make_gate0(n: int = 256, steps: int = 300):
                         resting_final=np.float64(np.sum(state.b_eff_m) * cfg.dx_m * cfg.dy_m))
 
 
+def make_fractal():
+    """slope_model.fractal_perlin_noise, the reference's training-patch noise
+    (slope_model.py:77-129): default parameters at 128^2 for seeds 0 and
+    19999, a non-square field and non-default parameters."""
+    import slope_model as S
+    cases = [((128, 128, 0), {}), ((128, 128, 19999), {}), ((64, 96, 5), {}),
+             ((50, 70, 3), {"base_cells": 4, "octaves": 3, "persistence": 0.4,
+                            "lacunarity": 2.5})]
+    arrays = {"count": np.int64(len(cases))}
+    for k, (args, kw) in enumerate(cases):
+        arrays[f"{k}/args"] = np.asarray(args, np.int64)
+        arrays[f"{k}/kw"] = np.asarray([kw.get("base_cells", 3), kw.get("octaves", 5)], np.int64)
+        arrays[f"{k}/kwf"] = np.asarray([kw.get("persistence", 0.52), kw.get("lacunarity", 2.0)])
+        arrays[f"{k}/noise"] = S.fractal_perlin_noise(*args, **kw)
+    np.savez_compressed(HERE / "fractal.npz", **arrays)
+
+
+def make_event():
+    """solvers.EventDrivenMinimumSlopeAdapter (solvers/event_driven_slope.py:
+    16-302), the reached-bbox MiniSlope backend: the three scenarios of the
+    reference's tests/test_minislope_dynamic_frontier_acceptance.py (single
+    bump, toe excavation of a near-critical plane, whole-pile stress with the
+    avalanche threshold below the iteration count) plus two seeded events on
+    non-square grids (one with dx != dy), closed boundary, tile size 8."""
+    from isaac_bulk_pipeline.config import SolverConfig
+    from isaac_bulk_pipeline.solvers import EventDrivenMinimumSlopeAdapter
+    from isaac_bulk_pipeline.terrain import TerrainGrid
+
+    def config(angle=30.0, max_iterations=5000):
+        return SolverConfig(critical_angle_deg=angle, max_iterations=max_iterations,
+                            large_avalanche_iteration_threshold=max_iterations,
+                            numerical_safety_max_iterations=max(10_000, max_iterations),
+                            tolerance=1.0e-8, boundary_condition="closed",
+                            conservation_tolerance_m3=1.0e-7)
+
+    def plane(shape, dx, fraction):
+        drop = np.tan(np.deg2rad(30.0)) * dx
+        prof = 1.0 + np.arange(shape[1], dtype=np.float64) * (fraction * drop)
+        return np.repeat(prof[None, :], shape[0], axis=0)
+
+    cases = []
+    base = np.ones((96, 96))
+    dist = base.copy()
+    dist[47, 53] += 0.30
+    cases.append(("bump96", (96, 96, 0.05, 0.05), base, dist, config()))
+    base = plane((65, 65), 0.05, 0.99)
+    dist = base.copy()
+    dist[28:37, 0] -= 0.10
+    cases.append(("toe65", (65, 65, 0.05, 0.05), base, dist, config()))
+    base = plane((33, 33), 0.05, 1.0)
+    dist = base.copy()
+    dist[:, 0] -= 0.10
+    cases.append(("stress33", (33, 33, 0.05, 0.05), base, dist, config(max_iterations=100)))
+    for name, (ny, nx), (dx, dy), seed in (("seeded70x90", (70, 90), (0.05, 0.05), 4),
+                                           ("seeded41x57_aniso", (41, 57), (0.05, 0.04), 9)):
+        rng = np.random.default_rng(seed)
+        base = 0.5 + 0.2 * rng.random((ny, nx)) * 0.01
+        dist = base.copy()
+        for _ in range(3):
+            r, c = rng.integers(3, ny - 4), rng.integers(3, nx - 4)
+            dist[r - 2:r + 3, c - 2:c + 3] += rng.uniform(0.15, 0.35)
+        cases.append((name, (nx, ny, dx, dy), base, dist, config(angle=33.0)))
+    arrays = {"names": np.asarray([c[0] for c in cases])}
+    for name, (nx, ny, dx, dy), base, dist, cfg in cases:
+        grid = TerrainGrid(nx, ny, dx, dy, 0.0, 0.0, "/World/Terrain")
+        solver = EventDrivenMinimumSlopeAdapter(grid, cfg, tile_size=8)
+        solver.set_reference_height(base)
+        res = solver.solve(dist)
+        arrays[f"{name}/grid"] = np.asarray([nx, ny, dx, dy], np.float64)
+        arrays[f"{name}/angle"] = np.float64(cfg.critical_angle_deg)
+        arrays[f"{name}/threshold"] = np.int64(cfg.large_avalanche_iteration_threshold)
+        arrays[f"{name}/base"] = base
+        arrays[f"{name}/initial"] = dist
+        arrays[f"{name}/stable"] = np.asarray(res.heightmap_stable)
+        arrays[f"{name}/iterations"] = np.int64(res.iteration_count)
+        arrays[f"{name}/classification"] = np.asarray(
+            res.diagnostics["avalanche_classification"])
+        arrays[f"{name}/propagation_bbox"] = np.asarray(
+            res.diagnostics["propagation_bbox_yx"], np.int64)
+        print(name, res.iteration_count, res.diagnostics["avalanche_classification"],
+              res.diagnostics["propagation_bbox_yx"], flush=True)
+    np.savez_compressed(HERE / "event.npz", **arrays)
+
+
 if __name__ == "__main__":
+    if "--event" in sys.argv:
+        make_event()
+        sys.exit(0)
+    if "--fractal" in sys.argv:
+        make_fractal()
+        sys.exit(0)
     if "--gate0" in sys.argv:
         make_gate0()
         sys.exit(0)

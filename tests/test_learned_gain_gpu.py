@@ -1,0 +1,84 @@
+"""What the trained repose network gains over the method without it.
+
+The shipped network (``data/repose_net_c3.npz``, trained on config-3 patches
+by the library's own tensor-core kernels) proposes per-face outflows that are
+applied in flux form; plain sweeps then finish until every face slope is at
+most tan(35 deg) + eps (eps = 1e-4, i.e. a height tolerance of eps * dx).
+On post-cut config-1 surfaces that the network never saw (seeds 2 and 4: not
+used for training nor for choosing the proposal schedule), the learned method
+must
+
+* converge to the same tolerance as the plain sweep (the plain relaxation is
+  the judge of the end state),
+* keep the volume ledger exact (integer quanta, both arms),
+* need far fewer sweeps (at most half the plain sweep count), and
+* be faster in device time by at least 1.5x (median of three runs; the
+  measured held-out gain is 2.0-3.0x, the bench surface 3.1-3.2x).
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import soilb200
+from soilb200 import learned, workloads
+from soilb200.train_repose import DEFAULT_WEIGHTS
+
+pytestmark = pytest.mark.gpu
+
+DX = 0.05
+DT = 1.0 / 60.0
+EPS = 1.0e-4
+SCALES = (1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5)
+MIN_SPEEDUP = 1.5
+
+
+def _post_cut(seed: int, n: int = 701) -> np.ndarray:
+    cfg = workloads.config1(n, seed=seed, dx=DX)
+    b = cfg["b_eff"].copy()
+    for k in range(1, 721):  # the whole 12 s straight cut
+        idx, tgt = cfg["cut"].footprint(k * DT)
+        b.flat[idx] = np.minimum(b.flat[idx], tgt)
+    return b
+
+
+@pytest.mark.parametrize("seed", [2, 4])
+def test_trained_network_reaches_repose_faster_than_plain_sweeps(seed):
+    assert DEFAULT_WEIGHTS.exists(), DEFAULT_WEIGHTS
+    net = learned.ReposeNet.load(DEFAULT_WEIGHTS)
+    b = _post_cut(seed)
+    k, datum = soilb200.choose_quantization(b)
+    q = 2.0 ** k
+    tol = EPS * DX
+    grid = soilb200.DeviceGrid(b.shape, DX, DX, precision="fx32", height_exponent=k,
+                               datum_m=datum)
+    grid.upload("z_base", np.zeros_like(b))
+    lr = learned.LearnedRelaxation(grid, net, 35.0)
+    stream = torch.cuda.ExternalStream(grid.stream_handle())
+
+    def run(rounds):
+        grid.upload("b_eff", b)
+        s0 = int(np.rint((grid.download("b_eff") - datum) * q).astype(np.int64).sum())
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        st = lr.relax(tol, max_iterations=400000, rounds=rounds,
+                      plain_between=5 if rounds else 0, scales=SCALES[:rounds])
+        e1.record(stream)
+        e1.synchronize()
+        s1 = int(np.rint((grid.download("b_eff") - datum) * q).astype(np.int64).sum())
+        return e0.elapsed_time(e1), int(st.iterations), bool(st.converged), s0 == s1
+
+    run(0)  # warm-up: graphs and the network's workspace
+    run(len(SCALES))
+    plain = [run(0) for _ in range(3)]
+    learn = [run(len(SCALES)) for _ in range(3)]
+    grid.close()
+    assert all(p[2] for p in plain + learn), "every run must reach the tolerance"
+    assert all(p[3] for p in plain + learn), "volume ledger must stay exact"
+    plain_sweeps, learned_sweeps = plain[0][1], learn[0][1]
+    assert learned_sweeps * 2 <= plain_sweeps, (learned_sweeps, plain_sweeps)
+    plain_ms = float(np.median([p[0] for p in plain]))
+    learned_ms = float(np.median([p[0] for p in learn]))
+    assert plain_ms / learned_ms >= MIN_SPEEDUP, (plain_ms, learned_ms)

@@ -13,6 +13,7 @@ import pytest
 
 from oracle import fixed_point as fx
 from oracle import mobile_v2 as m
+from oracle import relax as R
 
 from conftest import GOLDEN
 
@@ -134,3 +135,20 @@ def test_deposition_oracle_matches_reference_cpu_operator():
         assert np.array_equal(b, z[f"{n}/resting_out"]), n
         assert np.array_equal(h, z[f"{n}/mobile_out"]), n
         assert vol == pytest.approx(float(z[f"{n}/volume"]), abs=1e-15), n
+
+
+def test_reached_relax_bit_identical_to_event_driven_adapter():
+    """oracle.relax.reached_relax == EventDrivenMinimumSlopeAdapter.solve
+    (golden fixture written by the reference): stable heights bit for bit and
+    equal iteration counts, seeds = cells that differ from the reference
+    height by more than the tolerance."""
+    g = np.load(GOLDEN / "event.npz")
+    for name in g["names"]:
+        nx, ny, dx, dy = g[f"{name}/grid"]
+        base, init = g[f"{name}/base"], g[f"{name}/initial"]
+        seeds = np.abs(init - base) > 1e-8
+        crit = float(np.tan(np.deg2rad(float(g[f"{name}/angle"]))))
+        h, reached, it = R.reached_relax(init.T, seeds.T, (dx, dy), crit, 1e-8)
+        assert it == int(g[f"{name}/iterations"]), name
+        assert np.array_equal(h.T, g[f"{name}/stable"]), name
+        assert reached.T[seeds].all(), name
