@@ -33,6 +33,8 @@
  *       (runtime/gpu_large_avalanche.py:541-676)
  *   sb_relax_full
  *       slope_model.relax_critical_slope (slope_model.py:273-343)
+ *   sb_relax_reached
+ *       EventDrivenMinimumSlopeAdapter.solve (solvers/event_driven_slope.py:83-302)
  *   sb_frontier_seed / sb_frontier_run
  *       EarthmovingPhysicsCore._seed_gpu_residual_frontier and
  *       _advance_gpu_residual_frontier (runtime/v2_physics_core.py:1153-1254)
@@ -241,6 +243,16 @@ int sb_relax_full(sb_ctx* ctx, const sb_relax_params* params, sb_relax_stats* ou
  * reading statistics back (at most max_iterations; for interleaving with other
  * device work, e.g. learned proposals). */
 int sb_relax_sweeps(sb_ctx* ctx, const sb_relax_params* params);
+/* Event-driven reached-bbox MiniSlope on SB_FIELD_B_EFF
+ * (EventDrivenMinimumSlopeAdapter._relax_dynamic_frontier,
+ * solvers/event_driven_slope.py:166-302): seeds = the current
+ * SB_FIELD_FRONTIER_REACHED mask; every iteration runs the eight colour
+ * sub-phases on pairs with a reached endpoint only, marks both endpoints of
+ * every moved pair reached, and the solve ends after a confirming scan of the
+ * reachable pairs shows max excess <= tolerance.  The grown reached mask is
+ * left in SB_FIELD_FRONTIER_REACHED.  iterations > max_iterations ->
+ * SB_ERR_NONCONVERGENCE (the reference's numerical safety limit). */
+int sb_relax_reached(sb_ctx* ctx, const sb_relax_params* params, sb_relax_stats* out);
 /* Frontier seeds: reached := 1 at the cells and their 3x3-stencil tiles become
  * active (_seed_gpu_residual_frontier, v2_physics_core.py:1153-1170). */
 int sb_frontier_seed_cells(sb_ctx* ctx, const int32_t* flat_indices, int count);

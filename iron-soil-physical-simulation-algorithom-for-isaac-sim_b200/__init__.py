@@ -31,8 +31,11 @@ from .avalanche import (  # noqa: F401
     largest_connected_region,
 )
 from .relax import (  # noqa: F401
+    EventDrivenMinimumSlopeAdapter,
+    EventRelaxationResult,
     FrontierRelaxation,
     FrontierStats,
+    MiniSlopeConfig,
     RelaxationStats,
     relax_critical_slope,
 )
@@ -51,4 +54,5 @@ __all__ = [
     "MaterialScenario", "FrontierRelaxation", "FrontierStats", "RelaxationStats",
     "relax_critical_slope", "label_mask", "largest_connected_region",
     "label_mask_preallocated", "B200PatchBatch", "DeviceLargeAvalancheResult",
+    "EventDrivenMinimumSlopeAdapter", "EventRelaxationResult", "MiniSlopeConfig",
 ]

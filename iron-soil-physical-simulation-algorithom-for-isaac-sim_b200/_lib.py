@@ -242,6 +242,7 @@ _PROTOTYPES = {
                                        C.POINTER(LabelStats)]),
     "sb_relax_full": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams), C.POINTER(RelaxStats)]),
     "sb_relax_sweeps": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams)]),
+    "sb_relax_reached": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams), C.POINTER(RelaxStats)]),
     "sb_frontier_seed_cells": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "sb_frontier_seed_tiles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "sb_frontier_run": (C.c_int, [C.c_void_p, C.POINTER(RelaxParams), C.POINTER(RelaxStats)]),

@@ -23,6 +23,8 @@
 //                           endpoints, final scan -> next active tiles.
 #pragma once
 
+#include <climits>
+
 #include "sb_common.cuh"
 #include "sb_fv.cuh"
 
@@ -55,7 +57,8 @@ struct RelaxControl {
   int n_active;      // frontier: active tiles at the start of the last round
   int rounds;
   int moved_edges;
-  int pad;
+  int confirm;       // reached-gated sweep: 1 while the confirming scan is pending
+  int bb[4];         // reached-gated sweep: bounding box of reached cells (min0, max0, min1, max1)
 };
 
 __device__ __forceinline__ void dir_of(int d, int& d0, int& d1) {
@@ -198,6 +201,289 @@ __global__ void __launch_bounds__(kThreads)
   }
   __threadfence();
   if (use_handle) cudaGraphSetConditional(handle, ctl->done ? 0u : 1u);
+}
+
+// ------------------------------------------------------------------------
+// Reached-gated full-domain iteration: the event-driven reached-bbox
+// MiniSlope backend (EventDrivenMinimumSlopeAdapter._relax_dynamic_frontier,
+// solvers/event_driven_slope.py:166-302).
+//
+// Same temporal blocking as relax_full_kernel (48^2 box, 8 sub-phases in
+// shared memory, 32^2 interior written back), plus the reached mask staged
+// in a second TMA box: a pair moves only if one endpoint is reached, both
+// endpoints of a moved pair become reached (the mask can spread one cell per
+// sub-phase, so the 8-cell halo stays exact), and the iteration maximum takes
+// only reachable pairs.  A box that holds no reached cell when its CTA starts
+// cannot change its interior within one iteration, so CTAs whose box misses
+// the reached bounding box (grown with atomics, never shrunk) skip the
+// iteration; both ping-pong buffers hold the same values for such tiles
+// (begin kernel), so nothing needs writing.  An iteration whose maximum is
+// <= tolerance is followed by a confirming scan of all reachable pairs on the
+// post-iteration state (no update, not counted); the solve ends when that
+// scan is <= tolerance too, otherwise the iterations continue.
+// ------------------------------------------------------------------------
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    relax_reached_kernel(const RelaxConst c, const __grid_constant__ CUtensorMap tm0,
+                         const __grid_constant__ CUtensorMap tm1,
+                         const __grid_constant__ CUtensorMap tr0,
+                         const __grid_constant__ CUtensorMap tr1,
+                         typename FvTypes<FX>::H* __restrict__ f0,
+                         typename FvTypes<FX>::H* __restrict__ f1, int* __restrict__ r0,
+                         int* __restrict__ r1, RelaxControl* ctl,
+                         cudaGraphConditionalHandle handle, int use_handle) {
+  using H = typename FvTypes<FX>::H;
+  __shared__ alignas(128) H s[kRelaxBox * kRelaxBox];
+  __shared__ alignas(128) int rs[kRelaxBox * kRelaxBox];
+  __shared__ alignas(8) uint64_t bar;
+  __shared__ double red[kThreads / 32];
+  __shared__ int bbs[4];
+  __shared__ int last;
+  if (*(volatile int*)&ctl->done) return;
+  const int parity_buf = ctl->parity;
+  const int confirm = ctl->confirm;
+  const int t1 = blockIdx.x % c.tiles1, t0 = blockIdx.x / c.tiles1;
+  const int g0 = t0 * kRelaxTile - kRelaxHalo, g1 = t1 * kRelaxTile - kRelaxHalo;
+  const volatile int* vb = ctl->bb;
+  const int bmin0 = vb[0], bmax0 = vb[1], bmin1 = vb[2], bmax1 = vb[3];
+  const bool work = bmin0 <= bmax0 && bmax0 >= g0 && bmin0 < g0 + kRelaxBox && bmax1 >= g1 &&
+                    bmin1 < g1 + kRelaxBox;  // block-uniform
+  double worst = 0.0;
+  bool loaded = true;
+  if (work) {
+    if (threadIdx.x == 0) {
+      mbar_init(&bar, 1);
+      bbs[0] = INT_MAX;
+      bbs[1] = INT_MIN;
+      bbs[2] = INT_MAX;
+      bbs[3] = INT_MIN;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(&bar, kRelaxBox * kRelaxBox * (unsigned)(sizeof(H) + sizeof(int)));
+      tma_load_2d(s, parity_buf ? &tm1 : &tm0, g1, g0, &bar);
+      tma_load_2d(rs, parity_buf ? &tr1 : &tr0, g1, g0, &bar);
+    }
+    loaded = mbar_wait(&bar, 0);
+    if (confirm) {
+      // all reachable pairs owned by the interior, every direction, no update
+      for (int d = 0; d < 4 && loaded; ++d) {
+        int d0, d1;
+        dir_of(d, d0, d1);
+        for (int k = threadIdx.x; k < kRelaxTile * kRelaxTile; k += kThreads) {
+          const int la0 = kRelaxHalo + k / kRelaxTile, la1 = kRelaxHalo + k % kRelaxTile;
+          const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
+          if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+          const int ia = la0 * kRelaxBox + la1, ib = (la0 + d0) * kRelaxBox + la1 + d1;
+          if (!(rs[ia] | rs[ib])) continue;
+          double ex;
+          if constexpr (FX) {
+            const long long df = (long long)s[ia] - (long long)s[ib];
+            ex = (double)(df < 0 ? -df : df) - c.crit_q[d];
+          } else {
+            ex = fabs(s[ia] - s[ib]) - c.crit[d];
+          }
+          worst = fmax(worst, ex);
+        }
+      }
+    } else {
+      for (int d = 0; d < 4; ++d) {
+        int d0, d1;
+        dir_of(d, d0, d1);
+        for (int par = 0; par < 2; ++par) {
+          // (1) reachable inactive-parity pairs owned by the interior, before
+          // this sub-phase's update
+          constexpr int kHalfTile = kRelaxTile / 2;
+          const int ifirst = d0 ? ((1 - par - g0) & 1) : ((1 - par - g1) & 1);
+          for (int k = threadIdx.x; k < kHalfTile * kRelaxTile; k += kThreads) {
+            const int la0 = kRelaxHalo + (d0 ? ifirst + 2 * (k / kRelaxTile) : k / kHalfTile);
+            const int la1 = kRelaxHalo + (d0 ? k % kRelaxTile : ifirst + 2 * (k % kHalfTile));
+            const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
+            if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+            const int ia = la0 * kRelaxBox + la1, ib = (la0 + d0) * kRelaxBox + la1 + d1;
+            if (!(rs[ia] | rs[ib])) continue;
+            double ex;
+            if constexpr (FX) {
+              const long long df = (long long)s[ia] - (long long)s[ib];
+              ex = (double)(df < 0 ? -df : df) - c.crit_q[d];
+            } else {
+              ex = fmax(fabs(s[ia] - s[ib]) - c.crit[d], 0.0);
+            }
+            worst = fmax(worst, ex);
+          }
+          __syncthreads();
+          // (2) gated Jacobi update of the active-parity pairs inside the box
+          if (loaded) {
+            constexpr int kHalf = kRelaxBox / 2;
+            const int first = d0 ? ((par - g0) & 1) : ((par - g1) & 1);
+            for (int k = threadIdx.x; k < kHalf * kRelaxBox; k += kThreads) {
+              int la0, la1;
+              if (d0) {
+                la0 = first + 2 * (k / kRelaxBox);
+                la1 = k % kRelaxBox;
+              } else {
+                la0 = k / kHalf;
+                la1 = first + 2 * (k % kHalf);
+              }
+              const int lb0 = la0 + d0, lb1 = la1 + d1;
+              if (lb0 >= kRelaxBox || lb1 < 0 || lb1 >= kRelaxBox) continue;
+              const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
+              if (a0 < 0 || a1 < 0 || a0 >= c.n0 || a1 >= c.n1) continue;
+              if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+              const int ia = la0 * kRelaxBox + la1, ib = lb0 * kRelaxBox + lb1;
+              if (!(rs[ia] | rs[ib])) continue;
+              const bool owned = la0 >= kRelaxHalo && la0 < kRelaxHalo + kRelaxTile &&
+                                 la1 >= kRelaxHalo && la1 < kRelaxHalo + kRelaxTile;
+              if constexpr (FX) {
+                const long long df = (long long)s[ia] - (long long)s[ib];
+                const double ex = (double)(df < 0 ? -df : df) - c.crit_q[d];
+                if (owned) worst = fmax(worst, ex);
+                if (ex > 0.0) {
+                  const long long t = (long long)ceil(ex * 0.5);
+                  const long long st = df < 0 ? -t : t;
+                  s[ia] = (H)(s[ia] - st);
+                  s[ib] = (H)(s[ib] + st);
+                  rs[ia] = 1;
+                  rs[ib] = 1;
+                }
+              } else {
+                const double diff = s[ia] - s[ib];
+                const double ex = fmax(fabs(diff) - c.crit[d], 0.0);
+                if (owned) worst = fmax(worst, ex);
+                if (ex > 0.0) {
+                  const double sg = diff > 0.0 ? 1.0 : (diff < 0.0 ? -1.0 : 0.0);
+                  const double t = 0.5 * ex * sg;
+                  s[ia] = s[ia] - t;
+                  s[ib] = s[ib] + t;
+                  rs[ia] = 1;
+                  rs[ib] = 1;
+                }
+              }
+            }
+          }
+          __syncthreads();
+        }
+      }
+      // write back the interior (heights and reached) into the other buffers,
+      // and grow the reached bounding box by the interior's reached cells
+      H* dst = parity_buf ? f0 : f1;
+      int* rdst = parity_buf ? r0 : r1;
+      int lo0 = INT_MAX, hi0 = INT_MIN, lo1 = INT_MAX, hi1 = INT_MIN;
+      for (int k = threadIdx.x; k < kRelaxTile * kRelaxTile; k += kThreads) {
+        const int la0 = kRelaxHalo + k / kRelaxTile, la1 = kRelaxHalo + k % kRelaxTile;
+        const int a0 = g0 + la0, a1 = g1 + la1;
+        if (a0 < c.n0 && a1 < c.n1 && loaded) {
+          const int li = la0 * kRelaxBox + la1;
+          dst[(size_t)a0 * c.pitch + a1] = s[li];
+          rdst[(size_t)a0 * c.pitch + a1] = rs[li];
+          if (rs[li]) {
+            lo0 = min(lo0, a0);
+            hi0 = max(hi0, a0);
+            lo1 = min(lo1, a1);
+            hi1 = max(hi1, a1);
+          }
+        }
+      }
+      if (lo0 <= hi0) {
+        atomicMin(&bbs[0], lo0);
+        atomicMax(&bbs[1], hi0);
+        atomicMin(&bbs[2], lo1);
+        atomicMax(&bbs[3], hi1);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0 && bbs[0] <= bbs[1]) {
+        atomicMin(&ctl->bb[0], bbs[0]);
+        atomicMax(&ctl->bb[1], bbs[1]);
+        atomicMin(&ctl->bb[2], bbs[2]);
+        atomicMax(&ctl->bb[3], bbs[3]);
+      }
+    }
+  }
+  worst = warp_max(worst);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = worst;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) m = fmax(m, red[w]);
+    if (!loaded) atomicExch(&ctl->status, 6);
+    atomicMax(&ctl->max_excess_bits, (unsigned long long)__double_as_longlong(m));
+    __threadfence();
+    last = atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  const double m = __longlong_as_double((long long)ctl->max_excess_bits);
+  const double tol = FX ? c.tol_q : c.tol;
+  ctl->arrive = 0;
+  ctl->max_excess_bits = 0;
+  if (ctl->status) {
+    ctl->done = 1;
+  } else if (confirm) {
+    if (m <= tol) {
+      ctl->converged = 1;
+      ctl->done = 1;
+    }
+    ctl->confirm = 0;
+  } else {
+    ctl->iterations += 1;
+    ctl->parity = parity_buf ^ 1;
+    if (m <= tol) ctl->confirm = 1;
+  }
+  // the safety cap: a next iteration beyond max_iterations is an error
+  if (!ctl->done && !ctl->confirm && ctl->iterations >= c.max_iterations) {
+    ctl->status = 4;  // SB_ERR_NONCONVERGENCE
+    ctl->done = 1;
+  }
+  __threadfence();
+  if (use_handle) cudaGraphSetConditional(handle, ctl->done ? 0u : 1u);
+}
+
+// Start of a reached-gated solve: loop control reset, both ping-pong buffers
+// made equal (heights and reached) and the reached bounding box from the seeds.
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    relax_reached_begin_kernel(const RelaxConst c, const typename FvTypes<FX>::H* __restrict__ f0,
+                               typename FvTypes<FX>::H* __restrict__ f1,
+                               const int* __restrict__ r0, int* __restrict__ r1,
+                               RelaxControl* ctl) {
+  __shared__ int bbs[4];
+  if (threadIdx.x == 0) {
+    bbs[0] = INT_MAX;
+    bbs[1] = INT_MIN;
+    bbs[2] = INT_MAX;
+    bbs[3] = INT_MIN;
+  }
+  __syncthreads();
+  int lo0 = INT_MAX, hi0 = INT_MIN, lo1 = INT_MAX, hi1 = INT_MIN;
+  const long long n = (long long)c.n0 * c.n1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int a0 = (int)(i / c.n1), a1 = (int)(i % c.n1);
+    const size_t gi = (size_t)a0 * c.pitch + a1;
+    f1[gi] = f0[gi];
+    const int r = r0[gi] != 0;
+    r1[gi] = r;
+    if (r) {
+      lo0 = min(lo0, a0);
+      hi0 = max(hi0, a0);
+      lo1 = min(lo1, a1);
+      hi1 = max(hi1, a1);
+    }
+  }
+  if (lo0 <= hi0) {
+    atomicMin(&bbs[0], lo0);
+    atomicMax(&bbs[1], hi0);
+    atomicMin(&bbs[2], lo1);
+    atomicMax(&bbs[3], hi1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && bbs[0] <= bbs[1]) {
+    atomicMin(&ctl->bb[0], bbs[0]);
+    atomicMax(&ctl->bb[1], bbs[1]);
+    atomicMin(&ctl->bb[2], bbs[2]);
+    atomicMax(&ctl->bb[3], bbs[3]);
+  }
 }
 
 // ------------------------------------------------------------------------
@@ -507,6 +793,15 @@ template <bool FX>
 __global__ void relax_copyback_kernel(const typename FvTypes<FX>::B* __restrict__ src,
                                       typename FvTypes<FX>::B* __restrict__ dst, long long count,
                                       const RelaxControl* ctl) {
+  if (!ctl->parity) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+// reached mask back into the caller-visible field after a reached-gated solve
+__global__ void reached_copyback_kernel(const int* __restrict__ src, int* __restrict__ dst,
+                                        long long count, const RelaxControl* ctl) {
   if (!ctl->parity) return;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;
        i += (long long)gridDim.x * blockDim.x)

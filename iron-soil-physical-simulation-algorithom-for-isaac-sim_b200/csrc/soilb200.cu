@@ -153,6 +153,8 @@ struct sb_ctx {
   // relaxation
   void* b_alt = nullptr;
   CUtensorMap tm_relax[2];
+  CUtensorMap tm_reached[2];  // frontier_reached and its ping-pong partner (reached-gated sweep)
+  int* reached_alt = nullptr;
   int ftiles0 = 0, ftiles1 = 0;
   int* ftile_next = nullptr;   // next-round active tiles (seeded by labels / seeds)
   int* phase[2] = {nullptr, nullptr};
@@ -160,6 +162,7 @@ struct sb_ctx {
   RelaxControl* rctl_host = nullptr;
   LoopGraph relax_full;
   LoopGraph relax_full2;  // second cached relaxation graph (e.g. short sweeps vs. to tolerance)
+  LoopGraph relax_reached;  // reached-gated (event-driven) sweep to tolerance
   int relax_lru = 0;
   LoopGraph frontier;
   // fused plain-path step
@@ -790,6 +793,14 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
       return rc;
     if ((rc = encode_2d(ctx, &ctx->tm_relax[1], ctx->b_alt, dt, ctx->esize, kRelaxBox, kRelaxBox)))
       return rc;
+    SB_CUDA(ctx, cudaMalloc(&ctx->reached_alt, (size_t)ctx->pitch * d.ny * sizeof(int32_t)));
+    SB_CUDA(ctx, cudaMemsetAsync(ctx->reached_alt, 0, (size_t)ctx->pitch * d.ny * 4, ctx->stream));
+    if ((rc = encode_2d(ctx, &ctx->tm_reached[0], ctx->reached, CU_TENSOR_MAP_DATA_TYPE_INT32, 4,
+                        kRelaxBox, kRelaxBox)))
+      return rc;
+    if ((rc = encode_2d(ctx, &ctx->tm_reached[1], ctx->reached_alt, CU_TENSOR_MAP_DATA_TYPE_INT32,
+                        4, kRelaxBox, kRelaxBox)))
+      return rc;
   }
   if (fx(ctx)) {
     using Tl = FvTile<true>;
@@ -840,6 +851,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   if (ctx->mobile.graph) cudaGraphDestroy(ctx->mobile.graph);
   ctx->relax_full.reset();
   ctx->relax_full2.reset();
+  ctx->relax_reached.reset();
   ctx->frontier.reset();
   void* ptrs[] = {ctx->b, ctx->z, ctx->h[0], ctx->h[1], ctx->qx[0], ctx->qx[1], ctx->qy[0],
                   ctx->qy[1], ctx->ext_x, ctx->ext_y, ctx->reached, ctx->staging,
@@ -854,7 +866,7 @@ int sb_ctx_destroy(sb_ctx* ctx) {
                   ctx->path_count, ctx->forcing, ctx->m2r, ctx->dep_out, ctx->owned_surface,
                   ctx->act_count, ctx->act_first, ctx->act_last, ctx->r2m, ctx->initial_b,
                   ctx->ptiles, ctx->mob_out, ctx->pers_out, ctx->surf_before, ctx->dtiles,
-                  ctx->q_rows, ctx->q_cols, ctx->q_out};
+                  ctx->q_rows, ctx->q_cols, ctx->q_out, ctx->reached_alt};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->lout_host) cudaFreeHost(ctx->lout_host);
@@ -1320,6 +1332,11 @@ static int relax_const(sb_ctx* ctx, const sb_relax_params* p, RelaxConst* c, int
 
 __global__ void relax_reset_kernel(RelaxControl* ctl) {
   if (threadIdx.x == 0) {
+    ctl->confirm = 0;
+    ctl->bb[0] = INT_MAX;
+    ctl->bb[1] = INT_MIN;
+    ctl->bb[2] = INT_MAX;
+    ctl->bb[3] = INT_MIN;
     ctl->iterations = 0;
     ctl->done = 0;
     ctl->converged = 0;
@@ -1436,6 +1453,109 @@ extern "C" int sb_relax_full(sb_ctx* ctx, const sb_relax_params* p, sb_relax_sta
   out->status = k.status;
   if (k.status == SB_ERR_WAIT_LIMIT)
     return fail(ctx, SB_ERR_WAIT_LIMIT, "[soilb200] a bounded device wait gave up (TMA tile load)");
+  return SB_OK;
+}
+
+// Reached-gated sweep graph: reset + begin (equal ping-pong buffers, seed
+// bounding box), a WHILE loop over relax_reached_kernel (iterations and
+// confirming scans), then heights and reached mask back into b_eff /
+// frontier_reached.
+template <bool FX>
+static int build_relax_reached(sb_ctx* ctx, const RelaxConst& c, LoopGraph& lg) {
+  lg.reset();
+  cudaGraph_t g;
+  SB_CUDA(ctx, cudaGraphCreate(&g, 0));
+  lg.graph = g;
+  cudaGraphConditionalHandle handle;
+  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNode_t n_reset, n_begin, n_loop, n_body;
+  int rc;
+  {
+    void* args[] = {(void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_reset, nullptr, 0, (void*)relax_reset_kernel, dim3(1), 0,
+                         args)))
+      return rc;
+  }
+  RelaxConst ck = c;
+  ck.tiles1 = (c.n1 + kRelaxTile - 1) / kRelaxTile;
+  const int tiles0 = (c.n0 + kRelaxTile - 1) / kRelaxTile;
+  {
+    void* args[] = {(void*)&ck, (void*)&ctx->b, (void*)&ctx->b_alt, (void*)&ctx->reached,
+                    (void*)&ctx->reached_alt, (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_begin, &n_reset, 1, (void*)relax_reached_begin_kernel<FX>,
+                         dim3(grid_for((long long)c.n0 * c.n1)), 0, args)))
+      return rc;
+  }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_begin, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  int use_handle = 1;
+  {
+    void* args[] = {(void*)&ck, (void*)&ctx->tm_relax[0], (void*)&ctx->tm_relax[1],
+                    (void*)&ctx->tm_reached[0], (void*)&ctx->tm_reached[1], (void*)&ctx->b,
+                    (void*)&ctx->b_alt, (void*)&ctx->reached, (void*)&ctx->reached_alt,
+                    (void*)&ctx->rctl, (void*)&handle, (void*)&use_handle};
+    if ((rc = add_kernel(ctx, body, &n_body, nullptr, 0, (void*)relax_reached_kernel<FX>,
+                         dim3(tiles0 * ck.tiles1), 0, args)))
+      return rc;
+  }
+  cudaGraphNode_t n_copy, n_rcopy, n_par;
+  long long count = (long long)ctx->pitch * ctx->d.ny;
+  {
+    void* cargs[] = {(void*)&ctx->b_alt, (void*)&ctx->b, (void*)&count, (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_copy, &n_loop, 1, (void*)relax_copyback_kernel<FX>,
+                         dim3(grid_for(count)), 0, cargs)))
+      return rc;
+  }
+  {
+    void* cargs[] = {(void*)&ctx->reached_alt, (void*)&ctx->reached, (void*)&count,
+                     (void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_rcopy, &n_copy, 1, (void*)reached_copyback_kernel,
+                         dim3(grid_for(count)), 0, cargs)))
+      return rc;
+  }
+  {
+    void* pargs[] = {(void*)&ctx->rctl};
+    if ((rc = add_kernel(ctx, g, &n_par, &n_rcopy, 1, (void*)relax_parity_clear_kernel, dim3(1),
+                         0, pargs)))
+      return rc;
+  }
+  SB_CUDA(ctx, cudaGraphInstantiate(&lg.exec, g, 0));
+  lg.key = c;
+  lg.valid = true;
+  return SB_OK;
+}
+
+extern "C" int sb_relax_reached(sb_ctx* ctx, const sb_relax_params* p, sb_relax_stats* out) {
+  if (!ctx || !p || !out) return SB_ERR_BAD_ARG;
+  RelaxConst c;
+  int rc = relax_const(ctx, p, &c, kRelaxTile);
+  if (rc) return rc;
+  LoopGraph& lg = ctx->relax_reached;
+  if (!lg.valid || std::memcmp(&lg.key, &c, sizeof(RelaxConst)) != 0) {
+    rc = fx(ctx) ? build_relax_reached<true>(ctx, c, lg) : build_relax_reached<false>(ctx, c, lg);
+    if (rc) return rc;
+  }
+  SB_CUDA(ctx, cudaGraphLaunch(lg.exec, ctx->stream));
+  SB_CUDA(ctx, cudaMemcpyAsync(ctx->rctl_host, ctx->rctl, sizeof(RelaxControl),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const RelaxControl& k = *ctx->rctl_host;
+  ctx->launches += 5 + k.iterations;
+  std::memset(out, 0, sizeof(*out));
+  out->iterations = k.iterations;
+  out->converged = k.converged;
+  out->status = k.status;
+  if (k.status == SB_ERR_WAIT_LIMIT)
+    return fail(ctx, SB_ERR_WAIT_LIMIT, "[soilb200] a bounded device wait gave up (TMA tile load)");
+  if (k.status == SB_ERR_NONCONVERGENCE)
+    return fail(ctx, SB_ERR_NONCONVERGENCE,
+                "NUMERICAL_NONCONVERGENCE: reached-bbox MiniSlope exceeded the numerical safety "
+                "limit");
   return SB_OK;
 }
 

@@ -8,6 +8,10 @@
   vs the reference's ``SparseTileFrontierMinimumSlopeAdapter``; weighted
   (Triangle-A-C) production semantics and FX32 vs the oracle schedule,
   including exact conservation of sum(w * h).
+* event-driven reached-bbox backend (``EventDrivenMinimumSlopeAdapter``,
+  FP64): bit-identical heights, equal iteration counts, classification and
+  propagation bounding box vs the reference's adapter (golden fixture), and
+  vs the oracle on a larger event.
 """
 
 import numpy as np
@@ -151,3 +155,74 @@ def test_relax_validation_messages():
         soilb200.relax_critical_slope(np.ones((4, 4)), (0.05, 0.05), 95.0)
     with pytest.raises(ValueError, match="both dimensions >= 2"):
         soilb200.relax_critical_slope(np.ones((1, 4)), (0.05, 0.05))
+
+
+class _Grid:
+    def __init__(self, nx, ny, dx, dy):
+        self.nx, self.ny, self.dx, self.dy = int(nx), int(ny), float(dx), float(dy)
+
+
+def test_event_driven_adapter_bit_identical_to_reference():
+    """soilb200.EventDrivenMinimumSlopeAdapter (sb_relax_reached) against the
+    reference's EventDrivenMinimumSlopeAdapter.solve (golden fixture): stable
+    heights bit for bit, equal iteration counts, the same classification and
+    propagation bounding box; volume unchanged."""
+    g = np.load(GOLDEN / "event.npz")
+    for name in g["names"]:
+        nx, ny, dx, dy = g[f"{name}/grid"]
+        thr = int(g[f"{name}/threshold"])
+        cfg = soilb200.MiniSlopeConfig(critical_angle_deg=float(g[f"{name}/angle"]),
+                                       tolerance=1e-8, large_avalanche_iteration_threshold=thr,
+                                       numerical_safety_max_iterations=max(10_000, thr))
+        solver = soilb200.EventDrivenMinimumSlopeAdapter(_Grid(nx, ny, dx, dy), cfg, tile_size=8)
+        solver.set_reference_height(g[f"{name}/base"])
+        res = solver.solve(g[f"{name}/initial"])
+        assert res.converged, name
+        assert res.iteration_count == int(g[f"{name}/iterations"]), name
+        assert np.array_equal(res.heightmap_stable, g[f"{name}/stable"]), name
+        d = res.diagnostics
+        assert d["avalanche_classification"] == str(g[f"{name}/classification"]), name
+        assert d["propagation_bbox_yx"] == [int(v) for v in g[f"{name}/propagation_bbox"]], name
+        assert res.volume_after_m3 == pytest.approx(res.volume_before_m3, rel=1e-12)
+        # a second solve of the stable state has nothing to do
+        again = solver.solve(res.heightmap_stable)
+        assert again.iteration_count == 0
+        assert d["avalanche_classification"] != solver.NO_EVENT
+        solver.close()
+
+
+def test_event_driven_adapter_matches_oracle_on_a_larger_event():
+    """A 300 x 260 event (many 32-cell tiles, most of them never reached, so
+    the kernel's bounding-box skip is exercised) against oracle.relax.reached_relax."""
+    rng = np.random.default_rng(21)
+    ny, nx = 300, 260
+    base = 0.4 + 0.002 * rng.random((ny, nx))
+    init = base.copy()
+    for _ in range(5):
+        r, c = rng.integers(20, ny - 20), rng.integers(20, nx - 20)
+        init[r - 3:r + 4, c - 3:c + 4] += rng.uniform(0.2, 0.5)
+    seeds = np.abs(init - base) > 1e-8
+    crit = float(np.tan(np.deg2rad(32.0)))
+    want, reached, it = R.reached_relax(init.T, seeds.T, (0.05, 0.05), crit, 1e-8)
+    cfg = soilb200.MiniSlopeConfig(critical_angle_deg=32.0, tolerance=1e-8)
+    solver = soilb200.EventDrivenMinimumSlopeAdapter(_Grid(nx, ny, 0.05, 0.05), cfg)
+    solver.set_reference_height(base)
+    res = solver.solve(init)
+    assert res.iteration_count == it
+    assert np.array_equal(res.heightmap_stable, want.T)
+    assert res.diagnostics["reached_cell_count"] == int(reached.sum())
+    solver.close()
+
+
+def test_event_driven_adapter_safety_limit_raises():
+    g = np.load(GOLDEN / "event.npz")
+    name = "toe65"
+    nx, ny, dx, dy = g[f"{name}/grid"]
+    cfg = soilb200.MiniSlopeConfig(critical_angle_deg=30.0, tolerance=1e-8,
+                                   large_avalanche_iteration_threshold=10,
+                                   numerical_safety_max_iterations=20)
+    solver = soilb200.EventDrivenMinimumSlopeAdapter(_Grid(nx, ny, dx, dy), cfg, tile_size=8)
+    solver.set_reference_height(g[f"{name}/base"])
+    with pytest.raises(soilb200.NumericalNonconvergenceError, match="NUMERICAL_NONCONVERGENCE"):
+        solver.solve(g[f"{name}/initial"])
+    solver.close()
