@@ -25,6 +25,11 @@ need the reference at run time.  Cases:
   (bulk_interaction/deposition.py:67-160) on the three scenarios of the
   reference's device-deposition tests (tests/test_device_bulk_state.py:150-230)
   and a seeded static blanket below the stop angle.
+* ``reference_checkpoint.npz`` -- an archive written by the reference's
+  ``write_device_checkpoint`` from a stub core (``--checkpoint``).
+* ``avalanche.npz``     -- ``LargeAvalancheTransitionController.observe_and_maybe_mobilize``
+  (the CPU resting->mobile activation) called repeatedly on a pile and on a
+  45 deg plane (``--avalanche``).
 * ``event.npz``         -- ``EventDrivenMinimumSlopeAdapter.solve`` (the
   reached-bbox MiniSlope backend) on the reference's three acceptance
   scenarios and two seeded events (``--event``).
@@ -477,7 +482,100 @@ def make_event():
     np.savez_compressed(HERE / "event.npz", **arrays)
 
 
+def make_avalanche():
+    """LargeAvalancheTransitionController.observe_and_maybe_mobilize
+    (bulk_interaction/large_avalanche.py:289-422), the reference's CPU
+    resting->mobile activation, called repeatedly (no transport in between)
+    on a cohesionless pile and on the 45 deg plane of the reference's
+    tests/test_large_avalanche_transition.py; z_base = 0, so its resting
+    thickness is b_eff.  Per call: transition flag, transferred volume,
+    persistence, unstable / largest counts and the fields after the call."""
+    from isaac_bulk_pipeline.bulk_interaction import (LargeAvalancheTransitionConfig,
+                                                      LargeAvalancheTransitionController)
+    from isaac_bulk_pipeline.bulk_state import MaterialScenario, TerrainVolumeIntegrator
+    from isaac_bulk_pipeline.terrain import TerrainGrid
+
+    mat = MaterialScenario(name="golden_pile", assumed_bulk_density_kg_m3=1600.0,
+                           internal_friction_angle_deg=35.0, cohesion_proxy_pa=0.0,
+                           tool_friction_coefficient=0.5, start_angle_deg=38.0,
+                           stop_angle_deg=30.0, mobile_friction_coefficient=0.55)
+    n = 64
+    ys, xs = np.indices((n, n), dtype=np.float64)
+    pile = np.maximum(0.0, 1.6 - 1.1 * np.hypot(xs - n / 2, ys - n / 2) * 0.05) \
+        + 0.02 * (1.0 + np.sin(xs / 3.0))
+    plane = np.repeat((2.0 - np.tan(np.deg2rad(45.0)) * np.arange(21) * 0.05)[None, :], 21, axis=0)
+    cases = [("pile64", pile, 12), ("plane21", plane, 10)]
+    arrays = {"names": np.asarray([c[0] for c in cases]), "dt": np.float64(1.0 / 60.0)}
+    for name, resting, calls in cases:
+        ny, nx = resting.shape
+        grid = TerrainGrid(nx, ny, 0.05, 0.05, 0.0, 0.0, "/World/Terrain")
+        integ = TerrainVolumeIntegrator.from_grid(grid)
+        ctrl = LargeAvalancheTransitionController(LargeAvalancheTransitionConfig())
+        mobile = np.zeros_like(resting)
+        momentum = np.zeros(resting.shape + (2,))
+        arrays[f"{name}/resting0"] = resting.copy()
+        rec = []
+        for k in range(calls):
+            res = ctrl.observe_and_maybe_mobilize(resting, mobile, momentum, mat, grid, integ,
+                                                  1.0 / 60.0)
+            d = res.diagnostics
+            resting = np.asarray(res.H_resting_m).copy()
+            mobile = np.asarray(res.mobile_height_m).copy()
+            momentum = np.asarray(res.mobile_momentum_m2_s).copy()
+            rec.append([float(res.transitioned), res.transferred_volume_m3, ctrl.persistence_s,
+                        float(d.unstable_cell_count), float(d.largest_connected_cell_count)])
+            arrays[f"{name}/resting_{k}"] = resting
+            arrays[f"{name}/mobile_{k}"] = mobile
+        arrays[f"{name}/record"] = np.asarray(rec)
+        print(name, [(int(r[0]), round(r[1], 6), round(r[2], 4), int(r[3]), int(r[4])) for r in rec])
+    np.savez_compressed(HERE / "avalanche.npz", **arrays)
+
+
+def make_checkpoint():
+    """An archive written by the reference's own write_device_checkpoint
+    (runtime/device_checkpoint.py:65-124).  The writer only reads named
+    attributes of the physics core, so a stub core stands in for the GPU
+    runtime: a 24 x 32 grid whose every field holds distinct seeded values,
+    large-avalanche persistence, frontier tiles and dirty tiles."""
+    from types import SimpleNamespace
+
+    from isaac_bulk_pipeline.runtime import device_checkpoint as D
+
+    ny, nx = 24, 32
+    rng = np.random.default_rng(17)
+    fields = {}
+    for name in D.FLOAT_FIELDS:
+        fields[name] = rng.random((ny, nx))
+    fields["z_base"] = 0.1 * rng.random((ny, nx))
+    fields["b_eff"] = fields["z_base"] + 0.5 + rng.random((ny, nx))
+    fields["mobile"] = np.where(rng.random((ny, nx)) < 0.3, 0.05 * rng.random((ny, nx)), 0.0)
+    for name in D.INT_FIELDS:
+        fields[name] = rng.integers(0, 2, (ny, nx)).astype(np.int32)
+    fields["avalanche_activation_count"] = rng.integers(0, 4, (ny, nx)).astype(np.int32)
+
+    runtime = SimpleNamespace(download=lambda name: fields[name].ravel().copy())
+    state = SimpleNamespace(runtime=runtime, shape=(ny, nx),
+                            authority=SimpleNamespace(value="DEVICE"),
+                            timestamp_device_s=12.25, _dirty_tile_ids={3, 1})
+    chain = SimpleNamespace(large_avalanche=SimpleNamespace(_persistence_s=0.0833,
+                                                            _has_previous=True))
+    metadata = SimpleNamespace(checkpoint_record=lambda: {"source": "golden_stub"})
+    core = SimpleNamespace(runtime_backend="GPU_RUNTIME", device_state=state, gpu_chain=chain,
+                           gpu_metadata=metadata, grid=SimpleNamespace(dx=0.05, dy=0.05),
+                           _gpu_frontier_active_tiles=np.asarray([0, 2], np.int32),
+                           _gpu_frontier_iterations=7, _static_relaxation_pending=False)
+    out = D.write_device_checkpoint(core, HERE / "reference_checkpoint.npz",
+                                    provenance={"writer": "reference write_device_checkpoint"})
+    print("checkpoint", out["terrain_hash_sha256"], out["checkpoint_hash_sha256"])
+
+
 if __name__ == "__main__":
+    if "--checkpoint" in sys.argv:
+        make_checkpoint()
+        sys.exit(0)
+    if "--avalanche" in sys.argv:
+        make_avalanche()
+        sys.exit(0)
     if "--event" in sys.argv:
         make_event()
         sys.exit(0)

@@ -101,3 +101,34 @@ def test_observe_and_maybe_mobilize_record():
     assert res.cumulative_resting_to_mobile_m3 == pytest.approx(res.transferred_volume_m3, rel=1e-9)
     assert res.current_mobile_volume_m3 == pytest.approx(res.transferred_volume_m3, rel=1e-9)
     st.close()
+
+
+@pytest.mark.parametrize("name", ["pile64", "plane21"])
+def test_observe_and_maybe_mobilize_matches_reference_cpu_controller(name):
+    """B200LargeAvalancheBridge.observe_and_maybe_mobilize (FP64) against the
+    reference's CPU LargeAvalancheTransitionController.observe_and_maybe_mobilize
+    (golden fixture written by the reference), called repeatedly with no
+    transport in between, z_base = 0: per call the transition flag, the
+    persistence time, the unstable and largest-component counts and the
+    transferred volume; after every call b_eff and mobile height bit for bit.
+    (The CPU controller also gives the new mobile material a launch velocity,
+    the device path a zero-momentum exchange as the reference's Warp kernel
+    does, so momentum is not compared.)"""
+    from conftest import GOLDEN
+    g = np.load(GOLDEN / "avalanche.npz")
+    dt = float(g["dt"])
+    b0 = g[f"{name}/resting0"]
+    st = B200BulkState(b0.shape, DX, DX, b0, precision="fp64", mobile_headroom_m=1.0)
+    mat = soilb200.MaterialScenario("golden_pile", 1600.0, 35.0, 0.0, 0.5, 38.0, 30.0, 0.55)
+    br = soilb200.B200LargeAvalancheBridge(st.grid, mat, soilb200.LargeAvalancheTransitionConfig(),
+                                           state=st)
+    for k, (transitioned, volume, persistence, unstable, largest) in enumerate(g[f"{name}/record"]):
+        res = br.observe_and_maybe_mobilize(dt)
+        assert res.transitioned == bool(transitioned), (name, k)
+        assert res.transferred_volume_m3 == pytest.approx(volume, rel=1e-12, abs=1e-15), (name, k)
+        assert res.persistence_s == pytest.approx(persistence, rel=1e-12, abs=1e-15), (name, k)
+        assert res.unstable_cell_count == int(unstable), (name, k)
+        assert res.largest_connected_cell_count == int(largest), (name, k)
+        assert np.array_equal(st.grid.download("b_eff"), g[f"{name}/resting_{k}"]), (name, k)
+        assert np.array_equal(st.grid.download("mobile"), g[f"{name}/mobile_{k}"]), (name, k)
+    st.close()

@@ -89,3 +89,37 @@ def test_restore_older_archive_defaults(tmp_path):
         finally:
             st_small.close()
     st.close()
+
+
+class _Bridge:
+    _persistence_s = 0.0
+    _has_previous = False
+
+
+def test_restore_archive_written_by_the_reference(tmp_path):
+    """An archive written by the reference's write_device_checkpoint (golden
+    fixture) restores into a B200BulkState: every modelled field bit for bit,
+    the bridge's persistence state, the device time; written back by this
+    library, the modelled fields and the terrain hash are unchanged."""
+    from conftest import GOLDEN
+    path = GOLDEN / "reference_checkpoint.npz"
+    with np.load(path) as z:
+        fields = {name: z[name].copy() for name in z.files if name != "checkpoint_record_json"}
+    st = B200BulkState(fields["b_eff"].shape, DX, DX, fields["b_eff"], precision="fp64",
+                       mobile_headroom_m=1.0)
+    br = _Bridge()
+    rec = ck.restore_device_checkpoint(st, path, bridge=br)
+    assert br._persistence_s == 0.0833 and br._has_previous
+    assert st.timestamp_device_s == rec["device_timestamp_s"]
+    for name, dev in ck._DEVICE_NAME.items():
+        if dev is None:
+            continue
+        got = st.grid.download(dev)
+        assert np.array_equal(got, fields[name].astype(got.dtype)), name
+    out = ck.write_device_checkpoint(st, tmp_path / "back.npz", provenance={}, bridge=br)
+    assert out["terrain_hash_sha256"] == rec["terrain_hash_sha256"]
+    with np.load(tmp_path / "back.npz") as z:
+        for name, dev in ck._DEVICE_NAME.items():
+            if dev is not None:
+                assert np.array_equal(z[name], fields[name]), name
+    st.close()
