@@ -177,6 +177,8 @@ __device__ __forceinline__ void path_classify_body(const PathConst& c, const Lab
   rctl->n_active = 0;
   rctl->rounds = 0;
   rctl->moved_edges = 0;
+  rctl->list_len = 0;
+  rctl->sub_len = 0;
 }
 
 // The component reduction and, in the thread that finishes it, the

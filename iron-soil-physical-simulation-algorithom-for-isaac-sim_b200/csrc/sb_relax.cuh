@@ -17,10 +17,13 @@
 //                           the convergence test on the device.
 // frontier_*_kernel      -- production compact-frontier rounds
 //                           (runtime/v2_physics_core.py:1172-1254 over
-//                           solvers/warp_compact_frontier.py:56-130): per tile
-//                           CTAs, reached-gated weighted transfers, tile
-//                           activation of the 3x3 cell stencil around moved
-//                           endpoints, final scan -> next active tiles.
+//                           solvers/warp_compact_frontier.py:56-130): the
+//                           round's active tiles compacted into a list with
+//                           warp ballots, a fixed grid striding over the list,
+//                           reached-gated weighted transfers, tile activation
+//                           of the 3x3 cell stencil around moved endpoints
+//                           (appended to the list), final scan -> next active
+//                           tiles.
 #pragma once
 
 #include <climits>
@@ -59,6 +62,8 @@ struct RelaxControl {
   int moved_edges;
   int confirm;       // reached-gated sweep: 1 while the confirming scan is pending
   int bb[4];         // reached-gated sweep: bounding box of reached cells (min0, max0, min1, max1)
+  int list_len;      // frontier: tiles in this round's compacted phase-tile list
+  int sub_len;       // frontier: list entries the current sub-phase / scan processes
 };
 
 __device__ __forceinline__ void dir_of(int d, int& d0, int& d1) {
@@ -507,32 +512,45 @@ __device__ __forceinline__ long long gcd_ll(long long a, long long b) {
   return a;
 }
 
-// Round start: next-active flags -> phase buffer 0; decides termination.
-// Body for one block of kThreads threads.
+// Round start: the pending tile flags (scan results and seeds) are compacted
+// into this round's tile list with warp ballots -- one atomicAdd per warp on a
+// shared counter, each active lane writing its tile at the warp's base plus the
+// count of active lanes below it -- and become the round's membership flags;
+// the flags are cleared for the next round.  Decides termination.  Body for
+// one block of kThreads threads (the list order is irrelevant: tiles of one
+// sub-phase never share a pair endpoint).
 __device__ __forceinline__ void frontier_begin_body(const RelaxConst& c, int* __restrict__ unstable,
-                                                    int* __restrict__ phase0,
-                                                    int* __restrict__ phase1, RelaxControl* ctl,
+                                                    int* __restrict__ member,
+                                                    int* __restrict__ list, RelaxControl* ctl,
                                                     cudaGraphConditionalHandle handle) {
-  __shared__ int cnt[kThreads / 32];
+  __shared__ int count;
   if (*(volatile int*)&ctl->done) {  // loop disabled before it started: keep the flags
     if (threadIdx.x == 0) cudaGraphSetConditional(handle, 0u);
     return;
   }
-  int n = 0;
-  for (int t = threadIdx.x; t < c.ntiles; t += blockDim.x) {
-    const int a = unstable[t];
-    phase0[t] = a;
-    phase1[t] = 0;
-    unstable[t] = 0;
-    n += a;
+  if (threadIdx.x == 0) count = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  for (int base = 0; base < c.ntiles; base += blockDim.x) {  // uniform trip count
+    const int t = base + threadIdx.x;
+    int a = 0;
+    if (t < c.ntiles) {
+      a = unstable[t] != 0;
+      member[t] = a;
+      unstable[t] = 0;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, a);
+    int off = 0;
+    if (lane == 0 && mask) off = atomicAdd(&count, __popc(mask));
+    off = __shfl_sync(0xffffffffu, off, 0);
+    if (a) list[off + __popc(mask & ((1u << lane) - 1u))] = t;
   }
-  n = warp_sum(n);
-  if ((threadIdx.x & 31) == 0) cnt[threadIdx.x >> 5] = n;
   __syncthreads();
   if (threadIdx.x == 0) {
-    int tot = 0;
-    for (int w = 0; w < kThreads / 32; ++w) tot += cnt[w];
+    const int tot = count;
     ctl->n_active = tot;
+    ctl->list_len = tot;
+    ctl->sub_len = tot;
     if (tot == 0) {
       ctl->converged = 1;
       ctl->done = 1;
@@ -548,149 +566,178 @@ __device__ __forceinline__ void frontier_begin_body(const RelaxConst& c, int* __
 }
 
 __global__ void frontier_begin_kernel(const RelaxConst c, int* __restrict__ unstable,
-                                      int* __restrict__ phase0, int* __restrict__ phase1,
+                                      int* __restrict__ member, int* __restrict__ list,
                                       RelaxControl* ctl, cudaGraphConditionalHandle handle) {
-  frontier_begin_body(c, unstable, phase0, phase1, ctl, handle);
+  frontier_begin_body(c, unstable, member, list, ctl, handle);
 }
 
+// One colour sub-phase over the round's compacted tile list: a fixed grid of
+// CTAs strides over the first ctl->sub_len entries (the tiles active when the
+// sub-phase starts), one 32 x T tile per entry.  Tiles of the 3x3 cell stencil
+// around moved endpoints join the list (membership flag taken by atomicExch,
+// so each tile is appended once per round) and are processed from the next
+// sub-phase on; the last CTA publishes the new length.
 template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     frontier_subphase_kernel(const RelaxConst c, int dir, int par,
                              typename FvTypes<FX>::H* __restrict__ hfield,
-                             int* __restrict__ reached, const int* __restrict__ phase_src,
-                             int* __restrict__ phase_dst, RelaxControl* ctl) {
+                             int* __restrict__ reached, int* __restrict__ member,
+                             int* __restrict__ list, RelaxControl* ctl) {
   using H = typename FvTypes<FX>::H;
   __shared__ int trig[9];
   __shared__ int moved_count;
-  const int t = blockIdx.x;
-  if (*(volatile int*)&ctl->done || !phase_src[t]) return;
+  __shared__ int last;
+  if (*(volatile int*)&ctl->done) return;  // uniform across the grid
+  const int len = *(volatile int*)&ctl->sub_len;
   const int T = c.ftile;
-  const int tr = t / c.tiles1, tc = t % c.tiles1;
-  if (threadIdx.x < 9) trig[threadIdx.x] = 0;
-  if (threadIdx.x == 0) {
-    moved_count = 0;
-    phase_dst[t] = 1;
-  }
-  __syncthreads();
   int d0, d1;
   dir_of(dir, d0, d1);
-  int moved = 0;
-  // only the tile's rows (d0 != 0) or columns (d0 == 0) of parity par hold an
-  // active endpoint a: enumerate those lines alone
-  const int first = d0 ? ((par - tr * T) & 1) : ((par - tc * T) & 1);
-  const int half = (T - first + 1) / 2;
-  for (int k = threadIdx.x; k < half * T; k += kThreads) {
-    int la0, la1;
-    if (d0) {
-      la0 = first + 2 * (k / T);
-      la1 = k % T;
-    } else {
-      la0 = k / half;
-      la1 = first + 2 * (k % half);
-    }
-    const int a0 = tr * T + la0, a1 = tc * T + la1;
-    const int b0 = a0 + d0, b1 = a1 + d1;
-    if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
-    const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
-    if (!reached[ia] && !reached[ib]) continue;
-    bool did = false;
-    if constexpr (FX) {
-      const long long df = (long long)hfield[ia] - (long long)hfield[ib];
-      const double ex = (double)(df < 0 ? -df : df) - c.crit_q[dir];
-      if (ex > 0.0) {
-        long long ua = 1, ub = 1;
-        if (c.weighted) {
-          const long long wa = vertex_weight6(a0, a1, c.n0, c.n1);
-          const long long wb = vertex_weight6(b0, b1, c.n0, c.n1);
-          const long long g = gcd_ll(wa, wb);
-          ua = wb / g;
-          ub = wa / g;
-        }
-        const long long kk = (long long)ceil(ex / (double)(ua + ub));
-        const long long sg = df < 0 ? -1 : 1;
-        hfield[ia] = (H)(hfield[ia] - sg * kk * ua);
-        hfield[ib] = (H)(hfield[ib] + sg * kk * ub);
-        did = true;
+  int moved_total = 0;
+  for (int e = blockIdx.x; e < len; e += gridDim.x) {
+    const int t = list[e];
+    const int tr = t / c.tiles1, tc = t % c.tiles1;
+    if (threadIdx.x < 9) trig[threadIdx.x] = 0;
+    __syncthreads();
+    int moved = 0;
+    // only the tile's rows (d0 != 0) or columns (d0 == 0) of parity par hold an
+    // active endpoint a: enumerate those lines alone
+    const int first = d0 ? ((par - tr * T) & 1) : ((par - tc * T) & 1);
+    const int half = (T - first + 1) / 2;
+    for (int k = threadIdx.x; k < half * T; k += kThreads) {
+      int la0, la1;
+      if (d0) {
+        la0 = first + 2 * (k / T);
+        la1 = k % T;
+      } else {
+        la0 = k / half;
+        la1 = first + 2 * (k % half);
       }
-    } else {
-      const double diff = hfield[ia] - hfield[ib];
-      const double ex = fabs(diff) - c.crit[dir];
-      if (ex > 0.0) {
-        const double signed_ex = diff < 0.0 ? -ex : ex;
-        double wa = 1.0, wb = 1.0;
-        if (c.weighted) {
-          wa = vertex_weight_fp64(a0, a1, c.n0, c.n1, c.f);
-          wb = vertex_weight_fp64(b0, b1, c.n0, c.n1, c.f);
-        }
-        const double ws = wa + wb;
-        const double ta = signed_ex * wb / ws, tb = signed_ex * wa / ws;
-        hfield[ia] = hfield[ia] - ta;
-        hfield[ib] = hfield[ib] + tb;
-        did = true;
-      }
-    }
-    if (did) {
-      reached[ia] = 1;
-      reached[ib] = 1;
-      ++moved;
-      // tiles of the 3x3 cell stencil around both endpoints (within the 3x3 tile block)
-      const int ends[4] = {a0, a1, b0, b1};
-      for (int e = 0; e < 2; ++e) {
-        const int p0 = ends[2 * e], p1 = ends[2 * e + 1];
-        for (int o0 = -1; o0 <= 1; ++o0)
-          for (int o1 = -1; o1 <= 1; ++o1) {
-            const int q0 = p0 + o0, q1 = p1 + o1;
-            if (q0 < 0 || q1 < 0 || q0 >= c.n0 || q1 >= c.n1) continue;
-            const int rt = q0 / T - tr, ct = q1 / T - tc;  // in [-1, 1]
-            trig[(rt + 1) * 3 + ct + 1] = 1;
+      const int a0 = tr * T + la0, a1 = tc * T + la1;
+      const int b0 = a0 + d0, b1 = a1 + d1;
+      if (a0 >= c.n0 || a1 >= c.n1 || b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+      const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
+      if (!reached[ia] && !reached[ib]) continue;
+      bool did = false;
+      if constexpr (FX) {
+        const long long df = (long long)hfield[ia] - (long long)hfield[ib];
+        const double ex = (double)(df < 0 ? -df : df) - c.crit_q[dir];
+        if (ex > 0.0) {
+          long long ua = 1, ub = 1;
+          if (c.weighted) {
+            const long long wa = vertex_weight6(a0, a1, c.n0, c.n1);
+            const long long wb = vertex_weight6(b0, b1, c.n0, c.n1);
+            const long long g = gcd_ll(wa, wb);
+            ua = wb / g;
+            ub = wa / g;
           }
+          const long long kk = (long long)ceil(ex / (double)(ua + ub));
+          const long long sg = df < 0 ? -1 : 1;
+          hfield[ia] = (H)(hfield[ia] - sg * kk * ua);
+          hfield[ib] = (H)(hfield[ib] + sg * kk * ub);
+          did = true;
+        }
+      } else {
+        const double diff = hfield[ia] - hfield[ib];
+        const double ex = fabs(diff) - c.crit[dir];
+        if (ex > 0.0) {
+          const double signed_ex = diff < 0.0 ? -ex : ex;
+          double wa = 1.0, wb = 1.0;
+          if (c.weighted) {
+            wa = vertex_weight_fp64(a0, a1, c.n0, c.n1, c.f);
+            wb = vertex_weight_fp64(b0, b1, c.n0, c.n1, c.f);
+          }
+          const double ws = wa + wb;
+          const double ta = signed_ex * wb / ws, tb = signed_ex * wa / ws;
+          hfield[ia] = hfield[ia] - ta;
+          hfield[ib] = hfield[ib] + tb;
+          did = true;
+        }
+      }
+      if (did) {
+        reached[ia] = 1;
+        reached[ib] = 1;
+        ++moved;
+        // tiles of the 3x3 cell stencil around both endpoints (within the 3x3 tile block)
+        const int ends[4] = {a0, a1, b0, b1};
+        for (int q = 0; q < 2; ++q) {
+          const int p0 = ends[2 * q], p1 = ends[2 * q + 1];
+          for (int o0 = -1; o0 <= 1; ++o0)
+            for (int o1 = -1; o1 <= 1; ++o1) {
+              const int q0 = p0 + o0, q1 = p1 + o1;
+              if (q0 < 0 || q1 < 0 || q0 >= c.n0 || q1 >= c.n1) continue;
+              const int rt = q0 / T - tr, ct = q1 / T - tc;  // in [-1, 1]
+              trig[(rt + 1) * 3 + ct + 1] = 1;
+            }
+        }
       }
     }
+    moved_total += moved;
+    __syncthreads();
+    if (threadIdx.x < 9 && trig[threadIdx.x]) {
+      const int rt = tr + threadIdx.x / 3 - 1, ct = tc + threadIdx.x % 3 - 1;
+      const int nt = rt * c.tiles1 + ct;
+      if (atomicExch(&member[nt], 1) == 0) list[atomicAdd(&ctl->list_len, 1)] = nt;
+    }
+    __syncthreads();  // trig is reset by the next entry
   }
-  moved = warp_sum(moved);
-  if ((threadIdx.x & 31) == 0 && moved) atomicAdd(&moved_count, moved);
+  moved_total = warp_sum(moved_total);
+  if (threadIdx.x == 0) moved_count = 0;
   __syncthreads();
-  if (threadIdx.x < 9 && trig[threadIdx.x]) {
-    const int rt = tr + threadIdx.x / 3 - 1, ct = tc + threadIdx.x % 3 - 1;
-    phase_dst[rt * c.tiles1 + ct] = 1;
+  if ((threadIdx.x & 31) == 0 && moved_total) atomicAdd(&moved_count, moved_total);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (moved_count) atomicAdd(&ctl->moved_edges, moved_count);
+    __threadfence();
+    last = atomicAdd(&ctl->arrive, 1u) == gridDim.x - 1;
   }
-  if (threadIdx.x == 0 && moved_count) atomicAdd(&ctl->moved_edges, moved_count);
+  __syncthreads();
+  if (!last || threadIdx.x != 0) return;
+  __threadfence();
+  ctl->arrive = 0;
+  ctl->sub_len = *(volatile int*)&ctl->list_len;  // appended tiles join the next sub-phase
 }
 
+// Final scan of a round over the compacted list: tiles owning a reachable
+// pair whose excess is above the tolerance become pending for the next round.
 template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     frontier_scan_kernel(const RelaxConst c, const typename FvTypes<FX>::H* __restrict__ hfield,
-                         const int* __restrict__ reached, const int* __restrict__ phase,
+                         const int* __restrict__ reached, const int* __restrict__ list,
                          int* __restrict__ unstable, RelaxControl* ctl) {
   __shared__ int bad;
-  const int t = blockIdx.x;
-  if (*(volatile int*)&ctl->done || !phase[t]) return;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
+  if (*(volatile int*)&ctl->done) return;
+  const int len = *(volatile int*)&ctl->sub_len;
   const int T = c.ftile;
-  const int tr = t / c.tiles1, tc = t % c.tiles1;
-  int found = 0;
-  for (int k = threadIdx.x; k < T * T && !found; k += kThreads) {
-    const int a0 = tr * T + k / T, a1 = tc * T + k % T;
-    if (a0 >= c.n0 || a1 >= c.n1) continue;
-    for (int d = 0; d < 4 && !found; ++d) {
-      int d0, d1;
-      dir_of(d, d0, d1);
-      const int b0 = a0 + d0, b1 = a1 + d1;
-      if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
-      const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
-      if (!reached[ia] && !reached[ib]) continue;
-      if constexpr (FX) {
-        const long long df = (long long)hfield[ia] - (long long)hfield[ib];
-        if ((double)(df < 0 ? -df : df) - c.crit_q[d] > c.tol_q) found = 1;
-      } else {
-        if (fabs(hfield[ia] - hfield[ib]) - c.crit[d] > c.tol) found = 1;
+  for (int e = blockIdx.x; e < len; e += gridDim.x) {
+    const int t = list[e];
+    if (threadIdx.x == 0) bad = 0;
+    __syncthreads();
+    const int tr = t / c.tiles1, tc = t % c.tiles1;
+    int found = 0;
+    for (int k = threadIdx.x; k < T * T && !found; k += kThreads) {
+      const int a0 = tr * T + k / T, a1 = tc * T + k % T;
+      if (a0 >= c.n0 || a1 >= c.n1) continue;
+      for (int d = 0; d < 4 && !found; ++d) {
+        int d0, d1;
+        dir_of(d, d0, d1);
+        const int b0 = a0 + d0, b1 = a1 + d1;
+        if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+        const size_t ia = (size_t)a0 * c.pitch + a1, ib = (size_t)b0 * c.pitch + b1;
+        if (!reached[ia] && !reached[ib]) continue;
+        if constexpr (FX) {
+          const long long df = (long long)hfield[ia] - (long long)hfield[ib];
+          if ((double)(df < 0 ? -df : df) - c.crit_q[d] > c.tol_q) found = 1;
+        } else {
+          if (fabs(hfield[ia] - hfield[ib]) - c.crit[d] > c.tol) found = 1;
+        }
       }
     }
+    if (found) bad = 1;
+    __syncthreads();
+    if (threadIdx.x == 0 && bad) unstable[t] = 1;
+    __syncthreads();
   }
-  if (found) bad = 1;
-  __syncthreads();
-  if (threadIdx.x == 0 && bad) unstable[t] = 1;
 }
 
 __global__ void frontier_finish_kernel(const RelaxConst c, int* __restrict__ reached,

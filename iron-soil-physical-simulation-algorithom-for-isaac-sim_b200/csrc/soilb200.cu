@@ -157,7 +157,10 @@ struct sb_ctx {
   int* reached_alt = nullptr;
   int ftiles0 = 0, ftiles1 = 0;
   int* ftile_next = nullptr;   // next-round active tiles (seeded by labels / seeds)
+  // residual frontier: phase[0] = the round's tile membership flags,
+  // phase[1] = the round's compacted tile list (both ntiles ints)
   int* phase[2] = {nullptr, nullptr};
+  int frontier_grid = 1;  // CTAs of the list-driven frontier kernels
   RelaxControl* rctl = nullptr;
   RelaxControl* rctl_host = nullptr;
   LoopGraph relax_full;
@@ -762,6 +765,14 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMemsetAsync(ctx->b_alt, 0, field_bytes, ctx->stream));
   ctx->ftiles0 = (d.ny + d.tile_size - 1) / d.tile_size;
   ctx->ftiles1 = (d.nx + d.tile_size - 1) / d.tile_size;
+  {
+    // list-driven frontier kernels: eight 256-thread CTAs per SM stride over
+    // the active tiles (never more CTAs than tiles)
+    int sms = 0;
+    SB_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, d.device));
+    ctx->frontier_grid =
+        (int)std::min<long long>((long long)ctx->ftiles0 * ctx->ftiles1, 8LL * std::max(sms, 1));
+  }
   const size_t nt = (size_t)ctx->ftiles0 * ctx->ftiles1;
   SB_CUDA(ctx, cudaMalloc(&ctx->ptiles, nt * sizeof(int)));
   SB_CUDA(ctx, cudaMalloc(&ctx->dtiles, nt * sizeof(int)));
@@ -1347,6 +1358,8 @@ __global__ void relax_reset_kernel(RelaxControl* ctl) {
     ctl->n_active = 0;
     ctl->rounds = 0;
     ctl->moved_edges = 0;
+    ctl->list_len = 0;
+    ctl->sub_len = 0;
   }
 }
 
@@ -1688,19 +1701,20 @@ static int build_frontier(sb_ctx* ctx, const RelaxConst& c) {
   for (int k = 0; k < 8; ++k) {
     cudaGraphNode_t node;
     void* args[] = {(void*)&cc, (void*)&dirs[k], (void*)&pars[k], (void*)&hf,
-                    (void*)&ctx->reached, (void*)&ctx->phase[k & 1],
-                    (void*)&ctx->phase[(k + 1) & 1], (void*)&ctx->rctl};
+                    (void*)&ctx->reached, (void*)&ctx->phase[0], (void*)&ctx->phase[1],
+                    (void*)&ctx->rctl};
     if ((rc = add_kernel(ctx, body, &node, prev ? &prev : nullptr, prev ? 1 : 0,
-                         (void*)frontier_subphase_kernel<FX>, dim3(c.ntiles), 0, args)))
+                         (void*)frontier_subphase_kernel<FX>, dim3(ctx->frontier_grid), 0,
+                         args)))
       return rc;
     prev = node;
   }
   cudaGraphNode_t n_scan, n_begin;
   {
-    void* args[] = {(void*)&cc, (void*)&hf, (void*)&ctx->reached, (void*)&ctx->phase[0],
+    void* args[] = {(void*)&cc, (void*)&hf, (void*)&ctx->reached, (void*)&ctx->phase[1],
                     (void*)&ctx->ftile_next, (void*)&ctx->rctl};
     if ((rc = add_kernel(ctx, body, &n_scan, &prev, 1, (void*)frontier_scan_kernel<FX>,
-                         dim3(c.ntiles), 0, args)))
+                         dim3(ctx->frontier_grid), 0, args)))
       return rc;
   }
   if ((rc = add_kernel(ctx, body, &n_begin, &n_scan, 1, (void*)frontier_begin_kernel, dim3(1), 0,
@@ -2312,16 +2326,17 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     for (int k = 0; k < 8; ++k) {
       dirs[k] = k / 2;
       pars[k] = k % 2;
-      void* args[] = {&rcn, &dirs[k], &pars[k], &hf, &ctx->reached, &ctx->phase[k & 1],
-                      &ctx->phase[(k + 1) & 1], &ctx->rctl};
+      void* args[] = {&rcn, &dirs[k], &pars[k], &hf, &ctx->reached, &ctx->phase[0],
+                      &ctx->phase[1], &ctx->rctl};
       if ((rc = add_kernel(ctx, body, &bnode, bprev ? &bprev : nullptr, bprev ? 1 : 0,
-                           (void*)frontier_subphase_kernel<FX>, dim3(rcn.ntiles), 0, args)))
+                           (void*)frontier_subphase_kernel<FX>, dim3(ctx->frontier_grid), 0,
+                           args)))
         return rc;
       bprev = bnode;
     }
-    void* sargs[] = {&rcn, &hf, &ctx->reached, &ctx->phase[0], &ctx->ftile_next, &ctx->rctl};
+    void* sargs[] = {&rcn, &hf, &ctx->reached, &ctx->phase[1], &ctx->ftile_next, &ctx->rctl};
     if ((rc = add_kernel(ctx, body, &bnode, &bprev, 1, (void*)frontier_scan_kernel<FX>,
-                         dim3(rcn.ntiles), 0, sargs)))
+                         dim3(ctx->frontier_grid), 0, sargs)))
       return rc;
     bprev = bnode;
     if ((rc = add_kernel(ctx, body, &bnode, &bprev, 1, (void*)frontier_begin_kernel, dim3(1), 0,

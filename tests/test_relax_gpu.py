@@ -226,3 +226,34 @@ def test_event_driven_adapter_safety_limit_raises():
     with pytest.raises(soilb200.NumericalNonconvergenceError, match="NUMERICAL_NONCONVERGENCE"):
         solver.solve(g[f"{name}/initial"])
     solver.close()
+
+
+def test_weighted_frontier_compacted_list_beyond_one_wave():
+    """More active tiles than the list-driven kernels have CTAs (a 512^2 grid of
+    8-cell tiles, 4096 tiles, events scattered over all of it): the ballot-
+    compacted tile list with appended stencil tiles must still reproduce the
+    oracle's compact-frontier schedule bit for bit, with equal round counts."""
+    rng = np.random.default_rng(99)
+    shape = (512, 512)
+    h = 0.5 + 0.003 * rng.random(shape)
+    seeds = np.zeros(shape, dtype=bool)
+    for _ in range(1500):
+        r, c = rng.integers(2, shape[0] - 3), rng.integers(2, shape[1] - 3)
+        h[r - 1:r + 2, c - 1:c + 2] += rng.uniform(0.1, 0.25)
+        seeds[r - 1:r + 2, c - 1:c + 2] = True
+    tile = 8
+    crit = float(np.tan(np.deg2rad(33.0)))
+    w = R.vertex_weights(shape, 0.05, 0.05)
+    want, reached, rounds, hist = R.frontier_relax(h, seeds, R.seed_tiles(seeds, tile), tile=tile,
+                                                   spacing=(0.05, 0.05), crit_tan=crit,
+                                                   tolerance=1e-8, weights=w, record=True)
+    assert len(hist[0]["active"]) > 1184  # more list entries than CTAs in the first round
+    grid = soilb200.DeviceGrid(shape, 0.05, 0.05, precision="fp64", tile_size=tile)
+    grid.upload("b_eff", h)
+    front = soilb200.FrontierRelaxation(grid, weighted=True)
+    front.seed_mask(seeds)
+    st = front.run(crit, 1e-8)
+    assert st.rounds == rounds
+    assert np.array_equal(grid.download("b_eff"), want)
+    assert not grid.download("frontier_reached").any()
+    grid.close()
