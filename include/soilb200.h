@@ -486,6 +486,13 @@ int sb_batch_step(sb_batch* batch, double dt_s, const sb_mobile_params* params,
  * and keeps the fastest; best_ms = substep-loop time of one step with it. */
 int sb_batch_autotune(sb_batch* batch, double dt_s, const sb_mobile_params* params, int trials,
                       double* best_ms);
+/* Large-avalanche labelling of every patch's current state: the single-grid
+ * sb_label yield + canonical union-find (runtime/gpu_large_avalanche.py:
+ * 58-275), patch by patch; out[n_patches] receives each patch's record.  A
+ * batch models no latches or previous components (none set, none released). */
+int sb_batch_label(sb_batch* batch, const sb_label_params* params, sb_label_stats* out);
+/* Canonical labels of one patch after sb_batch_label (ny*nx int32, -1 = stable). */
+int sb_batch_download_labels(sb_batch* batch, int patch, int32_t* host);
 int sb_batch_last_error(sb_batch* batch, char* buffer, size_t length);
 int64_t sb_batch_kernel_launch_count(sb_batch* batch);
 void* sb_batch_stream(sb_batch* batch);

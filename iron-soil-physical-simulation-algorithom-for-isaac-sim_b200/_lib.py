@@ -281,6 +281,8 @@ _PROTOTYPES = {
     "sb_batch_autotune": (C.c_int, [C.c_void_p, C.c_double, C.POINTER(MobileParams), C.c_int,
                                     C.POINTER(C.c_double)]),
     "sb_batch_last_error": (C.c_int, [C.c_void_p, C.c_char_p, C.c_size_t]),
+    "sb_batch_label": (C.c_int, [C.c_void_p, C.POINTER(LabelParams), C.c_void_p]),
+    "sb_batch_download_labels": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "sb_batch_kernel_launch_count": (C.c_int64, [C.c_void_p]),
     "sb_batch_stream": (C.c_void_p, [C.c_void_p]),
     "sb_learned_last_error": (C.c_char_p, []),

@@ -187,15 +187,22 @@ class B200LargeAvalancheBridge:
         self._persistence_s = 0.0
         self._has_previous = False
 
-    def _params(self, release: bool) -> _lib.LabelParams:
-        start = float(np.deg2rad(self.material.start_angle_deg))
-        stop = float(np.deg2rad(self.material.stop_angle_deg))
+    @staticmethod
+    def label_params(material: MaterialScenario, config: LargeAvalancheTransitionConfig, *,
+                     release: bool, gravity: float = 9.81) -> _lib.LabelParams:
+        """The C-ABI labelling parameters of a material and transition config."""
+        start = float(np.deg2rad(material.start_angle_deg))
+        stop = float(np.deg2rad(material.stop_angle_deg))
         return _lib.LabelParams(
             float(np.tan(start)), float(np.tan(stop)), start, stop,
-            float(self.material.assumed_bulk_density_kg_m3), self.gravity,
-            float(self.material.cohesion_proxy_pa), float(self.config.mobilization_depth_m),
-            float(self.config.dry_tolerance_m), float(self.config.mobile_activity_speed_m_s),
-            int(self.config.connectivity), 1 if release else 0)
+            float(material.assumed_bulk_density_kg_m3), float(gravity),
+            float(material.cohesion_proxy_pa), float(config.mobilization_depth_m),
+            float(config.dry_tolerance_m), float(config.mobile_activity_speed_m_s),
+            int(config.connectivity), 1 if release else 0)
+
+    def _params(self, release: bool) -> _lib.LabelParams:
+        return self.label_params(self.material, self.config, release=release,
+                                 gravity=self.gravity)
 
     def label(self, *, release_settled_latches: bool = True) -> _lib.LabelStats:
         """Yield + components + component reductions (no classification)."""

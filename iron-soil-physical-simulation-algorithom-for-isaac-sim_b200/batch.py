@@ -141,6 +141,25 @@ class B200PatchBatch:
                            quantum=2.0 ** -self.quantization[i][0])
                 for i, st in enumerate(stats)]
 
+    def label(self, material, config=None) -> list:
+        """Large-avalanche labelling of every patch's current state (yield +
+        canonical union-find, as ``B200LargeAvalancheBridge.label`` on a
+        single grid, without latches); returns one ``LabelStats`` per patch."""
+        from .avalanche import B200LargeAvalancheBridge, LargeAvalancheTransitionConfig
+        cfg = config or LargeAvalancheTransitionConfig()
+        params = B200LargeAvalancheBridge.label_params(material, cfg, release=False)
+        out = (_lib.LabelStats * self.n_patches)()
+        self._check(_lib.load().sb_batch_label(self._batch, params, out), "batch label")
+        return list(out)
+
+    def labels(self, patch: int) -> np.ndarray:
+        """Canonical labels of one patch after :meth:`label` (-1 = stable)."""
+        ny, nx = self.shapes[patch]
+        out = np.empty((ny, nx), dtype=np.int32)
+        self._check(_lib.load().sb_batch_download_labels(self._batch, int(patch),
+                                                          out.ctypes.data), "batch labels")
+        return out
+
     def kernel_launches(self) -> int:
         return int(_lib.load().sb_batch_kernel_launch_count(self._batch))
 

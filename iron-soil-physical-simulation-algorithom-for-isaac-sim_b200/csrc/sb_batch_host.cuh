@@ -37,6 +37,21 @@ struct sb_batch {
   int rows_version = 0;
   int graph_rows_version = -1;
   long long launches = 0;
+  // per-patch labelling (sb_batch_label): scratch for the largest patch,
+  // reused patch by patch, and the labels of every patch (flat ny*nx each)
+  long long max_cells = 0;
+  int* lab_parent = nullptr;
+  float* lab_slope = nullptr;
+  float* lab_severity = nullptr;
+  int* lab_zero_i = nullptr;        // latch / previous component: all zero in a batch
+  double* lab_zero_d = nullptr;     // export ledgers: all zero
+  sb::LabelRoots lab_roots{};
+  int* lab_root_list = nullptr;
+  sb::LabelOut* lab_out = nullptr;  // one record per patch
+  sb::LabelOut* lab_out_host = nullptr;
+  unsigned int* lab_arrive = nullptr;
+  int32_t* labels = nullptr;
+  std::vector<long long> label_base;
   char err[512] = {0};
 };
 
@@ -288,10 +303,15 @@ int sb_batch_create(int device, int n_patches, const sb_patch_desc* patches, sb_
     bt->base.push_back(off);
     off += (long long)pitch * bt->desc[i].ny;
     max_cells = std::max(max_cells, (long long)bt->desc[i].ny * bt->desc[i].nx);
+    bt->label_base.push_back(bt->label_base.empty()
+                                 ? 0
+                                 : bt->label_base.back() +
+                                       (long long)bt->desc[i - 1].ny * bt->desc[i - 1].nx);
     bt->rows.push_back(16);
     bt->parity.push_back(0);
   }
   bt->elems = off;
+  bt->max_cells = max_cells;
   const size_t bytes = (size_t)off * 4;
   void** fields[] = {(void**)&bt->b, (void**)&bt->z, (void**)&bt->h[0], (void**)&bt->h[1],
                      (void**)&bt->qx[0], (void**)&bt->qx[1], (void**)&bt->qy[0], (void**)&bt->qy[1]};
@@ -324,9 +344,15 @@ int sb_batch_destroy(sb_batch* bt) {
   void* dev[] = {bt->b, bt->z, bt->h[0], bt->h[1], bt->qx[0], bt->qx[1], bt->qy[0], bt->qy[1],
                  bt->staging, bt->range_error, bt->d_patches, bt->d_item_patch, bt->d_band_patch,
                  bt->d_ctl, bt->d_g, bt->d_item_partials, bt->d_band_partials,
-                 bt->d_band_ipartials, bt->dt_dev};
+                 bt->d_band_ipartials, bt->dt_dev, bt->lab_parent, bt->lab_slope,
+                 bt->lab_severity, bt->lab_zero_i, bt->lab_zero_d, bt->lab_roots.count,
+                 bt->lab_roots.area6, bt->lab_roots.volume, bt->lab_roots.exc_start,
+                 bt->lab_roots.exc_stop, bt->lab_roots.max_exc_start, bt->lab_roots.max_exc_stop,
+                 bt->lab_roots.prev_overlap, bt->lab_root_list, bt->lab_out, bt->lab_arrive,
+                 bt->labels};
   for (void* p : dev)
     if (p) cudaFree(p);
+  if (bt->lab_out_host) cudaFreeHost(bt->lab_out_host);
   if (bt->h_ctl) cudaFreeHost(bt->h_ctl);
   if (bt->dt_host) cudaFreeHost(bt->dt_host);
   for (cudaEvent_t e : bt->ev)
@@ -554,6 +580,130 @@ int sb_batch_autotune(sb_batch* bt, double dt_s, const sb_mobile_params* params,
   if (rc) return rc;
   if (best_ms) *best_ms = best_t / trials;
   return sb_batch_set_rows(bt, best.data());
+}
+
+// Per-patch labelling: the single-grid yield + union-find kernels run patch by
+// patch on the batch arena (each patch's current ping-pong buffer, its own
+// quantum and datum), scratch reused, labels kept per patch.
+static int batch_label_alloc(sb_batch* bt) {
+  if (bt->lab_parent) return SB_OK;
+  const size_t n = (size_t)bt->max_cells;
+  long long total = 0;
+  for (int i = 0; i < bt->npatch; ++i) total += (long long)bt->desc[i].ny * bt->desc[i].nx;
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_parent, n * 4));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_slope, n * 4));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_severity, n * 4));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_zero_i, n * 4));
+  SB_BCUDA(bt, cudaMemsetAsync(bt->lab_zero_i, 0, n * 4, bt->stream));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_zero_d, n * 8));
+  SB_BCUDA(bt, cudaMemsetAsync(bt->lab_zero_d, 0, n * 8, bt->stream));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.count, n * 4));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.area6, n * 8));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.volume, n * 8));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.exc_start, n * 8));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.exc_stop, n * 8));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.max_exc_start, n * 8));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.max_exc_stop, n * 8));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_roots.prev_overlap, n * 4));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_root_list, n * 4));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_out, (size_t)bt->npatch * sizeof(LabelOut)));
+  SB_BCUDA(bt, cudaMallocHost(&bt->lab_out_host, (size_t)bt->npatch * sizeof(LabelOut)));
+  SB_BCUDA(bt, cudaMalloc(&bt->lab_arrive, sizeof(unsigned int)));
+  SB_BCUDA(bt, cudaMemsetAsync(bt->lab_arrive, 0, sizeof(unsigned int), bt->stream));
+  SB_BCUDA(bt, cudaMalloc(&bt->labels, (size_t)total * 4));
+  return SB_OK;
+}
+
+int sb_batch_label(sb_batch* bt, const sb_label_params* p, sb_label_stats* out) {
+  if (!bt || !p || !out) return SB_ERR_BAD_ARG;
+  if (p->connectivity != 4 && p->connectivity != 8)
+    return bfail(bt, SB_ERR_BAD_ARG, "[LargeAvalanche] connectivity must be 4 or 8");
+  SB_BCUDA(bt, cudaSetDevice(bt->device));
+  int rc = batch_label_alloc(bt);
+  if (rc) return rc;
+  SB_BCUDA(bt, cudaMemsetAsync(bt->lab_out, 0, (size_t)bt->npatch * sizeof(LabelOut), bt->stream));
+  for (int i = 0; i < bt->npatch; ++i) {
+    const sb_patch_desc& d = bt->desc[i];
+    LabelConst c{};
+    c.ny = d.ny;
+    c.nx = d.nx;
+    c.pitch = bt->pitch[i];
+    c.tiles_x = (d.nx + kLabelTile - 1) / kLabelTile;
+    c.connectivity = p->connectivity;
+    c.dx = d.dx_m;
+    c.dy = d.dy_m;
+    c.tan_start = p->tan_start;
+    c.tan_stop = p->tan_stop;
+    c.density = p->density_kg_m3;
+    c.gravity = p->gravity_m_s2;
+    c.cohesion = p->cohesion_pa;
+    c.mob_depth = p->mobilization_depth_m;
+    c.dry = p->dry_tolerance_m;
+    c.activity_speed = p->activity_speed_m_s;
+    c.start_rad = p->start_rad;
+    c.stop_rad = p->stop_rad;
+    c.Q = std::ldexp(1.0, -d.height_exponent);
+    c.datum = d.datum_m;
+    c.release_latches = 0;  // no latches in a batch
+    const long long base = bt->base[i];
+    const int tiles = c.tiles_x * ((d.ny + kLabelTile - 1) / kLabelTile);
+    LabelOut* lo = bt->lab_out + i;
+    label_init_local_kernel<true><<<tiles, kLabelInitThreads, 0, bt->stream>>>(
+        c, bt->b + base, bt->z + base, bt->h[0] + base, bt->h[1] + base, bt->qx[0] + base,
+        bt->qx[1] + base, bt->qy[0] + base, bt->qy[1] + base, &bt->d_ctl[i].k, bt->lab_parent,
+        bt->lab_slope, bt->lab_severity, bt->lab_zero_i, bt->lab_zero_d, bt->lab_zero_d,
+        bt->lab_roots);
+    label_merge_kernel<<<tiles, kThreads, 0, bt->stream>>>(c, bt->lab_parent, lo);
+    label_compress_kernel<true><<<grid_for((long long)d.ny * d.nx), kThreads, 0, bt->stream>>>(
+        c, bt->lab_parent, bt->b + base, bt->z + base, bt->lab_slope, bt->lab_severity,
+        bt->lab_zero_i, bt->lab_zero_i, bt->lab_roots, bt->lab_root_list, lo, 0);
+    label_reduce_kernel<<<32, kThreads, 0, bt->stream>>>(bt->lab_roots, bt->lab_root_list, lo,
+                                                          bt->lab_arrive);
+    SB_BCUDA(bt, cudaGetLastError());
+    SB_BCUDA(bt, cudaMemcpyAsync(bt->labels + bt->label_base[i], bt->lab_parent,
+                                 (size_t)d.ny * d.nx * 4, cudaMemcpyDeviceToDevice, bt->stream));
+    bt->launches += 4;
+  }
+  SB_BCUDA(bt, cudaMemcpyAsync(bt->lab_out_host, bt->lab_out,
+                               (size_t)bt->npatch * sizeof(LabelOut), cudaMemcpyDeviceToHost,
+                               bt->stream));
+  SB_BCUDA(bt, cudaStreamSynchronize(bt->stream));
+  int status = SB_OK;
+  for (int i = 0; i < bt->npatch; ++i) {
+    const LabelOut& o = bt->lab_out_host[i];
+    const sb_patch_desc& d = bt->desc[i];
+    sb_label_stats& s = out[i];
+    std::memset(&s, 0, sizeof(s));
+    s.status = o.status;
+    s.unstable_cell_count = o.total_unstable;
+    s.connected_region_count = o.regions;
+    s.largest_connected_cell_count = o.largest;
+    s.winner_root = o.winner;
+    s.union_passes = 2;
+    const double f = d.dx_m * d.dy_m / 6.0;
+    s.largest_connected_area_m2 = (double)o.area6 * f;
+    s.largest_connected_mobilizable_volume_m3 =
+        (double)o.volume * std::ldexp(1.0, -d.height_exponent) * f;
+    s.excess_start_sum_rad = (double)o.exc_start / kExcessScale;
+    s.excess_start_max_rad = (double)o.max_exc_start / kExcessScale;
+    s.excess_stop_sum_rad = (double)o.exc_stop / kExcessScale;
+    s.excess_stop_max_rad = (double)o.max_exc_stop / kExcessScale;
+    if (o.status && status == SB_OK)
+      status = bfail(bt, SB_ERR_NONCONVERGENCE,
+                     "NUMERICAL_NONCONVERGENCE: device avalanche connected components (patch %d)",
+                     i);
+  }
+  return status;
+}
+
+int sb_batch_download_labels(sb_batch* bt, int patch, int32_t* host) {
+  if (!bt || !host || patch < 0 || patch >= bt->npatch) return SB_ERR_BAD_ARG;
+  if (!bt->labels) return bfail(bt, SB_ERR_STATE, "[soilb200] sb_batch_label has not run");
+  const sb_patch_desc& d = bt->desc[patch];
+  SB_BCUDA(bt, cudaMemcpyAsync(host, bt->labels + bt->label_base[patch], (size_t)d.ny * d.nx * 4,
+                               cudaMemcpyDeviceToHost, bt->stream));
+  SB_BCUDA(bt, cudaStreamSynchronize(bt->stream));
+  return SB_OK;
 }
 
 int sb_batch_last_error(sb_batch* bt, char* buf, size_t len) {

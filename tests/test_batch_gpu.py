@@ -135,3 +135,43 @@ def test_batch_argument_errors():
     with pytest.raises(ValueError):
         batch.upload(0, "mobile", np.zeros((3, 3)))
     batch.close()
+
+
+def test_batch_labels_equal_patches_labelled_alone():
+    """Config 2's label check: after three batched steps every patch's
+    canonical labels and component statistics equal those of the same patch
+    stepped and labelled alone on its own grid (bit for bit; the resting layer
+    z_base = b_eff - 0.2 m gives the yield detector material to fail)."""
+    cfg = soilb200.MobileV2Config()
+    patches = _patches()[:-1]
+    states = [soilb200.MobileV2State(b, h, q) for b, h, q in patches]
+    zs = [b - 0.2 for b, _, _ in patches]
+    batch = B200PatchBatch(states, cfg, z_base=zs)
+    for _ in range(3):
+        batch.step_stats(DT)
+    mat = soilb200.MaterialScenario("batch", 1600.0, 35.0, 0.0, 0.5, 38.0, 30.0, 0.55)
+    stats = batch.label(mat)
+    assert sum(s.unstable_cell_count for s in stats) > 0
+    for i, (b, h, q) in enumerate(patches):
+        k, datum = batch.quantization[i]
+        grid = DeviceGrid(b.shape, cfg.dx_m, cfg.dy_m, precision="fx32", height_exponent=k,
+                          datum_m=datum)
+        for name, val in (("z_base", zs[i]), ("b_eff", b), ("mobile", h),
+                          ("momentum_x", q[..., 0]), ("momentum_y", q[..., 1])):
+            grid.upload(name, val)
+        for _ in range(3):
+            st = _lib.MobileStats()
+            _lib.check(grid.ctx, _lib.load().sb_mobile_step(grid.ctx, DT, mobile_params(cfg), st))
+        bridge = soilb200.B200LargeAvalancheBridge(grid, mat)
+        ref = bridge.label(release_settled_latches=False)
+        assert np.array_equal(batch.labels(i), bridge.labels()), i
+        got = stats[i]
+        assert (got.unstable_cell_count, got.connected_region_count,
+                got.largest_connected_cell_count, got.winner_root) == \
+            (ref.unstable_cell_count, ref.connected_region_count,
+             ref.largest_connected_cell_count, ref.winner_root), i
+        assert got.largest_connected_area_m2 == ref.largest_connected_area_m2, i
+        assert got.largest_connected_mobilizable_volume_m3 == \
+            ref.largest_connected_mobilizable_volume_m3, i
+        grid.close()
+    batch.close()
