@@ -279,6 +279,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     h_fx = grid.download("mobile")
     b_fx = grid.download("b_eff")
     wet_cells = int(np.count_nonzero(h_fx > 0.0))
+    site_extra = site_report(path, st, h_fx, local_rank) if site else None
     ref64 = PlainPath(cfg["b_eff"], cfg["z_base"], dx=DX, material=material(),
                       device=local_rank, residual="gated", precision="fp64")
     for k in range(total_steps):
@@ -337,6 +338,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             "wet_cells": wet_cells,
             "wet_fraction": wet_cells / cells,
             "max_abs_dh_vs_fp64_m": dh_max,
+            **({"site": site_extra} if site_extra else {}),
             "precision_vs_fp64": {
                 "max_abs_dh_m": dh_max, "max_abs_db_m": db_max, "bound_m": 1.0e-5,
                 "steps_compared": total_steps,
@@ -345,6 +347,39 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                        "last step"},
         }
     return result
+
+
+def site_report(path, last, h, device: int, reps: int = 10, tile: int = 64):
+    """Config-4 extras for the site line: the labelling (yield + union-find +
+    component reductions, sb_label) timed alone on the final state with CUDA
+    events, the component count of the last step, and the fraction of 64^2
+    tiles that hold mobile material or unstable cells."""
+    import torch
+    grid = path.grid
+    stream = torch.cuda.ExternalStream(grid.stream_handle(), device=device)
+    path.avalanche.label(release_settled_latches=False)  # warm
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        st = path.avalanche.label(release_settled_latches=False)
+    e1.record(stream)
+    e1.synchronize()
+    labels = grid.download("labels")
+    ny, nx = h.shape
+    ty, tx = (ny + tile - 1) // tile, (nx + tile - 1) // tile
+    busy = (h > 0.0) | (labels >= 0)
+    pad = np.zeros((ty * tile, tx * tile), dtype=bool)
+    pad[:ny, :nx] = busy
+    tiles = pad.reshape(ty, tile, tx, tile).any(axis=(1, 3))
+    return {"labelling_ms": e0.elapsed_time(e1) / reps,
+            "labelling_what": "sb_label on the final state: cohesive yield, block-local "
+                              "union-find, border merge, compression, component reductions",
+            "components": int(last.regions), "unstable_cells": int(last.unstable_cells),
+            "largest_component_cells": int(last.largest),
+            "active_tile_fraction": float(tiles.mean()),
+            "active_tile_rule": f"{tile}x{tile} tiles holding mobile material or unstable cells",
+            "label_regions_check": int(st.connected_region_count)}
 
 
 def run_mobile_large(args, n: int = 4096):
