@@ -64,6 +64,8 @@ struct FvControl {
   int neg_flag;                  // this substep's positivity failure (atomicOr)
   int pad;
   unsigned long long pmax[4];    // "before" ledger maxima for the prologue: external, |q|, grad, wave
+  unsigned int gen;              // persistent substep loop: barrier generation
+  int pad2;
 };
 
 // Ledger record layout (filled by the ledger kernels of sb_ledger.cuh).
@@ -295,6 +297,34 @@ __device__ __forceinline__ void plan_substep(const FvConst& c, FvControl* ctl) {
   ctl->sub_dt = sub;
 }
 
+// Loop control after the last block of a substep has arrived (one thread):
+// substep count, remaining time, ping-pong parity, error status and the next
+// substep's dt from this substep's wave-speed maximum.
+__device__ __forceinline__ void fv_advance(const FvConst& c, FvControl* ctl, double sub_dt,
+                                           int parity) {
+  const double w = __longlong_as_double((long long)atomicExch(&ctl->wave_bits, 0ull));
+  const int failed = atomicExch(&ctl->neg_flag, 0);
+  ctl->substeps += 1;
+  ctl->remaining -= sub_dt;
+  ctl->parity = parity ^ 1;
+  ctl->wave = w;
+  ctl->arrive = 0;
+  if (ctl->wait_fail) {
+    ctl->status = 6;  // SB_ERR_WAIT_LIMIT
+    ctl->done = 1;
+  } else if (failed) {
+    ctl->status = 3;  // SB_ERR_POSITIVITY
+    ctl->done = 1;
+  } else if (!(ctl->remaining > 1.0e-14)) {
+    ctl->done = 1;
+  } else if (ctl->substeps >= c.max_substeps) {
+    ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
+    ctl->done = 1;
+  } else {
+    plan_substep(c, ctl);
+  }
+}
+
 // End of one substep.  Every block folds its impulse/energy sums, wave
 // maximum and positivity flag (fixed order); the sums are added to the block's
 // own accumulators (diag_acc[k * nblocks + block], summed over the step's
@@ -331,27 +361,7 @@ __device__ __forceinline__ void fv_finish(const FvConst& c, FvControl* ctl, doub
   __syncthreads();
   if (!*flag || threadIdx.x != 0) return;
   __threadfence();
-  const double w = __longlong_as_double((long long)atomicExch(&ctl->wave_bits, 0ull));
-  const int failed = atomicExch(&ctl->neg_flag, 0);
-  ctl->substeps += 1;
-  ctl->remaining -= sub_dt;
-  ctl->parity = parity ^ 1;
-  ctl->wave = w;
-  ctl->arrive = 0;
-  if (ctl->wait_fail) {
-    ctl->status = 6;  // SB_ERR_WAIT_LIMIT
-    ctl->done = 1;
-  } else if (failed) {
-    ctl->status = 3;  // SB_ERR_POSITIVITY
-    ctl->done = 1;
-  } else if (!(ctl->remaining > 1.0e-14)) {
-    ctl->done = 1;
-  } else if (ctl->substeps >= c.max_substeps) {
-    ctl->status = 2;  // SB_ERR_SUBSTEP_CAP
-    ctl->done = 1;
-  } else {
-    plan_substep(c, ctl);
-  }
+  fv_advance(c, ctl, sub_dt, parity);
   __threadfence();
   if (use_handle) cudaGraphSetConditional(loop_handle, ctl->done ? 0u : 1u);
 }
@@ -636,6 +646,10 @@ struct FxCell {
   float qx, qy, u, v, cel;
 };
 
+// CG = false: read-only-cache loads (fields written by an earlier launch);
+// CG = true: L2-coherent loads (fields written by other CTAs of the same
+// persistent launch in the previous substep).
+template <bool CG>
 __device__ __forceinline__ void fx_load(const FvConst& c, const int32_t* __restrict__ b,
                                         const int32_t* __restrict__ h,
                                         const float* __restrict__ qx,
@@ -643,10 +657,16 @@ __device__ __forceinline__ void fx_load(const FvConst& c, const int32_t* __restr
                                         FxCell& x) {
   if (colok && row >= 0 && row < c.ny) {
     const size_t gi = (size_t)row * c.pitch + gx;
-    x.b = __ldg(b + gi);
-    x.h = __ldg(h + gi);
-    x.qx = __ldg(qx + gi);
-    x.qy = __ldg(qy + gi);
+    x.b = __ldg(b + gi);  // the support does not change during a substep loop
+    if constexpr (CG) {
+      x.h = __ldcg(h + gi);
+      x.qx = __ldcg(qx + gi);
+      x.qy = __ldcg(qy + gi);
+    } else {
+      x.h = __ldg(h + gi);
+      x.qx = __ldg(qx + gi);
+      x.qy = __ldg(qy + gi);
+    }
   } else {
     x.b = 0;
     x.h = 0;
@@ -675,7 +695,7 @@ __device__ __forceinline__ void fx_prepare(const FvConst& c, FxCell& x) {
 // of a grid whose row 0 starts at the given field pointers (row pitch
 // c.pitch).  Accumulates the impulse/energy sums into acc and the largest
 // next-substep wave speed into wave.  Every lane of the warp must call it.
-template <bool FAST = false>
+template <bool FAST = false, bool CG = false>
 __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __restrict__ bsrc,
                                              const int32_t* __restrict__ hsrc,
                                              const float* __restrict__ qxsrc,
@@ -698,14 +718,14 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
   float fa[kFvDiag] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   float fwave = 0.f;
   FxCell cur, nxt, nn;
-  fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0, gx, colok, cur);
-  fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 + 1, gx, colok, nxt);
+  fx_load<CG>(c, bsrc, hsrc, qxsrc, qysrc, y0, gx, colok, cur);
+  fx_load<CG>(c, bsrc, hsrc, qxsrc, qysrc, y0 + 1, gx, colok, nxt);
   // south face of the first row (the previous row's north face)
   int ms = 0;
   float nts = 0.f, nnps = 0.f;
   {
     FxCell prv;
-    fx_load(c, bsrc, hsrc, qxsrc, qysrc, y0 - 1, gx, colok, prv);
+    fx_load<CG>(c, bsrc, hsrc, qxsrc, qysrc, y0 - 1, gx, colok, prv);
     fx_prepare<FAST>(c, prv);
     fx_prepare<FAST>(c, cur);
     if (y0 > 0 && colok) {
@@ -717,7 +737,7 @@ __device__ __forceinline__ void fx_strip_run(const FvConst& c, const int32_t* __
   fx_prepare<FAST>(c, nxt);
 #pragma unroll 2
   for (int r = y0; r < y1; ++r) {
-    fx_load(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
+    fx_load<CG>(c, bsrc, hsrc, qxsrc, qysrc, r + 2, gx, colok, nn);
     // east face: this column and the next lane's
     const int eb = __shfl_down_sync(0xffffffffu, cur.b, 1);
     const int eh = __shfl_down_sync(0xffffffffu, cur.h, 1);
@@ -829,6 +849,94 @@ __global__ void __launch_bounds__(kThreads, 4)
                parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x, ext_y,
                gw % c.tiles_x, y0, y1, sub_dt, acc, wave);
   fv_finish(c, ctl, diag_acc, acc, wave, 0, &flag, sub_dt, parity, loop_handle, use_handle);
+}
+
+// --------------------------------------------------------------------------
+// Persistent FX32 substep loop: one cooperative launch (every CTA resident)
+// runs all CFL substeps of a physics step.  Each warp keeps its strip chunk
+// for the whole step; between substeps the CTAs meet at a grid barrier whose
+// last arrival advances the loop control (fv_advance: count, remaining time,
+// parity, status, next dt from the substep's wave-speed maximum, which every
+// CTA sent by atomicMax) and releases the others by bumping a generation
+// word.  The impulse/energy sums stay in each lane's registers across the
+// substeps and are folded once per step, so a substep ends with one warp
+// maximum and one atomic per CTA.  Field loads in the loop are L2-coherent
+// (the previous substep's writes come from other CTAs of this launch).  The
+// barrier wait is bounded: after kFvBarrierPolls polls the CTA records a wait
+// failure (SB_ERR_WAIT_LIMIT) and the loop ends.
+// --------------------------------------------------------------------------
+constexpr unsigned kFvBarrierPolls = 1u << 22;
+
+template <bool FAST>
+__global__ void __launch_bounds__(kThreads, 4)
+    fv_loop_kernel(const FvConst c, const int32_t* __restrict__ bsrc, int32_t* h0, int32_t* h1,
+                   float* qx0, float* qx1, float* qy0, float* qy1,
+                   const float* __restrict__ ext_x, const float* __restrict__ ext_y,
+                   FvControl* ctl, double* __restrict__ diag_acc) {
+  __shared__ double fold[fold_words(kFvDiag)];
+  __shared__ double wred[kThreads / 32];
+  __shared__ int s_done;
+  __shared__ unsigned s_gen;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (kThreads / 32) + warp;
+  const int j = gw / c.tiles_x, nchunk = c.row_chunks;
+  const int y0 = j < nchunk ? (int)((long long)j * c.ny / nchunk) : c.ny;
+  const int y1 = j < nchunk ? (int)((long long)(j + 1) * c.ny / nchunk) : c.ny;
+  const int strip = gw % c.tiles_x;
+  double acc[kFvDiag];
+#pragma unroll
+  for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      s_done = *(volatile int*)&ctl->done;
+      s_gen = *(volatile unsigned*)&ctl->gen;
+    }
+    __syncthreads();
+    if (s_done) break;
+    const double sub_dt = *(volatile double*)&ctl->sub_dt;
+    const int parity = *(volatile int*)&ctl->parity;
+    double wave = 0.0;
+    fx_strip_run<FAST, true>(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
+                             parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x,
+                             ext_y, strip, y0, y1, sub_dt, acc, wave);
+    wave = warp_max(wave);
+    if (lane == 0) wred[warp] = wave;
+    __threadfence();  // this thread's field writes before the arrival
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0;
+#pragma unroll
+      for (int w = 0; w < kThreads / 32; ++w) m = fmax(m, wred[w]);
+      atomicMax(&ctl->wave_bits, (unsigned long long)__double_as_longlong(m));
+      __threadfence();
+      const unsigned prev = atomicAdd(&ctl->arrive, 1u);
+      if (prev == gridDim.x - 1) {
+        __threadfence();
+        fv_advance(c, ctl, sub_dt, parity);
+        __threadfence();
+        atomicAdd(&ctl->gen, 1u);  // release
+      } else {
+        unsigned polls = 0;
+        while (*(volatile unsigned*)&ctl->gen == s_gen) {
+          if (++polls > kFvBarrierPolls) {
+            ctl->wait_fail = 1;
+            ctl->status = 6;  // SB_ERR_WAIT_LIMIT
+            ctl->done = 1;
+            break;
+          }
+          __nanosleep(32);
+        }
+        __threadfence();
+      }
+    }
+    __syncthreads();
+  }
+  // the step's impulse/energy sums of this CTA, once
+  const double* bt = block_fold<double, kFvDiag, kFvDiag>(acc, fold);
+  if (threadIdx.x < kFvDiag) {
+    double* a = diag_acc + (size_t)threadIdx.x * c.nblocks + blockIdx.x;
+    *a = *a + bt[threadIdx.x];
+  }
 }
 
 }  // namespace sb

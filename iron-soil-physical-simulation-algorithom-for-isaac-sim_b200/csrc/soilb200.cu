@@ -45,6 +45,7 @@ namespace sb {
 // with FMA contraction); this file only ever instantiates the exact variant.
 const void* fv_stream_fast_kernel();
 const void* batch_fv_fast_kernel();  // batch_fv_kernel<true>, same translation unit
+const void* fv_loop_fast_kernel();   // fv_loop_kernel<true>, same translation unit
 }  // namespace sb
 
 namespace {
@@ -129,6 +130,7 @@ struct sb_ctx {
   // chunks per strip
   int fv_stream = 0;
   int fv_exact = 0;  // 1: FX32 strip kernel with the CPU mirror's IEEE arithmetic
+  int fv_persistent = 0;  // 1: step graphs run the substeps in one cooperative launch
   int fv_rows = 0;  // FX streaming kernel: row chunks per strip
   int fv_strips = 0;
   int fv_stream_blocks = 0;
@@ -356,6 +358,47 @@ void fv_launch(sb_ctx* ctx, const FvConst& c, cudaGraphConditionalHandle* handle
   L.grid = dim3(c.nblocks);
 }
 
+int add_kernel(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps,
+               size_t ndeps, void* func, dim3 grid, size_t smem, void** args,
+               unsigned threads = kThreads);
+
+// Adds a step graph's substep loop after `dep`: the persistent cooperative
+// kernel (all substeps in one launch) when ctx->fv_persistent, else a WHILE
+// conditional node whose body runs two substep launches per iteration (the
+// second returns at once when the first ended the step).
+template <bool FX>
+int add_substep_loop(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t dep, const FvConst& c,
+                     cudaGraphConditionalHandle* handle, int* use_handle,
+                     cudaGraphNode_t* out) {
+  if (FX && ctx->fv_stream && ctx->fv_persistent) {
+    FvConst cc = c;
+    void* args[] = {(void*)&cc,         (void*)&ctx->b,     (void*)&ctx->h[0],  (void*)&ctx->h[1],
+                    (void*)&ctx->qx[0], (void*)&ctx->qx[1], (void*)&ctx->qy[0], (void*)&ctx->qy[1],
+                    (void*)&ctx->ext_x, (void*)&ctx->ext_y, (void*)&ctx->ctl,   (void*)&ctx->fv_diag};
+    void* fn = ctx->fv_exact ? (void*)fv_loop_kernel<false>
+                             : const_cast<void*>(fv_loop_fast_kernel());
+    int rc = add_kernel(ctx, g, out, &dep, 1, fn, dim3(ctx->fv_stream_blocks), 0, args, kThreads);
+    if (rc) return rc;
+    cudaLaunchAttributeValue v{};
+    v.cooperative = 1;
+    SB_CUDA(ctx, cudaGraphKernelNodeSetAttribute(*out, cudaLaunchAttributeCooperative, &v));
+    return SB_OK;
+  }
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = *handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  SB_CUDA(ctx, cudaGraphAddNode(out, g, &dep, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  FvLaunch L;
+  fv_launch<FX>(ctx, c, handle, use_handle, L);
+  cudaGraphNode_t n1, n2;
+  int rc = add_kernel(ctx, body, &n1, nullptr, 0, L.func, L.grid, L.smem, L.args.data(), kThreads);
+  if (rc) return rc;
+  return add_kernel(ctx, body, &n2, &n1, 1, L.func, L.grid, L.smem, L.args.data(), kThreads);
+}
+
 template <bool FX>
 void ledger_args(sb_ctx* ctx, const FvConst& c, double* datum, double* static_limit, int* mode,
                  cudaGraphConditionalHandle* handle, int* use_handle, std::vector<void*>& args) {
@@ -370,7 +413,7 @@ void ledger_args(sb_ctx* ctx, const FvConst& c, double* datum, double* static_li
 
 int add_kernel(sb_ctx* ctx, cudaGraph_t g, cudaGraphNode_t* node, const cudaGraphNode_t* deps,
                size_t ndeps, void* func, dim3 grid, size_t smem, void** args,
-               unsigned threads = kThreads) {
+               unsigned threads) {
   cudaKernelNodeParams kp{};
   kp.func = func;
   kp.gridDim = grid;
@@ -404,7 +447,7 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
   int mode0 = 0, mode1 = 2;  // 2: after-step ledger + substep diagnostics fold
   FvConst cc = c;
 
-  cudaGraphNode_t n_begin, n_pro, n_loop, n_after, n_body;
+  cudaGraphNode_t n_begin, n_pro, n_loop, n_after;
   {
     void* dt_mapped = nullptr;
     SB_CUDA(ctx, cudaHostGetDevicePointer(&dt_mapped, ctx->dt_host, 0));
@@ -415,7 +458,9 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
   }
   {
     std::vector<void*> args;
-    ledger_args<FX>(ctx, cc, &datum, &limit, &mode0, &handle, &use_handle, args);
+    // the prologue sets the WHILE condition only when the loop is one
+    int pro_handle = (FX && ctx->fv_stream && ctx->fv_persistent) ? 0 : use_handle;
+    ledger_args<FX>(ctx, cc, &datum, &limit, &mode0, &handle, &pro_handle, args);
     int rc = add_kernel(ctx, g, &n_pro, &n_begin, 1, (void*)ledger_kernel<FX>,
                         dim3(ctx->ledger_blocks), 0, args.data());
     if (rc) return rc;
@@ -423,21 +468,7 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
   cudaGraphNode_t n_ev0, n_ev1;
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&n_ev0, g, &n_pro, 1, ctx->ev_loop[0]));
   {
-    cudaGraphNodeParams cp{};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = handle;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    SB_CUDA(ctx, cudaGraphAddNode(&n_loop, g, &n_ev0, 1, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    FvLaunch L;
-    fv_launch<FX>(ctx, cc, &handle, &use_handle, L);
-    // two substeps per loop iteration (the second returns at once when the
-    // first ended the step): half the conditional-node relaunches
-    int rc = add_kernel(ctx, body, &n_body, nullptr, 0, L.func, L.grid, L.smem, L.args.data());
-    if (rc) return rc;
-    cudaGraphNode_t n_body2;
-    rc = add_kernel(ctx, body, &n_body2, &n_body, 1, L.func, L.grid, L.smem, L.args.data());
+    int rc = add_substep_loop<FX>(ctx, g, n_ev0, cc, &handle, &use_handle, &n_loop);
     if (rc) return rc;
   }
   {
@@ -688,6 +719,15 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
     ctx->fv_rows = (int)chunks;
     const long long warps = (long long)ctx->fv_strips * chunks;
     ctx->fv_stream_blocks = (int)((warps + kThreads / 32 - 1) / (kThreads / 32));
+    // the persistent substep loop needs every CTA resident at once
+    const void* loop_fn = ctx->fv_exact ? (const void*)fv_loop_kernel<false> : fv_loop_fast_kernel();
+    int per_sm = 0;
+    SB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, loop_fn, kThreads, 0));
+    const char* pers_env = std::getenv("SOILB200_FV_PERSISTENT");
+    ctx->fv_persistent = (!(pers_env && pers_env[0] == '0') &&
+                          (long long)per_sm * sms >= ctx->fv_stream_blocks)
+                             ? 1
+                             : 0;
   }
   // grid-stride reductions: three CTAs per SM (the ledger kernel's register
   // bound) keep the final fold short
@@ -1106,7 +1146,9 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
   const FvControl& k = *ctx->ctl_host;
   // graph: begin, two ledgers, records + two substep launches per loop
   // iteration; host loop: begin, two ledgers + one launch per substep
-  ctx->launches += ctx->use_graphs ? 4 + (k.substeps + 1) / 2 * 2 : 3 + k.substeps;
+  ctx->launches += !ctx->use_graphs ? 3 + k.substeps
+                   : (fx(ctx) && ctx->fv_stream && ctx->fv_persistent) ? 5
+                                                                        : 4 + (k.substeps + 1) / 2 * 2;
   rc = fill_mobile_stats(ctx, params, out);
   if (rc) return rc;
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
@@ -2199,8 +2241,10 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   dat = ctx->d.datum_m;
   int mode0 = 0, mode1 = 2, use_h = 1, no_h = 0;  // 2: after + diagnostics fold
   {
+    // the prologue sets the WHILE condition only when the loop is one
+    int pro_h = (FX && ctx->fv_stream && ctx->fv_persistent) ? 0 : use_h;
     std::vector<void*> args;
-    ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode0, &h_mob, &use_h, args);
+    ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode0, &h_mob, &pro_h, args);
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks),
                          0, args.data())))
       return rc;
@@ -2208,26 +2252,8 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   }
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[0]));
   prev = node;
-  {
-    cudaGraphNodeParams cp{};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h_mob;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    SB_CUDA(ctx, cudaGraphAddNode(&node, g, &prev, 1, &cp));
-    prev = node;
-    FvLaunch L;
-    fv_launch<FX>(ctx, fc, &h_mob, &use_h, L);
-    // two substeps per loop iteration (the second returns at once when the
-    // first ended the step): half the conditional-node relaunches
-    cudaGraphNode_t body_node, body_node2;
-    if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node, nullptr, 0, L.func,
-                         L.grid, L.smem, L.args.data())))
-      return rc;
-    if ((rc = add_kernel(ctx, cp.conditional.phGraph_out[0], &body_node2, &body_node, 1, L.func,
-                         L.grid, L.smem, L.args.data())))
-      return rc;
-  }
+  if ((rc = add_substep_loop<FX>(ctx, g, prev, fc, &h_mob, &use_h, &node))) return rc;
+  prev = node;
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[1]));
   prev = node;
   // The after-step ledger and the labelling chain both only read the final
@@ -2476,7 +2502,10 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
   const FvControl& k = *ctx->ctl_host;
   // ten kernels outside the loops, two substep launches per loop iteration,
   // ten kernels per residual round
-  ctx->launches += 10 + (k.substeps + 1) / 2 * 2 + 10LL * r.rounds;
+  ctx->launches += 10 +
+                   ((fx(ctx) && ctx->fv_stream && ctx->fv_persistent) ? 1
+                                                                      : (k.substeps + 1) / 2 * 2) +
+                   10LL * r.rounds;
   if (ctx->xout_host->bad_index)
     return fail(ctx, SB_ERR_BAD_ARG, "[DeviceBulkState] entrainment index outside state");
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
