@@ -336,6 +336,193 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
   if (warp == 0) tmem_free(tmem, S::TMEM_COLS);
 }
 
+// ------------------------------------------- forward, rotating accumulators
+// Each staged input row is read by the tensor core once instead of three
+// times.  Input row r feeds output rows r+1, r and r-1 through the kernel
+// rows dy = 0, 1, 2; three TMEM accumulators of COUT columns (slot s holds
+// output rows y with y % 3 == s) sit side by side, and for every column
+// offset dx one MMA of N = 3 * COUT writes all three: its B operand is the
+// three dy weight blocks in the order the slots want for this r.  The weights
+// are staged per dx as five blocks W(2) W(1) W(0) W(2) W(1), so the operand
+// for row r is the three consecutive blocks starting at block (1 - r) mod 3.
+// Every MMA accumulates; a slot is cleared (tcgen05.st of zeros) right after
+// its output row has been read, before the next row's MMAs add to it.  Per
+// output row this issues 3 * CIN/16 MMAs (N = 3 * COUT) instead of
+// 9 * CIN/16 (N = COUT): 2.1x less operand traffic from shared memory, which
+// bounds the M128 x N32 form.  A CTA reads input rows y0-1 .. y1, so it runs
+// two extra rows per row band.
+template <int CIN, int COUT>
+struct ConvRotSmem {
+  static constexpr int W_BLOCK = COUT * CIN * 2;         // one (dy, dx) weight block
+  static constexpr int W_BYTES = 15 * W_BLOCK;           // 3 dx x 5 staged blocks
+  static constexpr int ROW_BYTES = (CIN / 8) * kRowLbo;  // one staged input row
+  static constexpr int SLOTS = 4;                        // row in the MMA + three in flight
+  static constexpr int BYTES = W_BYTES + SLOTS * ROW_BYTES + 64;
+  static constexpr uint32_t TMEM_COLS = 3 * COUT <= 64 ? 64 : 128;
+};
+
+// Zeros COLS consecutive f32 columns of this thread's TMEM lane.
+template <int COLS>
+__device__ __forceinline__ void tmem_zero(uint32_t taddr) {
+  static_assert(COLS == 16 || COLS == 32, "16 or 32 columns");
+  const uint32_t z = 0u;
+  if constexpr (COLS == 32) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+        "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+        "r"(z)
+        : "memory");
+  } else {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+        "%1,%1};" ::"r"(taddr),
+        "r"(z)
+        : "memory");
+  }
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+// MMAs of input row r (staged in its ring slot) into the three accumulators.
+template <int CIN, int COUT>
+__device__ __forceinline__ void conv_rot_issue(uint32_t tmem, uint32_t slot_addr, uint32_t w_base,
+                                               int r, uint32_t idesc) {
+  using S = ConvRotSmem<CIN, COUT>;
+  const int first = ((1 - r) % 3 + 3) % 3;  // staged block that feeds accumulator slot 0
+  const uint64_t adesc0 = umma_desc(slot_addr, kRowLbo, 128);
+  const uint64_t bdesc0 = umma_desc(w_base, 128, (CIN / 8) * 128);
+#pragma unroll
+  for (int dx = 0; dx < 3; ++dx) {
+#pragma unroll
+    for (int kk = 0; kk < CIN / 16; ++kk)
+      umma_bf16(tmem, adesc0 + (uint64_t)((kk * 2 * kRowLbo + dx * 16) >> 4),
+                bdesc0 + (uint64_t)(((dx * 5 + first) * S::W_BLOCK + kk * 256) >> 4), idesc, 1);
+  }
+}
+
+template <int CIN, int COUT>
+__global__ void __launch_bounds__(kConvThreads) conv3x3_rot_kernel(const ConvArgs a) {
+  using S = ConvRotSmem<CIN, COUT>;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* wsm = smem;
+  unsigned char* ring = smem + S::W_BYTES;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ring + S::SLOTS * S::ROW_BYTES);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int x0 = blockIdx.x * kConvTileOut;
+  const int y0 = blockIdx.y * a.rows_per_cta;
+  const int y1 = min(y0 + a.rows_per_cta, a.h);
+  const int b = blockIdx.z;
+  auto slot = [&](int r) { return ring + ((r + S::SLOTS) % S::SLOTS) * S::ROW_BYTES; };
+
+  // weights -> shared memory: per dx the blocks of dy = 2, 1, 0, 2, 1 (the
+  // packed input holds block (dy * 3 + dx) for each (dy, dx))
+  {
+    constexpr int kDyOf[5] = {2, 1, 0, 2, 1};
+    constexpr int kChunks = S::W_BLOCK / 16;
+    const uint4* src = reinterpret_cast<const uint4*>(a.wpk);
+    uint4* dst = reinterpret_cast<uint4*>(wsm);
+    for (int i = tid; i < 15 * kChunks; i += kConvThreads) {
+      const int blk = i / kChunks, off = i % kChunks;
+      const int dx = blk / 5, j = blk % 5;
+      dst[i] = src[(kDyOf[j] * 3 + dx) * kChunks + off];
+    }
+  }
+  if (tid == 0) mbar_init(bar, 1);
+  if (warp == 0) tmem_alloc(tslot, S::TMEM_COLS);
+  const int r_first = y0 - 1, r_last = y1;  // input rows this CTA reads
+  int issued = r_first - 1;                 // last input row whose copy has been started
+  for (int r = r_first; r <= r_first + S::SLOTS - 1 && r <= r_last; ++r) {
+    conv_row_async<CIN>(a.in, b, a.h, a.w, r, x0, slot(r));
+    issued = r;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = umma_idesc_bf16(128, 3 * COUT);
+  const uint32_t w_base = smem_u32(wsm);
+  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  // all three accumulators start at zero
+#pragma unroll
+  for (int sl = 0; sl < 3; ++sl) tmem_zero<COUT>(lane_addr + (uint32_t)(sl * COUT));
+  conv_row_wait_pending(issued - r_first);  // row r_first has landed
+  fence_async_smem();                       // the weights (generic stores) too
+  tc_fence_before();
+  __syncthreads();
+  unsigned phase = 0;
+  bool ok = true;
+  if (y0 < y1 && tid == 0) {
+    tc_fence_after();
+    conv_rot_issue<CIN, COUT>(tmem, smem_u32(slot(r_first)), w_base, r_first, idesc);
+    umma_commit(bar);
+  }
+  for (int r = r_first; r <= r_last && y0 < y1; ++r) {
+    ok = mbar_wait(bar, phase) && ok;
+    phase ^= 1;
+    tc_fence_after();
+    // output row r - 1 is complete: read its accumulator, then clear the slot
+    // for the output row r + 2 that the next MMAs start
+    const int yo = r - 1;
+    const uint32_t acc = lane_addr + (uint32_t)((((yo % 3) + 3) % 3) * COUT);
+    float d[COUT];
+    if constexpr (COUT == 32)
+      tmem_ld32(acc, d);
+    else
+      tmem_ld16(acc, d);
+    tmem_zero<COUT>(acc);
+    tc_fence_before();
+    if (r + 1 <= r_last) conv_row_wait_pending(issued - (r + 1));  // row r + 1 has landed
+    __syncthreads();  // accumulator read and cleared by every thread, row r + 1 staged
+    if (r + 1 <= r_last) {
+      if (tid == 0) {
+        tc_fence_after();
+        conv_rot_issue<CIN, COUT>(tmem, smem_u32(slot(r + 1)), w_base, r + 1, idesc);
+        umma_commit(bar);
+      }
+      // row r's MMAs have completed: its slot takes row r + SLOTS
+      if (issued + 1 <= r_last && issued + 1 <= r + S::SLOTS) {
+        conv_row_async<CIN>(a.in, b, a.h, a.w, issued + 1, x0, slot(issued + 1));
+        ++issued;
+      }
+    }
+    const int xo = x0 + tid;
+    if (yo >= y0 && yo < y1 && xo < a.w) {
+      const size_t pix = ((size_t)b * a.h + yo) * a.w + xo;
+#pragma unroll
+      for (int c8 = 0; c8 < COUT; c8 += 8) {
+        float o[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) o[j] = a.relu ? fmaxf(d[c8 + j], 0.f) : d[c8 + j];
+        if (a.mask) {
+          const uint4 mv = *reinterpret_cast<const uint4*>(a.mask + pix * COUT + c8);
+          const __nv_bfloat16* mk = reinterpret_cast<const __nv_bfloat16*>(&mv);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (!(__bfloat162float(mk[j]) > 0.f)) o[j] = 0.f;
+        }
+        if (a.out_f32) {
+          float* op = reinterpret_cast<float*>(a.out) + pix * a.out_f32 + c8;
+          if (c8 < a.out_f32) *reinterpret_cast<float4*>(op) = make_float4(o[0], o[1], o[2], o[3]);
+          if (c8 + 4 < a.out_f32)
+            *reinterpret_cast<float4*>(op + 4) = make_float4(o[4], o[5], o[6], o[7]);
+        } else {
+          __align__(16) __nv_bfloat162 ob[4];
+#pragma unroll
+          for (int j = 0; j < 4; ++j) ob[j] = __floats2bfloat162_rn(o[2 * j], o[2 * j + 1]);
+          *reinterpret_cast<uint4*>(reinterpret_cast<__nv_bfloat16*>(a.out) + pix * COUT + c8) =
+              *reinterpret_cast<const uint4*>(ob);
+        }
+      }
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+  if (!ok && tid == 0 && a.status) atomicExch(a.status, 1);
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, S::TMEM_COLS);
+}
+
 // ----------------------------------------------------------- weight grad
 struct WgradArgs {
   const __nv_bfloat16* in;    // layer input [batch][h][w][cin]

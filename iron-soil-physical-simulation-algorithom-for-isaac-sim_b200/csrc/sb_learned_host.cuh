@@ -8,20 +8,34 @@ namespace {
 
 using namespace sb;
 
+// Forward / data-gradient convolution.  Default: the rotating-accumulator
+// kernel (each input row read once, N = 3 * COUT); SOILB200_CONV_ROT=0
+// selects the nine-tap kernel (N = COUT), which computes the same sums.
 template <int CIN, int COUT>
 cudaError_t launch_conv(const ConvArgs& a, int rows, cudaStream_t st) {
-  using S = ConvSmem<CIN, COUT>;
   static bool attr_set[16] = {false};
+  static const bool rot = [] {
+    const char* e = std::getenv("SOILB200_CONV_ROT");
+    return !(e && e[0] == '0');
+  }();
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 16 && !attr_set[dev]) {
     cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, COUT>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, S::BYTES);
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         ConvSmem<CIN, COUT>::BYTES);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(conv3x3_rot_kernel<CIN, COUT>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               ConvRotSmem<CIN, COUT>::BYTES);
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
   dim3 grid((a.w + kConvTileOut - 1) / kConvTileOut, (a.h + rows - 1) / rows, a.batch);
-  conv3x3_tc_kernel<CIN, COUT><<<grid, kConvThreads, S::BYTES, st>>>(a);
+  if (rot)
+    conv3x3_rot_kernel<CIN, COUT><<<grid, kConvThreads, ConvRotSmem<CIN, COUT>::BYTES, st>>>(a);
+  else
+    conv3x3_tc_kernel<CIN, COUT><<<grid, kConvThreads, ConvSmem<CIN, COUT>::BYTES, st>>>(a);
   return cudaGetLastError();
 }
 
