@@ -240,6 +240,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
 
     launches0 = grid.kernel_launches()
     step_ms, substeps, loop_ms = [], [], []
+    stage_sum = {}
     h2d = d2h = 0
     stats_bytes = 2 * 400  # MobileStats + LabelOut records read back per step (approx, fixed)
     wall = 0.0
@@ -268,6 +269,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
                 wall += time.perf_counter() - t0
                 step_ms.append(e0.elapsed_time(e1))
             substeps.append(st.substeps)
+            if args.stages:
+                for name, ms in path.stage_times().items():
+                    stage_sum[name] = stage_sum.get(name, 0.0) + ms
             ls = path.mobile.last_stats
             if ls is not None and ls.substeps:
                 loop_ms.append((ls.substep_loop_ms, ls.substeps))
@@ -339,6 +343,9 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             "wet_fraction": wet_cells / cells,
             "max_abs_dh_vs_fp64_m": dh_max,
             **({"site": site_extra} if site_extra else {}),
+            **({"stage_ms_per_step": {k: v / args.steps for k, v in stage_sum.items()},
+                "stage_note": "event nodes between the step graph's stages (they add a "
+                              "little time of their own)"} if stage_sum else {}),
             "precision_vs_fp64": {
                 "max_abs_dh_m": dh_max, "max_abs_db_m": db_max, "bound_m": 1.0e-5,
                 "steps_compared": total_steps,
@@ -715,6 +722,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--stages", action="store_true",
+                    help="per-stage device times of the step graph (event nodes between stages)")
     ap.add_argument("--no-repose", action="store_true",
                     help="leave the learned-repose sub-object out of the default line")
     ap.add_argument("--workload", default="config1_plain_path_701",
@@ -722,6 +731,8 @@ def main():
                              "repose_701", "site_c4_4096"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.stages:
+        os.environ["SOILB200_STAGE_EVENTS"] = "1"
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

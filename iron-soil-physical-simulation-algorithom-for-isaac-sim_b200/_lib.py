@@ -252,6 +252,7 @@ _PROTOTYPES = {
     "sb_path_step": (C.c_int, [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_int,
                                C.POINTER(PathParams), C.POINTER(PathStats)]),
     "sb_path_reset": (C.c_int, [C.c_void_p]),
+    "sb_path_stage_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
     "sb_entrain": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                              C.POINTER(C.c_double)]),
     "sb_entrain_to_surface": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,

@@ -138,6 +138,13 @@ struct sb_ctx {
   MobileGraph mobile;
   cudaEvent_t ev_loop[2] = {nullptr, nullptr};  // around the substep WHILE node
   cudaEvent_t ev_path[2] = {nullptr, nullptr};  // first and last node of the step graph
+  // optional event nodes between the stages of the step graph's main chain
+  // (SOILB200_STAGE_EVENTS=1): a device-time breakdown of one step
+  static constexpr int kStages = 10;
+  bool stage_events = false;
+  cudaEvent_t ev_stage[kStages] = {};
+  int n_stage = 0;
+  float stage_ms[kStages] = {};
   bool use_graphs = true;  // false: host-driven launches (profilers that cannot see
                            // kernels inside conditional graphs)
   // labelling (flat ny*nx arrays)
@@ -753,6 +760,12 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaEventCreate(&ctx->ev_loop[1]));
   SB_CUDA(ctx, cudaEventCreate(&ctx->ev_path[0]));
   SB_CUDA(ctx, cudaEventCreate(&ctx->ev_path[1]));
+  {
+    const char* env = std::getenv("SOILB200_STAGE_EVENTS");
+    ctx->stage_events = env && env[0] == '1';
+    if (ctx->stage_events)
+      for (cudaEvent_t& e : ctx->ev_stage) SB_CUDA(ctx, cudaEventCreate(&e));
+  }
   // labelling buffers (flat ny*nx)
   const size_t n = (size_t)d.ny * d.nx;
   SB_CUDA(ctx, cudaMalloc(&ctx->parent, n * 4));
@@ -925,6 +938,8 @@ int sb_ctx_destroy(sb_ctx* ctx) {
   for (cudaEvent_t e : ctx->ev_loop)
     if (e) cudaEventDestroy(e);
   for (cudaEvent_t e : ctx->ev_path)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->ev_stage)
     if (e) cudaEventDestroy(e);
   if (ctx->xout_host) cudaFreeHost(ctx->xout_host);
   if (ctx->dep_out_host) cudaFreeHost(ctx->dep_out_host);
@@ -2211,6 +2226,15 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   double Q = ctx->quantum, datum = ctx->d.datum_m, f = ctx->d.dx_m * ctx->d.dy_m / 6.0;
   cudaGraphNode_t prev, node;
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&prev, g, nullptr, 0, ctx->ev_path[0]));
+  ctx->n_stage = 0;
+  // stage boundary on the main chain (only with stage events enabled)
+  auto mark = [&]() -> int {
+    if (!ctx->stage_events || ctx->n_stage >= sb_ctx::kStages) return SB_OK;
+    cudaGraphNode_t ev;
+    SB_CUDA(ctx, cudaGraphAddEventRecordNode(&ev, g, &prev, 1, ctx->ev_stage[ctx->n_stage++]));
+    prev = ev;
+    return SB_OK;
+  };
   // 1. step start (loop control, cleared records), cut entrainment
   {
     void* in_dev = nullptr;
@@ -2220,6 +2244,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_begin_kernel, dim3(1), 0, args)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   {
     int pitch = ctx->pitch;
@@ -2232,6 +2257,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_entrain_kernel<FX>, dim3(64), 0, args)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   // 2. Mobile V2 (same kernels as the standalone step graph)
   FvConst fc;
@@ -2249,6 +2275,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          0, args.data())))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[0]));
   prev = node;
@@ -2279,12 +2306,14 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          0, args, kLabelInitThreads)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   {
     void* args[] = {&lc, &ctx->parent, &ctx->lout};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)label_merge_kernel, dim3(ltiles), 0, args)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   {
     int mask_only = 0;
@@ -2294,6 +2323,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          dim3(grid_for((long long)ny * nx)), 0, args)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   // 4. component reduction + classification / persistence / gate, then
   // previous mask + seeding
@@ -2323,6 +2353,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          args)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   // 5. previous mask + frontier seeds; its last block opens the gated
   // residual frontier loop (same kernels as sb_frontier_run)
@@ -2335,6 +2366,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          dim3(grid_for((long long)ny * nx)), 0, args)))
       return rc;
     prev = node;
+    if ((rc = mark())) return rc;
   }
   {
     cudaGraphNodeParams cp{};
@@ -2344,6 +2376,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     cp.conditional.size = 1;
     SB_CUDA(ctx, cudaGraphAddNode(&node, g, &prev, 1, &cp));
     prev = node;
+    if ((rc = mark())) return rc;
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     int dirs[8], pars[8];
     typename T::H* hf;
@@ -2404,6 +2437,15 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
 }
 
 }  // namespace
+
+// Device-time breakdown of the last sb_path_step (SOILB200_STAGE_EVENTS=1 at
+// context creation): out[k] = ms from the previous boundary to stage k's end.
+extern "C" int sb_path_stage_times(sb_ctx* ctx, float* out_ms, int capacity) {
+  if (!ctx || !out_ms || capacity < 0) return -SB_ERR_BAD_ARG;
+  const int n = ctx->stage_events ? std::min(ctx->n_stage, capacity) : 0;
+  for (int k = 0; k < n; ++k) out_ms[k] = ctx->stage_ms[k];
+  return n;
+}
 
 extern "C" int sb_path_reset(sb_ctx* ctx) {
   if (!ctx) return SB_ERR_BAD_ARG;
@@ -2499,6 +2541,13 @@ extern "C" int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_idx,
   float step_ms = 0.f;
   SB_CUDA(ctx, cudaEventElapsedTime(&step_ms, ctx->ev_path[0], ctx->ev_path[1]));
   out->device_ms = step_ms;
+  if (ctx->stage_events) {
+    cudaEvent_t prev_ev = ctx->ev_path[0];
+    for (int k = 0; k < ctx->n_stage; ++k) {
+      SB_CUDA(ctx, cudaEventElapsedTime(&ctx->stage_ms[k], prev_ev, ctx->ev_stage[k]));
+      prev_ev = ctx->ev_stage[k];
+    }
+  }
   const FvControl& k = *ctx->ctl_host;
   // ten kernels outside the loops, two substep launches per loop iteration,
   // ten kernels per residual round

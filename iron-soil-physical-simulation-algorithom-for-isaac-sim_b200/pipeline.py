@@ -143,5 +143,16 @@ class PlainPath:
                              diag.largest_connected_cell_count, rounds,
                              float(mob.volume_after_m3), float(mob.maximum_speed_m_s))
 
+    STAGES = ("start", "entrainment", "before_ledger", "substeps_and_yield_tiles", "border_merge",
+              "compression", "reduction_classification", "previous_and_seeds", "residual_frontier")
+
+    def stage_times(self) -> dict:
+        """Device ms per stage of the last fused step (needs the context created
+        with SOILB200_STAGE_EVENTS=1; empty otherwise)."""
+        import numpy as _np
+        out = _np.zeros(16, dtype=_np.float32)
+        n = int(_lib.load().sb_path_stage_times(self.grid.ctx, out.ctypes.data, out.size))
+        return {name: float(out[k]) for k, name in enumerate(self.STAGES[:max(n, 0)])}
+
     def close(self) -> None:
         self.state.close()
