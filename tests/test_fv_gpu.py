@@ -71,9 +71,8 @@ def _fx_run(solver, b, h, q, dt, steps, mu, cfl):
 
 def test_fx32_kernel_bitwise_equals_cpu_mirror(fv_golden, monkeypatch):
     cfg = soilb200.MobileV2Config()
-    monkeypatch.setenv("SOILB200_FV_EXACT", "1")
+    monkeypatch.setenv("SOILB200_FV_EXACT", "1")  # read when the solver creates its grids
     solver = soilb200.B200MobileV2Solver(cfg, precision="fx32")
-    monkeypatch.delenv("SOILB200_FV_EXACT")
     for name in fv_golden["names"]:
         b, h, q = fv_golden[f"{name}/b"], fv_golden[f"{name}/h"], fv_golden[f"{name}/q"]
         st, hq, qx, qy, n, k = _fx_run(solver, b, h, q, float(fv_golden[f"{name}/dt"]), 1,
@@ -144,15 +143,15 @@ def test_fx32_and_fp64_ragged_shapes(shape, monkeypatch):
     assert np.array_equal(st.state.h_m, ref.h)
     assert np.array_equal(st.state.q_m2_s, ref.q)
     s64.close()
-    monkeypatch.setenv("SOILB200_FV_EXACT", "1")
+    monkeypatch.setenv("SOILB200_FV_EXACT", "1")  # read when the solver creates its grid
     s32 = soilb200.B200MobileV2Solver(cfg, precision="fx32")
-    monkeypatch.delenv("SOILB200_FV_EXACT")
     st2, hq, qx, qy, n, k = _fx_run(s32, b, h, q, 0.02, 1, cfg.basal_friction_coefficient, cfg.cfl)
     assert st2.substeps == n
     assert np.array_equal(st2.state.h_m, fx.dequantize(hq, 0.0, k))
     assert np.array_equal(st2.state.q_m2_s[..., 0], qx.astype(np.float64))
     assert st2.mass_residual_m3 == 0.0
     s32.close()
+    monkeypatch.delenv("SOILB200_FV_EXACT")
     fast = soilb200.B200MobileV2Solver(cfg, precision="fx32")  # production kernel
     st3 = fast.step(soilb200.MobileV2State(b, h, q), 0.02)
     assert st3.substeps == n

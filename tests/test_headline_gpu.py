@@ -26,6 +26,7 @@ import pytest
 import soilb200
 from oracle import fixed_point as fx
 from oracle import labels as L
+from oracle import relax as R
 from oracle.path import PathOracle, PathOracleConfig
 from soilb200 import workloads
 from soilb200.pipeline import PlainPath
@@ -55,6 +56,19 @@ def _oracle_cfg(mat, **kw):
 def _fields(path):
     g = path.grid
     return {k: g.download(k) for k in ("b_eff", "mobile", "momentum_x", "momentum_y")}
+
+
+def _steep_cells(b, angle_deg):
+    """Cells with a neighbour slope above the angle (axis-aligned pairs)."""
+    crit = np.tan(np.deg2rad(angle_deg)) * DX
+    m = np.zeros(b.shape, dtype=bool)
+    d0 = np.abs(np.diff(b, axis=0)) > crit
+    d1 = np.abs(np.diff(b, axis=1)) > crit
+    m[:-1] |= d0
+    m[1:] |= d0
+    m[:, :-1] |= d1
+    m[:, 1:] |= d1
+    return m
 
 
 def _compare_step(k, g, o):
@@ -143,9 +157,10 @@ def test_fx32_headline_path_labels_bound_and_volume(headline_runs):
 
 @pytest.mark.parametrize("residual,seed", [("always", 3), ("gated", 5)])
 def test_fp64_small_path_with_residual_matches_oracle(residual, seed):
-    """A 192^2 pile with the residual frontier on (``always``) and gated:
-    frontier seeding from local instabilities, the gate and the compact-frontier
-    rounds against the oracle, fields bit-identical."""
+    """A 192^2 pile with the residual frontier on (``always``) and gated, with
+    residual seeds queued at the start: the gate, seeding from local
+    instabilities and the compact-frontier rounds against the oracle, fields
+    bit-identical."""
     n = 192
     b = workloads.noise_pile(n, seed, DX)
     cut = workloads.BucketCut((n, n), DX, b, start=(0.25 * n * DX, 0.5 * n * DX))
@@ -153,6 +168,13 @@ def test_fp64_small_path_with_residual_matches_oracle(residual, seed):
     path = PlainPath(b, np.zeros_like(b), dx=DX, material=mat, precision="fp64", tile_size=32,
                      residual=residual)
     oracle = PathOracle(b, np.zeros_like(b), _oracle_cfg(mat, tile=32, residual=residual))
+    # pending residual seeds at the start (the steepest cells of the pile, as
+    # the reference's _seed_gpu_residual_frontier queues changed cells): the
+    # reached mask and the 3x3-stencil tiles, on both sides
+    seeds = _steep_cells(b, mat.stop_angle_deg)
+    path.frontier.seed_mask(seeds)
+    oracle.reached |= seeds
+    oracle.pending = R.seed_tiles(seeds, 32)
     ran = 0
     for k in range(40):
         idx, tgt = cut.footprint((k + 1) * DT)
