@@ -72,9 +72,11 @@ int bfail(sb_batch* bt, int code, const char* fmt, ...) {
 #define SB_BCUDA(bt, call)                                                                   \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
+    if (e_ != cudaSuccess) {                                                                 \
+      cudaGetLastError(); /* a failed call must not surface again in a later check */       \
       return bfail((bt), SB_ERR_CUDA, "CUDA error %s at %s:%d (%s)", cudaGetErrorString(e_), \
                    __FILE__, __LINE__, #call);                                               \
+    }                                                                                        \
   } while (0)
 
 constexpr int kBatchMinRows = 4;

@@ -8,16 +8,15 @@ namespace {
 
 using namespace sb;
 
-// Forward / data-gradient convolution.  Default: the rotating-accumulator
-// kernel (each input row read once, N = 3 * COUT); SOILB200_CONV_ROT=0
-// selects the nine-tap kernel (N = COUT), which computes the same sums.
+// Forward / data-gradient convolution.  Default: the nine-tap kernel
+// (N = COUT), measured faster at the proposal's sizes; SOILB200_CONV_ROT=1
+// selects the rotating-accumulator kernel (each input row read once,
+// N = 3 * COUT), which computes the same sums in another order.
 template <int CIN, int COUT>
 cudaError_t launch_conv(const ConvArgs& a, int rows, cudaStream_t st) {
   static bool attr_set[16] = {false};
-  static const bool rot = [] {
-    const char* e = std::getenv("SOILB200_CONV_ROT");
-    return !(e && e[0] == '0');
-  }();
+  const char* rot_env = std::getenv("SOILB200_CONV_ROT");
+  const bool rot = rot_env && rot_env[0] == '1';
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 16 && !attr_set[dev]) {

@@ -240,9 +240,11 @@ int fail(sb_ctx* ctx, int code, const char* fmt, ...) {
 #define SB_CUDA(ctx, call)                                                                  \
   do {                                                                                      \
     cudaError_t e_ = (call);                                                                \
-    if (e_ != cudaSuccess)                                                                  \
+    if (e_ != cudaSuccess) {                                                                \
+      cudaGetLastError(); /* a failed call must not surface again in a later check */      \
       return fail((ctx), SB_ERR_CUDA, "CUDA error %s at %s:%d (%s)", cudaGetErrorString(e_), \
                   __FILE__, __LINE__, #call);                                               \
+    }                                                                                       \
   } while (0)
 
 bool fx(const sb_ctx* c) { return c->d.precision == SB_FX32; }
@@ -447,7 +449,11 @@ int build_mobile_graph(sb_ctx* ctx, const FvConst& c, double static_limit) {
   SB_CUDA(ctx, cudaGraphCreate(&g, 0));
   mg.graph = g;
   cudaGraphConditionalHandle handle;
-  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
+  // a conditional handle without a conditional node can fail instantiation:
+  // the persistent substep loop needs none
+  handle = 0;
+  if (!(FX && ctx->fv_stream && ctx->fv_persistent))
+    SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, g, 0, cudaGraphCondAssignDefault));
   int use_handle = 1;
   double datum = ctx->d.datum_m;
   double limit = static_limit;
@@ -2219,7 +2225,11 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   SB_CUDA(ctx, cudaGraphCreate(&g, 0));
   ctx->path_graph = g;
   cudaGraphConditionalHandle h_mob, h_front;
-  SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_mob, g, 0, cudaGraphCondAssignDefault));
+  // a conditional handle without a conditional node can fail instantiation:
+  // the persistent substep loop needs none
+  h_mob = 0;
+  if (!(FX && ctx->fv_stream && ctx->fv_persistent))
+    SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_mob, g, 0, cudaGraphCondAssignDefault));
   SB_CUDA(ctx, cudaGraphConditionalHandleCreate(&h_front, g, 0, cudaGraphCondAssignDefault));
   int rc, one = 1, zero = 0;
   const int ny = ctx->d.ny, nx = ctx->d.nx;

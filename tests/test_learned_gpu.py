@@ -1,8 +1,9 @@
 """GPU tests of the learned repose proposal's tensor-core kernels.
 
 The CPU oracle (oracle/learned.py, float64) is the checker:
-* forward convolutions: f32 outputs within 1e-4 of the largest |value| (FP32
-  accumulation of exact BF16 products), BF16 outputs within BF16 rounding;
+* forward convolutions (the nine-tap kernel and the rotating-accumulator
+  kernel, SOILB200_CONV_ROT=1): f32 outputs within 1e-4 of the largest |value|
+  (FP32 accumulation of exact BF16 products), BF16 outputs within BF16 rounding;
 * weight gradients within 1e-4 (relative to the largest |value|);
 * full back-propagation of the training loss: the GPU keeps activations in
   BF16, so each layer's gradient is compared by relative L2 error <= 5e-2;
@@ -38,7 +39,9 @@ def _learned():
 
 @pytest.mark.parametrize("cin,cout", [(16, 32), (32, 32), (32, 16), (16, 16)])
 @pytest.mark.parametrize("relu", [False, True])
-def test_conv_matches_oracle(cin, cout, relu):
+@pytest.mark.parametrize("rot", ["0", "1"])  # nine-tap / rotating-accumulator kernel
+def test_conv_matches_oracle(cin, cout, relu, rot, monkeypatch):
+    monkeypatch.setenv("SOILB200_CONV_ROT", rot)
     ln = _learned()
     rng = np.random.default_rng(cin * 100 + cout + relu)
     x = bf16(rng.normal(size=(2, 19, 300, cin)))
@@ -60,7 +63,9 @@ def test_conv_matches_oracle(cin, cout, relu):
     assert int(status.item()) == 0
 
 
-def test_conv_mask_and_rows():
+@pytest.mark.parametrize("rot", ["0", "1"])
+def test_conv_mask_and_rows(rot, monkeypatch):
+    monkeypatch.setenv("SOILB200_CONV_ROT", rot)
     ln = _learned()
     rng = np.random.default_rng(3)
     x = bf16(rng.normal(size=(1, 40, 130, 32)))
