@@ -544,7 +544,7 @@ REPOSE_SCALES = (1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5)
 
 
 def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: float = 1e-4,
-               seed: int = 1):
+               seed: int = 1, surface=None, label=None):
     """Second headline metric: ms to repose at 701^2 after the cut, the learned
     proposal (tensor-core conv net, flux form, exact quanta) + plain sweeps
     against plain sweeps alone, same tolerance (eps * dx m), same start.  The
@@ -558,7 +558,7 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
     if not DEFAULT_WEIGHTS.exists():
         raise SystemExit(f"trained weights missing: {DEFAULT_WEIGHTS} (python -m soilb200.train_repose)")
     net = learned.ReposeNet.load(DEFAULT_WEIGHTS)
-    b = c1_after_cut(seed=seed)
+    b = c1_after_cut(seed=seed) if surface is None else surface
     k, datum = soilb200.choose_quantization(b)
     tol = eps_slope * DX
     q = 2.0 ** k
@@ -601,11 +601,13 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
         g.close()
     pm = statistics.median(p[0] for p in plain)
     lm = statistics.median(p[0] for p in learn)
-    return {"metric": "ms to repose at 701^2 after the cut, learned proposal + plain sweeps (35 deg, eps 1e-4)",
+    n = b.shape[0]
+    return {"metric": f"ms to repose at {n}^2 after the cut, learned proposal + plain sweeps (35 deg, eps 1e-4)",
             "value": lm, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": lm, "higher_is_better": False, "dtype": "int32-quanta (bf16 net, f32 accumulate)",
-            "data": f"synthetic (config-1 pile, seed {seed}, after the full straight cut)",
-            "config": {"workload": "repose_701", "seed": seed, "proposal_rounds": rounds,
+            "data": label or f"synthetic (config-1 pile, seed {seed}, after the full straight cut)",
+            "config": {"workload": "repose_701" if surface is None else "repose_site_4096",
+                       "seed": seed, "proposal_rounds": rounds,
                        "proposal_scales": list(scales),
                        "plain_sweeps_between_proposals": plain_between, "tolerance_m": tol,
                        "plain_ms": pm, "speedup_vs_plain": pm / lm,
@@ -728,7 +730,7 @@ def main():
                     help="leave the learned-repose sub-object out of the default line")
     ap.add_argument("--workload", default="config1_plain_path_701",
                     choices=["config1_plain_path_701", "mobile_v2_4096", "batched_c2_512",
-                             "repose_701", "site_c4_4096"])
+                             "repose_701", "site_c4_4096", "repose_site_4096"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.stages:
@@ -748,6 +750,12 @@ def main():
         return
     if args.workload == "repose_701":
         print(json.dumps(run_repose(args)))
+        return
+    if args.workload == "repose_site_4096":
+        from soilb200 import workloads
+        site = workloads.site_after_cuts(workloads.config4(4096, seed=4, dx=DX))
+        print(json.dumps(run_repose(args, surface=site, seed=4, label=(
+            "synthetic (config-4 site, seed 4, after all 64 cuts ran their full travel)"))))
         return
     if world > 1:
         import datetime

@@ -272,6 +272,26 @@ class SiteCut:
         return self._flat[inside], self._target[inside]
 
 
+    def swept(self):
+        """Flat indices of every cell the footprint covers over the whole
+        travel (leading edge from 0 to ``travel``, trailing edge ``length``
+        behind it) and their target surfaces."""
+        inside = ((self._along <= self.travel) & (self._along >= -self.length)
+                  & (np.abs(self._across) <= 0.5 * self.width))
+        return self._flat[inside], self._target[inside]
+
+
+def site_after_cuts(cfg) -> np.ndarray:
+    """b_eff of a config-4 site after all its cuts have run their full travel
+    (every swept cell lowered to its target surface)."""
+    b = cfg["b_eff"].copy()
+    flat = b.reshape(-1)
+    for cut in cfg["cuts"]:
+        idx, tgt = cut.swept()
+        flat[idx] = np.minimum(flat[idx], tgt)
+    return b
+
+
 def merged_footprint(cuts, t_s: float):
     """Union of several cuts' footprints: each cell once, at its lowest target."""
     parts = [c.footprint(t_s) for c in cuts]
