@@ -330,7 +330,7 @@ int sb_path_step(sb_ctx* ctx, double dt_s, const int32_t* cut_flat_indices,
 int sb_path_reset(sb_ctx* ctx);
 /* Device-time breakdown of the last sb_path_step when the context was created
  * with SOILB200_STAGE_EVENTS=1 (event nodes between the stages of the step
- * graph: start, entrainment, before-ledger, substep loop + yield/union-find
+ * graph: start + entrainment, before-ledger, substep loop + yield/union-find
  * tile pass, border merge, compression, reduction/classification, previous
  * mask + seeding, residual frontier).  No counterpart in the reference (a
  * profiling aid).  Returns the number of stage times written (ms), 0 when

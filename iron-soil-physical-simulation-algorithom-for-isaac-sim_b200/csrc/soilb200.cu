@@ -845,6 +845,7 @@ int sb_ctx_create(const sb_grid_desc* desc, sb_ctx** out) {
   SB_CUDA(ctx, cudaMalloc(&ctx->xidx, n * 4));
   SB_CUDA(ctx, cudaMalloc(&ctx->xval, n * 8));
   SB_CUDA(ctx, cudaMalloc(&ctx->xout, sizeof(ExchangeOut)));
+  SB_CUDA(ctx, cudaMemsetAsync(ctx->xout, 0, sizeof(ExchangeOut), ctx->stream));  // arrive = 0
   static_assert(offsetof(ExchangeOut, momentum_w) == offsetof(ExchangeOut, volume_w_fp64) + 8,
                 "exchange_fold writes volume and momentum sums as one array");
   SB_CUDA(ctx, cudaMalloc(&ctx->xpart, 3 * 148 * 8 * sizeof(double)));
@@ -2245,25 +2246,18 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     prev = ev;
     return SB_OK;
   };
-  // 1. step start (loop control, cleared records), cut entrainment
-  {
-    void* in_dev = nullptr;
-    SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
-    void* args[] = {(void*)&ctx->ctl, &in_dev, (void*)&ctx->dt_dev, (void*)&ctx->path_count,
-                    (void*)&ctx->xout, (void*)&ctx->lout};
-    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_begin_kernel, dim3(1), 0, args)))
-      return rc;
-    prev = node;
-    if ((rc = mark())) return rc;
-  }
+  // 1. step start (loop control, cleared labelling record) fused with the cut
+  // entrainment
   {
     int pitch = ctx->pitch;
     int nyv = ny, nxv = nx;
-    void *idx_dev = nullptr, *val_dev = nullptr;
+    void *idx_dev = nullptr, *val_dev = nullptr, *in_dev = nullptr;
     SB_CUDA(ctx, cudaHostGetDevicePointer(&idx_dev, ctx->path_idx, 0));
     SB_CUDA(ctx, cudaHostGetDevicePointer(&val_dev, ctx->path_val, 0));
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
     void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
-                    &ctx->ctl, &idx_dev, &val_dev, &ctx->path_count, &ctx->xout, &ctx->xpart};
+                    &ctx->ctl, &idx_dev, &val_dev, &in_dev, &ctx->dt_dev, &ctx->xout,
+                    &ctx->lout, &ctx->xpart};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_entrain_kernel<FX>, dim3(64), 0, args)))
       return rc;
     prev = node;
@@ -2294,16 +2288,11 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
   SB_CUDA(ctx, cudaGraphAddEventRecordNode(&node, g, &prev, 1, ctx->ev_loop[1]));
   prev = node;
   // The after-step ledger and the labelling chain both only read the final
-  // state: they run as two branches of the graph (the ledger's final fold on
-  // one SM overlaps the labelling) and join at the component reduction.
+  // state: the ledger runs as a second branch that starts after the yield /
+  // tile union-find pass (which fills the SMs on its own) and overlaps the
+  // border merge and compression (short dependent chains that leave the SMs
+  // idle); the branches join at the component reduction.
   cudaGraphNode_t n_after;
-  {
-    std::vector<void*> args;
-    ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode1, &h_mob, &no_h, args);
-    if ((rc = add_kernel(ctx, g, &n_after, &prev, 1, (void*)ledger_kernel<FX>,
-                         dim3(ctx->ledger_blocks), 0, args.data())))
-      return rc;
-  }
   // 3. labelling
   LabelConst lc;
   lc = make_label_const(ctx, &p->label);
@@ -2316,6 +2305,13 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
                          0, args, kLabelInitThreads)))
       return rc;
     prev = node;
+  }
+  {
+    std::vector<void*> args;
+    ledger_args<FX>(ctx, fc, &dat, &static_limit, &mode1, &h_mob, &no_h, args);
+    if ((rc = add_kernel(ctx, g, &n_after, &prev, 1, (void*)ledger_kernel<FX>,
+                         dim3(ctx->ledger_blocks), 0, args.data())))
+      return rc;
     if ((rc = mark())) return rc;
   }
   {
