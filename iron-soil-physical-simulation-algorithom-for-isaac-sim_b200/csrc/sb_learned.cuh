@@ -33,6 +33,9 @@
 namespace sb {
 
 constexpr int kConvThreads = 128;   // 4 warps: TMEM lanes 0..127 = tile pixels
+// Forward kernel: the four pixel warps plus one warp whose lane 0 issues the
+// MMAs, so that a row's MMA issue overlaps the pixel warps' epilogue.
+constexpr int kConvFwdThreads = 160;
 constexpr int kConvTileOut = 128;   // output pixels per CTA row tile
 
 // ---------------------------------------------------------------- tcgen05
@@ -156,10 +159,10 @@ struct ConvSmem {
 
 // Starts the asynchronous copy of input row r (pixels x0-1 .. x0+128) into
 // a ring slot; 16-byte cp.async chunks, zero-filled outside the image.
-template <int CIN>
+template <int CIN, int NT = kConvThreads>
 __device__ __forceinline__ void conv_row_async(const __nv_bfloat16* __restrict__ in, int b, int h,
                                                int w, int r, int x0, unsigned char* slot) {
-  for (int j = threadIdx.x; j < kRowPixels; j += kConvThreads) {
+  for (int j = threadIdx.x; j < kRowPixels; j += NT) {
     const int x = x0 - 1 + j;
     const bool ok = r >= 0 && r < h && x >= 0 && x < w;
     const __nv_bfloat16* src = in + (((size_t)b * h + (ok ? r : 0)) * w + (ok ? x : 0)) * CIN;
@@ -225,7 +228,7 @@ __device__ __forceinline__ void conv_issue_row(uint32_t tmem, uint32_t ring_base
 // tensor core's shared-memory operand reads -- 40 wavefronts per
 // M128 x N32 x K16 MMA -- not by the copies.)
 template <int CIN, int COUT>
-__global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs a) {
+__global__ void __launch_bounds__(kConvFwdThreads) conv3x3_tc_kernel(const ConvArgs a) {
   using S = ConvSmem<CIN, COUT>;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char* wsm = smem;
@@ -244,13 +247,13 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
   {
     const uint4* src = reinterpret_cast<const uint4*>(a.wpk);
     uint4* dst = reinterpret_cast<uint4*>(wsm);
-    for (int i = tid; i < S::W_BYTES / 16; i += kConvThreads) dst[i] = src[i];
+    for (int i = tid; i < S::W_BYTES / 16; i += kConvFwdThreads) dst[i] = src[i];
   }
   if (tid == 0) mbar_init(bar, 1);
   if (warp == 0) tmem_alloc(tslot, S::TMEM_COLS);
-  conv_row_async<CIN>(a.in, b, a.h, a.w, y0 - 1, x0, slot(y0 - 1));
-  conv_row_async<CIN>(a.in, b, a.h, a.w, y0, x0, slot(y0));
-  conv_row_async<CIN>(a.in, b, a.h, a.w, y0 + 1, x0, slot(y0 + 1));
+  conv_row_async<CIN, kConvFwdThreads>(a.in, b, a.h, a.w, y0 - 1, x0, slot(y0 - 1));
+  conv_row_async<CIN, kConvFwdThreads>(a.in, b, a.h, a.w, y0, x0, slot(y0));
+  conv_row_async<CIN, kConvFwdThreads>(a.in, b, a.h, a.w, y0 + 1, x0, slot(y0 + 1));
   conv_row_wait();
   fence_async_smem();  // the weights (generic stores) too
   tc_fence_before();
@@ -259,48 +262,52 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const ConvArgs
   const uint32_t tmem = *tslot;
   const uint32_t idesc = umma_idesc_bf16(128, COUT);
   const uint32_t w_base = smem_u32(wsm), ring_base = smem_u32(ring);
-  const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  const bool issuer = tid == 4 * 32;  // lane 0 of warp 4
+  const bool pixel = warp < 4;         // the epilogue warps (TMEM lanes 0..127)
   unsigned phase = 0;
   bool ok = true;
   int issued = y0 + 1;  // last input row whose copy has been started
   if (y0 < y1) {
-    if (tid == 0) {
+    if (issuer) {
       conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y0, idesc);
       umma_commit(bar);
     }
     // rows up to y1 are read (the last MMA batch, row y1-1, reads y1)
     for (int r = y0 + 2; r <= y0 + S::SLOTS - 2 && r <= y1; ++r) {
-      conv_row_async<CIN>(a.in, b, a.h, a.w, r, x0, slot(r));
+      conv_row_async<CIN, kConvFwdThreads>(a.in, b, a.h, a.w, r, x0, slot(r));
       issued = r;
     }
   }
 
   for (int y = y0; y < y1; ++y) {
-    ok = mbar_wait(bar, phase) && ok;
-    phase ^= 1;
-    tc_fence_after();
     float d[COUT];  // this thread's pixel of the output row
-    if constexpr (COUT == 32)
-      tmem_ld32(lane_addr, d);
-    else
-      tmem_ld16(lane_addr, d);
+    if (pixel) {
+      ok = mbar_wait(bar, phase) && ok;
+      tc_fence_after();
+      if constexpr (COUT == 32)
+        tmem_ld32(lane_addr, d);
+      else
+        tmem_ld16(lane_addr, d);
+    }
+    phase ^= 1;
     tc_fence_before();
     if (y + 1 < y1) conv_row_wait_pending(issued - (y + 2));  // row y+2 has landed
     __syncthreads();                                         // everyone has read the accumulator
     if (y + 1 < y1) {
-      if (tid == 0) {
+      if (issuer) {
         tc_fence_after();
         conv_issue_row<CIN, COUT>(tmem, ring_base, w_base, y + 1, idesc);
         umma_commit(bar);
       }
       // the slot of row y-1 (= row y-1+SLOTS) is free: row y's MMAs have completed
       if (issued + 1 <= y1 && issued + 1 <= y + S::SLOTS - 1) {
-        conv_row_async<CIN>(a.in, b, a.h, a.w, issued + 1, x0, slot(issued + 1));
+        conv_row_async<CIN, kConvFwdThreads>(a.in, b, a.h, a.w, issued + 1, x0, slot(issued + 1));
         ++issued;
       }
     }
     const int xo = x0 + tid;
-    if (xo < a.w) {
+    if (pixel && xo < a.w) {
       const size_t pix = ((size_t)b * a.h + y) * a.w + xo;
 #pragma unroll
       for (int c8 = 0; c8 < COUT; c8 += 8) {

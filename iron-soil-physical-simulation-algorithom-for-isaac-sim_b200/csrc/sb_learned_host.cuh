@@ -34,7 +34,7 @@ cudaError_t launch_conv(const ConvArgs& a, int rows, cudaStream_t st) {
   if (rot)
     conv3x3_rot_kernel<CIN, COUT><<<grid, kConvThreads, ConvRotSmem<CIN, COUT>::BYTES, st>>>(a);
   else
-    conv3x3_tc_kernel<CIN, COUT><<<grid, kConvThreads, ConvSmem<CIN, COUT>::BYTES, st>>>(a);
+    conv3x3_tc_kernel<CIN, COUT><<<grid, kConvFwdThreads, ConvSmem<CIN, COUT>::BYTES, st>>>(a);
   return cudaGetLastError();
 }
 
