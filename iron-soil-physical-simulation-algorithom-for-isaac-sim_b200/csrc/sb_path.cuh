@@ -138,18 +138,27 @@ __global__ void __launch_bounds__(kThreads)
   __syncthreads();
   if (threadIdx.x == 0) last = atomicAdd(&out->arrive, 1u) == gridDim.x - 1 ? 1 : 0;
   __syncthreads();
-  if (!last || threadIdx.x != 0) return;
+  if (!last) return;
   __threadfence();
+  // the block partials land in shared memory in parallel (gridDim.x <=
+  // kThreads), then one thread adds them in block order: deterministic
+  __shared__ double vpart[kThreads];
+  __shared__ int fpart[kThreads];
+  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+    vpart[k] = __ldcg(bpart + k);
+    fpart[k] = __ldcg(bpart + gridDim.x + k) != 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
   long long tq = 0;
   double ts = 0.0;
   int tb = 0;
-  for (int k = 0; k < (int)gridDim.x; ++k) {  // block order: deterministic
-    const double x = __ldcg(bpart + k);
+  for (int k = 0; k < (int)gridDim.x; ++k) {
     if constexpr (FX)
-      tq += __double_as_longlong(x);
+      tq += __double_as_longlong(vpart[k]);
     else
-      ts += x;
-    tb |= __ldcg(bpart + gridDim.x + k) != 0.0;
+      ts += vpart[k];
+    tb |= fpart[k];
   }
   out->volume_w6_quanta = tq;
   out->volume_w_fp64 = ts;
