@@ -53,40 +53,44 @@ struct PathInput {
   int pad;
 };
 
-// Step start fused with the bucket-cut entrainment to target surfaces (one
-// node instead of two).  Every block reads the command length from the
-// host-mapped inputs (uncached, once per block); idx / target are the
-// host-mapped command (read once each, uncached).  Each block stores its
-// volume sum and bad-index flag as partials; the last block to finish folds
-// them in block order and WRITES the exchange record (so it needs no clearing
-// beforehand), clears the labelling record for this step, and starts the
-// Mobile V2 loop control from the host-mapped dt (fv_begin).  The entrained
-// cells' h lives in the current ping-pong buffer, which fv_begin leaves as is.
+// Step start: dt and the cut command length from the host-mapped inputs into
+// device copies, the Mobile V2 loop control for dt (fv_begin) and cleared
+// exchange and labelling records.  One block.
+__global__ void path_begin_kernel(FvControl* ctl, const PathInput* in, double* dt_dev,
+                                  int* count_dev, ExchangeOut* xout, LabelOut* lout) {
+  if (threadIdx.x == 0) {
+    *dt_dev = __ldcv(&in->dt);
+    *count_dev = __ldcv(&in->count);
+    fv_begin_body(ctl, dt_dev);
+  }
+  unsigned* xw = reinterpret_cast<unsigned*>(xout);
+  unsigned* lw = reinterpret_cast<unsigned*>(lout);
+  for (int k = threadIdx.x; k < (int)(sizeof(ExchangeOut) / 4); k += blockDim.x) xw[k] = 0u;
+  for (int k = threadIdx.x; k < (int)(sizeof(LabelOut) / 4); k += blockDim.x) lw[k] = 0u;
+}
+
+// Bucket-cut entrainment to target surfaces; the command length is read on
+// the device so the graph is independent of it (mode 1 of entrain_kernel).
+// idx / target are the host-mapped command (read once each, uncached).
 template <bool FX>
 __global__ void __launch_bounds__(kThreads)
     path_entrain_kernel(int ny, int nx, int pitch, double Q, double datum, double f,
                         typename FvTypes<FX>::B* __restrict__ b,
                         const typename FvTypes<FX>::B* __restrict__ z,
                         typename FvTypes<FX>::H* __restrict__ h0,
-                        typename FvTypes<FX>::H* __restrict__ h1, FvControl* ctl,
-                        const int32_t* __restrict__ idx, const double* __restrict__ target,
-                        const PathInput* in, double* dt_dev, ExchangeOut* out, LabelOut* lout,
-                        double* __restrict__ part) {
-  __shared__ int count;
-  __shared__ int last;
-  __shared__ long long qsum[kThreads / 32];
-  __shared__ int bsum[kThreads / 32];
-  if (threadIdx.x == 0) count = __ldcv(&in->count);
-  __syncthreads();
+                        typename FvTypes<FX>::H* __restrict__ h1,
+                        const FvControl* ctl, const int32_t* __restrict__ idx,
+                        const double* __restrict__ target, const int* count_dev,
+                        ExchangeOut* out, double* __restrict__ part) {
+  const int count = *count_dev;
   typename FvTypes<FX>::H* h = ctl->parity ? h1 : h0;
   long long vq = 0;
   double vs = 0.0;
-  int bad = 0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
     const int i = __ldcv(idx + k);
     const double tk = __ldcv(target + k);
     if (i < 0 || i >= ny * nx) {
-      bad = 1;
+      atomicExch(&out->bad_index, 1);
       continue;
     }
     const int r = i / nx, c = i % nx;
@@ -108,68 +112,14 @@ __global__ void __launch_bounds__(kThreads)
       vs += d * ((double)w6 * f);
     }
   }
-  // block partials: slot 0 = volume (FX: the int64 bits), slot 1 = bad flag
-  double* bpart = part;
   if constexpr (FX) {
     vq = (long long)warp_sum_u64((unsigned long long)vq);
-    const int wb = __any_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0) {
-      qsum[threadIdx.x >> 5] = vq;
-      bsum[threadIdx.x >> 5] = wb;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      long long t = 0;
-      int bb = 0;
-      for (int w = 0; w < kThreads / 32; ++w) {
-        t += qsum[w];
-        bb |= bsum[w];
-      }
-      bpart[blockIdx.x] = __longlong_as_double(t);
-      bpart[gridDim.x + blockIdx.x] = bb ? 1.0 : 0.0;
-    }
+    if ((threadIdx.x & 31) == 0 && vq)
+      atomicAdd((unsigned long long*)&out->volume_w6_quanta, (unsigned long long)vq);
   } else {
-    __shared__ double fold[fold_words(2)];
-    const double v[2] = {vs, bad ? 1.0 : 0.0};
-    const double* bt = block_fold<double, 2, 1>(v, fold);  // slot 1: maximum
-    if (threadIdx.x < 2) bpart[(size_t)threadIdx.x * gridDim.x + blockIdx.x] = bt[threadIdx.x];
+    const double v[1] = {vs};
+    exchange_fold<1>(v, part, &out->arrive, &out->volume_w_fp64);
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) last = atomicAdd(&out->arrive, 1u) == gridDim.x - 1 ? 1 : 0;
-  __syncthreads();
-  if (!last) return;
-  __threadfence();
-  // the block partials land in shared memory in parallel (gridDim.x <=
-  // kThreads), then one thread adds them in block order: deterministic
-  __shared__ double vpart[kThreads];
-  __shared__ int fpart[kThreads];
-  for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
-    vpart[k] = __ldcg(bpart + k);
-    fpart[k] = __ldcg(bpart + gridDim.x + k) != 0.0;
-  }
-  __syncthreads();
-  if (threadIdx.x != 0) return;
-  long long tq = 0;
-  double ts = 0.0;
-  int tb = 0;
-  for (int k = 0; k < (int)gridDim.x; ++k) {
-    if constexpr (FX)
-      tq += __double_as_longlong(vpart[k]);
-    else
-      ts += vpart[k];
-    tb |= fpart[k];
-  }
-  out->volume_w6_quanta = tq;
-  out->volume_w_fp64 = ts;
-  out->momentum_w[0] = 0.0;
-  out->momentum_w[1] = 0.0;
-  out->bad_index = tb;
-  out->arrive = 0u;
-  unsigned* lw = reinterpret_cast<unsigned*>(lout);
-  for (int k = 0; k < (int)(sizeof(LabelOut) / 4); ++k) lw[k] = 0u;
-  *dt_dev = __ldcv(&in->dt);
-  fv_begin_body(ctl, dt_dev);
 }
 
 // Classification, persistence and gating (reference gpu_large_avalanche.py

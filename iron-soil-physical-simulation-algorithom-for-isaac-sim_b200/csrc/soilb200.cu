@@ -2246,18 +2246,25 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     prev = ev;
     return SB_OK;
   };
-  // 1. step start (loop control, cleared labelling record) fused with the cut
-  // entrainment
+  // 1. step start (loop control, cleared records), cut entrainment
+  {
+    void* in_dev = nullptr;
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
+    void* args[] = {(void*)&ctx->ctl, &in_dev, (void*)&ctx->dt_dev, (void*)&ctx->path_count,
+                    (void*)&ctx->xout, (void*)&ctx->lout};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_begin_kernel, dim3(1), 0, args)))
+      return rc;
+    prev = node;
+    if ((rc = mark())) return rc;
+  }
   {
     int pitch = ctx->pitch;
     int nyv = ny, nxv = nx;
-    void *idx_dev = nullptr, *val_dev = nullptr, *in_dev = nullptr;
+    void *idx_dev = nullptr, *val_dev = nullptr;
     SB_CUDA(ctx, cudaHostGetDevicePointer(&idx_dev, ctx->path_idx, 0));
     SB_CUDA(ctx, cudaHostGetDevicePointer(&val_dev, ctx->path_val, 0));
-    SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
     void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
-                    &ctx->ctl, &idx_dev, &val_dev, &in_dev, &ctx->dt_dev, &ctx->xout,
-                    &ctx->lout, &ctx->xpart};
+                    &ctx->ctl, &idx_dev, &val_dev, &ctx->path_count, &ctx->xout, &ctx->xpart};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_entrain_kernel<FX>, dim3(64), 0, args)))
       return rc;
     prev = node;

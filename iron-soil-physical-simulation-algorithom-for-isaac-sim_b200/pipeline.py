@@ -143,7 +143,7 @@ class PlainPath:
                              diag.largest_connected_cell_count, rounds,
                              float(mob.volume_after_m3), float(mob.maximum_speed_m_s))
 
-    STAGES = ("start_and_entrainment", "before_ledger", "substeps_and_yield_tiles", "border_merge",
+    STAGES = ("start", "entrainment", "before_ledger", "substeps_and_yield_tiles", "border_merge",
               "compression", "reduction_classification", "previous_and_seeds", "residual_frontier")
 
     def stage_times(self) -> dict:
