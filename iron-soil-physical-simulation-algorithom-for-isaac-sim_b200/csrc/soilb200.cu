@@ -579,6 +579,16 @@ static int mobile_step_host_loop(sb_ctx* ctx, const FvConst& c, double static_li
   SB_CUDA(ctx, cudaLaunchKernel((void*)ledger_kernel<FX>, dim3(ctx->ledger_blocks), dim3(kThreads),
                                 args.data(), 0, ctx->stream));
   SB_CUDA(ctx, cudaEventRecord(ctx->ev_loop[0], ctx->stream));
+  if (FX && ctx->fv_stream && ctx->fv_persistent) {
+    // the step graph's persistent substep loop, as one cooperative launch
+    void* pargs[] = {(void*)&cc,         (void*)&ctx->b,     (void*)&ctx->h[0],  (void*)&ctx->h[1],
+                     (void*)&ctx->qx[0], (void*)&ctx->qx[1], (void*)&ctx->qy[0], (void*)&ctx->qy[1],
+                     (void*)&ctx->ext_x, (void*)&ctx->ext_y, (void*)&ctx->ctl,   (void*)&ctx->fv_diag};
+    void* fn = ctx->fv_exact ? (void*)fv_loop_kernel<false>
+                             : const_cast<void*>(fv_loop_fast_kernel());
+    SB_CUDA(ctx, cudaLaunchCooperativeKernel(fn, dim3(ctx->fv_stream_blocks), dim3(kThreads),
+                                             pargs, 0, ctx->stream));
+  }
   FvLaunch L;
   fv_launch<FX>(ctx, cc, &handle, &no_handle, L);
   for (int it = 0; it <= c.max_substeps; ++it) {
@@ -1167,10 +1177,12 @@ int sb_mobile_step(sb_ctx* ctx, double dt_s, const sb_mobile_params* params, sb_
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   const FvControl& k = *ctx->ctl_host;
   // graph: begin, two ledgers, records + two substep launches per loop
-  // iteration; host loop: begin, two ledgers + one launch per substep
-  ctx->launches += !ctx->use_graphs ? 3 + k.substeps
-                   : (fx(ctx) && ctx->fv_stream && ctx->fv_persistent) ? 5
-                                                                        : 4 + (k.substeps + 1) / 2 * 2;
+  // iteration; host loop: begin, two ledgers + one launch per substep; the
+  // persistent loop is one launch either way
+  const bool pers = fx(ctx) && ctx->fv_stream && ctx->fv_persistent;
+  ctx->launches += !ctx->use_graphs ? 3 + (pers ? 1 : k.substeps)
+                   : pers           ? 5
+                                    : 4 + (k.substeps + 1) / 2 * 2;
   rc = fill_mobile_stats(ctx, params, out);
   if (rc) return rc;
   if (k.status == SB_ERR_POSITIVITY) return fail(ctx, SB_ERR_POSITIVITY, "MobileV2 positivity failure");
