@@ -285,7 +285,7 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     wet_cells = int(np.count_nonzero(h_fx > 0.0))
     site_extra = site_report(path, st, h_fx, local_rank) if site else None
     ref64 = PlainPath(cfg["b_eff"], cfg["z_base"], dx=DX, material=material(),
-                      device=local_rank, residual="gated", precision="fp64")
+                      device=local_rank, residual="gated", precision="fp64", fused=fused)
     for k in range(total_steps):
         idx, tgt = sched[k]
         ref64.step(DT, idx, tgt)
