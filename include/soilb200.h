@@ -535,6 +535,16 @@ int sb_learned_loss(const float* flux, const float* target_dh, float* resid, voi
                     double* loss_part, int batch, int h, int w, double dx, double dy,
                     double tan_crit, float inv_scale2_n, void* stream);
 int sb_learned_loss_blocks(int batch, int h, int w);
+/* Inference of the whole 4-layer network in one launch: features bf16
+ * [batch][h][w][16] -> f32 fluxes [batch][h][w][4] (the last layer's first
+ * four channels), equal bit for bit to the four sb_learned_conv calls (ReLU
+ * after the first three, BF16 activations).  w1..w4: packed weights of the
+ * layers 16->32, 32->32, 32->32, 32->16.  rows_per_cta = 0 picks about one
+ * wave of CTAs.  Activations stay in shared memory: one CTA per SM streams a
+ * 122-pixel column strip down a band of rows. */
+int sb_learned_forward(const void* feat, float* flux, const void* w1, const void* w2,
+                       const void* w3, const void* w4, int batch, int h, int w, int rows_per_cta,
+                       int* d_status, void* stream);
 /* On a context's resident b_eff (SB_FX32): features, then the network's
  * fluxes (f32 [ny][nx][4]) applied in whole height quanta (tq: int32
  * [ny][nx][4] scratch). */

@@ -300,6 +300,9 @@ _PROTOTYPES = {
                                            C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double,
                                            C.c_double, C.c_double, C.c_float, C.c_void_p]),
     "sb_learned_loss_blocks": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "sb_learned_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                     C.c_void_p, C.c_void_p]),
     "sb_learned_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_double]),
     "sb_learned_apply": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double]),
 }

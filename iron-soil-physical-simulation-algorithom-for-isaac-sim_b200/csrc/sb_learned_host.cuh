@@ -157,6 +157,56 @@ int sb_learned_loss(const float* flux, const float* target_dh, float* resid, voi
   return lcuda(cudaGetLastError());
 }
 
+// The whole network's forward pass in one kernel (inference only): features
+// bf16 [batch][h][w][16] in, the last layer's first four channels as f32
+// [batch][h][w][4] out; w1..w4 are the layers' packed weights.
+int sb_learned_forward(const void* feat, float* flux, const void* w1, const void* w2,
+                       const void* w3, const void* w4, int batch, int h, int w, int rows_per_cta,
+                       int* d_status, void* stream) {
+  if (!feat || !flux || !w1 || !w2 || !w3 || !w4 || batch <= 0 || h <= 0 || w <= 0 ||
+      rows_per_cta < 0 || batch > 65535)
+    return lfail(SB_ERR_BAD_ARG, "[soilb200] forward: bad arguments");
+  if (((uintptr_t)feat | (uintptr_t)flux | (uintptr_t)w1 | (uintptr_t)w2 | (uintptr_t)w3 |
+       (uintptr_t)w4) & 15)
+    return lfail(SB_ERR_BAD_ARG, "[soilb200] forward: buffers must be 16-byte aligned");
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return lfail(SB_ERR_CUDA, "[soilb200] forward: cuTensorMapEncodeTiled unavailable");
+  // features as a 4-D tensor (channel, x, y, image); one box = one channel
+  // chunk of a staged row: 8 channels x 130 pixels, zeros outside the image
+  CUtensorMap map;
+  const cuuint64_t dims[4] = {16, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)batch};
+  const cuuint64_t strides[3] = {32, (cuuint64_t)w * 32, (cuuint64_t)w * (cuuint64_t)h * 32};
+  const cuuint32_t box[4] = {8, (cuuint32_t)kRowPixels, 1, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(feat), dims, strides, box,
+          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return lfail(SB_ERR_CUDA, "[soilb200] forward: feature tensor map rejected");
+  const int strips = (w + kNetTileOut - 1) / kNetTileOut;
+  int rows = rows_per_cta;
+  if (rows == 0) {  // one CTA per SM: about one wave over the 148 SMs
+    const long long per_band = (long long)strips * batch;
+    const int bands = per_band >= 148 ? 1 : (int)(148 / per_band);
+    rows = (h + bands - 1) / bands;
+  }
+  static bool attr_set[16] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 16 && !attr_set[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(net_forward_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         NetSmem::BYTES);
+    if (e != cudaSuccess) return lcuda(e);
+    attr_set[dev] = true;
+  }
+  NetArgs a{{(const __nv_bfloat16*)w1, (const __nv_bfloat16*)w2, (const __nv_bfloat16*)w3,
+             (const __nv_bfloat16*)w4},
+            flux, batch, h, w, rows, d_status};
+  dim3 grid(strips, (h + rows - 1) / rows, batch);
+  net_forward_kernel<<<grid, kNetThreads, NetSmem::BYTES, (cudaStream_t)stream>>>(map, a);
+  return lcuda(cudaGetLastError());
+}
+
 int sb_learned_loss_blocks(int batch, int h, int w) {
   return grid_for((long long)batch * h * w);
 }

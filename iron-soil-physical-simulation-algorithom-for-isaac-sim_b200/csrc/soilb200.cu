@@ -37,6 +37,7 @@
 #include "sb_path.cuh"
 #include "sb_batch.cuh"
 #include "sb_learned.cuh"
+#include "sb_learned_net.cuh"
 
 using namespace sb;
 

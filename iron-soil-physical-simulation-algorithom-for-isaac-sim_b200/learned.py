@@ -164,6 +164,24 @@ def network_forward(net: ReposeNet, feat, packed=None, stream=None):
     return acts, a
 
 
+def network_forward_fused(net: ReposeNet, feat, packed=None, stream=None, rows: int = 0):
+    """The f32 fluxes [B, H, W, 4] of the whole network in one kernel
+    (inference: no activations are kept).  Equal bit for bit to
+    ``network_forward``'s output; ``rows`` = rows per CTA (0: about one wave)."""
+    torch = _torch()
+    packed = packed or net.packed()
+    b, h, w, c = feat.shape
+    if c != LAYERS[0][0]:
+        raise ValueError(f"[soilb200] features have {c} channels, expected {LAYERS[0][0]}")
+    flux = torch.empty(b, h, w, 4, dtype=torch.float32, device=feat.device)
+    st = stream if stream is not None else torch.cuda.current_stream(feat.device).cuda_stream
+    _ok(_lib.load().sb_learned_forward(feat.data_ptr(), flux.data_ptr(), packed[0].data_ptr(),
+                                       packed[1].data_ptr(), packed[2].data_ptr(),
+                                       packed[3].data_ptr(), b, h, w, int(rows),
+                                       net.status.data_ptr(), st), "forward")
+    return flux
+
+
 def features_f64(heights, dx: float, dy: float, tan_crit: float):
     """BF16 features [B, H, W, 16] of float64 device heights [B, H, W]."""
     torch = _torch()
@@ -257,8 +275,10 @@ class LearnedRelaxation:
     """Learned proposal rounds on a fixed-point grid's resident b_eff, then the
     plain sweep to the tolerance."""
 
-    def __init__(self, grid, net: ReposeNet, critical_angle_deg: float) -> None:
+    def __init__(self, grid, net: ReposeNet, critical_angle_deg: float,
+                 fused: bool = True) -> None:
         torch = _torch()
+        self.fused = bool(fused)  # False: one launch per layer (the training path's kernels)
         if grid.precision != "fx32":
             raise ValueError("[soilb200] the learned proposal runs on fx32 grids")
         self.grid = grid
@@ -288,8 +308,12 @@ class LearnedRelaxation:
                 _lib.check(self.grid.ctx, lib.sb_learned_features(self.grid.ctx,
                                                                   self._feat.data_ptr(),
                                                                   self.tan_crit), "features")
-                _, flux = network_forward(self.net, self._feat, self._packed,
-                                          stream=self._stream)
+                if self.fused:
+                    flux = network_forward_fused(self.net, self._feat, self._packed,
+                                                 stream=self._stream)
+                else:
+                    _, flux = network_forward(self.net, self._feat, self._packed,
+                                              stream=self._stream)
                 # the transfer is flux * tan * dx, so the scale rides on tan
                 _lib.check(self.grid.ctx, lib.sb_learned_apply(self.grid.ctx, flux.data_ptr(),
                                                                self._tq.data_ptr(),

@@ -4,6 +4,9 @@ The CPU oracle (oracle/learned.py, float64) is the checker:
 * forward convolutions (the nine-tap kernel and the rotating-accumulator
   kernel, SOILB200_CONV_ROT=1): f32 outputs within 1e-4 of the largest |value|
   (FP32 accumulation of exact BF16 products), BF16 outputs within BF16 rounding;
+* the one-kernel inference of the whole network equals the four layer
+  launches bit for bit, and the float64 oracle network within 2e-2 of the
+  largest |value| (BF16 activations between layers);
 * weight gradients within 1e-4 (relative to the largest |value|);
 * full back-propagation of the training loss: the GPU keeps activations in
   BF16, so each layer's gradient is compared by relative L2 error <= 5e-2;
@@ -195,3 +198,38 @@ def test_scaled_proposal_schedule():
     sum1 = int(np.rint((grid.download("b_eff") - datum) * q).astype(np.int64).sum())
     assert sum1 == sum0
     grid.close()
+
+
+@pytest.mark.parametrize("b,h,w,rows", [(1, 701, 701, 0), (2, 37, 300, 0), (1, 130, 123, 5),
+                                        (1, 9, 250, 1), (3, 64, 128, 0), (1, 1, 5, 0)])
+def test_fused_forward_equals_layer_path(b, h, w, rows):
+    """One-kernel inference (activations in shared memory, 122-pixel strips,
+    two-row layer skew) equals the four layer launches bit for bit, on the
+    shipped network and on a random one, with every band height."""
+    ln = _learned()
+    from soilb200.train_repose import DEFAULT_WEIGHTS
+    rng = np.random.default_rng(b * 1000 + h + w)
+    feat = to_dev(bf16(rng.normal(size=(b, h, w, 16))), torch.bfloat16)
+    for net in (ln.ReposeNet.load(DEFAULT_WEIGHTS), ln.ReposeNet(seed=h + w)):
+        packed = net.packed()
+        _, ref = ln.network_forward(net, feat, packed)
+        got = ln.network_forward_fused(net, feat, packed, rows=rows)
+        torch.cuda.synchronize()
+        assert int(net.status.item()) == 0
+        assert got.shape == ref.shape
+        assert torch.equal(got, ref), float((got - ref).abs().max())
+
+
+def test_fused_forward_matches_oracle():
+    """The fused forward against the float64 oracle network on BF16-rounded
+    inputs and weights: within the BF16 rounding of the three hidden layers."""
+    ln = _learned()
+    rng = np.random.default_rng(17)
+    x = bf16(rng.normal(size=(1, 40, 260, 16)))
+    net = ln.ReposeNet(seed=5)
+    ws = [bf16(wt) for wt in net.numpy_weights()]
+    ref = L.forward(x, ws)[1][..., :4]
+    got = ln.network_forward_fused(net, to_dev(x, torch.bfloat16)).cpu().numpy()
+    assert int(net.status.item()) == 0
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 2e-2 * scale + 1e-6
