@@ -163,14 +163,16 @@ class ClockSampler:
                 "samples": len(self.samples), "source": self.source}
 
 
-# DRAM bytes (read + write) of one FV substep launch, from one ncu capture of
-# the same workload (dram__bytes_read.sum + dram__bytes_write.sum).
+# DRAM bytes (read + write) per FV substep, from one ncu capture of the
+# persistent substep-loop kernel on the same workload (dram__bytes_read.sum +
+# dram__bytes_write.sum of the launch, divided by the substeps it ran).
 NCU_TRAFFIC_BYTES = {
-    # fv_stream_kernel at 701^2, ncu --set full of one launch: 7.987712 MB read
-    # (cold L2 under ncu; the state fits in L2, so writes stay there)
-    "config1_plain_path_701": 7_987_712,
-    # fv_stream_kernel at 4096^2: 275.369216 MB read + 164.824064 MB written
-    "mobile_v2_4096": 440_193_280,
+    # fv_loop_kernel at 701^2, 3 substeps in the captured launch: 8.028672 MB
+    # read + 1.536 KB written (cold L2 under ncu; the state then stays in L2)
+    "config1_plain_path_701": (8_028_672 + 1_536) // 3,
+    # fv_loop_kernel at 4096^2, 4 substeps in the captured launch: 1.130031 GB
+    # read + 805.078784 MB written
+    "mobile_v2_4096": (1_130_031_000 + 805_078_784) // 4,
 }
 
 
@@ -329,14 +331,16 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
             "e2e": {"value": cell_substeps / wall if wall > 0 else 0.0, "unit": UNIT,
                     "h2d_bytes_per_step": h2d // max(args.steps, 1),
                     "d2h_bytes_per_step": d2h // max(args.steps, 1)},
-            "roofline": {"bound": "hbm", "kernel": "fv_stream_kernel (FX32 substep)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "fv_loop_kernel (FX32 persistent substep loop; per substep)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "mean_launch_ms": per_launch_ms,
                          "traffic": NCU_TRAFFIC_BYTES.get(args.workload),
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"},
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of one loop launch / its substeps"},
             "gpu_launches": int(launches),
             "clocks": clocks.summary(),
             "wet_cells": wet_cells,
@@ -435,7 +439,8 @@ def run_mobile_large(args, n: int = 4096):
                          "frac": ach / peak, "peak_source": kind, "mean_launch_ms": per,
                          "algorithmic_bytes_per_launch": alg,
                          "traffic": NCU_TRAFFIC_BYTES["mobile_v2_4096"],
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch"}}
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of one loop launch / its substeps"}}
 
 
 def _c2_cpu_patch(args):
@@ -557,6 +562,7 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
     if not DEFAULT_WEIGHTS.exists():
         raise SystemExit(f"trained weights missing: {DEFAULT_WEIGHTS} (python -m soilb200.train_repose)")
     net = learned.ReposeNet.load(DEFAULT_WEIGHTS)
+    fused_net = getattr(args, "net", "fused") == "fused"
     b = c1_after_cut(seed=seed) if surface is None else surface
     k, datum = soilb200.choose_quantization(b)
     tol = eps_slope * DX
@@ -569,7 +575,7 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
     for r in (0, rounds):
         g = soilb200.DeviceGrid(b.shape, DX, DX, precision="fx32", height_exponent=k, datum_m=datum)
         g.upload("z_base", np.zeros_like(b))
-        grids[r] = (g, learned.LearnedRelaxation(g, net, 35.0))
+        grids[r] = (g, learned.LearnedRelaxation(g, net, 35.0, fused=fused_net))
 
     def one(r):
         g, lr = grids[r]
@@ -607,6 +613,8 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
             "data": label or f"synthetic (config-1 pile, seed {seed}, after the full straight cut)",
             "config": {"workload": "repose_701" if surface is None else "repose_site_4096",
                        "seed": seed, "proposal_rounds": rounds,
+                       "network": ("one kernel for the four layers" if fused_net
+                                   else "one launch per layer"),
                        "proposal_scales": list(scales),
                        "plain_sweeps_between_proposals": plain_between, "tolerance_m": tol,
                        "plain_ms": pm, "speedup_vs_plain": pm / lm,
@@ -727,6 +735,9 @@ def main():
                     help="per-stage device times of the step graph (event nodes between stages)")
     ap.add_argument("--no-repose", action="store_true",
                     help="leave the learned-repose sub-object out of the default line")
+    ap.add_argument("--net", default="fused", choices=["fused", "layers"],
+                    help="repose workloads: the network's inference in one kernel or one "
+                         "launch per layer")
     ap.add_argument("--workload", default="config1_plain_path_701",
                     choices=["config1_plain_path_701", "mobile_v2_4096", "batched_c2_512",
                              "repose_701", "site_c4_4096", "repose_site_4096"])

@@ -21,17 +21,22 @@
 // B-3+L+u), so a layer trails the one before it by two rows: the rows it
 // reads were finished in an earlier round, and the four layers of a round
 // are independent.  Warp roles:
-//   warps 0-3  epilogue: TMEM lane = pixel slot; ReLU, BF16, into the ring
-//              (or the last layer's four f32 outputs to global memory);
-//   warp 4     one thread issues the MMAs (tcgen05.mma, accumulators double
+//   warps 0-15 epilogue, one group of four warps per layer (TMEM lane =
+//              pixel slot): ReLU, BF16, into the layer's ring (the last
+//              layer: its four f32 outputs to global memory).  A row's
+//              epilogue is a chain of dependent steps (TMEM load, convert,
+//              stores, proxy fence, arrival) of about a microsecond, so the
+//              four layers' epilogues run side by side;
+//   warp 16    one thread issues the MMAs (tcgen05.mma, accumulators double
 //              buffered per layer in TMEM);
-//   warp 5     one thread issues the TMA loads of feature rows (6-row ring).
+//   warp 17    one thread issues the TMA loads of feature rows (6-row ring).
 // Every hand-off is an mbarrier: feature row landed (TMA transaction bytes),
 // feature slot free and accumulator ready (tcgen05.commit), epilogue done
 // (128 arrivals: the accumulator buffer is free and the output row is in the
-// ring).  Ring slots need no barrier of their own: a slot is rewritten two
-// rounds after the MMAs that last read it, and the epilogue threads have
-// waited for those MMAs' completion (in issue order) in between.
+// ring).  Ring slots need no barrier of their own: layer L's use u rewrites
+// the slot of its use u-4, whose last reader is layer L+1's use u-4, issued
+// one round before layer L's use u; MMAs complete in issue order, so the
+// completion that the epilogue waits for before writing use u implies it.
 //
 // The MMAs of a row are issued in the same order (dy, dx, K chunk) as the
 // layer kernels', and the epilogue rounds the same way, so the output equals
@@ -44,7 +49,8 @@
 
 namespace sb {
 
-constexpr int kNetThreads = 192;
+constexpr int kNetEpiGroups = 4;                           // one epilogue warp group per layer
+constexpr int kNetThreads = (4 * kNetEpiGroups + 2) * 32;  // + MMA warp + TMA warp
 constexpr int kNetHalo = 3;                                // slots lost per side, layers 2-4
 constexpr int kNetTileOut = kConvTileOut - 2 * kNetHalo;   // 122 valid output pixels per strip
 constexpr int kNetFeatSlots = 6;
@@ -193,7 +199,7 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   const uint32_t sbase = smem_u32(smem);
   const int rounds = n + 9;
 
-  if (warp == 5) {
+  if (warp == 4 * kNetEpiGroups + 1) {
     // ---- feature rows B-4 .. B+n+3 by TMA (relative row f, slot f % 6)
     if ((tid & 31) == 0) {
       prefetch_tmap(&feat_map);
@@ -219,7 +225,7 @@ __global__ void __launch_bounds__(kNetThreads, 1)
       for (int g = f > kNetFeatSlots ? f - kNetFeatSlots : 0; g < f; ++g)
         mbar_wait(&feat_full[g % kNetFeatSlots], (unsigned)((g / kNetFeatSlots) & 1));
     }
-  } else if (warp == 4) {
+  } else if (warp == 4 * kNetEpiGroups) {
     // ---- MMA issue
     if ((tid & 31) == 0) {
       bool ok = true;
@@ -267,13 +273,15 @@ __global__ void __launch_bounds__(kNetThreads, 1)
       mbar_wait(fin, 0);
     }
   } else {
-    // ---- epilogue: pixel slot p = TMEM lane
-    const int p = tid;
+    // ---- epilogue: group g = warp / 4 owns the layers L with L % groups == g;
+    // pixel slot p = TMEM lane (warp w reads lanes 32 (w % 4) ..)
+    const int g = warp >> 2;
+    const int p = ((warp & 3) << 5) | (tid & 31);
     const int x = x0 + p;
-    const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
     bool ok = true;
     for (int s = 0; s < rounds && ok; ++s) {
-      for (int L = 0; L < 4; ++L) {
+      for (int L = g; L < 4; L += kNetEpiGroups) {
         const int u = s - 3 * L;
         if (u < 0 || u > n + 5 - 2 * L) continue;
         if (!net_wait(&mma_done[L * 2 + (u & 1)], (unsigned)((u >> 1) & 1), abort_flag)) {
