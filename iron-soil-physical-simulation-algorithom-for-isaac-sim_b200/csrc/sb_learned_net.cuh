@@ -12,37 +12,51 @@
 // pixel slot p needs its input at p-1 .. p+1, so the valid slots shrink by
 // one on each side per layer after the first: 122 of the 128 slots of the
 // last layer are valid, and strips advance by 122 pixels (slot p of strip s
-// is pixel x = 122 s - 3 + p).  Rows: for the band [B, B+n) the layers
-// compute rows B-3 .. B+n+2, B-2 .. B+n+1, B-1 .. B+n and B .. B+n-1; the
-// features rows B-4 .. B+n+3 arrive by TMA.  Positions outside the image are
-// stored as zeros, which is the zero padding of every layer.
+// is pixel x = 122 s - 3 + p).  Rows: for the band [B, B+n) layer L (0-3)
+// reads input rows B-4+L .. B+n+3-L (input i = row B-4+L+i) and produces the
+// rows B-3+L .. B+n+2-L; the feature rows arrive by TMA.  Positions outside
+// the image are stored as zeros, which is the zero padding of every layer.
 //
-// Schedule.  In round s layer L (0-based) computes its use u = s - 3L (row
-// B-3+L+u), so a layer trails the one before it by two rows: the rows it
-// reads were finished in an earlier round, and the four layers of a round
-// are independent.  Warp roles:
-//   warps 0-15 epilogue, one group of four warps per layer (TMEM lane =
-//              pixel slot): ReLU, BF16, into the layer's ring (the last
-//              layer: its four f32 outputs to global memory).  A row's
-//              epilogue is a chain of dependent steps (TMEM load, convert,
-//              stores, proxy fence, arrival) of about a microsecond, so the
-//              four layers' epilogues run side by side;
-//   warp 16    one thread issues the MMAs (tcgen05.mma, accumulators double
-//              buffered per layer in TMEM);
-//   warp 17    one thread issues the TMA loads of feature rows (6-row ring).
-// Every hand-off is an mbarrier: feature row landed (TMA transaction bytes),
-// feature slot free and accumulator ready (tcgen05.commit), epilogue done
-// (128 arrivals: the accumulator buffer is free and the output row is in the
-// ring).  Ring slots need no barrier of their own: layer L's use u rewrites
-// the slot of its use u-4, whose last reader is layer L+1's use u-4, issued
-// one round before layer L's use u; MMAs complete in issue order, so the
-// completion that the epilogue waits for before writing use u implies it.
+// Rotating accumulators.  A tcgen05.mma instruction costs tens of cycles
+// whatever its size (measured: ~50 ns per M128 x N32 x K16 MMA issued from
+// one thread, most of it not tensor-pipe time), so small MMAs leave the
+// tensor core idle.  Each input row is therefore consumed once, by
+// 3 x CIN/16 MMAs of N = 3 x COUT: input i feeds the outputs i, i+1, i+2
+// (numbered from the layer's first input) through the kernel rows dy = 2,
+// 1, 0, into three accumulators side by side in TMEM.  Output j lives in
+// slot j % 3, and the staged weights per dx are the five blocks
+// W(2) W(1) W(0) W(2) W(1), so the operand for input i is the three
+// consecutive blocks from (3 - i % 3) % 3.  Output j is complete after input
+// j; its epilogue reads the slot and clears it (tcgen05.st of zeros) before
+// input j+1 adds to it as output j+3.  Every output thus receives its inputs
+// j-2, j-1, j in the (dy, dx, K chunk) order of the layer kernels, starting
+// from zero, and the epilogue rounds the same way, so the fluxes equal the
+// layer-by-layer path's.  Outputs 0 and 1 only collect partial sums and are
+// dropped.
 //
-// The MMAs of a row are issued in the same order (dy, dx, K chunk) as the
-// layer kernels', and the epilogue rounds the same way, so the output equals
-// the layer-by-layer path bit for bit.  All waits are bounded; a wait that
-// gives up sets the CTA's abort flag (the other roles leave their loops) and
-// the caller's status word.
+// Roles.
+//   warps 0-15  epilogue, one group of four warps per layer (TMEM lane =
+//               pixel slot): ReLU, BF16, into the layer's ring (the last
+//               layer: its four f32 outputs to global memory);
+//   warp 16     one thread issues the MMAs in rounds: round s issues input
+//               s - 3L of every layer L that has one.  Layer L's input i is
+//               layer L-1's output i+2, finished in the previous round, and
+//               the accumulator slot it starts held output i-1, drained in
+//               the previous round, so a round's MMAs overlap the previous
+//               round's epilogues;
+//   warp 17     one thread issues the TMA loads of feature rows (6-row ring).
+// Hand-offs are mbarriers (feature row landed: TMA transaction bytes; the
+// MMAs of an input done, feature slot free: tcgen05.commit; epilogue of an
+// output done: 128 arrivals), two per layer used alternately.  A
+// phase-parity wait only tells completion #k from #k-1, so each barrier's
+// completions are waited for in order, and no barrier runs two completions
+// ahead of a waiter (checked by a protocol simulation over band heights 1-40
+// and random interleavings).  Ring slots need no barrier of their own: the
+// ring entry that input i of layer L writes (entry i-2) last held entry i-6,
+// read by layer L+1's input i-6, issued three rounds earlier; the commit that
+// the epilogue waits for tracks every MMA issued before it.  All waits are
+// bounded; a wait that gives up sets the CTA's abort flag (the other roles
+// leave their loops) and the caller's status word.
 #pragma once
 
 #include "sb_learned.cuh"
@@ -57,12 +71,16 @@ constexpr int kNetFeatSlots = 6;
 constexpr int kNetActSlots = 4;
 constexpr uint32_t kNetFeatLbo = 2176;  // 130 pixels x 16 B rounded up to 128 B (TMA destination)
 
+__host__ __device__ constexpr int net_cin(int L) { return L == 0 ? 16 : 32; }
+__host__ __device__ constexpr int net_cout(int L) { return L == 3 ? 16 : 32; }
+
 struct NetSmem {
-  static constexpr int W1 = 0;                                 // 16 -> 32, 9 taps
-  static constexpr int W2 = W1 + 9 * 32 * 16 * 2;              // 32 -> 32
-  static constexpr int W3 = W2 + 9 * 32 * 32 * 2;              // 32 -> 32
-  static constexpr int W4 = W3 + 9 * 32 * 32 * 2;              // 32 -> 16
-  static constexpr int W_END = W4 + 9 * 16 * 32 * 2;
+  // weights per layer: 3 dx x 5 staged blocks of COUT x CIN
+  static constexpr int W1 = 0;
+  static constexpr int W2 = W1 + 15 * 32 * 16 * 2;
+  static constexpr int W3 = W2 + 15 * 32 * 32 * 2;
+  static constexpr int W4 = W3 + 15 * 32 * 32 * 2;
+  static constexpr int W_END = W4 + 15 * 16 * 32 * 2;
   static constexpr int FEAT_SLOT = 2 * (int)kNetFeatLbo;       // 16 channels
   static constexpr int FEAT = W_END;
   static constexpr int ACT_SLOT = 4 * (int)kRowLbo;            // 32 channels
@@ -71,22 +89,24 @@ struct NetSmem {
   static constexpr int BARS = ACT + 3 * ACT_RING;
   static constexpr int NBARS = 2 * kNetFeatSlots + 8 + 8 + 1;  // full, free, mma, epilogue, final
   static constexpr int BYTES = BARS + NBARS * 8 + 16;
-  static constexpr uint32_t TMEM_COLS = 256;
-  // accumulator of layer L, buffer j: 32 columns each for layers 0-2, 16 for layer 3
-  __host__ __device__ static constexpr uint32_t acc_col(int L, int j) {
-    return L < 3 ? (uint32_t)(L * 64 + j * 32) : (uint32_t)(192 + j * 16);
+  static constexpr uint32_t TMEM_COLS = 512;
+  // first accumulator column of layer L (three slots of COUT columns)
+  __host__ __device__ static constexpr uint32_t acc_col(int L) { return (uint32_t)(L * 96); }
+  __host__ __device__ static constexpr int w_off(int L) {
+    return L == 0 ? W1 : L == 1 ? W2 : L == 2 ? W3 : W4;
   }
 };
 static_assert(NetSmem::FEAT % 128 == 0 && NetSmem::FEAT_SLOT % 128 == 0,
               "TMA destinations are 128-byte aligned");
 static_assert(NetSmem::BYTES <= 227 * 1024, "one CTA per SM");
+static_assert(NetSmem::acc_col(3) + 3 * 16 <= NetSmem::TMEM_COLS, "accumulators fit in TMEM");
 
 struct NetArgs {
   const __nv_bfloat16* wpk[4];  // packed weights of the four layers (layer kernels' packing)
-  float* flux;                // [batch][h][w][4]
+  float* flux;                  // [batch][h][w][4]
   int batch, h, w;
   int rows_per_cta;
-  int* status;                // set to 1 if a bounded wait gave up
+  int* status;                  // set to 1 if a bounded wait gave up
 };
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -119,27 +139,23 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
-// One output row of a layer: nine taps (dy, dx) x CIN/16 K chunks of
-// M = 128 pixels x N = COUT, in the layer kernels' order.  r0..r2: the
-// staged input rows y-1, y, y+1; LBO: their channel-chunk stride.
+// The MMAs of one input row of a layer: per (dx, K chunk) one M = 128
+// pixels x N = 3 COUT MMA into the layer's three accumulator slots.  row:
+// the staged input row, LBO its channel-chunk stride; first: the staged
+// weight block (of five per dx) that feeds slot 0.
 template <int CIN, int COUT, uint32_t LBO>
-__device__ __forceinline__ void net_issue(uint32_t tmem_d, uint32_t r0, uint32_t r1, uint32_t r2,
-                                          uint32_t w_base) {
+__device__ __forceinline__ void net_issue_input(uint32_t tmem_d, uint32_t row, uint32_t w_base,
+                                                int first) {
   constexpr int W_BLOCK = COUT * CIN * 2;
-  constexpr uint32_t idesc = umma_idesc_bf16(128, COUT);
+  constexpr uint32_t idesc = umma_idesc_bf16(128, 3 * COUT);
+  const uint64_t adesc0 = umma_desc(row, LBO, 128);
   const uint64_t bdesc0 = umma_desc(w_base, 128, (CIN / 8) * 128);
 #pragma unroll
-  for (int dy = 0; dy < 3; ++dy) {
-    const uint64_t adesc0 = umma_desc(dy == 0 ? r0 : dy == 1 ? r1 : r2, LBO, 128);
+  for (int dx = 0; dx < 3; ++dx)
 #pragma unroll
-    for (int dx = 0; dx < 3; ++dx) {
-#pragma unroll
-      for (int kk = 0; kk < CIN / 16; ++kk)
-        umma_bf16(tmem_d, adesc0 + (uint64_t)((kk * 2 * LBO + dx * 16) >> 4),
-                  bdesc0 + (uint64_t)(((dy * 3 + dx) * W_BLOCK + kk * 256) >> 4), idesc,
-                  (dy | dx | kk) != 0);
-    }
-  }
+    for (int kk = 0; kk < CIN / 16; ++kk)
+      umma_bf16(tmem_d, adesc0 + (uint64_t)((kk * 2 * LBO + dx * 16) >> 4),
+                bdesc0 + (uint64_t)(((dx * 5 + first) * W_BLOCK + kk * 256) >> 4), idesc, 1);
 }
 
 __global__ void __launch_bounds__(kNetThreads, 1)
@@ -149,8 +165,8 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::BARS);
   uint64_t* feat_full = bars;
   uint64_t* feat_free = bars + kNetFeatSlots;
-  uint64_t* mma_done = bars + 2 * kNetFeatSlots;  // [layer][buffer]
-  uint64_t* epi_done = mma_done + 8;              // [layer][buffer]
+  uint64_t* mma_done = bars + 2 * kNetFeatSlots;  // [layer][input & 1]
+  uint64_t* epi_done = mma_done + 8;              // [layer][output & 1]
   uint64_t* fin = epi_done + 8;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
@@ -161,14 +177,20 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   const int n = min(a.rows_per_cta, a.h - B);
   const int img = blockIdx.z;
 
-  {
-    constexpr int kOff[4] = {S::W1, S::W2, S::W3, S::W4};
-    constexpr int kEnd[4] = {S::W2, S::W3, S::W4, S::W_END};
+  // weights: per layer and dx the blocks of dy = 2, 1, 0, 2, 1 (the packed
+  // input holds block dy * 3 + dx)
 #pragma unroll
-    for (int L = 0; L < 4; ++L) {
-      const uint4* src = reinterpret_cast<const uint4*>(a.wpk[L]);
-      uint4* dst = reinterpret_cast<uint4*>(smem + kOff[L]);
-      for (int i = tid; i < (kEnd[L] - kOff[L]) / 16; i += kNetThreads) dst[i] = src[i];
+  for (int L = 0; L < 4; ++L) {
+    constexpr int kChunks[4] = {32 * 16 * 2 / 16, 32 * 32 * 2 / 16, 32 * 32 * 2 / 16,
+                                16 * 32 * 2 / 16};
+    const int chunks = kChunks[L];
+    const uint4* src = reinterpret_cast<const uint4*>(a.wpk[L]);
+    uint4* dst = reinterpret_cast<uint4*>(smem + S::w_off(L));
+    for (int i = tid; i < 15 * chunks; i += kNetThreads) {
+      const int blk = i / chunks, c = i - blk * chunks;
+      const int dx = blk / 5, jj = blk - dx * 5;
+      const int dy = (jj == 0 || jj == 3) ? 2 : (jj == 1 || jj == 4) ? 1 : 0;
+      dst[i] = src[(dy * 3 + dx) * chunks + c];
     }
   }
   // staged pixels 0 and 129 of the activation rings feed only invalid slots;
@@ -197,10 +219,21 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tslot;
   const uint32_t sbase = smem_u32(smem);
-  const int rounds = n + 9;
+  // epilogue warps: every layer's three accumulator slots start at zero
+  if (warp < 4 * kNetEpiGroups) {
+    const int L = warp >> 2;
+    const uint32_t lanes = tmem + ((uint32_t)((warp & 3) * 32) << 16) + S::acc_col(L);
+    if (L < 3)
+      for (int sl = 0; sl < 3; ++sl) tmem_zero<32>(lanes + (uint32_t)(sl * 32));
+    else
+      for (int sl = 0; sl < 3; ++sl) tmem_zero<16>(lanes + (uint32_t)(sl * 16));
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
 
   if (warp == 4 * kNetEpiGroups + 1) {
-    // ---- feature rows B-4 .. B+n+3 by TMA (relative row f, slot f % 6)
+    // ---- feature rows B-4 .. B+n+3 by TMA (input i of layer 0, slot i % 6)
     if ((tid & 31) == 0) {
       prefetch_tmap(&feat_map);
       bool ok = true;
@@ -226,43 +259,45 @@ __global__ void __launch_bounds__(kNetThreads, 1)
         mbar_wait(&feat_full[g % kNetFeatSlots], (unsigned)((g / kNetFeatSlots) & 1));
     }
   } else if (warp == 4 * kNetEpiGroups) {
-    // ---- MMA issue
+    // ---- MMA issue in rounds: round s issues input s - 3L of every layer L
+    // that has one; each needs only epilogues of earlier rounds
     if ((tid & 31) == 0) {
       bool ok = true;
+      const int rounds = n + 8 + 3 * 3;
       for (int s = 0; s < rounds && ok; ++s) {
+#pragma unroll
         for (int L = 0; L < 4; ++L) {
-          const int u = s - 3 * L;
-          if (u < 0 || u > n + 5 - 2 * L) continue;
-          if (L == 0) {
-            for (int f = (u == 0 ? 0 : u + 2); f <= u + 2 && ok; ++f)
-              ok = net_wait(&feat_full[f % kNetFeatSlots], (unsigned)((f / kNetFeatSlots) & 1),
-                            abort_flag);
-          } else {
-            const int v = u + 2;  // the newest input row is use v of layer L-1
+          const int i = s - 3 * L;
+          if (i < 0 || i >= n + 8 - 2 * L) continue;
+          if (L == 0) {  // feature row i landed
+            ok = net_wait(&feat_full[i % kNetFeatSlots], (unsigned)((i / kNetFeatSlots) & 1),
+                          abort_flag);
+          } else {  // output i + 2 of layer L-1 (issued in the previous round) in the ring
+            const int v = i + 2;
             ok = net_wait(&epi_done[(L - 1) * 2 + (v & 1)], (unsigned)((v >> 1) & 1), abort_flag);
           }
-          if (ok && u >= 2)  // accumulator buffer: use u-2 drained
-            ok = net_wait(&epi_done[L * 2 + (u & 1)], (unsigned)(((u - 2) >> 1) & 1), abort_flag);
+          if (ok && i >= 1)  // output i-1 drained: the slot that output i+2 starts is clear
+            ok = net_wait(&epi_done[L * 2 + ((i - 1) & 1)], (unsigned)(((i - 1) >> 1) & 1),
+                          abort_flag);
           if (!ok) break;
           tc_fence_after();
-          const uint32_t d = tmem + S::acc_col(L, u & 1);
+          const uint32_t d = tmem + S::acc_col(L);
+          const int first = (3 - i % 3) % 3;
           if (L == 0) {
-            auto fs = [&](int f) {
-              return sbase + S::FEAT + (uint32_t)((f % kNetFeatSlots) * S::FEAT_SLOT);
-            };
-            net_issue<16, 32, kNetFeatLbo>(d, fs(u), fs(u + 1), fs(u + 2), sbase + S::W1);
+            net_issue_input<16, 32, kNetFeatLbo>(
+                d, sbase + S::FEAT + (uint32_t)((i % kNetFeatSlots) * S::FEAT_SLOT),
+                sbase + S::W1, first);
           } else {
-            const uint32_t ring = sbase + S::ACT + (uint32_t)((L - 1) * S::ACT_RING);
-            auto as = [&](int v) { return ring + (uint32_t)((v % kNetActSlots) * S::ACT_SLOT); };
-            if (L == 1)
-              net_issue<32, 32, kRowLbo>(d, as(u), as(u + 1), as(u + 2), sbase + S::W2);
-            else if (L == 2)
-              net_issue<32, 32, kRowLbo>(d, as(u), as(u + 1), as(u + 2), sbase + S::W3);
+            // input i of layer L = output i + 2 of layer L-1 = ring entry i
+            const uint32_t row = sbase + S::ACT + (uint32_t)((L - 1) * S::ACT_RING) +
+                                 (uint32_t)((i % kNetActSlots) * S::ACT_SLOT);
+            if (L == 3)
+              net_issue_input<32, 16, kRowLbo>(d, row, sbase + S::W4, first);
             else
-              net_issue<32, 16, kRowLbo>(d, as(u), as(u + 1), as(u + 2), sbase + S::W4);
+              net_issue_input<32, 32, kRowLbo>(d, row, sbase + (L == 1 ? S::W2 : S::W3), first);
           }
-          umma_commit(&mma_done[L * 2 + (u & 1)]);
-          if (L == 0) umma_commit(&feat_free[u % kNetFeatSlots]);  // feature row u is done
+          umma_commit(&mma_done[L * 2 + (i & 1)]);
+          if (L == 0) umma_commit(&feat_free[i % kNetFeatSlots]);  // feature row consumed
         }
       }
       if (!ok) {
@@ -273,52 +308,54 @@ __global__ void __launch_bounds__(kNetThreads, 1)
       mbar_wait(fin, 0);
     }
   } else {
-    // ---- epilogue: group g = warp / 4 owns the layers L with L % groups == g;
-    // pixel slot p = TMEM lane (warp w reads lanes 32 (w % 4) ..)
-    const int g = warp >> 2;
+    // ---- epilogue: warp group L = warp / 4 drains layer L; pixel slot p =
+    // TMEM lane (warp w reads lanes 32 (w % 4) ..)
+    const int L = warp >> 2;
     const int p = ((warp & 3) << 5) | (tid & 31);
     const int x = x0 + p;
-    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t lanes = tmem + ((uint32_t)((warp & 3) * 32) << 16) + S::acc_col(L);
+    const int outputs = n + 8 - 2 * L;
     bool ok = true;
-    for (int s = 0; s < rounds && ok; ++s) {
-      for (int L = g; L < 4; L += kNetEpiGroups) {
-        const int u = s - 3 * L;
-        if (u < 0 || u > n + 5 - 2 * L) continue;
-        if (!net_wait(&mma_done[L * 2 + (u & 1)], (unsigned)((u >> 1) & 1), abort_flag)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const int r = B - 3 + L + u;
-        const uint32_t taddr = lane_addr + S::acc_col(L, u & 1);
-        if (L < 3) {
-          float d[32];
-          tmem_ld32(taddr, d);
-          tc_fence_before();
+    for (int j = 0; j < outputs; ++j) {
+      if (!net_wait(&mma_done[L * 2 + (j & 1)], (unsigned)((j >> 1) & 1), abort_flag)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const int r = B - 5 + L + j;  // output j of layer L
+      if (L < 3) {
+        const uint32_t taddr = lanes + (uint32_t)((j % 3) * 32);
+        float d[32];
+        tmem_ld32(taddr, d);
+        tmem_zero<32>(taddr);
+        tc_fence_before();
+        if (j >= 2) {
           const bool inside = x >= 0 && x < a.w && r >= 0 && r < a.h;
-          unsigned char* dst = smem + S::ACT + L * S::ACT_RING + (u % kNetActSlots) * S::ACT_SLOT +
-                               (p + 1) * 16;
+          unsigned char* dst = smem + S::ACT + L * S::ACT_RING +
+                               ((j - 2) % kNetActSlots) * S::ACT_SLOT + (p + 1) * 16;
 #pragma unroll
           for (int c8 = 0; c8 < 4; ++c8) {
             __align__(16) __nv_bfloat162 ob[4];
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-              ob[j] = inside ? __floats2bfloat162_rn(fmaxf(d[c8 * 8 + 2 * j], 0.f),
-                                                     fmaxf(d[c8 * 8 + 2 * j + 1], 0.f))
+            for (int k = 0; k < 4; ++k)
+              ob[k] = inside ? __floats2bfloat162_rn(fmaxf(d[c8 * 8 + 2 * k], 0.f),
+                                                     fmaxf(d[c8 * 8 + 2 * k + 1], 0.f))
                              : __floats2bfloat162_rn(0.f, 0.f);
             *reinterpret_cast<uint4*>(dst + c8 * kRowLbo) = *reinterpret_cast<const uint4*>(ob);
           }
           fence_async_smem();  // the next layer's MMAs read this row
-        } else {
-          float d[16];
-          tmem_ld16(taddr, d);
-          tc_fence_before();
-          if (p >= kNetHalo && p < kNetHalo + kNetTileOut && x < a.w)
-            *reinterpret_cast<float4*>(a.flux + (((size_t)img * a.h + r) * a.w + x) * 4) =
-                make_float4(d[0], d[1], d[2], d[3]);
         }
-        mbar_arrive(&epi_done[L * 2 + (u & 1)]);
+      } else {
+        const uint32_t taddr = lanes + (uint32_t)((j % 3) * 16);
+        float d[16];
+        tmem_ld16(taddr, d);
+        tmem_zero<16>(taddr);
+        tc_fence_before();
+        if (j >= 2 && p >= kNetHalo && p < kNetHalo + kNetTileOut && x < a.w)
+          *reinterpret_cast<float4*>(a.flux + (((size_t)img * a.h + r) * a.w + x) * 4) =
+              make_float4(d[0], d[1], d[2], d[3]);
       }
+      mbar_arrive(&epi_done[L * 2 + (j & 1)]);
     }
     if (!ok) {
       *abort_flag = 1;
