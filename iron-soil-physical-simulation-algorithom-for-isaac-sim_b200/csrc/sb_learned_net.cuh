@@ -38,23 +38,24 @@
 //   warps 0-15  epilogue, one group of four warps per layer (TMEM lane =
 //               pixel slot): ReLU, BF16, into the layer's ring (the last
 //               layer: its four f32 outputs to global memory);
-//   warp 16     one thread issues the MMAs in rounds: round s issues input
-//               s - 3L of every layer L that has one.  Layer L's input i is
-//               layer L-1's output i+2, finished in the previous round, and
-//               the accumulator slot it starts held output i-1, drained in
-//               the previous round, so a round's MMAs overlap the previous
-//               round's epilogues;
-//   warp 17     one thread issues the TMA loads of feature rows (6-row ring).
-// Hand-offs are mbarriers (feature row landed: TMA transaction bytes; the
-// MMAs of an input done, feature slot free: tcgen05.commit; epilogue of an
-// output done: 128 arrivals), two per layer used alternately.  A
-// phase-parity wait only tells completion #k from #k-1, so each barrier's
-// completions are waited for in order, and no barrier runs two completions
-// ahead of a waiter (checked by a protocol simulation over band heights 1-40
-// and random interleavings).  Ring slots need no barrier of their own: the
-// ring entry that input i of layer L writes (entry i-2) last held entry i-6,
-// read by layer L+1's input i-6, issued three rounds earlier; the commit that
-// the epilogue waits for tracks every MMA issued before it.  All waits are
+//   warps 16-19 one thread per layer issues that layer's MMAs, input after
+//               input: input i of layer L is output i+2 of layer L-1, and
+//               the accumulator slot it starts held output i-1, so it waits
+//               for those two epilogues.  Issue from one thread is serial
+//               (about 60 ns per MMA and 70 ns per barrier wait, measured),
+//               so the four layers issue side by side;
+//   warp 20     one thread issues the TMA loads of feature rows (6-row ring).
+// Hand-offs are mbarriers: feature row landed (TMA transaction bytes); the
+// MMAs of an input done and feature slot free (tcgen05.commit); epilogue of
+// an output done (128 arrivals).  A phase-parity wait only tells completion
+// #k from #k-1, so each waiter observes a barrier's completions in order, and
+// the barriers of a kind rotate over four per layer: no producer gets two
+// completions ahead of a waiter (layer L-1 can finish at most three outputs
+// beyond the one layer L waits for).  Commits track only their own thread's
+// MMAs, so a ring slot is guarded explicitly: the epilogue that writes ring
+// entry j-2 (replacing entry j-6) first waits for layer L+1's input j-6.
+// The protocol (ordering, slot reuse, parity aliasing) was checked by a
+// simulation over band heights 1-40 and random interleavings.  All waits are
 // bounded; a wait that gives up sets the CTA's abort flag (the other roles
 // leave their loops) and the caller's status word.
 #pragma once
@@ -64,7 +65,8 @@
 namespace sb {
 
 constexpr int kNetEpiGroups = 4;                           // one epilogue warp group per layer
-constexpr int kNetThreads = (4 * kNetEpiGroups + 2) * 32;  // + MMA warp + TMA warp
+constexpr int kNetThreads = (4 * kNetEpiGroups + 4 + 1) * 32;  // + 4 MMA warps + TMA warp
+constexpr int kNetBars = 4;  // mbarriers per layer and kind, used in turn (see the protocol note)
 constexpr int kNetHalo = 3;                                // slots lost per side, layers 2-4
 constexpr int kNetTileOut = kConvTileOut - 2 * kNetHalo;   // 122 valid output pixels per strip
 constexpr int kNetFeatSlots = 6;
@@ -87,7 +89,7 @@ struct NetSmem {
   static constexpr int ACT_RING = kNetActSlots * ACT_SLOT;
   static constexpr int ACT = FEAT + kNetFeatSlots * FEAT_SLOT;
   static constexpr int BARS = ACT + 3 * ACT_RING;
-  static constexpr int NBARS = 2 * kNetFeatSlots + 8 + 8 + 1;  // full, free, mma, epilogue, final
+  static constexpr int NBARS = 2 * kNetFeatSlots + 2 * 4 * kNetBars + 4;  // + final per layer
   static constexpr int BYTES = BARS + NBARS * 8 + 16;
   static constexpr uint32_t TMEM_COLS = 512;
   // first accumulator column of layer L (three slots of COUT columns)
@@ -165,10 +167,10 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S::BARS);
   uint64_t* feat_full = bars;
   uint64_t* feat_free = bars + kNetFeatSlots;
-  uint64_t* mma_done = bars + 2 * kNetFeatSlots;  // [layer][input & 1]
-  uint64_t* epi_done = mma_done + 8;              // [layer][output & 1]
-  uint64_t* fin = epi_done + 8;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 1);
+  uint64_t* mma_done = bars + 2 * kNetFeatSlots;  // [layer][input % kNetBars]
+  uint64_t* epi_done = mma_done + 4 * kNetBars;   // [layer][output % kNetBars]
+  uint64_t* fin = epi_done + 4 * kNetBars;        // [layer]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -205,11 +207,11 @@ __global__ void __launch_bounds__(kNetThreads, 1)
       mbar_init(&feat_full[k], 1);
       mbar_init(&feat_free[k], 1);
     }
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < 4 * kNetBars; ++k) {
       mbar_init(&mma_done[k], 1);
       mbar_init(&epi_done[k], 128);
     }
-    mbar_init(fin, 1);
+    for (int k = 0; k < 4; ++k) mbar_init(&fin[k], 1);
     *abort_flag = 0;
   }
   if (warp == 0) tmem_alloc(tslot, S::TMEM_COLS);
@@ -232,7 +234,7 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   __syncthreads();
   tc_fence_after();
 
-  if (warp == 4 * kNetEpiGroups + 1) {
+  if (warp == 4 * kNetEpiGroups + 4) {
     // ---- feature rows B-4 .. B+n+3 by TMA (input i of layer 0, slot i % 6)
     if ((tid & 31) == 0) {
       prefetch_tmap(&feat_map);
@@ -258,54 +260,50 @@ __global__ void __launch_bounds__(kNetThreads, 1)
       for (int g = f > kNetFeatSlots ? f - kNetFeatSlots : 0; g < f; ++g)
         mbar_wait(&feat_full[g % kNetFeatSlots], (unsigned)((g / kNetFeatSlots) & 1));
     }
-  } else if (warp == 4 * kNetEpiGroups) {
-    // ---- MMA issue in rounds: round s issues input s - 3L of every layer L
-    // that has one; each needs only epilogues of earlier rounds
+  } else if (warp >= 4 * kNetEpiGroups) {
+    // ---- MMA issue: warp 16 + L issues layer L's inputs in order
+    const int L = warp - 4 * kNetEpiGroups;
     if ((tid & 31) == 0) {
       bool ok = true;
-      const int rounds = n + 8 + 3 * 3;
-      for (int s = 0; s < rounds && ok; ++s) {
-#pragma unroll
-        for (int L = 0; L < 4; ++L) {
-          const int i = s - 3 * L;
-          if (i < 0 || i >= n + 8 - 2 * L) continue;
-          if (L == 0) {  // feature row i landed
-            ok = net_wait(&feat_full[i % kNetFeatSlots], (unsigned)((i / kNetFeatSlots) & 1),
-                          abort_flag);
-          } else {  // output i + 2 of layer L-1 (issued in the previous round) in the ring
-            const int v = i + 2;
-            ok = net_wait(&epi_done[(L - 1) * 2 + (v & 1)], (unsigned)((v >> 1) & 1), abort_flag);
-          }
-          if (ok && i >= 1)  // output i-1 drained: the slot that output i+2 starts is clear
-            ok = net_wait(&epi_done[L * 2 + ((i - 1) & 1)], (unsigned)(((i - 1) >> 1) & 1),
-                          abort_flag);
-          if (!ok) break;
-          tc_fence_after();
-          const uint32_t d = tmem + S::acc_col(L);
-          const int first = (3 - i % 3) % 3;
-          if (L == 0) {
-            net_issue_input<16, 32, kNetFeatLbo>(
-                d, sbase + S::FEAT + (uint32_t)((i % kNetFeatSlots) * S::FEAT_SLOT),
-                sbase + S::W1, first);
-          } else {
-            // input i of layer L = output i + 2 of layer L-1 = ring entry i
-            const uint32_t row = sbase + S::ACT + (uint32_t)((L - 1) * S::ACT_RING) +
-                                 (uint32_t)((i % kNetActSlots) * S::ACT_SLOT);
-            if (L == 3)
-              net_issue_input<32, 16, kRowLbo>(d, row, sbase + S::W4, first);
-            else
-              net_issue_input<32, 32, kRowLbo>(d, row, sbase + (L == 1 ? S::W2 : S::W3), first);
-          }
-          umma_commit(&mma_done[L * 2 + (i & 1)]);
-          if (L == 0) umma_commit(&feat_free[i % kNetFeatSlots]);  // feature row consumed
+      const int inputs = n + 8 - 2 * L;
+      for (int i = 0; i < inputs && ok; ++i) {
+        if (L == 0) {  // feature row i landed
+          ok = net_wait(&feat_full[i % kNetFeatSlots], (unsigned)((i / kNetFeatSlots) & 1),
+                        abort_flag);
+        } else {  // output i + 2 of layer L-1 in the ring (outputs 0-2 first, in order)
+          for (int v = i == 0 ? 0 : i + 2; v <= i + 2 && ok; ++v)
+            ok = net_wait(&epi_done[(L - 1) * kNetBars + (v % kNetBars)],
+                          (unsigned)((v / kNetBars) & 1), abort_flag);
         }
+        if (ok && i >= 1)  // output i-1 drained: the slot that output i+2 starts is clear
+          ok = net_wait(&epi_done[L * kNetBars + ((i - 1) % kNetBars)],
+                        (unsigned)(((i - 1) / kNetBars) & 1), abort_flag);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t d = tmem + S::acc_col(L);
+        const int first = (3 - i % 3) % 3;
+        if (L == 0) {
+          net_issue_input<16, 32, kNetFeatLbo>(
+              d, sbase + S::FEAT + (uint32_t)((i % kNetFeatSlots) * S::FEAT_SLOT), sbase + S::W1,
+              first);
+        } else {
+          // input i of layer L = output i + 2 of layer L-1 = ring entry i
+          const uint32_t row = sbase + S::ACT + (uint32_t)((L - 1) * S::ACT_RING) +
+                               (uint32_t)((i % kNetActSlots) * S::ACT_SLOT);
+          if (L == 3)
+            net_issue_input<32, 16, kRowLbo>(d, row, sbase + S::W4, first);
+          else
+            net_issue_input<32, 32, kRowLbo>(d, row, sbase + (L == 1 ? S::W2 : S::W3), first);
+        }
+        umma_commit(&mma_done[L * kNetBars + (i % kNetBars)]);
+        if (L == 0) umma_commit(&feat_free[i % kNetFeatSlots]);  // feature row consumed
       }
       if (!ok) {
         *abort_flag = 1;
         if (a.status) atomicExch(a.status, 1);
       }
-      umma_commit(fin);  // completes once every MMA issued above has
-      mbar_wait(fin, 0);
+      umma_commit(&fin[L]);  // completes once every MMA this thread issued has
+      mbar_wait(&fin[L], 0);
     }
   } else {
     // ---- epilogue: warp group L = warp / 4 drains layer L; pixel slot p =
@@ -317,7 +315,8 @@ __global__ void __launch_bounds__(kNetThreads, 1)
     const int outputs = n + 8 - 2 * L;
     bool ok = true;
     for (int j = 0; j < outputs; ++j) {
-      if (!net_wait(&mma_done[L * 2 + (j & 1)], (unsigned)((j >> 1) & 1), abort_flag)) {
+      if (!net_wait(&mma_done[L * kNetBars + (j % kNetBars)], (unsigned)((j / kNetBars) & 1),
+                    abort_flag)) {
         ok = false;
         break;
       }
@@ -329,6 +328,12 @@ __global__ void __launch_bounds__(kNetThreads, 1)
         tmem_ld32(taddr, d);
         tmem_zero<32>(taddr);
         tc_fence_before();
+        // ring entry j-2 replaces entry j-6: layer L+1's input j-6 must be done
+        if (j >= 6 && !net_wait(&mma_done[(L + 1) * kNetBars + ((j - 6) % kNetBars)],
+                                (unsigned)(((j - 6) / kNetBars) & 1), abort_flag)) {
+          ok = false;
+          break;
+        }
         if (j >= 2) {
           const bool inside = x >= 0 && x < a.w && r >= 0 && r < a.h;
           unsigned char* dst = smem + S::ACT + L * S::ACT_RING +
@@ -355,7 +360,7 @@ __global__ void __launch_bounds__(kNetThreads, 1)
           *reinterpret_cast<float4*>(a.flux + (((size_t)img * a.h + r) * a.w + x) * 4) =
               make_float4(d[0], d[1], d[2], d[3]);
       }
-      mbar_arrive(&epi_done[L * 2 + (j & 1)]);
+      mbar_arrive(&epi_done[L * kNetBars + (j % kNetBars)]);
     }
     if (!ok) {
       *abort_flag = 1;
