@@ -46,8 +46,9 @@
 //               so the four layers issue side by side;
 //   warp 20     one thread issues the TMA loads of feature rows (6-row ring).
 // Hand-offs are mbarriers: feature row landed (TMA transaction bytes); the
-// MMAs of an input done and feature slot free (tcgen05.commit); epilogue of
-// an output done (128 arrivals).  A phase-parity wait only tells completion
+// MMAs of an input done and feature slot free (tcgen05.commit); an output's
+// accumulator read and cleared, then its row in the ring (128 arrivals each:
+// the issuer of the same layer needs only the first).  A phase-parity wait only tells completion
 // #k from #k-1, so each waiter observes a barrier's completions in order, and
 // the barriers of a kind rotate over four per layer: no producer gets two
 // completions ahead of a waiter (layer L-1 can finish at most three outputs
@@ -89,7 +90,7 @@ struct NetSmem {
   static constexpr int ACT_RING = kNetActSlots * ACT_SLOT;
   static constexpr int ACT = FEAT + kNetFeatSlots * FEAT_SLOT;
   static constexpr int BARS = ACT + 3 * ACT_RING;
-  static constexpr int NBARS = 2 * kNetFeatSlots + 2 * 4 * kNetBars + 4;  // + final per layer
+  static constexpr int NBARS = 2 * kNetFeatSlots + 3 * 4 * kNetBars + 4;  // + final per layer
   static constexpr int BYTES = BARS + NBARS * 8 + 16;
   static constexpr uint32_t TMEM_COLS = 512;
   // first accumulator column of layer L (three slots of COUT columns)
@@ -169,7 +170,8 @@ __global__ void __launch_bounds__(kNetThreads, 1)
   uint64_t* feat_free = bars + kNetFeatSlots;
   uint64_t* mma_done = bars + 2 * kNetFeatSlots;  // [layer][input % kNetBars]
   uint64_t* epi_done = mma_done + 4 * kNetBars;   // [layer][output % kNetBars]
-  uint64_t* fin = epi_done + 4 * kNetBars;        // [layer]
+  uint64_t* acc_free = epi_done + 4 * kNetBars;   // [layer][output % kNetBars]
+  uint64_t* fin = acc_free + 4 * kNetBars;        // [layer]
   uint32_t* tslot = reinterpret_cast<uint32_t*>(fin + 4);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
 
@@ -210,6 +212,7 @@ __global__ void __launch_bounds__(kNetThreads, 1)
     for (int k = 0; k < 4 * kNetBars; ++k) {
       mbar_init(&mma_done[k], 1);
       mbar_init(&epi_done[k], 128);
+      mbar_init(&acc_free[k], 128);
     }
     for (int k = 0; k < 4; ++k) mbar_init(&fin[k], 1);
     *abort_flag = 0;
@@ -275,8 +278,8 @@ __global__ void __launch_bounds__(kNetThreads, 1)
             ok = net_wait(&epi_done[(L - 1) * kNetBars + (v % kNetBars)],
                           (unsigned)((v / kNetBars) & 1), abort_flag);
         }
-        if (ok && i >= 1)  // output i-1 drained: the slot that output i+2 starts is clear
-          ok = net_wait(&epi_done[L * kNetBars + ((i - 1) % kNetBars)],
+        if (ok && i >= 1)  // output i-1 read and cleared: the slot output i+2 starts
+          ok = net_wait(&acc_free[L * kNetBars + ((i - 1) % kNetBars)],
                         (unsigned)(((i - 1) / kNetBars) & 1), abort_flag);
         if (!ok) break;
         tc_fence_after();
@@ -328,6 +331,7 @@ __global__ void __launch_bounds__(kNetThreads, 1)
         tmem_ld32(taddr, d);
         tmem_zero<32>(taddr);
         tc_fence_before();
+        mbar_arrive(&acc_free[L * kNetBars + (j % kNetBars)]);
         // ring entry j-2 replaces entry j-6: layer L+1's input j-6 must be done
         if (j >= 6 && !net_wait(&mma_done[(L + 1) * kNetBars + ((j - 6) % kNetBars)],
                                 (unsigned)(((j - 6) / kNetBars) & 1), abort_flag)) {
@@ -356,11 +360,12 @@ __global__ void __launch_bounds__(kNetThreads, 1)
         tmem_ld16(taddr, d);
         tmem_zero<16>(taddr);
         tc_fence_before();
+        mbar_arrive(&acc_free[L * kNetBars + (j % kNetBars)]);
         if (j >= 2 && p >= kNetHalo && p < kNetHalo + kNetTileOut && x < a.w)
           *reinterpret_cast<float4*>(a.flux + (((size_t)img * a.h + r) * a.w + x) * 4) =
               make_float4(d[0], d[1], d[2], d[3]);
       }
-      mbar_arrive(&epi_done[L * kNetBars + (j % kNetBars)]);
+      if (L < 3) mbar_arrive(&epi_done[L * kNetBars + (j % kNetBars)]);
     }
     if (!ok) {
       *abort_flag = 1;
