@@ -36,6 +36,12 @@ need the reference at run time.  Cases:
 * ``fractal.npz``       -- ``slope_model.fractal_perlin_noise`` (the
   generator of the config-3 training patches) on four seeds/parameter sets
   (``--fractal``).
+* ``surface.npz``       -- ``AirborneParcelModel._bilinear``
+  (bulk_exchange/airborne.py:587-600), the reference's CPU bilinear sample of
+  the free surface (resting + mobile), on seeded fields at in-range queries
+  (grid points, cell interiors, the last row and column) (``--surface``); the
+  Warp query kernel (runtime/bulk_state_authority.py:201-228) is the same
+  formula with the queries clamped to the grid first.
 * ``gate0.npz``         -- the 5 s config-0 gate: 256x256, seed 0, 300 steps of
   1/60 s at CFL 0.4 and mu = tan 35 deg, each followed by
   ``relax_critical_slope`` of ``b_eff`` at 35 deg (row-major array, spacing
@@ -415,6 +421,25 @@ def make_fractal():
     np.savez_compressed(HERE / "fractal.npz", **arrays)
 
 
+def make_surface():
+    """Bilinear surface samples from the reference's CPU sampler
+    (bulk_exchange/airborne.py:587-600) on resting + mobile fields."""
+    from isaac_bulk_pipeline.bulk_exchange.airborne import AirborneParcelModel
+    rng = np.random.default_rng(11)
+    ny, nx = 37, 53
+    resting = 0.4 + 0.3 * rng.random((ny, nx))
+    mobile = np.where(rng.random((ny, nx)) < 0.3, 0.05 * rng.random((ny, nx)), 0.0)
+    field = resting + mobile
+    q = np.concatenate([
+        np.column_stack([rng.uniform(0.0, ny - 1.0, 400), rng.uniform(0.0, nx - 1.0, 400)]),
+        np.column_stack([rng.integers(0, ny, 40), rng.integers(0, nx, 40)]).astype(np.float64),
+        np.asarray([[ny - 1.0, nx - 1.0], [0.0, 0.0], [ny - 1.0, 0.5], [3.25, nx - 1.0]]),
+    ])
+    values = np.asarray([AirborneParcelModel._bilinear(field, r, c) for r, c in q])
+    np.savez_compressed(HERE / "surface.npz", resting=resting, mobile=mobile, queries=q,
+                        values=values)
+
+
 def make_event():
     """solvers.EventDrivenMinimumSlopeAdapter (solvers/event_driven_slope.py:
     16-302), the reached-bbox MiniSlope backend: the three scenarios of the
@@ -578,6 +603,9 @@ if __name__ == "__main__":
         sys.exit(0)
     if "--event" in sys.argv:
         make_event()
+        sys.exit(0)
+    if "--surface" in sys.argv:
+        make_surface()
         sys.exit(0)
     if "--fractal" in sys.argv:
         make_fractal()

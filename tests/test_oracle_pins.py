@@ -14,6 +14,7 @@ import pytest
 from oracle import fixed_point as fx
 from oracle import mobile_v2 as m
 from oracle import relax as R
+from oracle import surface as Sf
 
 from conftest import GOLDEN
 
@@ -152,3 +153,14 @@ def test_reached_relax_bit_identical_to_event_driven_adapter():
         assert it == int(g[f"{name}/iterations"]), name
         assert np.array_equal(h.T, g[f"{name}/stable"]), name
         assert reached.T[seeds].all(), name
+
+
+def test_surface_oracle_matches_reference_cpu_sampler():
+    """The clamped bilinear query equals the reference's CPU sampler bit for
+    bit on in-range queries, and the reference test's known answers."""
+    z = np.load(GOLDEN / "surface.npz")
+    field = z["resting"] + z["mobile"]
+    q = z["queries"]
+    assert np.array_equal(Sf.bilinear(field, q[:, 0], q[:, 1]), z["values"])
+    grid = np.arange(256, dtype=np.float64).reshape(16, 16)
+    assert Sf.bilinear(grid, [1.0, 2.5], [2.0, 3.5]).tolist() == [18.0, 43.5]

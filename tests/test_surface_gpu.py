@@ -1,28 +1,20 @@
 """GPU tests of surface publication: dirty tiles after a mutation, tile
-downloads with their one-cell overlap, and batched bilinear queries
-(FP64: equal to the reference kernel's arithmetic restated in NumPy)."""
+downloads with their one-cell overlap, and batched bilinear queries (FP64:
+equal bit for bit to the reference's CPU sampler on its golden queries, and
+to the oracle's clamped restatement of the reference query kernel, which is
+pinned to that sampler, on queries outside the grid)."""
 
 import numpy as np
 import pytest
+
+from conftest import GOLDEN
+from oracle.surface import bilinear as _bilinear
 
 from soilb200.bulk_state import B200BulkState
 
 pytestmark = pytest.mark.gpu
 
 DX = 0.05
-
-
-def _bilinear(surface, rows, cols):
-    ny, nx = surface.shape
-    row = np.clip(rows, 0.0, ny - 1.0)
-    col = np.clip(cols, 0.0, nx - 1.0)
-    r0 = np.floor(row).astype(int)
-    c0 = np.floor(col).astype(int)
-    r1 = np.minimum(r0 + 1, ny - 1)
-    c1 = np.minimum(c0 + 1, nx - 1)
-    fr, fc = row - r0, col - c0
-    return ((1.0 - fr) * (1.0 - fc) * surface[r0, c0] + (1.0 - fr) * fc * surface[r0, c1]
-            + fr * (1.0 - fc) * surface[r1, c0] + fr * fc * surface[r1, c1])
 
 
 @pytest.mark.parametrize("precision", ["fp64", "fx32"])
@@ -57,4 +49,29 @@ def test_dirty_tiles_downloads_and_queries(precision):
         assert np.abs(vals - ref).max() <= 1e-12
     with pytest.raises(ValueError):
         st.sample_surface_bilinear(np.zeros((2, 3)), source="test")
+    st.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fx32"])
+def test_surface_queries_match_reference_sampler(precision):
+    z = np.load(GOLDEN / "surface.npz")
+    resting, mobile, q = z["resting"], z["mobile"], z["queries"]
+    st = B200BulkState(resting.shape, DX, DX, resting, precision=precision, tile_size=16,
+                       mobile_headroom_m=0.5)
+    st.grid.upload("mobile", mobile)
+    vals = st.sample_surface_bilinear(q, source="test")
+    if precision == "fp64":
+        assert np.array_equal(vals, z["values"])
+    else:  # heights held in int32 quanta: within one quantum per corner
+        assert np.abs(vals - z["values"]).max() <= 4.0 * st.grid.quantum
+    st.close()
+
+
+def test_surface_query_known_answers():
+    """The reference's own device-state test (tests/test_device_bulk_state.py:
+    116-126): resting heights 0..255 on a 16 x 16 grid."""
+    grid = np.arange(256, dtype=np.float64).reshape(16, 16)
+    st = B200BulkState(grid.shape, DX, DX, grid, precision="fp64", tile_size=4)
+    vals = st.sample_surface_bilinear(np.asarray([[1.0, 2.0], [2.5, 3.5]]), source="test")
+    assert vals.tolist() == [18.0, 43.5]
     st.close()
