@@ -1510,6 +1510,39 @@ static int relax_graph_for(sb_ctx* ctx, const RelaxConst& c, LoopGraph** out) {
   return SB_OK;
 }
 
+// SOILB200_NO_GRAPH=1 (profilers that cannot see kernel nodes of a graph
+// with conditional nodes): the sweep graph's kernels launched from the host,
+// the loop flag read back after every sweep.
+template <bool FX>
+static int relax_full_host_loop(sb_ctx* ctx, const RelaxConst& c) {
+  void* rargs[] = {(void*)&ctx->rctl};
+  SB_CUDA(ctx, cudaLaunchKernel((void*)relax_reset_kernel, dim3(1), dim3(kThreads), rargs, 0,
+                                ctx->stream));
+  RelaxConst ck = c;
+  ck.tiles1 = (c.n1 + kRelaxTile - 1) / kRelaxTile;
+  const int tiles0 = (c.n0 + kRelaxTile - 1) / kRelaxTile;
+  cudaGraphConditionalHandle handle{};
+  int no_handle = 0;
+  void* args[] = {(void*)&ck, (void*)&ctx->tm_relax[0], (void*)&ctx->tm_relax[1],
+                  (void*)&ctx->b, (void*)&ctx->b_alt, (void*)&ctx->rctl, (void*)&handle,
+                  (void*)&no_handle};
+  for (long long it = 0; it <= (long long)c.max_iterations; ++it) {
+    SB_CUDA(ctx, cudaLaunchKernel((void*)relax_full_kernel<FX>, dim3(tiles0 * ck.tiles1),
+                                  dim3(kThreads), args, 0, ctx->stream));
+    SB_CUDA(ctx, cudaMemcpyAsync(ctx->rctl_host, ctx->rctl, sizeof(RelaxControl),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->rctl_host->done) break;
+  }
+  long long count = (long long)ctx->pitch * ctx->d.ny;
+  void* cargs[] = {(void*)&ctx->b_alt, (void*)&ctx->b, (void*)&count, (void*)&ctx->rctl};
+  SB_CUDA(ctx, cudaLaunchKernel((void*)relax_copyback_kernel<FX>, dim3(grid_for(count)),
+                                dim3(kThreads), cargs, 0, ctx->stream));
+  SB_CUDA(ctx, cudaLaunchKernel((void*)relax_parity_clear_kernel, dim3(1), dim3(kThreads), rargs,
+                                0, ctx->stream));
+  return SB_OK;
+}
+
 // Queues max_iterations (or fewer, if converged) sweeps without waiting for
 // them or reading their statistics back.
 extern "C" int sb_relax_sweeps(sb_ctx* ctx, const sb_relax_params* p) {
@@ -1517,6 +1550,11 @@ extern "C" int sb_relax_sweeps(sb_ctx* ctx, const sb_relax_params* p) {
   RelaxConst c;
   int rc = relax_const(ctx, p, &c, kRelaxTile);
   if (rc) return rc;
+  if (!ctx->use_graphs) {
+    rc = fx(ctx) ? relax_full_host_loop<true>(ctx, c) : relax_full_host_loop<false>(ctx, c);
+    ctx->launches += 3 + ctx->rctl_host->iterations;
+    return rc;
+  }
   LoopGraph* lg = nullptr;
   if ((rc = relax_graph_for(ctx, c, &lg))) return rc;
   SB_CUDA(ctx, cudaGraphLaunch(lg->exec, ctx->stream));
@@ -1529,9 +1567,14 @@ extern "C" int sb_relax_full(sb_ctx* ctx, const sb_relax_params* p, sb_relax_sta
   RelaxConst c;
   int rc = relax_const(ctx, p, &c, kRelaxTile);
   if (rc) return rc;
-  LoopGraph* lg = nullptr;
-  if ((rc = relax_graph_for(ctx, c, &lg))) return rc;
-  SB_CUDA(ctx, cudaGraphLaunch(lg->exec, ctx->stream));
+  if (!ctx->use_graphs) {
+    rc = fx(ctx) ? relax_full_host_loop<true>(ctx, c) : relax_full_host_loop<false>(ctx, c);
+    if (rc) return rc;
+  } else {
+    LoopGraph* lg = nullptr;
+    if ((rc = relax_graph_for(ctx, c, &lg))) return rc;
+    SB_CUDA(ctx, cudaGraphLaunch(lg->exec, ctx->stream));
+  }
   SB_CUDA(ctx, cudaMemcpyAsync(ctx->rctl_host, ctx->rctl, sizeof(RelaxControl),
                                cudaMemcpyDeviceToHost, ctx->stream));
   SB_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

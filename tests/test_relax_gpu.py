@@ -257,3 +257,20 @@ def test_weighted_frontier_compacted_list_beyond_one_wave():
     assert np.array_equal(grid.download("b_eff"), want)
     assert not grid.download("frontier_reached").any()
     grid.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fx32"])
+def test_host_driven_sweeps_equal_sweep_graph(relax_golden, precision, monkeypatch):
+    """SOILB200_NO_GRAPH=1 (sweeps launched from the host, the mode profilers
+    use) gives the sweep graph's heights and iteration count."""
+    for name in relax_golden["full_names"][:3]:
+        h = relax_golden[f"full/{name}/h"]
+        spacing = tuple(relax_golden[f"full/{name}/spacing"])
+        angle = float(relax_golden[f"full/{name}/angle"])
+        monkeypatch.delenv("SOILB200_NO_GRAPH", raising=False)
+        a, sa = soilb200.relax_critical_slope(h, spacing, angle, 20000, 1e-8, precision=precision)
+        monkeypatch.setenv("SOILB200_NO_GRAPH", "1")
+        b, sb = soilb200.relax_critical_slope(h, spacing, angle, 20000, 1e-8, precision=precision)
+        monkeypatch.delenv("SOILB200_NO_GRAPH")
+        assert np.array_equal(a, b), name
+        assert sa.iterations == sb.iterations, name
