@@ -281,3 +281,80 @@ def physical_deposition(cfg: OracleConfig, b, h, q, depth):
     h2 = np.maximum(h - depth, 0.0)
     q2 = np.asarray(q) * keep[..., None]
     return (b2, h2, q2), energy_terms(cfg, b2, h2, q2)[3] - e_before
+
+
+# ---------------------------------------------------------------------------
+# Production record (reference bulk_interaction/warp_mobile_v2.py).
+# ---------------------------------------------------------------------------
+def vertex_weights(ny: int, nx: int, dx: float, dy: float) -> np.ndarray:
+    """Triangle-A-C vertex weights (runtime/bulk_state_authority.py:624-633)."""
+    w = np.zeros((ny, nx), dtype=np.float64)
+    f = dx * dy / 6.0
+    w[:-1, :-1] += 2.0 * f
+    w[:-1, 1:] += f
+    w[1:, 1:] += 2.0 * f
+    w[1:, :-1] += f
+    return w
+
+
+def production_summary(cfg: OracleConfig, density: float, b, h, q) -> np.ndarray:
+    """The seven weighted sums of the production ``summarize`` kernel
+    (warp_mobile_v2.py:28-54): volume, momentum x/y, max speed, kinetic,
+    potential and internal (pressure) energy."""
+    ny, nx = h.shape
+    w = vertex_weights(ny, nx, cfg.dx_m, cfg.dy_m)
+    wet = h > cfg.dry_tolerance_m
+    vel = _safe_div(q, h[..., None], wet[..., None])
+    spd = np.linalg.norm(vel, axis=-1)
+    g, K = cfg.gravity_m_s2, cfg.earth_pressure_coefficient
+    return np.asarray([
+        float(np.sum(h * w)),
+        float(np.sum(density * q[..., 0] * w)),
+        float(np.sum(density * q[..., 1] * w)),
+        float(np.max(np.where(wet, spd, 0.0), initial=0.0)),
+        float(np.sum(np.where(wet, 0.5 * density * h * spd * spd * w, 0.0))),
+        float(np.sum(density * g * h * b * w)),
+        float(np.sum(density * 0.5 * K * g * h * h * w)),
+    ])
+
+
+def production_record(cfg: OracleConfig, density: float, b0, h0, q0, st: OracleStep) -> dict:
+    """The WarpMobileStep fields of one production step (warp_mobile_v2.py:
+    151-245) from the state before it and the oracle's step.  The impulse and
+    dissipation totals are the reference solver's (``step`` above); the Warp
+    diagnostic kernel of the production path (mobile_v2_warp.py:178-232)
+    sums the same quantities and differs only in a cell that dries out within
+    a substep, where it adds the face update before the momentum is zeroed."""
+    before = production_summary(cfg, density, b0, h0, q0)
+    bp = np.asarray([before[1], before[2], 0.0])
+    if st.substeps == 0:
+        return dict(volume_before_m3=before[0], volume_after_m3=before[0],
+                    momentum_before_terrain_kg_m_s=bp, momentum_after_terrain_kg_m_s=bp,
+                    gravity_pressure_impulse_terrain_ns=np.zeros(3),
+                    basal_friction_impulse_terrain_ns=np.zeros(3),
+                    numerical_dissipative_impulse_terrain_ns=np.zeros(3),
+                    maximum_speed_m_s=before[3], substeps=0, cfl_limited=False,
+                    kinetic_energy_before_j=before[4], kinetic_energy_after_j=before[4],
+                    gravity_pressure_work_j=0.0, basal_friction_work_j=0.0,
+                    transport_numerical_energy_residual_j=0.0, transport_mass_residual_m3=0.0)
+    after = production_summary(cfg, density, st.b, st.h, st.q)
+    ap = np.asarray([after[1], after[2], 0.0])
+    gravity = np.asarray([st.conservative_impulse[0], st.conservative_impulse[1], 0.0]) * density
+    friction = np.asarray([st.friction_impulse[0], st.friction_impulse[1], 0.0]) * density
+    fwork = st.friction_dissipation * density
+    remaining, cfl_limited = st.dt_s, False
+    for sub in st.substep_dts:  # warp_mobile_v2.py:193-194
+        cfl_limited |= sub < remaining - 1.0e-14
+        remaining -= sub
+    return dict(volume_before_m3=before[0], volume_after_m3=after[0],
+                momentum_before_terrain_kg_m_s=bp, momentum_after_terrain_kg_m_s=ap,
+                gravity_pressure_impulse_terrain_ns=gravity,
+                basal_friction_impulse_terrain_ns=friction,
+                numerical_dissipative_impulse_terrain_ns=ap - bp - gravity - friction,
+                maximum_speed_m_s=after[3], substeps=st.substeps, cfl_limited=cfl_limited,
+                kinetic_energy_before_j=before[4], kinetic_energy_after_j=after[4],
+                gravity_pressure_work_j=(after[5] + after[6]) - (before[5] + before[6]),
+                basal_friction_work_j=fwork,
+                transport_numerical_energy_residual_j=(after[4] + after[5] + after[6])
+                - (before[4] + before[5] + before[6]) + fwork,
+                transport_mass_residual_m3=after[0] - before[0])
