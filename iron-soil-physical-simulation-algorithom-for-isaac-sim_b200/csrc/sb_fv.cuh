@@ -66,6 +66,9 @@ struct FvControl {
   unsigned long long pmax[4];    // "before" ledger maxima for the prologue: external, |q|, grad, wave
   unsigned int gen;              // persistent substep loop: barrier generation
   int pad2;
+  // persistent substep loop: substep k's wave-speed maximum goes to slot
+  // k % 3 (cleared two substeps ahead by the barrier)
+  unsigned long long wave3[3];
 };
 
 // Ledger record layout (filled by the ledger kernels of sb_ledger.cuh).
@@ -875,7 +878,6 @@ __global__ void __launch_bounds__(kThreads, 4)
                    FvControl* ctl, double* __restrict__ diag_acc) {
   __shared__ double fold[fold_words(kFvDiag)];
   __shared__ double wred[kThreads / 32];
-  __shared__ int s_done;
   __shared__ unsigned s_gen;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (kThreads / 32) + warp;
@@ -886,15 +888,32 @@ __global__ void __launch_bounds__(kThreads, 4)
   double acc[kFvDiag];
 #pragma unroll
   for (int k = 0; k < kFvDiag; ++k) acc[k] = 0.0;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      s_done = *(volatile int*)&ctl->done;
-      s_gen = *(volatile unsigned*)&ctl->gen;
-    }
-    __syncthreads();
-    if (s_done) break;
-    const double sub_dt = *(volatile double*)&ctl->sub_dt;
-    const int parity = *(volatile int*)&ctl->parity;
+  // The loop control (remaining time, dt, parity, substep count) is the same
+  // arithmetic in every CTA, so each CTA keeps its own copy in shared memory
+  // (thread 0 advances it): a barrier needs one wave-speed maximum (slot
+  // k % 3) and the release, and no CTA waits for one thread of another CTA to
+  // plan the next substep.
+  struct LoopCtl {
+    double remaining, sub_dt, max_cfl, wave;
+    int parity, substeps, cfl_limited, status, done;
+  };
+  __shared__ LoopCtl L;
+  if (threadIdx.x == 0) {
+    L.remaining = *(volatile double*)&ctl->remaining;
+    L.sub_dt = *(volatile double*)&ctl->sub_dt;
+    L.max_cfl = *(volatile double*)&ctl->max_cfl;
+    L.wave = *(volatile double*)&ctl->wave;
+    L.parity = *(volatile int*)&ctl->parity;
+    L.substeps = *(volatile int*)&ctl->substeps;
+    L.cfl_limited = *(volatile int*)&ctl->cfl_limited;
+    L.status = *(volatile int*)&ctl->status;
+    L.done = *(volatile int*)&ctl->done;
+  }
+  __syncthreads();
+  for (int k = 0; !L.done; ++k) {
+    const double sub_dt = L.sub_dt;
+    const int parity = L.parity;
+    if (threadIdx.x == 0) s_gen = *(volatile unsigned*)&ctl->gen;
     double wave = 0.0;
     fx_strip_run<FAST, true>(c, bsrc, parity ? h1 : h0, parity ? qx1 : qx0, parity ? qy1 : qy0,
                              parity ? h0 : h1, parity ? qx0 : qx1, parity ? qy0 : qy1, ext_x,
@@ -907,29 +926,65 @@ __global__ void __launch_bounds__(kThreads, 4)
       double m = 0.0;
 #pragma unroll
       for (int w = 0; w < kThreads / 32; ++w) m = fmax(m, wred[w]);
-      atomicMax(&ctl->wave_bits, (unsigned long long)__double_as_longlong(m));
+      atomicMax(&ctl->wave3[k % 3], (unsigned long long)__double_as_longlong(m));
       __threadfence();
       const unsigned prev = atomicAdd(&ctl->arrive, 1u);
+      bool failed = false;
       if (prev == gridDim.x - 1) {
-        __threadfence();
-        fv_advance(c, ctl, sub_dt, parity);
+        ctl->arrive = 0;
+        ctl->wave3[(k + 1) % 3] = 0ull;  // read by every CTA two barriers ago
         __threadfence();
         atomicAdd(&ctl->gen, 1u);  // release
       } else {
         unsigned polls = 0;
         while (*(volatile unsigned*)&ctl->gen == s_gen) {
           if (++polls > kFvBarrierPolls) {
-            ctl->wait_fail = 1;
-            ctl->status = 6;  // SB_ERR_WAIT_LIMIT
-            ctl->done = 1;
+            failed = true;
             break;
           }
-          __nanosleep(32);
+          if (polls > 64) __nanosleep(32);
         }
         __threadfence();
       }
+      // fv_advance on this CTA's copy
+      L.substeps += 1;
+      L.remaining -= sub_dt;
+      L.parity = parity ^ 1;
+      if (failed) {
+        L.status = 6;  // SB_ERR_WAIT_LIMIT
+        L.done = 1;
+        ctl->wait_fail = 1;
+      } else {
+        const double w = __longlong_as_double((long long)__ldcg(&ctl->wave3[k % 3]));
+        L.wave = w;
+        if (!(L.remaining > 1.0e-14)) {
+          L.done = 1;
+        } else if (L.substeps >= c.max_substeps) {
+          L.status = 2;  // SB_ERR_SUBSTEP_CAP
+          L.done = 1;
+        } else {  // plan_substep
+          const double rem = L.remaining;
+          const double stable = w <= 1.0e-14 ? rem : c.cfl * c.min_spacing / w;
+          const double sub = fmin(rem, stable);
+          if (sub < rem - 1.0e-14) L.cfl_limited = 1;
+          L.max_cfl = fmax(L.max_cfl, w * sub / c.min_spacing);
+          L.sub_dt = sub;
+        }
+      }
     }
     __syncthreads();
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // every CTA holds the same loop control; one writes it back
+    ctl->remaining = L.remaining;
+    ctl->sub_dt = L.sub_dt;
+    ctl->max_cfl = L.max_cfl;
+    ctl->wave = L.wave;
+    ctl->parity = L.parity;
+    ctl->substeps = L.substeps;
+    ctl->cfl_limited = L.cfl_limited;
+    ctl->status = L.status;
+    ctl->done = 1;
   }
   // the step's impulse/energy sums of this CTA, once
   const double* bt = block_fold<double, kFvDiag, kFvDiag>(acc, fold);

@@ -309,6 +309,7 @@ __device__ __forceinline__ void fv_begin_body(FvControl* ctl, const double* dt) 
     ctl->static_skip = 0;
     ctl->arrive = 0;
     ctl->wait_fail = 0;
+    for (int k = 0; k < 3; ++k) ctl->wave3[k] = 0ull;
   }
 }
 
