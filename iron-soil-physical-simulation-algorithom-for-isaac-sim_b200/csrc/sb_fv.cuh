@@ -920,7 +920,8 @@ __global__ void __launch_bounds__(kThreads, 4)
                              ext_y, strip, y0, y1, sub_dt, acc, wave);
     wave = warp_max(wave);
     if (lane == 0) wred[warp] = wave;
-    __threadfence();  // this thread's field writes before the arrival
+    // the CTA barrier orders every thread's field writes before thread 0's
+    // device-scope fence and arrival (the grid-barrier pattern: one fence)
     __syncthreads();
     if (threadIdx.x == 0) {
       double m = 0.0;
