@@ -544,11 +544,7 @@ def c1_after_cut(n: int = N, seed: int = 1):
     return b
 
 
-REPOSE_SCALES = (1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5)
-
-
-def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: float = 1e-4,
-               seed: int = 1, surface=None, label=None):
+def run_repose(args, eps_slope: float = 1e-4, seed: int = 1, surface=None, label=None):
     """Second headline metric: ms to repose at 701^2 after the cut, the learned
     proposal (tensor-core conv net, flux form, exact quanta) + plain sweeps
     against plain sweeps alone, same tolerance (eps * dx m), same start.  The
@@ -563,6 +559,8 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
         raise SystemExit(f"trained weights missing: {DEFAULT_WEIGHTS} (python -m soilb200.train_repose)")
     net = learned.ReposeNet.load(DEFAULT_WEIGHTS)
     fused_net = getattr(args, "net", "fused") == "fused"
+    sched = learned.SCHEDULE
+    scales, plain_between = sched["scales"], sched["plain_between"]
     b = c1_after_cut(seed=seed) if surface is None else surface
     k, datum = soilb200.choose_quantization(b)
     tol = eps_slope * DX
@@ -586,8 +584,10 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
         torch.cuda.synchronize()
         launches0 = g.kernel_launches()
         e0.record(stream)
+        adapt = dict(check_sweeps=sched["check_sweeps"], extra_scales=sched["extra_scales"],
+                     extra_between=sched["extra_between"]) if r else {}
         st = lr.relax(tol, max_iterations=400000, rounds=r,
-                      plain_between=plain_between if r else 0, scales=scales[:r])
+                      plain_between=plain_between if r else 0, scales=scales[:r], **adapt)
         e1.record(stream)
         e1.synchronize()
         s1 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())
@@ -616,7 +616,11 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
                        "network": ("one kernel for the four layers" if fused_net
                                    else "one launch per layer"),
                        "proposal_scales": list(scales),
-                       "plain_sweeps_between_proposals": plain_between, "tolerance_m": tol,
+                       "plain_sweeps_between_proposals": plain_between,
+                       "check_sweeps": sched["check_sweeps"],
+                       "extra_proposal_scales": list(sched["extra_scales"]),
+                       "plain_sweeps_between_extra_proposals": sched["extra_between"],
+                       "tolerance_m": tol,
                        "plain_ms": pm, "speedup_vs_plain": pm / lm,
                        "plain_iterations": plain[0][1], "learned_iterations": learn[0][1],
                        "converged": all(p[2] for p in plain + learn),
@@ -624,11 +628,12 @@ def run_repose(args, scales=REPOSE_SCALES, plain_between: int = 5, eps_slope: fl
             "gpu_launches": learn[0][4], "clocks": clocks.summary()}
 
 
-def repose_summary(seeds=(1, 2, 3, 4, 5), trials: int = 3):
+def repose_summary(seeds=(1, 2, 3, 4, 5, 6, 7, 8, 9), trials: int = 3):
     """The second metric for the default line: ms to repose, learned + plain
-    sweeps against plain sweeps, on the bench surface (seed 1) and on four
-    held-out surfaces (seeds 2-5, never used to train the network or to choose
-    its schedule), median of ``trials`` runs each."""
+    sweeps against plain sweeps, on the bench surface (seed 1), on four
+    held-out surfaces (seeds 2-5, never used to train the network or to tune
+    the adaptive part of its schedule) and on the four surfaces that tuned it
+    (seeds 6-9; 6 and 7 have long run-outs), median of ``trials`` runs each."""
     import math
     sub = argparse.Namespace(steps=trials, warmup=1)
     per = []
@@ -639,10 +644,11 @@ def repose_summary(seeds=(1, 2, 3, 4, 5), trials: int = 3):
                     "speedup": r["speedup_vs_plain"], "plain_sweeps": r["plain_iterations"],
                     "learned_sweeps": r["learned_iterations"], "converged": r["converged"],
                     "mass_ledger_exact": r["mass_ledger_exact"]})
-    held = [p["speedup"] for p in per if p["seed"] != 1]
+    held = [p["speedup"] for p in per if 2 <= p["seed"] <= 5]
     return {"metric": "ms to repose at 701^2 after the cut, learned proposal + plain sweeps vs "
                       "plain sweeps (35 deg, eps 1e-4)",
-            "bench_surface": per[0], "held_out": per[1:],
+            "bench_surface": per[0], "held_out": [p for p in per if 2 <= p["seed"] <= 5],
+            "tuning_surfaces": [p for p in per if p["seed"] >= 6],
             "held_out_geomean_speedup": math.exp(sum(math.log(x) for x in held) / len(held))
             if held else None,
             "all_geomean_speedup": math.exp(sum(math.log(p["speedup"]) for p in per) / len(per))}

@@ -271,6 +271,15 @@ def train(net: ReposeNet, pre: np.ndarray, post: np.ndarray, *, dx: float, dy: f
     return TrainStats(steps, first, last, time.perf_counter() - t0)
 
 
+# The proposal schedule the bench and the gain test use: four full-size and
+# four half-size rounds with 5 plain sweeps after each; a surface that is not
+# at the tolerance 20 sweeps later (a long run-out) gets six full and six
+# half rounds more, 2 sweeps after each (tuned on the post-cut config-1
+# surfaces of seeds 1 and 6-9; seeds 2-5 were kept for checking).
+SCHEDULE = dict(scales=(1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5), plain_between=5,
+                check_sweeps=20, extra_scales=(1.0,) * 6 + (0.5,) * 6, extra_between=2)
+
+
 class LearnedRelaxation:
     """Learned proposal rounds on a fixed-point grid's resident b_eff, then the
     plain sweep to the tolerance."""
@@ -320,7 +329,8 @@ class LearnedRelaxation:
                                                                self.tan_crit * scale), "apply")
 
     def relax(self, tolerance_m: float, max_iterations: int = 20000, rounds: int = 1,
-              spacing=None, plain_between: int = 0, scales=None):
+              spacing=None, plain_between: int = 0, scales=None, check_sweeps: int = 0,
+              extra_scales=None, extra_between: int = 0):
         """Learned rounds, then relax_critical_slope sweeps to the tolerance.
 
         With ``plain_between`` > 0 each proposal is followed by that many plain
@@ -329,24 +339,53 @@ class LearnedRelaxation:
         on the grid's stream without host round trips, and only the final
         sweeps to the tolerance report back.  ``scales`` (one positive factor
         per round, default 1.0 each) damps later proposals, whose full-size
-        transfers overshoot once the surface is near repose.  Returns that
-        RelaxStats, with ``iterations`` including the interleaved sweeps (as an
-        upper bound: the interleaved calls stop early when already converged)."""
+        transfers overshoot once the surface is near repose.
+
+        ``check_sweeps`` > 0 adapts the schedule to the surface: after the
+        rounds, at most that many plain sweeps run; a surface that has not
+        reached the tolerance by then (one whose run-out is long) gets the
+        further proposal rounds ``extra_scales`` (``extra_between`` sweeps
+        after each) before the sweeps to the tolerance.  Returns the final
+        RelaxStats, with ``iterations`` counting every sweep queued (the
+        interleaved calls as an upper bound: they stop early when already
+        converged)."""
         rounds = max(0, int(rounds))
         scales = [1.0] * rounds if scales is None else [float(x) for x in scales]
         if len(scales) != rounds:
             raise ValueError("[soilb200] scales needs one factor per proposal round")
+        extra = [float(x) for x in (extra_scales or ())]
         s0, s1 = spacing if spacing is not None else (self.grid.dy, self.grid.dx)
         lib = _lib.load()
-        between = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
-                                   int(max(plain_between, 1)), 0)
+
+        def sweeps(count: int):
+            p = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
+                                 int(max(count, 1)), 0)
+            _lib.check(self.grid.ctx, lib.sb_relax_sweeps(self.grid.ctx, p), "relax")
+
+        def full(limit: int):
+            p = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
+                                 int(limit), 0)
+            st = _lib.RelaxStats()
+            _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, p, st), "relax")
+            return st
+
+        done = 0
         for sc in scales:
             self.propose(1, sc)
             if plain_between > 0:
-                _lib.check(self.grid.ctx, lib.sb_relax_sweeps(self.grid.ctx, between), "relax")
-        params = _lib.RelaxParams(float(s0), float(s1), self.tan_crit, float(tolerance_m),
-                                  int(max_iterations), 0)
-        st = _lib.RelaxStats()
-        _lib.check(self.grid.ctx, lib.sb_relax_full(self.grid.ctx, params, st), "relax")
-        st.iterations = int(st.iterations) + rounds * max(plain_between, 0)
+                sweeps(plain_between)
+                done += plain_between
+        if check_sweeps > 0 and extra:
+            st = full(check_sweeps)
+            done += int(st.iterations)
+            if st.converged:
+                st.iterations = done
+                return st
+            for sc in extra:
+                self.propose(1, sc)
+                if extra_between > 0:
+                    sweeps(extra_between)
+                    done += extra_between
+        st = full(max_iterations)
+        st.iterations = int(st.iterations) + done
         return st

@@ -5,16 +5,17 @@ by the library's own tensor-core kernels) proposes per-face outflows that are
 applied in flux form; plain sweeps then finish until every face slope is at
 most tan(35 deg) + eps (eps = 1e-4, i.e. a height tolerance of eps * dx).
 On post-cut config-1 surfaces that the network never saw (seeds 2 and 4: not
-used for training nor for choosing the proposal schedule), the learned method
-must
+used for training nor for tuning the adaptive part of the proposal schedule,
+``learned.SCHEDULE``; and seed 6, whose long run-out takes the schedule's
+extra rounds), the learned method must
 
 * converge to the same tolerance as the plain sweep (the plain relaxation is
   the judge of the end state),
 * keep the volume ledger exact (integer quanta, both arms),
 * need far fewer sweeps (at most half the plain sweep count), and
 * be faster in device time by at least 2x (median of three runs; with the
-  one-kernel network inference the measured gain is 2.5x on seed 2 and
-  3.3x on seed 4, 3.9x on the bench surface).
+  one-kernel network inference the measured gain is 2.5-2.8x on seed 2,
+  3.3-3.7x on seed 4, 3.5-3.9x on seed 6, 3.9-4.3x on the bench surface).
 """
 
 import numpy as np
@@ -30,7 +31,8 @@ pytestmark = pytest.mark.gpu
 DX = 0.05
 DT = 1.0 / 60.0
 EPS = 1.0e-4
-SCALES = (1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5)
+SCHED = learned.SCHEDULE
+SCALES = SCHED["scales"]
 MIN_SPEEDUP = 2.0
 
 
@@ -43,7 +45,7 @@ def _post_cut(seed: int, n: int = 701) -> np.ndarray:
     return b
 
 
-@pytest.mark.parametrize("seed", [2, 4])
+@pytest.mark.parametrize("seed", [2, 4, 6])
 def test_trained_network_reaches_repose_faster_than_plain_sweeps(seed):
     assert DEFAULT_WEIGHTS.exists(), DEFAULT_WEIGHTS
     net = learned.ReposeNet.load(DEFAULT_WEIGHTS)
@@ -64,8 +66,11 @@ def test_trained_network_reaches_repose_faster_than_plain_sweeps(seed):
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
         e0.record(stream)
+        adapt = dict(check_sweeps=SCHED["check_sweeps"], extra_scales=SCHED["extra_scales"],
+                     extra_between=SCHED["extra_between"]) if rounds else {}
         st = lr.relax(tol, max_iterations=400000, rounds=rounds,
-                      plain_between=5 if rounds else 0, scales=SCALES[:rounds])
+                      plain_between=SCHED["plain_between"] if rounds else 0,
+                      scales=SCALES[:rounds], **adapt)
         e1.record(stream)
         e1.synchronize()
         s1 = int(np.rint((grid.download("b_eff") - datum) * q).astype(np.int64).sum())
