@@ -97,6 +97,8 @@ __global__ void __launch_bounds__(kThreads)
     tma_load_2d(s, parity_buf ? &tm1 : &tm0, g1, g0, &bar);
   }
   const bool loaded = mbar_wait(&bar, 0);
+  // a box wholly inside the domain needs no domain checks
+  const bool inner = g0 >= 0 && g1 >= 0 && g0 + kRelaxBox <= c.n0 && g1 + kRelaxBox <= c.n1;
   double worst = 0.0;
   for (int d = 0; d < 4; ++d) {
     int d0, d1;
@@ -125,24 +127,31 @@ __global__ void __launch_bounds__(kThreads)
       __syncthreads();
       // (2) Jacobi update of the active-parity pairs inside the box: only the
       // rows (d0 != 0) or columns (d0 == 0) whose global index has parity
-      // par hold an active endpoint a -- half the box, kRelaxBox/2 lines
+      // par hold an active endpoint a.  Sub-phase i (0-7) only needs pairs
+      // with endpoint a in [i, kRelaxBox - i) on both axes: every pair that
+      // touches a cell still exact after it (distance > i from the box edge)
+      // has a there, and its inputs are exact (distance >= i).
       if (loaded) {
-        constexpr int kHalf = kRelaxBox / 2;
+        const int lo = d * 2 + par, hi = kRelaxBox - lo, span = hi - lo;
         const int first = d0 ? ((par - g0) & 1) : ((par - g1) & 1);
-        for (int k = threadIdx.x; k < kHalf * kRelaxBox; k += kThreads) {
+        const int start = lo + ((first - lo) & 1);  // first line of the parity in [lo, hi)
+        const int lines = (hi - start + 1) >> 1;
+        for (int k = threadIdx.x; k < lines * span; k += kThreads) {
           int la0, la1;
           if (d0) {
-            la0 = first + 2 * (k / kRelaxBox);
-            la1 = k % kRelaxBox;
+            la0 = start + 2 * (k / span);
+            la1 = lo + k % span;
           } else {
-            la0 = k / kHalf;
-            la1 = first + 2 * (k % kHalf);
+            la0 = lo + k / lines;
+            la1 = start + 2 * (k % lines);
           }
           const int lb0 = la0 + d0, lb1 = la1 + d1;
           if (lb0 >= kRelaxBox || lb1 < 0 || lb1 >= kRelaxBox) continue;
           const int a0 = g0 + la0, a1 = g1 + la1, b0 = a0 + d0, b1 = a1 + d1;
-          if (a0 < 0 || a1 < 0 || a0 >= c.n0 || a1 >= c.n1) continue;
-          if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+          if (!inner) {
+            if (a0 < 0 || a1 < 0 || a0 >= c.n0 || a1 >= c.n1) continue;
+            if (b0 >= c.n0 || b1 < 0 || b1 >= c.n1) continue;
+          }
           const int ia = la0 * kRelaxBox + la1, ib = lb0 * kRelaxBox + lb1;
           const bool owned = la0 >= kRelaxHalo && la0 < kRelaxHalo + kRelaxTile &&
                              la1 >= kRelaxHalo && la1 < kRelaxHalo + kRelaxTile;
