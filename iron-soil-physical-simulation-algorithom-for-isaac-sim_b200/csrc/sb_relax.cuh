@@ -136,14 +136,18 @@ __global__ void __launch_bounds__(kThreads)
         const int first = d0 ? ((par - g0) & 1) : ((par - g1) & 1);
         const int start = lo + ((first - lo) & 1);  // first line of the parity in [lo, hi)
         const int lines = (hi - start + 1) >> 1;
+        // k / ncol by a multiply and shift (exact for k < 2^20 / 48)
+        const int ncol = d0 ? span : lines;
+        const unsigned inv = ((1u << 20) + (unsigned)ncol - 1u) / (unsigned)ncol;
         for (int k = threadIdx.x; k < lines * span; k += kThreads) {
+          const int q = (int)(((unsigned)k * inv) >> 20), rem = k - q * ncol;
           int la0, la1;
           if (d0) {
-            la0 = start + 2 * (k / span);
-            la1 = lo + k % span;
+            la0 = start + 2 * q;
+            la1 = lo + rem;
           } else {
-            la0 = lo + k / lines;
-            la1 = start + 2 * (k % lines);
+            la0 = lo + q;
+            la1 = start + 2 * rem;
           }
           const int lb0 = la0 + d0, lb1 = la1 + d1;
           if (lb0 >= kRelaxBox || lb1 < 0 || lb1 >= kRelaxBox) continue;
