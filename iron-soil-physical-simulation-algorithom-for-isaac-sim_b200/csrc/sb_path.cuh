@@ -126,6 +126,96 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Step start and bucket-cut entrainment in one block, for commands of up to
+// kPathStartCells cells: one thread reads dt and the command length from
+// the host-mapped inputs (one 16-byte read), starts the Mobile V2 loop
+// control and clears the labelling record; the block then entrains the
+// command (four host-link loads in flight per thread) and writes the
+// exchange record whole (block sums in a fixed order), so it needs no
+// clearing beforehand.  Same per-cell arithmetic as path_entrain_kernel.
+constexpr int kPathStartCells = 4096;
+
+template <bool FX>
+__global__ void __launch_bounds__(kThreads)
+    path_start_kernel(int ny, int nx, int pitch, double Q, double datum, double f,
+                      typename FvTypes<FX>::B* __restrict__ b,
+                      const typename FvTypes<FX>::B* __restrict__ z,
+                      typename FvTypes<FX>::H* __restrict__ h0,
+                      typename FvTypes<FX>::H* __restrict__ h1, FvControl* ctl,
+                      const PathInput* in, double* dt_dev, const int32_t* __restrict__ idx,
+                      const double* __restrict__ target, ExchangeOut* out, LabelOut* lout) {
+  __shared__ int s_count;
+  __shared__ double fold[fold_words(1)];
+  __shared__ long long ifold[fold_words(1)];
+  if (threadIdx.x == 0) {
+    const double2 v = __ldcv(reinterpret_cast<const double2*>(in));
+    *dt_dev = v.x;
+    s_count = (int)(unsigned)(__double_as_longlong(v.y) & 0xffffffffll);
+    fv_begin_body(ctl, dt_dev);
+  }
+  unsigned* lw = reinterpret_cast<unsigned*>(lout);
+  for (int k = threadIdx.x; k < (int)(sizeof(LabelOut) / 4); k += blockDim.x) lw[k] = 0u;
+  __syncthreads();
+  const int count = min(s_count, kPathStartCells);
+  typename FvTypes<FX>::H* h = ctl->parity ? h1 : h0;
+  long long vq = 0;
+  double vs = 0.0;
+  int bad = 0;
+  constexpr int kInFlight = 4;
+  for (int base = 0; base < count; base += kThreads * kInFlight) {
+    int iv[kInFlight];
+    double tv[kInFlight];
+#pragma unroll
+    for (int u = 0; u < kInFlight; ++u) {
+      const int k = base + u * kThreads + threadIdx.x;
+      iv[u] = k < count ? __ldcv(idx + k) : 0;
+      tv[u] = k < count ? __ldcv(target + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kInFlight; ++u) {
+      const int k = base + u * kThreads + threadIdx.x;
+      if (k >= count) continue;
+      const int i = iv[u];
+      const double tk = tv[u];
+      if (i < 0 || i >= ny * nx) {
+        bad = 1;
+        continue;
+      }
+      const int r = i / nx, c = i % nx;
+      const size_t gi = (size_t)r * pitch + c;
+      const int w6 = vertex_weight6(r, c, ny, nx);
+      if constexpr (FX) {
+        const long long avail = (long long)b[gi] - (long long)z[gi];
+        const long long req = (long long)b[gi] - (long long)rint((tk - datum) / Q);
+        long long d = req < avail ? req : avail;
+        if (d < 0) d = 0;
+        b[gi] = (int32_t)(b[gi] - d);
+        h[gi] = (int32_t)(h[gi] + d);
+        vq += d * w6;
+      } else {
+        const double avail = fmax(b[gi] - z[gi], 0.0);
+        const double d = fmin(fmax(b[gi] - tk, 0.0), avail);
+        b[gi] = b[gi] - d;
+        h[gi] = h[gi] + d;
+        vs += d * ((double)w6 * f);
+      }
+    }
+  }
+  const int any_bad = __syncthreads_or(bad);
+  const long long iv1[1] = {vq};
+  const double v1[1] = {vs};
+  const long long* qt = block_fold<long long, 1, 1>(iv1, ifold);
+  const double* st = block_fold<double, 1, 1>(v1, fold);
+  if (threadIdx.x == 0) {
+    out->volume_w6_quanta = qt[0];
+    out->volume_w_fp64 = st[0];
+    out->momentum_w[0] = 0.0;
+    out->momentum_w[1] = 0.0;
+    out->bad_index = any_bad ? 1 : 0;
+    out->arrive = 0u;
+  }
+}
+
 // Classification, persistence and gating (reference gpu_large_avalanche.py
 // :620-676 and the residual gate of v2_physics_core.py:930-1003).
 // One thread.

@@ -2302,7 +2302,26 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     prev = ev;
     return SB_OK;
   };
-  // 1. step start (loop control, cleared records), cut entrainment
+  // 1. step start (loop control, cleared records), cut entrainment: one
+  // block when the command buffer holds at most kPathStartCells cells (the
+  // entrainment stage is then part of the start stage), else a start kernel
+  // and a 64-block entrainment kernel
+  if (ctx->path_cap <= kPathStartCells) {
+    int pitch = ctx->pitch;
+    int nyv = ny, nxv = nx;
+    void *in_dev = nullptr, *idx_dev = nullptr, *val_dev = nullptr;
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&idx_dev, ctx->path_idx, 0));
+    SB_CUDA(ctx, cudaHostGetDevicePointer(&val_dev, ctx->path_val, 0));
+    void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
+                    &ctx->ctl, &in_dev, (void*)&ctx->dt_dev, &idx_dev, &val_dev, &ctx->xout,
+                    &ctx->lout};
+    if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_start_kernel<FX>, dim3(1), 0, args)))
+      return rc;
+    prev = node;
+    if ((rc = mark())) return rc;
+    if ((rc = mark())) return rc;
+  } else {
   {
     void* in_dev = nullptr;
     SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
@@ -2325,6 +2344,7 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
       return rc;
     prev = node;
     if ((rc = mark())) return rc;
+  }
   }
   // 2. Mobile V2 (same kernels as the standalone step graph)
   FvConst fc;

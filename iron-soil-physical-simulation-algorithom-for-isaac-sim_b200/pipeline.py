@@ -148,7 +148,10 @@ class PlainPath:
 
     def stage_times(self) -> dict:
         """Device ms per stage of the last fused step (needs the context created
-        with SOILB200_STAGE_EVENTS=1; empty otherwise)."""
+        with SOILB200_STAGE_EVENTS=1; empty otherwise).  While the cut command
+        buffer holds at most 4096 cells, one kernel starts the step and
+        entrains the cut: "start" then holds both and "entrainment" only the
+        stage marker."""
         import numpy as _np
         out = _np.zeros(16, dtype=_np.float32)
         n = int(_lib.load().sb_path_stage_times(self.grid.ctx, out.ctypes.data, out.size))
