@@ -173,6 +173,9 @@ NCU_TRAFFIC_BYTES = {
     # fv_loop_kernel at 4096^2, 4 substeps in the captured launch: 1.130031 GB
     # read + 805.078784 MB written
     "mobile_v2_4096": (1_130_031_000 + 805_078_784) // 4,
+    # fv_loop_kernel on the config-4 site (4096^2, 64 cuts), the first timed
+    # step's launch, 3 substeps: 841.548288 MB read + 592.439552 MB written
+    "site_c4_4096": (841_548_288 + 592_439_552) // 3,
 }
 
 
@@ -286,6 +289,8 @@ def run_gpu(args, rank: int, world: int, local_rank: int):
     b_fx = grid.download("b_eff")
     wet_cells = int(np.count_nonzero(h_fx > 0.0))
     site_extra = site_report(path, st, h_fx, local_rank) if site else None
+    if site_extra is not None and not args.no_repose:
+        site_extra["settle"] = site_settle(path, local_rank)
     ref64 = PlainPath(cfg["b_eff"], cfg["z_base"], dx=DX, material=material(),
                       device=local_rank, residual="gated", precision="fp64", fused=fused)
     for k in range(total_steps):
@@ -391,6 +396,51 @@ def site_report(path, last, h, device: int, reps: int = 10, tile: int = 64):
             "active_tile_fraction": float(tiles.mean()),
             "active_tile_rule": f"{tile}x{tile} tiles holding mobile material or unstable cells",
             "label_regions_check": int(st.connected_region_count)}
+
+
+def site_settle(path, device: int, trials: int = 3, eps_slope: float = 1e-4,
+                angle_deg: float = 35.0):
+    """Config-4 settle stage, on the site's own resident state after the timed
+    steps: PlainPath.settle relaxes the resting surface to 35 deg with the
+    learned proposal schedule + plain sweeps, and with the plain sweeps alone,
+    from the same start (restored untimed before every trial); device time
+    with CUDA events on the grid's stream, median of ``trials``."""
+    import torch
+    from soilb200 import learned
+    from soilb200.train_repose import DEFAULT_WEIGHTS
+    grid = path.grid
+    lr = learned.LearnedRelaxation(grid, learned.ReposeNet.load(DEFAULT_WEIGHTS), angle_deg)
+    stream = torch.cuda.ExternalStream(grid.stream_handle(), device=device)
+    start = grid.download("b_eff")
+    q = 2.0 ** grid.height_exponent
+
+    def quanta():
+        return int(np.rint((grid.download("b_eff") - grid.datum) * q).astype(np.int64).sum())
+
+    def one(schedule):
+        grid.upload("b_eff", start)
+        s0 = quanta()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        st = path.settle(lr, eps_slope * DX, schedule)
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), int(st.iterations), bool(st.converged), quanta() == s0
+
+    one(learned.PLAIN)  # warm: relaxation graphs, the network's workspace
+    one(learned.SCHEDULE)
+    plain = [one(learned.PLAIN) for _ in range(trials)]
+    learn = [one(learned.SCHEDULE) for _ in range(trials)]
+    grid.upload("b_eff", start)
+    pm = statistics.median(p[0] for p in plain)
+    lm = statistics.median(p[0] for p in learn)
+    return {"what": "PlainPath.settle on the site's resident state after the timed steps: "
+                    f"resting surface to {angle_deg:g} deg, eps {eps_slope:g}",
+            "learned_ms": lm, "plain_ms": pm, "speedup_vs_plain": pm / lm,
+            "learned_sweeps": learn[0][1], "plain_sweeps": plain[0][1],
+            "converged": all(p[2] for p in plain + learn),
+            "mass_ledger_exact": all(p[3] for p in plain + learn), "trials": trials}
 
 
 def run_mobile_large(args, n: int = 4096):
@@ -584,10 +634,7 @@ def run_repose(args, eps_slope: float = 1e-4, seed: int = 1, surface=None, label
         torch.cuda.synchronize()
         launches0 = g.kernel_launches()
         e0.record(stream)
-        adapt = dict(check_sweeps=sched["check_sweeps"], extra_scales=sched["extra_scales"],
-                     extra_between=sched["extra_between"]) if r else {}
-        st = lr.relax(tol, max_iterations=400000, rounds=r,
-                      plain_between=plain_between if r else 0, scales=scales[:r], **adapt)
+        st = lr.relax_scheduled(tol, sched if r else learned.PLAIN, max_iterations=400000)
         e1.record(stream)
         e1.synchronize()
         s1 = int(np.rint((g.download("b_eff") - datum) * q).astype(np.int64).sum())

@@ -278,6 +278,7 @@ def train(net: ReposeNet, pre: np.ndarray, post: np.ndarray, *, dx: float, dy: f
 # surfaces of seeds 1 and 6-9; seeds 2-5 were kept for checking).
 SCHEDULE = dict(scales=(1.0, 1.0, 1.0, 1.0, 0.5, 0.5, 0.5, 0.5), plain_between=5,
                 check_sweeps=20, extra_scales=(1.0,) * 6 + (0.5,) * 6, extra_between=2)
+PLAIN = dict(scales=())  # the plain sweep alone
 
 
 class LearnedRelaxation:
@@ -389,3 +390,19 @@ class LearnedRelaxation:
         st = full(max_iterations)
         st.iterations = int(st.iterations) + done
         return st
+
+    def relax_scheduled(self, tolerance_m: float, schedule=None, max_iterations: int = 400000,
+                        spacing=None):
+        """``relax`` with a whole proposal schedule (a dict with the keys of
+        ``SCHEDULE``, the default); ``schedule={"scales": ()}`` gives the plain
+        sweep alone."""
+        s = SCHEDULE if schedule is None else schedule
+        scales = tuple(s.get("scales", ()))
+        if not scales:
+            return self.relax(tolerance_m, max_iterations=max_iterations, rounds=0,
+                              spacing=spacing)
+        return self.relax(tolerance_m, max_iterations=max_iterations, rounds=len(scales),
+                          spacing=spacing, plain_between=int(s.get("plain_between", 0)),
+                          scales=scales, check_sweeps=int(s.get("check_sweeps", 0)),
+                          extra_scales=tuple(s.get("extra_scales", ())),
+                          extra_between=int(s.get("extra_between", 0)))

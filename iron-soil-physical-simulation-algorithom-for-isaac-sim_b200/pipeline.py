@@ -143,6 +143,21 @@ class PlainPath:
                              diag.largest_connected_cell_count, rounds,
                              float(mob.volume_after_m3), float(mob.maximum_speed_m_s))
 
+    def settle(self, relaxation, tolerance_m: float, schedule=None,
+               max_iterations: int = 400000):
+        """Relaxes this path's resting surface (the resident b_eff) to repose
+        in place, after the cuts: ``relaxation`` is a
+        ``learned.LearnedRelaxation`` bound to this path's grid; ``schedule``
+        its proposal schedule (``learned.SCHEDULE`` by default,
+        ``learned.PLAIN`` for the plain relax_critical_slope sweep alone,
+        reference ``slope_model.py:273-343``).  Either way the plain sweep
+        finishes until every face slope is at most tan(angle) + tolerance, and
+        the volume ledger stays exact (whole quanta).  Returns the RelaxStats
+        of the finishing sweeps, ``iterations`` counting every sweep."""
+        if relaxation.grid is not self.grid:
+            raise ValueError("[soilb200] settle needs a relaxation bound to this path's grid")
+        return relaxation.relax_scheduled(tolerance_m, schedule, max_iterations=max_iterations)
+
     STAGES = ("start", "entrainment", "before_ledger", "substeps_and_yield_tiles", "border_merge",
               "compression", "reduction_classification", "previous_and_seeds", "residual_frontier")
 
