@@ -351,9 +351,8 @@ int sb_path_stage_times(sb_ctx* ctx, float* out_ms, int capacity);
  * this call.  Limit: ny*nx <= 524288 cells (SB_ERR_CAPACITY beyond).  The
  * first call on a device looks up the scratch address with the device
  * current and keeps it for the process (after cudaDeviceReset the module is
- * reloaded at a new address, so do not call this across a device reset);
- * make that first call before any stream capture.  Every call
- * shares the one scratch array (its contents persist; each call clears what
+ * reloaded at a new address, so do not call this across a device reset).
+ * Every call shares the one scratch array (its contents persist; each call clears what
  * must start at zero), so calls that overlap on the GPU race: serialise them
  * (one stream, or wait between calls).  Blocks until the stats are read.
  * dx_m/dy_m only scale largest_connected_area_m2. */
