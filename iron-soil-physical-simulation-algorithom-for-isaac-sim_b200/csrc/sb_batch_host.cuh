@@ -100,6 +100,10 @@ FvConst batch_patch_const(const sb_patch_desc& d, int pitch, int rows, const sb_
   c.kg = p->earth_pressure_coefficient * p->gravity_m_s2;
   c.min_spacing = d.dx_m < d.dy_m ? d.dx_m : d.dy_m;
   c.Q = std::ldexp(1.0, -d.height_exponent);
+  c.gsx[0] = c.Q / (2.0 * c.dx);
+  c.gsx[1] = c.Q / c.dx;
+  c.gsy[0] = c.Q / (2.0 * c.dy);
+  c.gsy[1] = c.Q / c.dy;
   c.Kf = (float)c.K;
   c.KGf = (float)c.kg;
   c.HKGf = (float)c.c_half;

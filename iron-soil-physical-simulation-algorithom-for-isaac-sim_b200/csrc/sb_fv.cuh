@@ -40,6 +40,7 @@ struct FvConst {
   double dx, dy, K, g, cfl, dry, mu_g, c_half, kg, min_spacing;
   // fixed-point constants
   double Q;
+  double gsx[2], gsy[2];  // ledger gradient scales: {Q / (2 dx), Q / dx}, {Q / (2 dy), Q / dy}
   float Kf, KGf, HKGf, Qf, invQf, dryf, QKf;  // QKf = float(Q / K)
   int max_substeps;
   int has_external;

@@ -13,88 +13,70 @@
 
 namespace sb {
 
-// Ledger contributions of cell (r, col): sums into v[0 .. L_NSUM), maxima
-// into v[L_NSUM .. L_NP), exact quanta sums into iq0..iq2 (FX).
-template <bool FX>
-__device__ __forceinline__ void ledger_cell(const FvConst& c,
-                                            const typename FvTypes<FX>::B* __restrict__ b,
-                                            const typename FvTypes<FX>::B* __restrict__ z,
-                                            const typename FvTypes<FX>::H* __restrict__ h,
-                                            const typename FvTypes<FX>::R* __restrict__ qx,
-                                            const typename FvTypes<FX>::R* __restrict__ qy,
-                                            const typename FvTypes<FX>::R* __restrict__ ext_x,
-                                            const typename FvTypes<FX>::R* __restrict__ ext_y,
-                                            double datum, int r, int col, double* v,
-                                            long long& iq0, long long& iq1, long long& iq2) {
-  const size_t gi = (size_t)r * c.pitch + col;
-  const int w6 = vertex_weight6(r, col, c.ny, c.nx);
-  double hv, bv;
-  const double qxv = (double)qx[gi], qyv = (double)qy[gi];
-  // gradient of the free surface b + h (np.gradient, edge_order 1)
+// FX: squared free-surface gradient of cell (r, col) (np.gradient,
+// edge_order 1) from integer b + h differences, scaled by Q / (2 dx) inside
+// and Q / dx on the edges (c.gsx / c.gsy, computed on the host).
+__device__ __forceinline__ double fx_grad2(const FvConst& c, const int32_t* __restrict__ b,
+                                           const int32_t* __restrict__ h, int r, int col) {
+  const bool inx = col > 0 && col + 1 < c.nx, iny = r > 0 && r + 1 < c.ny;
   const int cl = col > 0 ? col - 1 : col, cr = col + 1 < c.nx ? col + 1 : col;
   const int rd = r > 0 ? r - 1 : r, ru = r + 1 < c.ny ? r + 1 : r;
-  const double denx = (col > 0 && col + 1 < c.nx) ? 2.0 * c.dx : c.dx;
-  const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
   const size_t il = (size_t)r * c.pitch + cl, ir = (size_t)r * c.pitch + cr;
   const size_t idn = (size_t)rd * c.pitch + col, iup = (size_t)ru * c.pitch + col;
-  double grad;  // FX: squared gradient (sqrt taken once, after the max)
-  if constexpr (FX) {
-    const int hq = h[gi];
-    hv = (double)hq * c.Q;
-    bv = (double)b[gi] * c.Q + datum;
-    iq0 += hq;
-    iq1 += (long long)hq * w6;
-    const long long rest = (long long)b[gi] - (long long)z[gi];
-    iq2 += (rest > 0 ? rest : 0) * w6;
-    const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
-    const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
-    // (H difference) * Q / spacing with the spacing folded into one constant
-    const double gx = (double)(Hr - Hl) * ((col > 0 && col + 1 < c.nx) ? c.Q / (2.0 * c.dx) : c.Q / c.dx);
-    const double gy = (double)(Hu - Hd) * ((r > 0 && r + 1 < c.ny) ? c.Q / (2.0 * c.dy) : c.Q / c.dy);
-    grad = gx * gx + gy * gy;
-  } else {
-    hv = h[gi];
-    bv = b[gi];
-    v[L_HSUM] += hv;
-    v[L_HSUM_W] += hv * w6;
-    v[L_REST_W] += fmax(b[gi] - z[gi], 0.0) * w6;
-    const double gx = ((b[ir] + h[ir]) - (b[il] + h[il])) / denx;
-    const double gy = ((b[iup] + h[iup]) - (b[idn] + h[idn])) / deny;
-    grad = hypot(gx, gy);
+  const long long Hl = (long long)b[il] + h[il], Hr = (long long)b[ir] + h[ir];
+  const long long Hd = (long long)b[idn] + h[idn], Hu = (long long)b[iup] + h[iup];
+  const double gx = (double)(Hr - Hl) * (inx ? c.gsx[0] : c.gsx[1]);
+  const double gy = (double)(Hu - Hd) * (iny ? c.gsy[0] : c.gsy[1]);
+  return gx * gx + gy * gy;
+}
+
+// FX ledger contributions of cell (r, col).  Every load of the cell is
+// issued before any branch (one memory round trip per cell).  A cell with no
+// mobile material and no momentum (most of a terrain) contributes an exact
+// zero to every sum and to every maximum other than the resting volume, the
+// gradient, the external forcing and the depth minimum; adding a zero leaves
+// a sum that starts at +0 bit for bit unchanged, so only those are evaluated.
+__device__ __forceinline__ void ledger_cell_fx(const FvConst& c, const int32_t* __restrict__ b,
+                                               const int32_t* __restrict__ z,
+                                               const int32_t* __restrict__ h,
+                                               const float* __restrict__ qx,
+                                               const float* __restrict__ qy,
+                                               const float* __restrict__ ext_x,
+                                               const float* __restrict__ ext_y, double datum,
+                                               int r, int col, double* v, long long& iq0,
+                                               long long& iq1, long long& iq2) {
+  const size_t gi = (size_t)r * c.pitch + col;
+  const int w6 = vertex_weight6(r, col, c.ny, c.nx);
+  const int hq = h[gi], bq = b[gi], zq = z[gi];
+  const float qxf = qx[gi], qyf = qy[gi];
+  const double grad = fx_grad2(c, b, h, r, col);  // squared; sqrt after the max
+  const long long rest = (long long)bq - (long long)zq;
+  iq2 += (rest > 0 ? rest : 0) * w6;
+  v[L_MAXGRAD] = fmax(v[L_MAXGRAD], grad);
+  if (c.has_external)
+    v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
+  const double hv = (double)hq * c.Q;
+  v[L_NEGMINH] = fmax(v[L_NEGMINH], -hv);
+  if (hq == 0 && qxf == 0.f && qyf == 0.f) return;
+  const double bv = (double)bq * c.Q + datum;
+  const double qxv = (double)qxf, qyv = (double)qyf;
+  iq0 += hq;
+  iq1 += (long long)hq * w6;
+  double s2 = 0.0, e = 0.0, wave = 0.0;  // empty cell: no velocity, no celerity
+  if (hq != 0) {
+    const float hn = (float)hq * c.Qf;
+    float vx = 0.f, vy = 0.f;
+    if (hn > c.dryf) {
+      const float inv = 1.0f / hn;
+      vx = qxf * inv;
+      vy = qyf * inv;
+    }
+    wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
   }
-  const bool wet = hv > c.dry;
-  double s2 = 0.0, spd = 0.0, e = 0.0, wave;
-  if constexpr (FX) {
-    if (h[gi] == 0) {
-      wave = 0.0;  // empty cell: no velocity, no celerity (the expression below gives 0)
-    } else {
-      const float hn = (float)h[gi] * c.Qf;
-      float vx = 0.f, vy = 0.f;
-      if (hn > c.dryf) {
-        const float inv = 1.0f / hn;
-        vx = qx[gi] * inv;
-        vy = qy[gi] * inv;
-      }
-      wave = (double)(sqrtf(vx * vx + vy * vy) + sqrtf(c.KGf * hn));
-    }
-    if (wet) {  // one reciprocal: e = |q|^2 / h (= h |u|^2), s2 = e / h
-      const double inv = 1.0 / hv;
-      e = (qxv * qxv + qyv * qyv) * inv;
-      s2 = e * inv;
-    }
-    spd = s2;  // squared speed; sqrt after the max
-  } else {
-    double vx = 0.0, vy = 0.0;
-    if (wet) {
-      vx = qxv / hv;
-      vy = qyv / hv;
-    }
-    wave = sqrt(vx * vx + vy * vy) + sqrt(c.kg * fmax(hv, 0.0));
-    if (wet) {
-      s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
-      spd = sqrt(s2);
-      e = hv * s2;
-    }
+  if (hv > c.dry) {  // one reciprocal: e = |q|^2 / h (= h |u|^2), s2 = e / h
+    const double inv = 1.0 / hv;
+    e = (qxv * qxv + qyv * qyv) * inv;
+    s2 = e * inv;
   }
   v[L_QX] += qxv;
   v[L_QY] += qyv;
@@ -106,13 +88,76 @@ __device__ __forceinline__ void ledger_cell(const FvConst& c,
   v[L_HB_W] += hv * bv * w6;
   v[L_HH] += hv * hv;
   v[L_HH_W] += hv * hv * w6;
-  v[L_MAXSPEED] = fmax(v[L_MAXSPEED], spd);
-  v[L_NEGMINH] = fmax(v[L_NEGMINH], -hv);
+  v[L_MAXSPEED] = fmax(v[L_MAXSPEED], s2);  // squared speed; sqrt after the max
   v[L_MAXQ] = fmax(v[L_MAXQ], fmax(fabs(qxv), fabs(qyv)));
-  v[L_MAXGRAD] = fmax(v[L_MAXGRAD], grad);
   v[L_MAXWAVE] = fmax(v[L_MAXWAVE], wave);
-  if (c.has_external)
-    v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
+}
+
+// Ledger contributions of cell (r, col): sums into v[0 .. L_NSUM), maxima
+// into v[L_NSUM .. L_NP), exact quanta sums into iq0..iq2 (FX: ledger_cell_fx).
+template <bool FX>
+__device__ __forceinline__ void ledger_cell(const FvConst& c,
+                                            const typename FvTypes<FX>::B* __restrict__ b,
+                                            const typename FvTypes<FX>::B* __restrict__ z,
+                                            const typename FvTypes<FX>::H* __restrict__ h,
+                                            const typename FvTypes<FX>::R* __restrict__ qx,
+                                            const typename FvTypes<FX>::R* __restrict__ qy,
+                                            const typename FvTypes<FX>::R* __restrict__ ext_x,
+                                            const typename FvTypes<FX>::R* __restrict__ ext_y,
+                                            double datum, int r, int col, double* v,
+                                            long long& iq0, long long& iq1, long long& iq2) {
+  if constexpr (FX) {
+    ledger_cell_fx(c, b, z, h, qx, qy, ext_x, ext_y, datum, r, col, v, iq0, iq1, iq2);
+  } else {
+    const size_t gi = (size_t)r * c.pitch + col;
+    const int w6 = vertex_weight6(r, col, c.ny, c.nx);
+    const double qxv = (double)qx[gi], qyv = (double)qy[gi];
+    // gradient of the free surface b + h (np.gradient, edge_order 1)
+    const int cl = col > 0 ? col - 1 : col, cr = col + 1 < c.nx ? col + 1 : col;
+    const int rd = r > 0 ? r - 1 : r, ru = r + 1 < c.ny ? r + 1 : r;
+    const double denx = (col > 0 && col + 1 < c.nx) ? 2.0 * c.dx : c.dx;
+    const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
+    const size_t il = (size_t)r * c.pitch + cl, ir = (size_t)r * c.pitch + cr;
+    const size_t idn = (size_t)rd * c.pitch + col, iup = (size_t)ru * c.pitch + col;
+    const double hv = h[gi];
+    const double bv = b[gi];
+    v[L_HSUM] += hv;
+    v[L_HSUM_W] += hv * w6;
+    v[L_REST_W] += fmax(b[gi] - z[gi], 0.0) * w6;
+    const double gx = ((b[ir] + h[ir]) - (b[il] + h[il])) / denx;
+    const double gy = ((b[iup] + h[iup]) - (b[idn] + h[idn])) / deny;
+    const double grad = hypot(gx, gy);
+    const bool wet = hv > c.dry;
+    double s2 = 0.0, spd = 0.0, e = 0.0;
+    double vx = 0.0, vy = 0.0;
+    if (wet) {
+      vx = qxv / hv;
+      vy = qyv / hv;
+    }
+    const double wave = sqrt(vx * vx + vy * vy) + sqrt(c.kg * fmax(hv, 0.0));
+    if (wet) {
+      s2 = (qxv * qxv + qyv * qyv) / (hv * hv);
+      spd = sqrt(s2);
+      e = hv * s2;
+    }
+    v[L_QX] += qxv;
+    v[L_QY] += qyv;
+    v[L_QX_W] += qxv * w6;
+    v[L_QY_W] += qyv * w6;
+    v[L_HS2] += e;
+    v[L_HS2_W] += e * w6;
+    v[L_HB] += hv * bv;
+    v[L_HB_W] += hv * bv * w6;
+    v[L_HH] += hv * hv;
+    v[L_HH_W] += hv * hv * w6;
+    v[L_MAXSPEED] = fmax(v[L_MAXSPEED], spd);
+    v[L_NEGMINH] = fmax(v[L_NEGMINH], -hv);
+    v[L_MAXQ] = fmax(v[L_MAXQ], fmax(fabs(qxv), fabs(qyv)));
+    v[L_MAXGRAD] = fmax(v[L_MAXGRAD], grad);
+    v[L_MAXWAVE] = fmax(v[L_MAXWAVE], wave);
+    if (c.has_external)
+      v[L_MAXEXT] = fmax(v[L_MAXEXT], fmax(fabs((double)ext_x[gi]), fabs((double)ext_y[gi])));
+  }
 }
 
 // Block reduction of per-thread ledger values into one block's partials, in a
@@ -221,6 +266,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     int it = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
     int r = it / strips, s = it - r * strips;
     const int dr = nwarps / strips, ds = nwarps - dr * strips;
+#pragma unroll 2
     for (; it < items; it += nwarps) {
       const int col = (s << 5) + lane;
       if (col < c.nx)

@@ -320,6 +320,10 @@ FvConst make_const(const sb_ctx* ctx, const sb_mobile_params* p) {
   c.kg = p->earth_pressure_coefficient * p->gravity_m_s2;
   c.min_spacing = ctx->d.dx_m < ctx->d.dy_m ? ctx->d.dx_m : ctx->d.dy_m;
   c.Q = ctx->quantum;
+  c.gsx[0] = c.Q / (2.0 * c.dx);
+  c.gsx[1] = c.Q / c.dx;
+  c.gsy[0] = c.Q / (2.0 * c.dy);
+  c.gsy[1] = c.Q / c.dy;
   c.Kf = (float)c.K;
   c.KGf = (float)c.kg;
   c.HKGf = (float)c.c_half;
