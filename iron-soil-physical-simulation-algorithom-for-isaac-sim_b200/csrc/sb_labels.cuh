@@ -87,6 +87,55 @@ __device__ __forceinline__ double free_surface_diff(const typename FvTypes<FX>::
   }
 }
 
+// Fixed-point yield constants in float32, each one rounding of its double
+// expression: gradient scales {Q / (2 dx), Q / dx} and {Q / (2 dy), Q / dy},
+// the quantum, the mobilization depth, density * gravity, cohesion, the start
+// and stop tangents, their difference and the dry tolerance.
+struct YieldF {
+  float sx[2], sy[2];
+  float Q, depth, rg, coh, ts, tp, dts, dry;
+};
+
+__device__ __forceinline__ YieldF yield_constants(const LabelConst& c) {
+  YieldF y;
+  y.sx[0] = (float)(c.Q / (2.0 * c.dx));
+  y.sx[1] = (float)(c.Q / c.dx);
+  y.sy[0] = (float)(c.Q / (2.0 * c.dy));
+  y.sy[1] = (float)(c.Q / c.dy);
+  y.Q = (float)c.Q;
+  y.depth = (float)c.mob_depth;
+  y.rg = (float)(c.density * c.gravity);
+  y.coh = (float)c.cohesion;
+  y.ts = (float)c.tan_start;
+  y.tp = (float)c.tan_stop;
+  y.dts = (float)(c.tan_start - c.tan_stop);
+  y.dry = (float)c.dry;
+  return y;
+}
+
+// Arc tangent of x >= 0 in float32 by the polynomial of Abramowitz & Stegun,
+// Handbook of Mathematical Functions, 4.4.49 (Hastings): on [0, 1]
+// atan(x) = x (1 + a2 x^2 + ... + a16 x^16) with |error| <= 2e-8; for x > 1,
+// pi/2 - atan(1/x).  Evaluated in float32 with separate multiplies and adds
+// (Horner), so a NumPy float32 restatement gives the same bits; error against
+// the exact value <= 2e-7 rad.
+__device__ __forceinline__ float atan_as4449(float x) {
+  const bool inv = x > 1.0f;
+  const float t = inv ? 1.0f / x : x;
+  const float t2 = t * t;
+  float p = 0.0028662257f;
+  p = -0.0161657367f + t2 * p;
+  p = 0.0429096138f + t2 * p;
+  p = -0.0752896400f + t2 * p;
+  p = 0.1065626393f + t2 * p;
+  p = -0.1420889944f + t2 * p;
+  p = 0.1999355085f + t2 * p;
+  p = -0.3333314528f + t2 * p;
+  p = 1.0f + t2 * p;
+  const float r = t * p;
+  return inv ? 1.5707963267948966f - r : r;
+}
+
 __device__ __forceinline__ int lfind(const int* lab, int x) {
   for (int i = 0; i < kLabelTile * kLabelTile && lab[x] != x; ++i) x = lab[x];
   return x;
@@ -160,6 +209,7 @@ __global__ void __launch_bounds__(kLabelInitThreads, 3)
   const typename FvTypes<FX>::H* h = P ? h1 : h0;
   const typename FvTypes<FX>::R* qx = P ? qx1 : qx0;
   const typename FvTypes<FX>::R* qy = P ? qy1 : qy0;
+  const YieldF yf = yield_constants(c);
   for (int li = threadIdx.x; li < kLabelTile * kLabelTile; li += kLabelInitThreads) {
     const int ly = li / kLabelTile, lx = li % kLabelTile;
     const int r = gy0 + ly, col = gx0 + lx;
@@ -169,31 +219,53 @@ __global__ void __launch_bounds__(kLabelInitThreads, 3)
       const long long flat = (long long)r * c.nx + col;
       const int cl = col > 0 ? col - 1 : col, cr = col + 1 < c.nx ? col + 1 : col;
       const int rd = r > 0 ? r - 1 : r, ru = r + 1 < c.ny ? r + 1 : r;
-      const double denx = (col > 0 && col + 1 < c.nx) ? 2.0 * c.dx : c.dx;
-      const double deny = (r > 0 && r + 1 < c.ny) ? 2.0 * c.dy : c.dy;
-      const double gx = free_surface_diff<FX>(b, h, (size_t)r * c.pitch + cr,
-                                              (size_t)r * c.pitch + cl, c.Q) / denx;
-      const double gy = free_surface_diff<FX>(b, h, (size_t)ru * c.pitch + col,
-                                              (size_t)rd * c.pitch + col, c.Q) / deny;
-      const double mag = sqrt(gx * gx + gy * gy);
-      double layer, mob;
+      const bool inx = col > 0 && col + 1 < c.nx, iny = r > 0 && r + 1 < c.ny;
+      double mob;
+      bool settled;  // stop margin <= 0
       if constexpr (FX) {
+        // float32 throughout (the ledger and the exchange sums are the only
+        // FP64 work of the fixed-point path)
+        const long long dxq = ((long long)b[(size_t)r * c.pitch + cr] + h[(size_t)r * c.pitch + cr]) -
+                              ((long long)b[(size_t)r * c.pitch + cl] + h[(size_t)r * c.pitch + cl]);
+        const long long dyq = ((long long)b[(size_t)ru * c.pitch + col] + h[(size_t)ru * c.pitch + col]) -
+                              ((long long)b[(size_t)rd * c.pitch + col] + h[(size_t)rd * c.pitch + col]);
+        const float gx = (float)dxq * (inx ? yf.sx[0] : yf.sx[1]);
+        const float gy = (float)dyq * (iny ? yf.sy[0] : yf.sy[1]);
+        const float mag = sqrtf(gx * gx + gy * gy);
         const long long dq = (long long)b[gi] - (long long)z[gi];
-        layer = fmin((double)(dq > 0 ? dq : 0) * c.Q, c.mob_depth);
+        const float layer = fminf((float)(dq > 0 ? dq : 0) * yf.Q, yf.depth);
         mob = (double)h[gi] * c.Q;
+        const float norm = sqrtf(1.0f + mag * mag);
+        const float drive = yf.rg * layer * mag / norm;
+        const float normal = yf.rg * layer / norm;
+        const float start_margin = drive - (yf.coh + normal * yf.ts);
+        const float stop_margin = drive - (yf.coh + normal * yf.tp);
+        const float sev = fminf(fmaxf(stop_margin / fmaxf(normal * yf.dts, 1.0e-12f), 0.f), 1.f);
+        slope_out[flat] = atan_as4449(mag);
+        severity_out[flat] = sev;
+        u = (layer > yf.dry && start_margin > 0.f) ? 1 : 0;
+        settled = stop_margin <= 0.f;
       } else {
-        layer = fmin(fmax(b[gi] - z[gi], 0.0), c.mob_depth);
+        const double denx = inx ? 2.0 * c.dx : c.dx;
+        const double deny = iny ? 2.0 * c.dy : c.dy;
+        const double gx = free_surface_diff<FX>(b, h, (size_t)r * c.pitch + cr,
+                                                (size_t)r * c.pitch + cl, c.Q) / denx;
+        const double gy = free_surface_diff<FX>(b, h, (size_t)ru * c.pitch + col,
+                                                (size_t)rd * c.pitch + col, c.Q) / deny;
+        const double mag = sqrt(gx * gx + gy * gy);
+        const double layer = fmin(fmax(b[gi] - z[gi], 0.0), c.mob_depth);
         mob = h[gi];
+        const double norm = sqrt(1.0 + mag * mag);
+        const double drive = c.density * c.gravity * layer * mag / norm;
+        const double normal = c.density * c.gravity * layer / norm;
+        const double start_margin = drive - (c.cohesion + normal * c.tan_start);
+        const double stop_margin = drive - (c.cohesion + normal * c.tan_stop);
+        const double sev = fmin(fmax(stop_margin / fmax(normal * (c.tan_start - c.tan_stop), 1.0e-12), 0.0), 1.0);
+        slope_out[flat] = atan(mag);
+        severity_out[flat] = sev;
+        u = (layer > c.dry && start_margin > 0.0) ? 1 : 0;
+        settled = stop_margin <= 0.0;
       }
-      const double norm = sqrt(1.0 + mag * mag);
-      const double drive = c.density * c.gravity * layer * mag / norm;
-      const double normal = c.density * c.gravity * layer / norm;
-      const double start_margin = drive - (c.cohesion + normal * c.tan_start);
-      const double stop_margin = drive - (c.cohesion + normal * c.tan_stop);
-      const double sev = fmin(fmax(stop_margin / fmax(normal * (c.tan_start - c.tan_stop), 1.0e-12), 0.0), 1.0);
-      slope_out[flat] = (typename FvTypes<FX>::R)atan(mag);
-      severity_out[flat] = (typename FvTypes<FX>::R)sev;
-      u = (layer > c.dry && start_margin > 0.0) ? 1 : 0;
       parent[flat] = u ? (int)flat : -1;
       if (u) {
         roots.count[flat] = 0;
@@ -215,7 +287,7 @@ __global__ void __launch_bounds__(kLabelInitThreads, 3)
         }
         const double w = (double)vertex_weight6(r, col, c.ny, c.nx) * (c.dx * c.dy / 6.0);
         const bool resolved = (export_cum[flat] - export_base[flat]) > c.dry * w;
-        if (speed <= c.activity_speed && (resolved || stop_margin <= 0.0)) latch[flat] = 0;
+        if (speed <= c.activity_speed && (resolved || settled)) latch[flat] = 0;
       }
     }
     lab[li] = u ? li : -1;

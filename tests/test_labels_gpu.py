@@ -99,6 +99,13 @@ def test_fx32_yield_labels_equal_fixed_point_oracle():
                      mobilization_depth=0.08, dry=1e-8, fixed_point=True, quantum=2.0 ** -k)
     want = L.canonical_labels(y["unstable"], 8)
     assert np.array_equal(labels, want)
+    # the float32 yield fields bit for bit, and the slope within the arc
+    # tangent's bound of the double-precision angle of the same gradient
+    slope = grid.download("slope").astype(np.float32)
+    assert np.array_equal(slope, y["slope"])
+    assert np.array_equal(grid.download("severity").astype(np.float32), y["severity"])
+    exact = np.arctan(np.hypot(y["gx"].astype(np.float64), y["gy"].astype(np.float64)))
+    assert np.abs(slope - exact).max() <= 3.0e-7
     regions, largest, winner, total = L.component_summary(want)
     assert (st.connected_region_count, st.largest_connected_cell_count, st.winner_root) == \
         (regions, largest, winner)
