@@ -132,7 +132,10 @@ __global__ void __launch_bounds__(kThreads)
 // control and clears the labelling record; the block then entrains the
 // command (four host-link loads in flight per thread) and writes the
 // exchange record whole (block sums in a fixed order), so it needs no
-// clearing beforehand.  Same per-cell arithmetic as path_entrain_kernel.
+// clearing beforehand.  The command's first kThreads * 4 entries are read
+// together with the length (the buffers hold ``cap`` entries; those past the
+// length are not used), so a command of up to 1024 cells costs one host-link
+// round trip.  Same per-cell arithmetic as path_entrain_kernel.
 constexpr int kPathStartCells = 4096;
 
 template <bool FX>
@@ -143,10 +146,20 @@ __global__ void __launch_bounds__(kThreads)
                       typename FvTypes<FX>::H* __restrict__ h0,
                       typename FvTypes<FX>::H* __restrict__ h1, FvControl* ctl,
                       const PathInput* in, double* dt_dev, const int32_t* __restrict__ idx,
-                      const double* __restrict__ target, ExchangeOut* out, LabelOut* lout) {
+                      const double* __restrict__ target, int cap, ExchangeOut* out,
+                      LabelOut* lout) {
   __shared__ int s_count;
   __shared__ double fold[fold_words(1)];
   __shared__ long long ifold[fold_words(1)];
+  constexpr int kInFlight = 4;
+  int iv0[kInFlight];
+  double tv0[kInFlight];
+#pragma unroll
+  for (int u = 0; u < kInFlight; ++u) {
+    const int k = u * kThreads + threadIdx.x;
+    iv0[u] = k < cap ? __ldcv(idx + k) : 0;
+    tv0[u] = k < cap ? __ldcv(target + k) : 0.0;
+  }
   if (threadIdx.x == 0) {
     const double2 v = __ldcv(reinterpret_cast<const double2*>(in));
     *dt_dev = v.x;
@@ -161,15 +174,19 @@ __global__ void __launch_bounds__(kThreads)
   long long vq = 0;
   double vs = 0.0;
   int bad = 0;
-  constexpr int kInFlight = 4;
   for (int base = 0; base < count; base += kThreads * kInFlight) {
     int iv[kInFlight];
     double tv[kInFlight];
 #pragma unroll
     for (int u = 0; u < kInFlight; ++u) {
       const int k = base + u * kThreads + threadIdx.x;
-      iv[u] = k < count ? __ldcv(idx + k) : 0;
-      tv[u] = k < count ? __ldcv(target + k) : 0.0;
+      if (base == 0) {
+        iv[u] = iv0[u];
+        tv[u] = tv0[u];
+      } else {
+        iv[u] = k < count ? __ldcv(idx + k) : 0;
+        tv[u] = k < count ? __ldcv(target + k) : 0.0;
+      }
     }
 #pragma unroll
     for (int u = 0; u < kInFlight; ++u) {

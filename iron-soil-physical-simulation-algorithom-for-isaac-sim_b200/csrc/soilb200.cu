@@ -2317,8 +2317,9 @@ int build_path_graph(sb_ctx* ctx, const sb_path_params* p) {
     SB_CUDA(ctx, cudaHostGetDevicePointer(&in_dev, ctx->path_in, 0));
     SB_CUDA(ctx, cudaHostGetDevicePointer(&idx_dev, ctx->path_idx, 0));
     SB_CUDA(ctx, cudaHostGetDevicePointer(&val_dev, ctx->path_val, 0));
+    int cap = ctx->path_cap;
     void* args[] = {&nyv, &nxv, &pitch, &Q, &datum, &f, &ctx->b, &ctx->z, &ctx->h[0], &ctx->h[1],
-                    &ctx->ctl, &in_dev, (void*)&ctx->dt_dev, &idx_dev, &val_dev, &ctx->xout,
+                    &ctx->ctl, &in_dev, (void*)&ctx->dt_dev, &idx_dev, &val_dev, &cap, &ctx->xout,
                     &ctx->lout};
     if ((rc = add_kernel(ctx, g, &node, &prev, 1, (void*)path_start_kernel<FX>, dim3(1), 0, args)))
       return rc;
