@@ -177,3 +177,30 @@ def test_fixed_point_yield_arc_tangent_within_its_bound():
     want = np.arctan(x.astype(np.float64))
     assert np.abs(got - want).max() <= 2.0e-7
     assert got[-3] == 0.0 and got[-1] == np.float32(np.pi / 2)
+
+
+def test_fixed_point_yield_tracks_the_fp64_yield():
+    """The float32 fixed-point yield against the FP64 yield (the reference's
+    arithmetic) on the same quantized surface: slope within 4e-7 rad,
+    severity within 1e-5, and the unstable masks equal up to cells whose
+    start margin lies within float rounding of zero (at most 0.1 %)."""
+    from oracle import labels as L
+    rng = np.random.default_rng(11)
+    ny, nx = 120, 140
+    ys, xs = np.indices((ny, nx))
+    b = 0.8 + 0.6 * np.sin(xs / 7.0) * np.cos(ys / 5.0) + 0.05 * rng.random((ny, nx))
+    z = b - 0.02 - 0.12 * rng.random((ny, nx))
+    k = 24
+    bq, zq = fx.quantize(b, 0.0, k), fx.quantize(z, 0.0, k)
+    hq = np.zeros_like(bq)
+    kw = dict(dx=0.05, dy=0.05, tan_start=np.tan(np.deg2rad(38.0)),
+              tan_stop=np.tan(np.deg2rad(30.0)), density=1600.0, gravity=9.81, cohesion=20.0,
+              mobilization_depth=0.08, dry=1e-8)
+    y32 = L.yield_init(bq, zq, hq, None, None, fixed_point=True, quantum=2.0 ** -k, **kw)
+    y64 = L.yield_init(fx.dequantize(bq, 0.0, k), fx.dequantize(zq, 0.0, k),
+                       np.zeros((ny, nx)), None, None, **kw)
+    assert np.abs(y32["slope"].astype(np.float64) - y64["slope"]).max() <= 4.0e-7
+    assert np.abs(y32["severity"].astype(np.float64) - y64["severity"]).max() <= 1.0e-5
+    assert 0 < int(y64["unstable"].sum()) < ny * nx
+    diff = int(np.count_nonzero(y32["unstable"] != y64["unstable"]))
+    assert diff <= int(1e-3 * ny * nx), diff
