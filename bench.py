@@ -465,18 +465,19 @@ def run_mobile_large(args, n: int = 4096):
     warm_subs = [int(solver.step_resident(DT).substeps) for _ in range(args.warmup)]
     torch.cuda.synchronize()
     dev_ms, subs, loop = 0.0, 0, []
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        rec = solver.step_resident(DT)
-        e1.record(stream)
-        e1.synchronize()
-        dev_ms += e0.elapsed_time(e1)
-        subs += rec.substeps
-        ls = solver.last_stats
-        loop.append((ls.substep_loop_ms, ls.substeps))
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rec = solver.step_resident(DT)
+            e1.record(stream)
+            e1.synchronize()
+            dev_ms += e0.elapsed_time(e1)
+            subs += rec.substeps
+            ls = solver.last_stats
+            loop.append((ls.substep_loop_ms, ls.substeps))
     peak, kind = measured_peak()
     per = sum(m for m, _ in loop) / max(sum(k for _, k in loop), 1)
     alg = BYTES_PER_CELL_SUBSTEP * n * n
@@ -490,7 +491,8 @@ def run_mobile_large(args, n: int = 4096):
                          "algorithmic_bytes_per_launch": alg,
                          "traffic": NCU_TRAFFIC_BYTES["mobile_v2_4096"],
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "of one loop launch / its substeps"}}
+                                           "of one loop launch / its substeps"},
+            "clocks": clocks.summary()}
 
 
 def _c2_cpu_patch(args):
