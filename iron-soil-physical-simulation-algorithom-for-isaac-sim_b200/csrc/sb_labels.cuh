@@ -21,6 +21,10 @@
 // Component sums are exact integers (area in units of dx*dy/6, mobilizable
 // volume in height quanta * area units, slope excesses in 2^-32 rad), so the
 // statistics are deterministic as well.
+//
+// Yield arithmetic: FP64 in the parity path (the reference's); float32 in the
+// fixed-point path (integer height differences, IEEE divisions and roots, the
+// slope angle by a published polynomial), restated bit for bit on the CPU.
 #pragma once
 
 #include "sb_common.cuh"
@@ -30,9 +34,10 @@ namespace sb {
 
 constexpr int kLabelTile = 32;
 // Threads of the yield/labelling tile kernel: 16 warps per 32x32 tile (two
-// cells per thread) and 3 tiles per SM; its FP64 yield arithmetic is latency
-// bound, and 12 warps per tile (4 tiles per SM) measured 1.3 % slower on the
-// whole 701^2 step, 8 warps 0.1 % slower still.
+// cells per thread) and 3 tiles per SM; measured with the FP64 yield (now the
+// parity path only; the fixed-point path's yield is float32), 12 warps per
+// tile (4 tiles per SM) were 1.3 % slower on the whole 701^2 step, 8 warps
+// 0.1 % slower still.
 constexpr int kLabelInitThreads = 512;
 // Fixed-point units of the per-root sums.  2^32 keeps the int64 sums free of
 // overflow up to 2^24 cells with slopes < pi/2 rad and failure depths < 8 m
